@@ -1,0 +1,108 @@
+/* libxkb200 -- C ABI of the B200 (sm_100a) implementation of XKRT's dataflow hot path.
+ *
+ * Every entry point takes plain pointers and sizes; device pointers are CUDA global
+ * memory of the current device, `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream). Return value: XKB_OK (0) or a negative XKB_E* code; the text
+ * of the last error is available from xkb_last_error(). No entry point aborts the
+ * process, and none falls back to a CPU implementation: without a usable GPU they
+ * return XKB_ENODEV.
+ *
+ * Reference interfaces replaced (XKRT, file:line within its repository) are cited on
+ * each declaration.
+ */
+#ifndef XKRT_B200_H
+#define XKRT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#  define XKB_API __attribute__((visibility("default")))
+#else
+#  define XKB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ---------------------------------------------------------------------- */
+#define XKB_OK          0
+#define XKB_EINVAL     (-22)   /* bad argument (sizes, alignment, mode bits)             */
+#define XKB_ENOMEM     (-12)   /* device or host allocation failed                       */
+#define XKB_ERANGE     (-34)   /* an output or scratch capacity is too small; the needed */
+                               /* capacity is reported through the call's out-parameter  */
+#define XKB_ETIMEDOUT  (-110)  /* a bounded device-side wait gave up (no hang, no trap)  */
+#define XKB_ENODEV     (-19)   /* no CUDA device / the library cannot reach the GPU       */
+#define XKB_ECUDA      (-1000) /* a CUDA runtime call failed; see xkb_last_error()       */
+
+/* Text of the last error set on the calling thread ("" if none). */
+XKB_API const char * xkb_last_error(void);
+
+/* Library version string and the device architecture it was compiled for ("sm_100a"). */
+XKB_API const char * xkb_version(void);
+
+/* ---- access records --------------------------------------------------------------------- */
+/* Access modes and types: same values as the reference's
+ * include/xkrt/memory/access/mode.h:54-66 and include/xkrt/memory/access/type.h. */
+#define XKB_ACCESS_MODE_R   1
+#define XKB_ACCESS_MODE_W   2
+#define XKB_ACCESS_MODE_RW  3
+#define XKB_ACCESS_MODE_V   4
+#define XKB_ACCESS_MODE_D   8
+#define XKB_ACCESS_TYPE_SEGMENT     1
+#define XKB_ACCESS_TYPE_BLAS_MATRIX 2
+
+/* One access of one task, 64 bytes, tasks in spawn order and each task's accesses in
+ * declaration order (the order in which the reference's spawning thread hands them to
+ * task_dependency_resolve, src/task/task.cc:285-299).
+ *  matrix : addr = storage base, ld, offset_m, offset_n, m, n, sizeof_type -- the
+ *           arguments of access_t's matrix constructor (include/xkrt/memory/access/access.hpp:539-574)
+ *  segment: byte interval [addr, ld)  -- access_t's segment constructor (access.hpp:479-514) */
+typedef struct xkb_access_rec_t {
+    uint32_t task;
+    uint8_t  type;
+    uint8_t  mode;
+    uint16_t reserved;
+    uint64_t addr;
+    uint64_t ld;
+    uint64_t offset_m;
+    uint64_t offset_n;
+    uint64_t m;
+    uint64_t n;
+    uint64_t sizeof_type;
+} xkb_access_rec_t;
+
+/* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
+/* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float
+ * storage, every cell update computed in double and rounded once to float on store. */
+#define XKB_F64 0
+#define XKB_F32 1
+
+/* One Jacobi step of the 5-point heat stencil on the tile task (tile_x, tile_y) of an
+ * nx x ny column-major grid (cell (i,j) at G[j*ld + i]):
+ *   D(i,j) = S(i,j) + c*( (S(i+1,j) - 2S(i,j) + S(i-1,j)) + (S(i,j+1) - 2S(i,j) + S(i,j-1)) )
+ * for the cells of rows [tile_x*tsx, tile_x*tsx+tsx) x cols [tile_y*tsy, tile_y*tsy+tsy)
+ * that are interior (0 < i < nx-1, 0 < j < ny-1); boundary cells are never written.
+ * src/dst are the WHOLE grids, resident on the device (this library keeps one replica per
+ * grid in the host layout instead of one compact replica per access).
+ * Replaces the tile body diffusion_cuda() of examples/heat-diffusion-2d/src/kernels/diffusion.cu:130-154
+ * (c = ALPHA*DT/(DX*DY) with DX = DY = 1, examples/heat-diffusion-2d/src/main.cc:408-421). */
+XKB_API int xkb_heat_tile(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
+                  int64_t tile_x, int64_t tile_y, int64_t tsx, int64_t tsy, double c, void * stream);
+
+/* One whole Jacobi step (every interior cell of the grid) in one launch: the fused form of
+ * all tile tasks of one step of examples/heat-diffusion-2d/src/main.cc:569-581 (update()). */
+XKB_API int xkb_heat_step(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
+                  double c, void * stream);
+
+/* ---- axpby tile body -------------------------------------------------------------------- */
+/* y[i] = a*x[i] + b*y[i] for i in [0, n), FP64, computed as (a*x) + (b*y) with no fused
+ * multiply-add. No reference kernel exists; nearest reference task body is the byte-wise
+ * z = x + y of examples/task-axpby.cc:43-52. */
+XKB_API int xkb_axpby(int64_t n, double a, const double * x, double b, double * y, void * stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XKRT_B200_H */

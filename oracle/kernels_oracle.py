@@ -1,0 +1,71 @@
+"""ORACLE -- test infrastructure only (imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py as the checker; never by the product).
+
+CPU restatement of the task bodies on the path, in numpy (each operation a separate IEEE
+double operation, so no fused multiply-add can occur):
+
+* heat_step: the heat-diffusion-2d update of examples/heat-diffusion-2d/src/main.cc:408-421
+  (update_cpu) with DX = DY = 1 and c = ALPHA*DT/(DX*DY):
+      D(i,j) = S(i,j) + c*( ((S(i+1,j) - 2S(i,j)) + S(i-1,j)) + ((S(i,j+1) - 2S(i,j)) + S(i,j-1)) )
+  on interior cells only; boundary cells of dst are left untouched. Grids are column-major
+  with leading dimension ld: numpy arrays of shape (ny, ld), cell (i, j) at G[j, i]
+  (GRID(G,I,J,L) = G[J*L+I], examples/heat-diffusion-2d/include/heat/consts.h:90).
+  FP32-storage mode: cells read as float32, promoted to double, updated in double, rounded
+  once to float32.
+* heat_tile: the same update restricted to one tile task's cells
+  (examples/heat-diffusion-2d/src/main.cc:508-566 decomposition, src/kernels/diffusion.cu:107-128).
+* axpby: y = (a*x) + (b*y) (no reference kernel exists; examples/task-axpby.cc:43-52 is the
+  byte-wise analogue).
+* heat_init: the seeded synthetic grid: interior U[0,1) from numpy's PCG64 generator with the
+  given seed, boundary 0 (Dirichlet).
+"""
+import numpy as np
+
+
+def heat_init(nx, ny, ld=None, seed=42, dtype=np.float64):
+    ld = nx if ld is None else ld
+    g = np.zeros((ny, ld), dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    g[1:ny - 1, 1:nx - 1] = rng.random((ny - 2, nx - 2))
+    return g.astype(dtype)
+
+
+def _update(S, c):
+    """Interior update of a (ny, nx') view S (float64). Returns the (ny-2, nx'-2) block."""
+    s = S[1:-1, 1:-1]
+    a = (S[1:-1, 2:] - 2.0 * s) + S[1:-1, :-2]      # rows i+1, i-1 (contiguous dim)
+    b = (S[2:, 1:-1] - 2.0 * s) + S[:-2, 1:-1]      # cols j+1, j-1
+    return s + c * (a + b)
+
+
+def heat_tile(src, dst, nx, ny, tile_x, tile_y, tsx, tsy, c):
+    """Update the interior cells of tile (tile_x, tile_y) of dst from src (in place on dst)."""
+    x0, y0 = tile_x * tsx, tile_y * tsy
+    rx0, rx1 = max(x0, 1), min(x0 + tsx, nx - 1)
+    cy0, cy1 = max(y0, 1), min(y0 + tsy, ny - 1)
+    if rx0 >= rx1 or cy0 >= cy1:
+        return dst
+    S = src[cy0 - 1:cy1 + 1, rx0 - 1:rx1 + 1].astype(np.float64)
+    dst[cy0:cy1, rx0:rx1] = _update(S, c).astype(dst.dtype)
+    return dst
+
+
+def heat_step(src, dst, nx, ny, c):
+    if nx >= 3 and ny >= 3:
+        S = src[:ny, :nx].astype(np.float64)
+        dst[1:ny - 1, 1:nx - 1] = _update(S, c).astype(dst.dtype)
+    return dst
+
+
+def heat_run(grid, nx, ny, steps, c, dtype=np.float64):
+    """Double-buffered Jacobi: returns the grid after `steps` steps."""
+    a = grid.astype(dtype).copy()
+    b = a.copy()
+    for _ in range(steps):
+        heat_step(a, b, nx, ny, c)
+        a, b = b, a
+    return a
+
+
+def axpby(a, x, b, y):
+    return (a * x) + (b * y)

@@ -1,0 +1,93 @@
+"""GPU parity of the heat-diffusion tile body against the numpy oracle (bit-exact in FP64;
+FP32-storage within 1e-5 relative of the FP64 oracle)."""
+import numpy as np
+import pytest
+
+import kernels_oracle as O
+import xkaapi_b200 as xk
+
+pytestmark = pytest.mark.gpu
+C = 0.2
+
+
+def to_dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("nx,ny,ld", [(64, 64, 64), (130, 97, 130), (131, 77, 136), (3, 3, 3), (5, 200, 7),
+                                      (1024, 1024, 1024), (257, 129, 257)])
+def test_step_f64_bit_exact(torch_cuda, nx, ny, ld):
+    torch = torch_cuda
+    g = O.heat_init(nx, ny, ld, seed=nx * 1000 + ny)
+    ref = O.heat_step(g, g.copy(), nx, ny, C)
+    s, d = to_dev(torch, g), to_dev(torch, g)
+    xk.heat_step(s, d, nx, ny, ld, C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("nx,ny,tsx,tsy", [(64, 64, 16, 16), (1024, 1024, 128, 128), (200, 136, 64, 48),
+                                           (130, 130, 128, 128), (97, 61, 33, 17)])
+def test_tiles_f64_bit_exact(torch_cuda, nx, ny, tsx, tsy):
+    torch = torch_cuda
+    g = O.heat_init(nx, ny, seed=3)
+    ref = g.copy()
+    s, d = to_dev(torch, g), to_dev(torch, g)
+    ntx, nty = -(-nx // tsx), -(-ny // tsy)
+    for tx in range(ntx):
+        for ty in range(nty):
+            O.heat_tile(g, ref, nx, ny, tx, ty, tsx, tsy, C)
+            xk.heat_tile(s, d, nx, ny, nx, tx, ty, tsx, tsy, C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), ref)
+    # a tile beyond the grid writes nothing
+    xk.heat_tile(s, d, nx, ny, nx, ntx + 1, 0, tsx, tsy, C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), ref)
+
+
+def test_run_100_steps_f64_1024(torch_cuda):
+    """Config: 1024x1024 FP64, c=0.2, Dirichlet 0, 100 double-buffered steps."""
+    torch = torch_cuda
+    nx = ny = 1024
+    g = O.heat_init(nx, ny, seed=42)
+    ref = O.heat_run(g, nx, ny, 100, C)
+    a, b = to_dev(torch, g), to_dev(torch, g)
+    for _ in range(100):
+        xk.heat_step(a, b, nx, ny, nx, C)
+        a, b = b, a
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("nx,ny", [(512, 384), (131, 77)])
+def test_f32_storage_matches_oracle_and_fp64(torch_cuda, nx, ny):
+    torch = torch_cuda
+    g64 = O.heat_init(nx, ny, seed=5)
+    g32 = g64.astype(np.float32)
+    steps = 20
+    ref32 = O.heat_run(g32, nx, ny, steps, C, dtype=np.float32)
+    ref64 = O.heat_run(g64, nx, ny, steps, C)
+    a, b = to_dev(torch, g32), to_dev(torch, g32)
+    for _ in range(steps):
+        xk.heat_step(a, b, nx, ny, nx, C)
+        a, b = b, a
+    torch.cuda.synchronize()
+    out = a.cpu().numpy()
+    np.testing.assert_array_equal(out, ref32)          # same rounding as the FP32-storage oracle
+    rel = np.abs(out.astype(np.float64) - ref64).max() / np.abs(ref64).max()
+    assert rel <= 1e-5, rel                            # FP32-storage error bound vs FP64
+
+
+def test_f32_tiles_bit_exact(torch_cuda):
+    torch = torch_cuda
+    nx, ny, ts = 300, 260, 128
+    g = O.heat_init(nx, ny, seed=9).astype(np.float32)
+    ref = g.copy()
+    s, d = to_dev(torch, g), to_dev(torch, g)
+    for tx in range(-(-nx // ts)):
+        for ty in range(-(-ny // ts)):
+            O.heat_tile(g, ref, nx, ny, tx, ty, ts, ts, C)
+            xk.heat_tile(s, d, nx, ny, nx, tx, ty, ts, ts, C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), ref)

@@ -1,0 +1,50 @@
+"""The dependency oracle restatement against golden edge sets produced by the reference's own
+dependency trees (tests/golden/make_golden.py), plus oracle self-checks. CPU only."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import streams as S
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = np.load(os.path.join(REPO, "tests", "golden", "deps_golden.npz"))
+CASES = sorted(k[:-len("__stream")] for k in GOLDEN.files if k.endswith("__stream"))
+
+
+def run_oracle(recs, tmp_path):
+    p = str(tmp_path / "s.bin")
+    S.write_stream(p, recs)
+    subprocess.run([os.path.join(REPO, "oracle", "_bin", "deps_oracle"), p, str(tmp_path / "o")],
+                   check=True, capture_output=True)
+    return S.read_edges(str(tmp_path / "o.edges"))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_matches_reference_golden(case, tmp_path):
+    edges = run_oracle(GOLDEN[case + "__stream"], tmp_path)
+    np.testing.assert_array_equal(edges, GOLDEN[case + "__edges"])
+
+
+def test_known_answer_orderings():
+    # reference tests/task-dependency-interval.cc and tests/task-dependency-interval-matrix.cc:
+    # both build the chain T0 -> T1 -> T2
+    for case in ("ref_interval_chain", "ref_interval_matrix_chain"):
+        e = set(map(tuple, GOLDEN[case + "__edges"].tolist()))
+        assert {(0, 1), (1, 2)} <= e, (case, e)
+
+
+def test_heat_oracle_properties():
+    import kernels_oracle as O
+    g = O.heat_init(40, 30, seed=1)
+    assert (g[0] == 0).all() and (g[:, 0] == 0).all() and (g[-1] == 0).all() and (g[:, 39] == 0).all()
+    out = O.heat_run(g, 40, 30, 5, 0.2)
+    assert (out[0] == 0).all() and (out[:, 39] == 0).all()          # Dirichlet boundary preserved
+    # tile decomposition == whole step (the task graph computes the same grid)
+    ref = O.heat_step(g, g.copy(), 40, 30, 0.2)
+    t = g.copy()
+    for tx in range(3):
+        for ty in range(3):
+            O.heat_tile(g, t, 40, 30, tx, ty, 16, 11, 0.2)
+    np.testing.assert_array_equal(t, ref)

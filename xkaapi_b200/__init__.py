@@ -1,0 +1,95 @@
+"""xkaapi_b200 -- B200 (sm_100a) implementation of XKRT's dataflow hot path.
+
+The product is the C-ABI shared library `libxkb200.so` (declared in include/xkrt_b200.h).
+This module loads it with ctypes and exposes thin Python wrappers that take torch CUDA
+tensors for device memory. There is no CPU fallback: if the library is missing or the GPU
+is unreachable, calls raise XkbError.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libxkb200.so")
+
+XKB_OK = 0
+XKB_EINVAL = -22
+XKB_ENOMEM = -12
+XKB_ERANGE = -34
+XKB_ETIMEDOUT = -110
+XKB_ENODEV = -19
+XKB_ECUDA = -1000
+F64, F32 = 0, 1
+
+_lib = None
+
+
+class XkbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libxkb200 error {code}: {msg}")
+        self.code = code
+
+
+_c = ctypes
+_i64, _dbl, _vp, _int = _c.c_int64, _c.c_double, _c.c_void_p, _c.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "xkb_last_error": (_c.c_char_p, []),
+    "xkb_version": (_c.c_char_p, []),
+    "xkb_heat_tile": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _dbl, _vp]),
+    "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
+    "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
+}
+
+
+def lib():
+    """Load libxkb200.so (built in-tree by xkaapi_b200/build.py). Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise XkbError(XKB_ENODEV, f"{LIB_PATH} is not built (run: python -m xkaapi_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != XKB_OK:
+        raise XkbError(rc, lib().xkb_last_error().decode())
+    return rc
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def _dtype_code(t):
+    import torch
+    if t.dtype == torch.float64:
+        return F64
+    if t.dtype == torch.float32:
+        return F32
+    raise XkbError(XKB_EINVAL, f"unsupported grid dtype {t.dtype}")
+
+
+def heat_tile(src, dst, nx, ny, ld, tile_x, tile_y, tsx, tsy, c, stream=None):
+    """One heat tile task on whole resident grids (torch CUDA tensors, column-major with ld)."""
+    return check(lib().xkb_heat_tile(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny,
+                                     tile_x, tile_y, tsx, tsy, c, _stream(stream)))
+
+
+def heat_step(src, dst, nx, ny, ld, c, stream=None):
+    """One whole Jacobi step over the grid in one launch."""
+    return check(lib().xkb_heat_step(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c,
+                                     _stream(stream)))
+
+
+def axpby(a, x, b, y, stream=None):
+    """y = a*x + b*y (FP64 torch CUDA tensors)."""
+    return check(lib().xkb_axpby(x.numel(), a, x.data_ptr(), b, y.data_ptr(), _stream(stream)))

@@ -1,0 +1,79 @@
+"""In-tree build of libxkb200.so (sm_100a) with nvcc.
+
+Every .cu/.cc under xkaapi_b200/csrc is compiled to an object in xkaapi_b200/_build and
+linked into xkaapi_b200/libxkb200.so. Objects are rebuilt when their source, any header of
+csrc/ or include/, or the flags change. nvcc cross-compiles: no GPU is needed to build.
+"""
+import concurrent.futures as cf
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libxkb200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include")]
+LINK_FLAGS = ["-shared", "-lcudart", "-lpthread"]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _headers_digest():
+    h = hashlib.sha256()
+    for d in (CSRC, os.path.join(REPO, "include")):
+        for root, _, files in os.walk(d):
+            for f in sorted(files):
+                if f.endswith((".h", ".cuh", ".hpp")):
+                    with open(os.path.join(root, f), "rb") as fh:
+                        h.update(f.encode()); h.update(fh.read())
+    return h.hexdigest()
+
+
+def _compile(src, extra, verbose):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    stamp = obj + ".stamp"
+    with open(src, "rb") as fh:
+        key = hashlib.sha256(fh.read() + extra.encode()).hexdigest()
+    if os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == key:
+        return obj
+    cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+    if verbose and r.stderr.strip():
+        print(r.stderr, file=sys.stderr)
+    with open(stamp, "w") as fh:
+        fh.write(key)
+    return obj
+
+
+def build(verbose=False):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cc")))
+    extra = _headers_digest() + " ".join(ARCH + NVCC_FLAGS)
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, extra, verbose), srcs))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        cmd = [nvcc()] + ARCH + ["-o", LIB] + objs + LINK_FLAGS
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))
