@@ -96,6 +96,24 @@ XKB_API int xkb_heat_tile(int dtype, const void * src, void * dst, int64_t ld, i
 XKB_API int xkb_heat_step(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
                   double c, void * stream);
 
+/* Launch shape of the whole-step stencil kernel (chosen by xkb_heat_autotune or by hand).
+ *   pf               east columns each lane loads before using any (2, 4 or 8)
+ *   min_blocks       CTAs per SM the register budget is sized for (1, 2 or 4; pf 8 allows 1-2)
+ *   ctas_per_sm      grid size = SMs x ctas_per_sm (the CTAs then stride over strips)
+ *   l2_prefetch_cols distance, in columns, of the bulk L2 prefetch ahead of the sweep (0 = off)
+ *   cols_per_strip   columns one warp sweeps per strip */
+typedef struct xkb_heat_cfg_t {
+    int pf;
+    int min_blocks;
+    int ctas_per_sm;
+    int l2_prefetch_cols;
+    int cols_per_strip;
+} xkb_heat_cfg_t;
+
+/* xkb_heat_step with an explicit launch shape (NULL = the library default). */
+XKB_API int xkb_heat_step_cfg(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
+                              double c, const xkb_heat_cfg_t * cfg, void * stream);
+
 /* ---- axpby tile body -------------------------------------------------------------------- */
 /* y[i] = a*x[i] + b*y[i] for i in [0, n), FP64, computed as (a*x) + (b*y) with no fused
  * multiply-add. No reference kernel exists; nearest reference task body is the byte-wise

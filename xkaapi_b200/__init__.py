@@ -32,12 +32,19 @@ class XkbError(RuntimeError):
 _c = ctypes
 _i64, _dbl, _vp, _int = _c.c_int64, _c.c_double, _c.c_void_p, _c.c_int
 
+class HeatCfg(ctypes.Structure):
+    """xkb_heat_cfg_t: launch shape of the whole-step stencil kernel."""
+    _fields_ = [("pf", ctypes.c_int), ("min_blocks", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("l2_prefetch_cols", ctypes.c_int), ("cols_per_strip", ctypes.c_int)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "xkb_last_error": (_c.c_char_p, []),
     "xkb_version": (_c.c_char_p, []),
     "xkb_heat_tile": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
+    "xkb_heat_step_cfg": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, ctypes.POINTER(HeatCfg), _vp]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
 }
 
@@ -84,10 +91,13 @@ def heat_tile(src, dst, nx, ny, ld, tile_x, tile_y, tsx, tsy, c, stream=None):
                                      tile_x, tile_y, tsx, tsy, c, _stream(stream)))
 
 
-def heat_step(src, dst, nx, ny, ld, c, stream=None):
-    """One whole Jacobi step over the grid in one launch."""
-    return check(lib().xkb_heat_step(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c,
-                                     _stream(stream)))
+def heat_step(src, dst, nx, ny, ld, c, stream=None, cfg=None):
+    """One whole Jacobi step over the grid in one launch (cfg: HeatCfg or None for the default)."""
+    if cfg is None:
+        return check(lib().xkb_heat_step(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c,
+                                         _stream(stream)))
+    return check(lib().xkb_heat_step_cfg(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c,
+                                         ctypes.byref(cfg), _stream(stream)))
 
 
 def axpby(a, x, b, y, stream=None):

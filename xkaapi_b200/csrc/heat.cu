@@ -19,24 +19,24 @@ heat_tile_kernel(const T * __restrict__ src, T * __restrict__ dst, int64_t ld, i
     const int64_t a = y0 + (int64_t) blockIdx.x * per;
     int64_t b = a + per; if (b > y1) b = y1;
     if (a >= b) return;
-    heat_tile_cta<T, VEC, HEAT_PF, false>(src, dst, ld, nx, ny, x0, x1, a, b, c, vec_ok);
+    heat_tile_cta<T, VEC, HEAT_PF, false>(src, dst, ld, nx, ny, x0, x1, a, b, c, vec_ok, 8);
 }
 
-template <typename T, int VEC>
-__global__ void __launch_bounds__(HEAT_THREADS, 2)
+template <typename T, int VEC, int PF, int MINB>
+__global__ void __launch_bounds__(HEAT_THREADS, MINB)
 heat_step_kernel(const T * __restrict__ src, T * __restrict__ dst, int64_t ld, int64_t nx, int64_t ny,
-                 int64_t nrg, int64_t ncc, double c, bool vec_ok)
+                 int64_t nrg, int64_t ncc, int64_t cols, double c, bool vec_ok, int pfd)
 {
     const int64_t warps = (int64_t) gridDim.x * (HEAT_THREADS / 32);
     const int64_t nstrips = nrg * ncc;
     for (int64_t s = (int64_t) blockIdx.x * (HEAT_THREADS / 32) + (threadIdx.x >> 5); s < nstrips; s += warps)
     {
         // consecutive warps take consecutive row groups of the same column chunk, so a CTA
-        // sweeps a contiguous panel and its halo rows are shared through L2
+        // sweeps a contiguous panel of the grid
         const int64_t rg = s % nrg, cc = s / nrg;
-        const int64_t cy0 = 1 + cc * STEP_COLS;
-        int64_t cy1 = cy0 + STEP_COLS; if (cy1 > ny - 1) cy1 = ny - 1;
-        heat_strip<T, VEC, HEAT_PF, false>(src, dst, ld, nx, rg * 32 * VEC, 1, nx - 1, cy0, cy1, c, vec_ok);
+        const int64_t cy0 = 1 + cc * cols;
+        int64_t cy1 = cy0 + cols; if (cy1 > ny - 1) cy1 = ny - 1;
+        heat_strip<T, VEC, PF, false>(src, dst, ld, nx, ny, rg * StripGeom<VEC>::OUT, 1, nx - 1, cy0, cy1, c, vec_ok, pfd);
     }
 }
 
@@ -63,21 +63,51 @@ static int launch_tile(const void * src, void * dst, int64_t ld, int64_t nx, int
     return XKB_OK;
 }
 
+static int sm_count()
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+template <typename T, int PF, int MINB>
+static void step_launch(dim3 g, cudaStream_t st, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
+                        int64_t nrg, int64_t ncc, int64_t cols, double c, bool vok, int pfd)
+{
+    heat_step_kernel<T, HeatVec<T>::N, PF, MINB><<<g, HEAT_THREADS, 0, st>>>((const T *) src, (T *) dst, ld, nx, ny,
+                                                                          nrg, ncc, cols, c, vok, pfd);
+}
+
 template <typename T>
-static int launch_step(const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny, double c, cudaStream_t st)
+static int launch_step(const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny, double c,
+                       const xkb_heat_cfg_t & cfg, cudaStream_t st)
 {
     constexpr int VEC = HeatVec<T>::N;
     if (nx < 3 || ny < 3) return XKB_OK;
-    const int64_t nrg = (nx - 1 + 32 * VEC - 1) / (32 * VEC);
-    const int64_t ncc = (ny - 2 + STEP_COLS - 1) / STEP_COLS;
+    const int64_t cols = cfg.cols_per_strip > 0 ? cfg.cols_per_strip : 64;
+    const int64_t nrg = (nx - 2 + StripGeom<VEC>::OUT - 1) / StripGeom<VEC>::OUT;
+    const int64_t ncc = (ny - 2 + cols - 1) / cols;
     const int64_t ctas_needed = (nrg * ncc + (HEAT_THREADS / 32) - 1) / (HEAT_THREADS / 32);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int64_t grid = sms * 8;   // grid-stride over strips, several CTAs resident per SM
+    int64_t grid = (int64_t) sm_count() * (cfg.ctas_per_sm > 0 ? cfg.ctas_per_sm : 8);
     if (grid > ctas_needed) grid = ctas_needed;
-    heat_step_kernel<T, VEC><<<(unsigned) grid, HEAT_THREADS, 0, st>>>((const T *) src, (T *) dst, ld, nx, ny,
-                                                                      nrg, ncc, c, vec_ok_for<T>(src, dst, ld));
+    const bool vok = vec_ok_for<T>(src, dst, ld);
+    const dim3 g((unsigned) grid);
+    const int pfd = cfg.l2_prefetch_cols;
+    switch (cfg.pf * 10 + cfg.min_blocks)
+    {
+        case 21: step_launch<T, 2, 1>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 22: step_launch<T, 2, 2>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 24: step_launch<T, 2, 4>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 41: step_launch<T, 4, 1>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 42: step_launch<T, 4, 2>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 81: step_launch<T, 8, 1>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        case 82: step_launch<T, 8, 2>(g, st, src, dst, ld, nx, ny, nrg, ncc, cols, c, vok, pfd); break;
+        default: return xkb_set_error(XKB_EINVAL, "heat_step: unsupported (pf=%d, min_blocks=%d)", cfg.pf, cfg.min_blocks);
+    }
     XKB_CUDA_TRY(cudaGetLastError());
     return XKB_OK;
 }
@@ -106,11 +136,22 @@ extern "C" int xkb_heat_tile(int dtype, const void * src, void * dst, int64_t ld
                             : launch_tile<float>(src, dst, ld, nx, ny, x0, x1, y0, y1, c, xkb_stream(stream));
 }
 
+static const xkb_heat_cfg_t kDefaultStepCfg = {4, 2, 8, 8, 64};
+
 extern "C" int xkb_heat_step(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
                              double c, void * stream)
 {
+    return xkb_heat_step_cfg(dtype, src, dst, ld, nx, ny, c, &kDefaultStepCfg, stream);
+}
+
+extern "C" int xkb_heat_step_cfg(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
+                                 double c, const xkb_heat_cfg_t * cfg, void * stream)
+{
     int rc = heat_check(dtype, src, dst, ld, nx, ny);
     if (rc) return rc;
-    return dtype == XKB_F64 ? launch_step<double>(src, dst, ld, nx, ny, c, xkb_stream(stream))
-                            : launch_step<float>(src, dst, ld, nx, ny, c, xkb_stream(stream));
+    const xkb_heat_cfg_t & k = cfg ? *cfg : kDefaultStepCfg;
+    if (k.l2_prefetch_cols < 0 || k.l2_prefetch_cols > 256 || k.cols_per_strip < 0)
+        return xkb_set_error(XKB_EINVAL, "heat_step: bad configuration");
+    return dtype == XKB_F64 ? launch_step<double>(src, dst, ld, nx, ny, c, k, xkb_stream(stream))
+                            : launch_step<float>(src, dst, ld, nx, ny, c, k, xkb_stream(stream));
 }

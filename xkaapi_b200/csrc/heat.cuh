@@ -5,9 +5,10 @@
 // Work unit = a warp STRIP: 32*VEC consecutive rows (each lane owns VEC consecutive rows,
 // loaded as one 16-byte vector) x a range of columns swept left to right. The sweep keeps
 // the west/centre/east columns in registers, so every input cell is read from HBM once per
-// strip; north/south neighbours come from the adjacent lanes by shuffle, and only lanes 0
-// and 31 fetch one halo cell per column. Each batch of PF east columns is loaded before any
-// of them is used, giving PF x 16 B per lane in flight.
+// strip; north/south neighbours come from the adjacent lanes by shuffle. Strips overlap by
+// two rows (a strip writes its 32*VEC-2 inner rows), so no lane needs a halo load. Each batch
+// of PF east columns is loaded before any is used, and one bulk L2 prefetch per column runs
+// `pfd` columns ahead, keeping enough HBM bytes in flight without spending registers.
 //
 // Arithmetic matches the reference formula (examples/heat-diffusion-2d/src/main.cc:408-421,
 // src/kernels/diffusion.cu:117-121) with DX = DY = 1, in its evaluation order and without
@@ -56,87 +57,133 @@ __device__ __forceinline__ Cells<T, VEC> ld_cells(const T * __restrict__ g, int6
 
 __device__ __forceinline__ double heat_update(double s, double up, double down, double w, double e, double c)
 {
-    const double a = __dadd_rn(__dsub_rn(down, __dmul_rn(2.0, s)), up);
-    const double b = __dadd_rn(__dsub_rn(e, __dmul_rn(2.0, s)), w);
+    const double s2 = __dmul_rn(2.0, s);
+    const double a = __dadd_rn(__dsub_rn(down, s2), up);
+    const double b = __dadd_rn(__dsub_rn(e, s2), w);
     return __dadd_rn(s, __dmul_rn(c, __dadd_rn(a, b)));
 }
 
-// One warp strip: rows [rbase, rbase + 32*VEC) intersected with [rx0, rx1), columns
-// [cy0, cy1). Preconditions: 1 <= rx0 < rx1 <= nx-1, 1 <= cy0 < cy1 <= ny-1, and rbase a
-// multiple of VEC. `vec_ok` = ld and both base pointers allow VEC-wide aligned accesses.
-template <typename T, int VEC, int PF, bool CG>
-__device__ __forceinline__ void heat_strip(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
-                                           int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
-                                           int64_t cy0, int64_t cy1, double c, bool vec_ok)
+// Bulk L2 prefetch of `bytes` (multiple of 16, 16-byte aligned source) with one instruction.
+__device__ __forceinline__ void l2_prefetch_bulk(const void * p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
+
+// Rows a warp strip loads (32 lanes x VEC) and writes: a strip based at row rbase writes rows
+// [rbase+1, rbase+1+OUT), so the north/south neighbours of every written row are in the
+// strip's own registers; consecutive strips step by OUT rows.
+template <int VEC> struct StripGeom {
+    static constexpr int LOAD = 32 * VEC;
+    static constexpr int OUT = LOAD - VEC;    // row step between strips (keeps VEC alignment)
+};
+
+// One warp strip: loads rows [rbase, rbase + 32*VEC) of columns [cy0-1, cy1], writes rows
+// [rbase+1, rbase+1+OUT) intersected with [rx0, rx1) of columns [cy0, cy1).
+// Preconditions: 1 <= rx0 < rx1 <= nx-1, 1 <= cy0 < cy1 <= ny-1, rbase a multiple of VEC,
+// rbase >= 0. `vec_ok` = ld and both base pointers allow VEC-wide aligned accesses.
+// FAST = every loaded row is inside [0, nx) and vec_ok (no per-load checks).
+template <typename T, int VEC, int PF, bool CG, bool FAST>
+__device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                                int64_t nx, int64_t ny, int64_t rbase, int64_t rx0, int64_t rx1,
+                                                int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
 {
     const int lane = threadIdx.x & 31;
     const int64_t r = rbase + (int64_t) lane * VEC;
-    const int64_t rn = rbase - 1;                   // north halo row of the strip
-    const int64_t rs = rbase + 32 * VEC;            // south halo row of the strip
-    const bool lane_rows = (r + VEC > rx0) && (r < rx1);
+    // rows of this lane that are written
+    const int64_t w0 = (r > rbase ? r : rbase + 1) > rx0 ? (r > rbase ? r : rbase + 1) : rx0;
+    int64_t w1 = r + VEC; if (w1 > rbase + 1 + StripGeom<VEC>::OUT) w1 = rbase + 1 + StripGeom<VEC>::OUT;
+    if (w1 > rx1) w1 = rx1;
+    const bool full_store = vec_ok && w0 == r && w1 == r + VEC;
+    int64_t pf_rows = nx - rbase; if (pf_rows > StripGeom<VEC>::LOAD) pf_rows = StripGeom<VEC>::LOAD;
+    const uint32_t pf_bytes = (uint32_t) ((pf_rows * (int64_t) sizeof(T)) & ~(int64_t) 15);
+    const bool pf_on = pfd > 0 && vec_ok && pf_bytes > 0;
 
-    Cells<T, VEC> west = ld_cells<T, VEC, CG>(src, ld, nx, r, cy0 - 1, vec_ok);
-    Cells<T, VEC> cur  = ld_cells<T, VEC, CG>(src, ld, nx, r, cy0, vec_ok);
+    const T * __restrict__ sp = src + r;
+    T * __restrict__ dp = dst + r;
+    auto load = [&](int64_t j) -> Cells<T, VEC> {
+        if constexpr (FAST) {
+            Cells<T, VEC> q;
+            const T * p = sp + j * ld;
+            if constexpr (VEC == 2 && sizeof(T) == 8) {
+                double2 v = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
+                q.v[0] = v.x; q.v[1] = v.y;
+            } else {
+                float4 v = CG ? __ldcg((const float4 *) p) : __ldg((const float4 *) p);
+                q.v[0] = v.x; q.v[1] = v.y; q.v[2] = v.z; q.v[3] = v.w;
+            }
+            return q;
+        } else {
+            return ld_cells<T, VEC, CG>(src, ld, nx, r, j, vec_ok);
+        }
+    };
 
+    Cells<T, VEC> west = load(cy0 - 1);
+    Cells<T, VEC> cur  = load(cy0);
     for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
     {
-        Cells<T, VEC> nxt[PF];
-        T hn[PF], hs[PF];
-#pragma unroll
-        for (int k = 0; k < PF; ++k)
+        if (pf_on && lane < PF)
         {
-            const int64_t je = j0 + k + 1;
-            if (je <= cy1) nxt[k] = ld_cells<T, VEC, CG>(src, ld, nx, r, je, vec_ok);
-            const int64_t jc = j0 + k;
-            hn[k] = T(0); hs[k] = T(0);
-            if (jc < cy1)
-            {
-                if (lane == 0 && rn >= 0)   hn[k] = ld_scalar<CG>(src + jc * ld + rn);
-                if (lane == 31 && rs < nx)  hs[k] = ld_scalar<CG>(src + jc * ld + rs);
-            }
+            // lane k prefetches column j0 + pfd + k of the strip into L2 with one bulk request
+            const int64_t jp = j0 + pfd + lane;
+            if (jp <= cy1) l2_prefetch_bulk(src + jp * ld + rbase, pf_bytes);
         }
+        Cells<T, VEC> nxt[PF];
+#pragma unroll
+        for (int k = 0; k < PF; ++k)
+            if (j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
 #pragma unroll
         for (int k = 0; k < PF; ++k)
         {
             const int64_t jc = j0 + k;
-            if (jc >= cy1) break;
-            // neighbours across lanes (warp-uniform control flow up to here)
-            T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
-            T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
-            if (lane == 0)  north = hn[k];
-            if (lane == 31) south = hs[k];
-            if (lane_rows)
+            if (jc >= cy1) break;                        // warp-uniform
+            const T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
+            const T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
+            Cells<T, VEC> out;
+#pragma unroll
+            for (int e = 0; e < VEC; ++e)
             {
-                Cells<T, VEC> out;
+                const double sv = (double) cur.v[e];
+                const double up = (double) (e == 0 ? north : cur.v[e - 1]);
+                const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
+                out.v[e] = (T) heat_update(sv, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
+            }
+            T * q = dp + jc * ld;
+            if (full_store)
+            {
+                if constexpr (VEC == 2 && sizeof(T) == 8) *(double2 *) q = make_double2(out.v[0], out.v[1]);
+                else *(float4 *) q = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
+            }
+            else
+            {
 #pragma unroll
                 for (int e = 0; e < VEC; ++e)
-                {
-                    const double s  = (double) cur.v[e];
-                    const double up = (double) (e == 0 ? north : cur.v[e - 1]);
-                    const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
-                    out.v[e] = (T) heat_update(s, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
-                }
-                T * q = dst + jc * ld + r;
-                if (vec_ok && r >= rx0 && r + VEC <= rx1)
-                {
-                    if constexpr (VEC == 2 && sizeof(T) == 8)      *(double2 *) q = make_double2(out.v[0], out.v[1]);
-                    else if constexpr (VEC == 4 && sizeof(T) == 4) *(float4 *) q = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
-                    else {
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) q[e] = out.v[e];
-                    }
-                }
-                else
-                {
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e)
-                        if (r + e >= rx0 && r + e < rx1) q[e] = out.v[e];
-                }
+                    if (r + e >= w0 && r + e < w1) q[e] = out.v[e];
             }
             west = cur;
             cur = nxt[k];
         }
     }
+}
+
+// Edge strips (grid bottom rows, unaligned grids) take a checked path kept out of line so the
+// fast path's register allocation stays small.
+template <typename T, int VEC, int PF, bool CG>
+__device__ __noinline__ void heat_strip_edge(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                             int64_t nx, int64_t ny, int64_t rbase, int64_t rx0, int64_t rx1,
+                                             int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
+{
+    heat_strip_impl<T, VEC, 2, CG, false>(src, dst, ld, nx, ny, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
+}
+
+template <typename T, int VEC, int PF, bool CG>
+__device__ __forceinline__ void heat_strip(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                           int64_t nx, int64_t ny, int64_t rbase, int64_t rx0, int64_t rx1,
+                                           int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
+{
+    if (vec_ok && rbase + StripGeom<VEC>::LOAD <= nx)
+        heat_strip_impl<T, VEC, PF, CG, true>(src, dst, ld, nx, ny, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
+    else
+        heat_strip_edge<T, VEC, PF, CG>(src, dst, ld, nx, ny, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
 }
 
 // Cells a tile task writes: its rows/cols clipped to the interior [1, n-1).
@@ -150,15 +197,15 @@ __host__ __device__ __forceinline__ TileBox heat_tile_box(int64_t nx, int64_t ny
     return b;
 }
 
-// Number of warp strips a tile box splits into when `nwarps` warps share it: row groups of
-// 32*VEC rows (aligned to VEC) times column groups, at least one column per strip.
+// Strips a tile box splits into when `nwarps` warps share it: row groups of OUT written rows
+// (first base = rx0-1 rounded down to a multiple of VEC) times column groups.
 template <int VEC>
 __host__ __device__ __forceinline__ void heat_tile_split(const TileBox & b, int nwarps, int64_t & rbase0,
                                                          int & nrg, int & ncg, int64_t & cols_per)
 {
-    rbase0 = b.rx0 - (b.rx0 % VEC);
-    const int64_t rows = b.rx1 - rbase0;
-    nrg = (int) ((rows + 32 * VEC - 1) / (32 * VEC));
+    rbase0 = (b.rx0 - 1) - ((b.rx0 - 1) % VEC);
+    const int64_t rows = b.rx1 - (rbase0 + 1);
+    nrg = (int) ((rows + StripGeom<VEC>::OUT - 1) / StripGeom<VEC>::OUT);
     ncg = nwarps / (nrg > 0 ? nrg : 1);
     if (ncg < 1) ncg = 1;
     const int64_t cols = b.cy1 - b.cy0;
@@ -169,7 +216,8 @@ __host__ __device__ __forceinline__ void heat_tile_split(const TileBox & b, int 
 // A whole CTA executes one tile task: the warps take the tile's strips round-robin.
 template <typename T, int VEC, int PF, bool CG>
 __device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld, int64_t nx, int64_t ny,
-                                              int64_t x0, int64_t x1, int64_t y0, int64_t y1, double c, bool vec_ok)
+                                              int64_t x0, int64_t x1, int64_t y0, int64_t y1, double c, bool vec_ok,
+                                              int pfd = 0)
 {
     const TileBox b = heat_tile_box(nx, ny, x0, x1, y0, y1);
     if (b.rx0 >= b.rx1 || b.cy0 >= b.cy1) return;
@@ -182,7 +230,7 @@ __device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld
         const int64_t cy0 = b.cy0 + cg * cols_per;
         int64_t cy1 = cy0 + cols_per; if (cy1 > b.cy1) cy1 = b.cy1;
         if (cy0 >= cy1) continue;
-        heat_strip<T, VEC, PF, CG>(src, dst, ld, nx, rbase0 + (int64_t) rg * 32 * VEC, b.rx0, b.rx1, cy0, cy1, c, vec_ok);
+        heat_strip<T, VEC, PF, CG>(src, dst, ld, nx, ny, rbase0 + (int64_t) rg * StripGeom<VEC>::OUT, b.rx0, b.rx1, cy0, cy1, c, vec_ok, pfd);
     }
 }
 
