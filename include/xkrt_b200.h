@@ -73,6 +73,48 @@ typedef struct xkb_access_rec_t {
     uint64_t sizeof_type;
 } xkb_access_rec_t;
 
+/* ---- dependency resolution ------------------------------------------------------------- */
+/* A resolver keeps, per dependency domain, the last writer and the readers since that write
+ * of every elementary cell, in HBM, so tasks can be added in batches (spawn order continues
+ * across batches). It computes the same dependency edges as the reference's domains:
+ * KBLASDependencyTree per (ld, sizeof) and IntervalDependencyTree, driven by
+ * task_dependency_resolve (src/task/task.cc:203-299; include/xkrt/memory/access/blas/dependency-tree.hpp:228-426;
+ * include/xkrt/memory/access/interval/dependency-tree.hpp:225-360), as the set of unique
+ * (predecessor task, successor task) pairs. No task completes while resolving, so no edge is
+ * dropped for a completed predecessor. */
+typedef struct xkb_resolver xkb_resolver_t;
+
+/* Successor graph in device memory (owned by the resolver, valid until its next call). */
+typedef struct xkb_task_graph_t {
+    uint64_t ntasks;
+    uint64_t nedges;
+    const uint32_t * succ_ptr;   /* [ntasks+1] CSR offsets into succ                           */
+    const uint32_t * succ;       /* [nedges] successor task ids, ascending within each task     */
+    const uint32_t * npred;      /* [ntasks] number of unique predecessors = initial wait count */
+} xkb_task_graph_t;
+
+/* Create a resolver working on `stream` (device = current device). Replaces the per-thread
+ * implicit task's dependency domains (include/xkrt/task/task.hpp task_dom_info_t;
+ * include/xkrt/thread/thread.h:159-196). */
+XKB_API int xkb_resolver_create(xkb_resolver_t ** resolver, void * stream);
+XKB_API int xkb_resolver_destroy(xkb_resolver_t * resolver);
+
+/* Resolve a batch of host-resident access records (tasks dense, in spawn order, the first
+ * one numbered like the number of tasks added so far). Replaces, for each task of the batch,
+ * thread_t::resolve (include/xkrt/thread/thread.h:264-271) -> task_dependency_resolve
+ * (src/task/task.cc:285-299). */
+XKB_API int xkb_resolver_add(xkb_resolver_t * resolver, const xkb_access_rec_t * accesses, size_t naccesses);
+
+/* Build (if needed) and return the successor CSR of every task added so far. */
+XKB_API int xkb_resolver_graph(xkb_resolver_t * resolver, xkb_task_graph_t * graph);
+
+/* Copy the unique (pred, succ) pairs, sorted by pred then succ, to host memory as uint32
+ * pairs. *nedges receives the count; XKB_ERANGE if cap_pairs is smaller. */
+XKB_API int xkb_resolver_edges(xkb_resolver_t * resolver, uint32_t * pairs, size_t cap_pairs, size_t * nedges);
+
+/* Counters: tasks added, unique edges, device+host time of the last batch in ms. */
+XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms);
+
 /* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
 /* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float
  * storage, every cell update computed in double and rounded once to float on store. */

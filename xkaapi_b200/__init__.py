@@ -38,6 +38,12 @@ class HeatCfg(ctypes.Structure):
                 ("l2_prefetch_cols", ctypes.c_int), ("cols_per_strip", ctypes.c_int)]
 
 
+class TaskGraph(ctypes.Structure):
+    """xkb_task_graph_t: successor CSR in device memory."""
+    _fields_ = [("ntasks", ctypes.c_uint64), ("nedges", ctypes.c_uint64), ("succ_ptr", ctypes.c_void_p),
+                ("succ", ctypes.c_void_p), ("npred", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "xkb_last_error": (_c.c_char_p, []),
@@ -46,6 +52,13 @@ SIGNATURES = {
     "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step_cfg": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, ctypes.POINTER(HeatCfg), _vp]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
+    "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
+    "xkb_resolver_destroy": (_int, [_vp]),
+    "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
+    "xkb_resolver_graph": (_int, [_vp, ctypes.POINTER(TaskGraph)]),
+    "xkb_resolver_edges": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "xkb_resolver_stats": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                  ctypes.POINTER(ctypes.c_double)]),
 }
 
 
@@ -103,3 +116,50 @@ def heat_step(src, dst, nx, ny, ld, c, stream=None, cfg=None):
 def axpby(a, x, b, y, stream=None):
     """y = a*x + b*y (FP64 torch CUDA tensors)."""
     return check(lib().xkb_axpby(x.numel(), a, x.data_ptr(), b, y.data_ptr(), _stream(stream)))
+
+
+class Resolver:
+    """Batched GPU dependency resolver (xkb_resolver_t). Feed access records (numpy structured
+    array with the 64-byte xkb_access_rec_t layout) in spawn order; read back unique edges or
+    the device successor graph."""
+
+    def __init__(self, stream=None):
+        self._h = ctypes.c_void_p()
+        check(lib().xkb_resolver_create(ctypes.byref(self._h), _stream(stream) if stream is not None else None))
+
+    def add(self, recs):
+        import numpy as np
+        recs = np.ascontiguousarray(recs)
+        assert recs.dtype.itemsize == 64
+        check(lib().xkb_resolver_add(self._h, recs.ctypes.data, len(recs)))
+
+    def edges(self):
+        import numpy as np
+        n = ctypes.c_size_t()
+        rc = lib().xkb_resolver_edges(self._h, None, 0, ctypes.byref(n))
+        if rc not in (XKB_OK, XKB_ERANGE):
+            check(rc)
+        out = np.zeros((n.value, 2), dtype=np.uint32)
+        check(lib().xkb_resolver_edges(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def graph(self):
+        g = TaskGraph()
+        check(lib().xkb_resolver_graph(self._h, ctypes.byref(g)))
+        return g
+
+    def stats(self):
+        nt, ne, ms = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
+        check(lib().xkb_resolver_stats(self._h, ctypes.byref(nt), ctypes.byref(ne), ctypes.byref(ms)))
+        return nt.value, ne.value, ms.value
+
+    def close(self):
+        if self._h:
+            lib().xkb_resolver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,774 @@
+// Batched dependency resolver for R/W/RW accesses on LD-strided matrices and segments.
+//
+// Semantics (what the reference's dependency domains compute; file:line in XKRT):
+//  * per task: LINK every access, then PUT every access (src/task/task.cc:285-299);
+//  * one interval domain for segments, one BLAS domain per (ld, sizeof) created by the first
+//    matrix access naming it, during that task's LINK pass (src/task/task.cc:153-201); a
+//    segment also goes to every BLAS domain that exists at that moment (:240-259), and a new
+//    BLAS domain first replays the PUT of every earlier segment newest-first
+//    (interval/dependency-tree.hpp:355-360 push_front, task.cc:177-198);
+//  * frames: matrix tile -> 1-2 rects (byte row mod ld*s, column) (access.hpp:204-287);
+//    segment -> [a, b) in the interval domain, 3 rects in a BLAS frame (access.hpp:76-139);
+//    a segment's PUT in a BLAS domain only touches rows [a, b) of column 0 of that frame,
+//    because BLAS on_insert tests the access's own rects, which a segment keeps in the
+//    ld = SIZE_MAX frame (access.hpp:479-514, blas/dependency-tree.hpp:228-256);
+//  * per point: LINK(A): W-mode A with readers -> edges from every reader, else edge from
+//    the writer; PUT(A): W-mode -> writer = A, readers = {}; mode == R exactly -> readers += A
+//    (blas/dependency-tree.hpp:295-355).
+//
+// Method (B200): the host turns the accesses of a batch into each domain's ordered op list
+// and keeps a coordinate compression of the domain (elementary cells between all rect
+// boundaries seen so far). On the GPU one CTA owns a region of RX x RY cells: it streams the
+// batch's ops, keeps those overlapping its region with a ballot + block prefix sum (order
+// preserving), and each thread then applies the ops to its own cell's writer/readers state,
+// emitting (pred, succ) pairs; lanes emitting the same pred for the same op are merged with
+// __match_any_sync. A GPU hash set keeps the unique pairs; finalising counts predecessors,
+// scans and scatters the pairs into a successor CSR. Cell state stays in HBM between batches.
+#include "common.cuh"
+#include "scan.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <utility>
+#include <vector>
+
+namespace xkb {
+
+constexpr uint8_t M_R = 1, M_W = 2;
+constexpr int RES_CHUNK_PER_THREAD = 4;
+constexpr unsigned long long EDGE_EMPTY = ~0ull;
+
+struct DOp {            // one op in cell coordinates (24 bytes)
+    int32_t task;
+    uint8_t link;
+    uint8_t mode;
+    uint16_t pad;
+    int32_t cx0, cx1, cy0, cy1;
+};
+
+struct ResolveArgs {
+    const DOp * ops;
+    int nops;
+    int ncx, ncy, nrx;
+    const int * state_in;     // per cell: writer, nreaders, readers[rcap]
+    int * state_out;
+    int rcap;
+    unsigned long long * emit;
+    unsigned long long * emit_count;
+    unsigned long long emit_cap;
+    int * max_readers;        // largest reader count seen (overflow when > rcap)
+};
+
+template <int RX, int RY>
+__global__ void __launch_bounds__(RX * RY)
+resolve_region_kernel(ResolveArgs a)
+{
+    constexpr int NT = RX * RY;
+    constexpr int NW = NT / 32;
+    constexpr int CHUNK = NT * RES_CHUNK_PER_THREAD;
+    extern __shared__ int rd[];                  // readers: rd[k * NT + tid]
+    __shared__ DOp list[CHUNK];
+    __shared__ int wcount[NW];
+    __shared__ int nlist_s;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int rx = blockIdx.x % a.nrx, ry = blockIdx.x / a.nrx;
+    const int gx0 = rx * RX, gy0 = ry * RY;
+    const int gx1 = min(gx0 + RX, a.ncx), gy1 = min(gy0 + RY, a.ncy);
+    const int cx = gx0 + tid % RX, cy = gy0 + tid / RX;
+    const bool valid = cx < a.ncx && cy < a.ncy;
+    const size_t cell = valid ? (size_t) cy * a.ncx + cx : 0;
+    const size_t stride = 2 + (size_t) a.rcap;
+
+    int writer = -1, nr = 0, maxnr = 0;
+    if (valid)
+    {
+        const int * st = a.state_in + cell * stride;
+        writer = st[0]; nr = st[1];
+        for (int k = 0; k < nr && k < a.rcap; ++k) rd[k * NT + tid] = st[2 + k];
+        maxnr = nr;
+    }
+
+    for (int base = 0; base < a.nops; base += CHUNK)
+    {
+        // ---- compact the ops of this chunk that overlap the region, in op order ----------
+        if (tid == 0) nlist_s = 0;
+        __syncthreads();
+        for (int j = 0; j < RES_CHUNK_PER_THREAD; ++j)
+        {
+            const int idx = base + j * NT + tid;
+            DOp op;
+            bool hit = false;
+            if (idx < a.nops)
+            {
+                op = a.ops[idx];
+                hit = op.cx0 < gx1 && gx0 < op.cx1 && op.cy0 < gy1 && gy0 < op.cy1;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) wcount[warp] = __popc(bal);
+            __syncthreads();
+            int off = nlist_s;
+            for (int w = 0; w < warp; ++w) off += wcount[w];
+            if (hit) list[off + __popc(bal & ((1u << lane) - 1))] = op;
+            __syncthreads();
+            if (tid == 0) { int t = 0; for (int w = 0; w < NW; ++w) t += wcount[w]; nlist_s += t; }
+            __syncthreads();
+        }
+        const int nlist = nlist_s;
+
+        // ---- apply them to this thread's cell -----------------------------------------------
+        for (int k = 0; k < nlist; ++k)
+        {
+            const DOp op = list[k];
+            const bool in = valid && op.cx0 <= cx && cx < op.cx1 && op.cy0 <= cy && cy < op.cy1;
+            if (op.link)
+            {
+                const bool from_readers = in && (op.mode & M_W) && nr > 0;
+                const int cnt = from_readers ? min(nr, a.rcap) : ((in && writer >= 0) ? 1 : 0);
+                const int maxcnt = __reduce_max_sync(0xffffffffu, cnt);
+                for (int q = 0; q < maxcnt; ++q)
+                {
+                    const int p = q < cnt ? (from_readers ? rd[q * NT + tid] : writer) : -1;
+                    const unsigned peers = __match_any_sync(0xffffffffu, p);
+                    const bool leader = p >= 0 && lane == __ffs(peers) - 1;
+                    const unsigned em = __ballot_sync(0xffffffffu, leader);
+                    unsigned long long slot0 = 0;
+                    if (lane == __ffs(em) - 1 && em) slot0 = atomicAdd(a.emit_count, (unsigned long long) __popc(em));
+                    slot0 = __shfl_sync(0xffffffffu, slot0, em ? __ffs(em) - 1 : 0);
+                    if (leader)
+                    {
+                        const unsigned long long slot = slot0 + __popc(em & ((1u << lane) - 1));
+                        if (slot < a.emit_cap)
+                            a.emit[slot] = ((unsigned long long) (uint32_t) p << 32) | (uint32_t) op.task;
+                    }
+                }
+            }
+            else if (in)
+            {
+                if (op.mode & M_W) { writer = op.task; nr = 0; }
+                else if (op.mode == M_R)
+                {
+                    if (nr < a.rcap) rd[nr * NT + tid] = op.task;
+                    ++nr;
+                    maxnr = max(maxnr, nr);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (valid)
+    {
+        int * st = a.state_out + cell * stride;
+        st[0] = writer; st[1] = min(nr, a.rcap);
+        for (int k = 0; k < nr && k < a.rcap; ++k) st[2 + k] = rd[k * NT + tid];
+    }
+    if (maxnr > a.rcap) atomicMax(a.max_readers, maxnr);
+}
+
+// New compression refines the old one: every new cell lies inside exactly one old cell (or
+// outside the old domain, where the state is empty).
+__global__ void refine_state_kernel(const int * __restrict__ old_state, int * __restrict__ new_state, size_t stride,
+                                    const int * __restrict__ map_x, const int * __restrict__ map_y, int ncx, int ncy, int old_ncx)
+{
+    const size_t cell = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= (size_t) ncx * ncy) return;
+    const int cx = (int) (cell % ncx), cy = (int) (cell / ncx);
+    const int ox = map_x[cx], oy = map_y[cy];
+    int * dst = new_state + cell * stride;
+    if (ox < 0 || oy < 0) { dst[0] = -1; dst[1] = 0; return; }
+    const int * src = old_state + ((size_t) oy * old_ncx + ox) * stride;
+    const int n = src[1];
+    dst[0] = src[0]; dst[1] = n;
+    for (int k = 0; k < n; ++k) dst[2 + k] = src[2 + k];
+}
+
+__global__ void init_state_kernel(int * state, size_t ncells, size_t stride)
+{
+    const size_t cell = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell < ncells) { state[cell * stride] = -1; state[cell * stride + 1] = 0; }
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long k)
+{
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+    return k;
+}
+
+__global__ void dedupe_kernel(const unsigned long long * __restrict__ emit, size_t n, unsigned long long * table,
+                              unsigned long long mask, unsigned long long * uniq, unsigned long long * nuniq,
+                              unsigned long long uniq_cap)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long key = emit[i];
+    unsigned long long h = mix64(key) & mask;
+    for (unsigned long long probe = 0; probe <= mask; ++probe)
+    {
+        const unsigned long long prev = atomicCAS(table + h, EDGE_EMPTY, key);
+        if (prev == EDGE_EMPTY)
+        {
+            const unsigned long long s = atomicAdd(nuniq, 1ull);
+            if (s < uniq_cap) uniq[s] = key;
+            return;
+        }
+        if (prev == key) return;
+        h = (h + 1) & mask;
+    }
+}
+
+__global__ void count_edges_kernel(const unsigned long long * __restrict__ e, size_t n, uint32_t * nsucc, uint32_t * npred)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = e[i];
+    atomicAdd(nsucc + (uint32_t) (k >> 32), 1u);
+    atomicAdd(npred + (uint32_t) k, 1u);
+}
+
+__global__ void scatter_edges_kernel(const unsigned long long * __restrict__ e, size_t n, uint32_t * cursor, uint32_t * succ)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = e[i];
+    const uint32_t pos = atomicAdd(cursor + (uint32_t) (k >> 32), 1u);
+    succ[pos] = (uint32_t) k;
+}
+
+// Sort each successor list ascending (deterministic CSR). Short lists: one thread, insertion sort.
+__global__ void sort_segments_kernel(const uint32_t * __restrict__ ptr, uint32_t * succ, uint32_t ntasks)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const uint32_t b = ptr[t], e = ptr[t + 1];
+    for (uint32_t i = b + 1; i < e; ++i)
+    {
+        const uint32_t v = succ[i];
+        uint32_t j = i;
+        while (j > b && succ[j - 1] > v) { succ[j] = succ[j - 1]; --j; }
+        succ[j] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+
+struct HRect { uint64_t x0, x1, y0, y1; };
+struct HOp { uint32_t task; uint8_t link; uint8_t mode; HRect r; };
+
+template <typename T>
+struct DevBuf {
+    T * p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    int reserve(size_t n)
+    {
+        if (n <= cap) return XKB_OK;
+        size_t c = cap ? cap : 1024;
+        while (c < n) c *= 2;
+        T * q = nullptr;
+        cudaError_t e = cudaMalloc(&q, c * sizeof(T));
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        if (p) cudaFree(p);
+        p = q; cap = c;
+        return XKB_OK;
+    }
+    int grow_keep(size_t n, size_t used, cudaStream_t st)
+    {
+        if (n <= cap) return XKB_OK;
+        size_t c = cap ? cap : 1024;
+        while (c < n) c *= 2;
+        T * q = nullptr;
+        cudaError_t e = cudaMalloc(&q, c * sizeof(T));
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        if (p && used) { e = cudaMemcpyAsync(q, p, used * sizeof(T), cudaMemcpyDeviceToDevice, st); if (e != cudaSuccess) { cudaFree(q); return xkb_set_cuda_error(e); } }
+        if (p) { cudaStreamSynchronize(st); cudaFree(p); }
+        p = q; cap = c;
+        return XKB_OK;
+    }
+};
+
+// Sorted unique values with a fast path for heavily repeated inputs.
+static void unique_sorted(std::vector<uint64_t> & v)
+{
+    if (v.empty()) return;
+    // linear-probing pre-filter: boundaries repeat massively (tile grids), so keep each value once
+    size_t cap = 1024;
+    std::vector<uint64_t> table(cap, ~0ull);
+    std::vector<uint64_t> out;
+    size_t used = 0;
+    for (uint64_t x : v)
+    {
+        if (x == ~0ull) { out.push_back(x); continue; }
+        if (used * 2 >= cap)
+        {
+            std::vector<uint64_t> t2(cap * 2, ~0ull);
+            for (uint64_t y : table) if (y != ~0ull) {
+                size_t h = (y * 0x9e3779b97f4a7c15ull) >> 20 & (cap * 2 - 1);
+                while (t2[h] != ~0ull) h = (h + 1) & (cap * 2 - 1);
+                t2[h] = y;
+            }
+            table.swap(t2); cap *= 2;
+        }
+        size_t h = (x * 0x9e3779b97f4a7c15ull) >> 20 & (cap - 1);
+        while (table[h] != ~0ull && table[h] != x) h = (h + 1) & (cap - 1);
+        if (table[h] == ~0ull) { table[h] = x; out.push_back(x); ++used; }
+    }
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+    v.swap(out);
+}
+
+struct Domain {
+    bool interval = false;
+    uint64_t ld = 0, s = 0;
+    std::vector<uint64_t> xs, ys;       // compression (sorted unique boundaries)
+    DevBuf<int> state[2];
+    int cur = 0;
+    size_t ncells = 0;
+    std::vector<HOp> ops;               // ops of the batch being resolved
+};
+
+} // namespace xkb
+
+using namespace xkb;
+
+struct xkb_resolver {
+    int rcap = 64;
+    cudaStream_t stream = nullptr;
+    Domain interval;
+    std::vector<std::unique_ptr<Domain>> blas;
+    std::map<std::pair<uint64_t, uint64_t>, size_t> blas_index;
+    std::vector<xkb_access_rec_t> segments;     // every segment so far, spawn order (replay)
+    uint32_t ntasks = 0;
+    // device work buffers
+    DevBuf<DOp> dops;
+    DevBuf<unsigned long long> emit, table, uniq;
+    DevBuf<unsigned long long> counters;        // [0] emit count, [1] unique count
+    DevBuf<int> maxr;
+    size_t nuniq = 0;
+    // graph
+    DevBuf<uint32_t> succ_ptr, succ, npred, tmp;
+    bool graph_valid = false;
+    double last_device_ms = 0;
+};
+
+namespace xkb {
+
+static int seg_rects_blas(uint64_t a, uint64_t b, uint64_t ld, uint64_t s, HRect out[3])
+{
+    const uint64_t LDs = ld * s, size = b - a;
+    const uint64_t x0 = a % LDs, x1 = std::min(x0 + size, LDs), dx10 = x1 - x0;
+    const uint64_t x3 = (size - dx10) % LDs;
+    const uint64_t y0 = a / LDs, y1 = y0 + 1;
+    const uint64_t y3 = y0 + (size - dx10 - x3) / LDs + 2, y2 = y3 - 1;
+    const HRect r[3] = {{x0, x1, y0, y1}, {0, LDs, y1, y2}, {0, x3, y2, y3}};
+    int n = 0;
+    for (const HRect & q : r) if (q.x0 < q.x1 && q.y0 < q.y1) out[n++] = q;
+    return n;
+}
+
+static int mat_rects(const xkb_access_rec_t & r, HRect out[2])
+{
+    const uint64_t s = r.sizeof_type, ld = r.ld, LDs = ld * s;
+    const uint64_t A = r.addr + (r.offset_n * ld + r.offset_m) * s;
+    const uint64_t x0 = A % LDs, y0 = A / LDs;
+    if (x0 + r.m * s <= LDs) { out[0] = {x0, x0 + r.m * s, y0, y0 + r.n}; return 1; }
+    out[0] = {x0, LDs, y0, y0 + r.n};
+    out[1] = {0, r.m * s - (LDs - x0), y0 + 1, y0 + r.n + 1};
+    return 2;
+}
+
+static void push_ops(Domain & d, bool link, const xkb_access_rec_t & r)
+{
+    HRect rects[3];
+    int n;
+    if (d.interval) { rects[0] = {r.addr, r.ld, 0, 1}; n = 1; }
+    else if (r.type == XKB_ACCESS_TYPE_SEGMENT) n = seg_rects_blas(r.addr, r.ld, d.ld, d.s, rects);
+    else n = mat_rects(r, rects);
+    for (int i = 0; i < n; ++i)
+    {
+        HRect q = rects[i];
+        if (!link && !d.interval && r.type == XKB_ACCESS_TYPE_SEGMENT)
+        {
+            q.x0 = std::max(q.x0, r.addr); q.x1 = std::min(q.x1, r.ld);
+            q.y1 = std::min<uint64_t>(q.y1, 1);
+            if (q.x0 >= q.x1 || q.y0 >= q.y1) continue;
+        }
+        d.ops.push_back({r.task, (uint8_t) link, r.mode, q});
+    }
+}
+
+static int validate(const xkb_access_rec_t * recs, size_t n, uint32_t first_task)
+{
+    uint32_t prev = first_task;
+    for (size_t i = 0; i < n; ++i)
+    {
+        const xkb_access_rec_t & r = recs[i];
+        if (r.task < prev || r.task > prev + 1 || (i == 0 && r.task != first_task))
+            return xkb_set_error(XKB_EINVAL, "resolver: access %zu: task ids must be dense, in spawn order, continuing at %u", i, first_task);
+        prev = r.task;
+        if (r.mode == 0 || (r.mode & ~15u)) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: bad mode %u", i, r.mode);
+        if (r.type == XKB_ACCESS_TYPE_SEGMENT) {
+            if (r.ld <= r.addr) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: empty segment", i);
+        } else if (r.type == XKB_ACCESS_TYPE_BLAS_MATRIX) {
+            if (!r.ld || !r.sizeof_type || !r.m || !r.n || r.m > r.ld)
+                return xkb_set_error(XKB_EINVAL, "resolver: access %zu: bad matrix tile", i);
+        } else return xkb_set_error(XKB_EINVAL, "resolver: access %zu: unsupported access type %u", i, r.type);
+    }
+    return XKB_OK;
+}
+
+// Build every domain's op list for the batch, in the order the reference performs them.
+static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
+{
+    for (size_t i = 0; i < n;)
+    {
+        size_t j = i;
+        while (j < n && recs[j].task == recs[i].task) ++j;
+        for (size_t a = i; a < j; ++a)                          // LINK pass
+        {
+            const xkb_access_rec_t & r = recs[a];
+            if (r.type == XKB_ACCESS_TYPE_SEGMENT)
+            {
+                push_ops(R->interval, true, r);
+                for (auto & d : R->blas) push_ops(*d, true, r);
+            }
+            else
+            {
+                const auto key = std::make_pair(r.ld, r.sizeof_type);
+                auto it = R->blas_index.find(key);
+                if (it == R->blas_index.end())
+                {
+                    std::unique_ptr<Domain> d(new Domain());
+                    d->ld = r.ld; d->s = r.sizeof_type;
+                    for (auto k = R->segments.rbegin(); k != R->segments.rend(); ++k) push_ops(*d, false, *k);
+                    R->blas.push_back(std::move(d));
+                    it = R->blas_index.emplace(key, R->blas.size() - 1).first;
+                }
+                push_ops(*R->blas[it->second], true, r);
+            }
+        }
+        for (size_t a = i; a < j; ++a)                          // PUT pass
+        {
+            const xkb_access_rec_t & r = recs[a];
+            if (r.type == XKB_ACCESS_TYPE_SEGMENT)
+            {
+                push_ops(R->interval, false, r);
+                for (auto & d : R->blas) push_ops(*d, false, r);
+                R->segments.push_back(r);
+            }
+            else
+                push_ops(*R->blas[R->blas_index.at({r.ld, r.sizeof_type})], false, r);
+        }
+        i = j;
+    }
+}
+
+// Extend the domain's compression with the batch's boundaries; remap the device state when
+// the cell grid changes.
+static int refine_domain(xkb_resolver * R, Domain & d)
+{
+    std::vector<uint64_t> xs = d.xs, ys = d.ys;
+    xs.reserve(xs.size() + 2 * d.ops.size()); ys.reserve(ys.size() + 2 * d.ops.size());
+    for (const HOp & o : d.ops) { xs.push_back(o.r.x0); xs.push_back(o.r.x1); ys.push_back(o.r.y0); ys.push_back(o.r.y1); }
+    unique_sorted(xs); unique_sorted(ys);
+    if (xs.size() < 2 || ys.size() < 2) { d.xs = xs; d.ys = ys; return XKB_OK; }
+    const bool same = xs == d.xs && ys == d.ys;
+    const size_t ncx = xs.size() - 1, ncy = ys.size() - 1, ncells = ncx * ncy;
+    const size_t stride = 2 + (size_t) R->rcap;
+    if (same && d.ncells == ncells) return XKB_OK;
+    int rc;
+    DevBuf<int> & out = d.state[d.cur ^ 1];
+    if ((rc = out.reserve(ncells * stride))) return rc;
+    if (d.ncells == 0)
+    {
+        init_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(out.p, ncells, stride);
+    }
+    else
+    {
+        const size_t old_ncx = d.xs.size() - 1;
+        std::vector<int> mx(ncx), my(ncy);
+        for (size_t i = 0; i < ncx; ++i) {
+            const uint64_t v = xs[i];
+            if (v < d.xs.front() || v >= d.xs.back()) mx[i] = -1;
+            else mx[i] = (int) (std::upper_bound(d.xs.begin(), d.xs.end(), v) - d.xs.begin()) - 1;
+        }
+        for (size_t i = 0; i < ncy; ++i) {
+            const uint64_t v = ys[i];
+            if (v < d.ys.front() || v >= d.ys.back()) my[i] = -1;
+            else my[i] = (int) (std::upper_bound(d.ys.begin(), d.ys.end(), v) - d.ys.begin()) - 1;
+        }
+        DevBuf<int> dm;
+        if ((rc = dm.reserve(ncx + ncy))) return rc;
+        XKB_CUDA_TRY(cudaMemcpyAsync(dm.p, mx.data(), ncx * sizeof(int), cudaMemcpyHostToDevice, R->stream));
+        XKB_CUDA_TRY(cudaMemcpyAsync(dm.p + ncx, my.data(), ncy * sizeof(int), cudaMemcpyHostToDevice, R->stream));
+        refine_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(
+            d.state[d.cur].p, out.p, stride, dm.p, dm.p + ncx, (int) ncx, (int) ncy, (int) old_ncx);
+        XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));   // dm is freed on return
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    d.cur ^= 1;
+    d.xs.swap(xs); d.ys.swap(ys); d.ncells = ncells;
+    return XKB_OK;
+}
+
+static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t nops, int rcap_smem_ok)
+{
+    (void) rcap_smem_ok;
+    const int ncx = (int) d.xs.size() - 1, ncy = (int) d.ys.size() - 1;
+    ResolveArgs a;
+    a.ops = R->dops.p + op_offset; a.nops = (int) nops;
+    a.ncx = ncx; a.ncy = ncy;
+    a.state_in = d.state[d.cur].p; a.state_out = d.state[d.cur ^ 1].p;
+    a.rcap = R->rcap;
+    a.emit = R->emit.p; a.emit_count = R->counters.p; a.emit_cap = R->emit.cap;
+    a.max_readers = R->maxr.p;
+    if (ncy == 1)
+    {
+        constexpr int RX = 64, RY = 1;
+        a.nrx = (ncx + RX - 1) / RX;
+        const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        resolve_region_kernel<RX, RY><<<(unsigned) a.nrx, RX * RY, smem, R->stream>>>(a);
+    }
+    else
+    {
+        constexpr int RX = 8, RY = 8;
+        a.nrx = (ncx + RX - 1) / RX;
+        const int nry = (ncy + RY - 1) / RY;
+        const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        resolve_region_kernel<RX, RY><<<(unsigned) (a.nrx * nry), RX * RY, smem, R->stream>>>(a);
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
+static int map_ops(Domain & d, std::vector<DOp> & out)
+{
+    for (const HOp & o : d.ops)
+    {
+        DOp q;
+        q.task = (int32_t) o.task; q.link = o.link; q.mode = o.mode; q.pad = 0;
+        q.cx0 = (int32_t) (std::lower_bound(d.xs.begin(), d.xs.end(), o.r.x0) - d.xs.begin());
+        q.cx1 = (int32_t) (std::lower_bound(d.xs.begin(), d.xs.end(), o.r.x1) - d.xs.begin());
+        q.cy0 = (int32_t) (std::lower_bound(d.ys.begin(), d.ys.end(), o.r.y0) - d.ys.begin());
+        q.cy1 = (int32_t) (std::lower_bound(d.ys.begin(), d.ys.end(), o.r.y1) - d.ys.begin());
+        out.push_back(q);
+    }
+    return XKB_OK;
+}
+
+static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
+{
+    int rc;
+    build_ops(R, recs, n);
+    std::vector<Domain *> doms;
+    if (!R->interval.ops.empty()) doms.push_back(&R->interval);
+    for (auto & d : R->blas) if (!d->ops.empty()) doms.push_back(d.get());
+
+    std::vector<DOp> all;
+    std::vector<size_t> offs;
+    for (Domain * d : doms)
+    {
+        if ((rc = refine_domain(R, *d))) return rc;
+        offs.push_back(all.size());
+        map_ops(*d, all);
+    }
+    if ((rc = R->dops.reserve(all.size() ? all.size() : 1))) return rc;
+    if (!all.empty())
+        XKB_CUDA_TRY(cudaMemcpyAsync(R->dops.p, all.data(), all.size() * sizeof(DOp), cudaMemcpyHostToDevice, R->stream));
+
+    size_t emit_guess = std::max<size_t>(1 << 16, all.size() * 2);
+    for (int attempt = 0; attempt < 6; ++attempt)
+    {
+        if ((rc = R->emit.reserve(emit_guess))) return rc;
+        if ((rc = R->counters.reserve(2))) return rc;
+        if ((rc = R->maxr.reserve(1))) return rc;
+        XKB_CUDA_TRY(cudaMemsetAsync(R->counters.p, 0, 2 * sizeof(unsigned long long), R->stream));
+        XKB_CUDA_TRY(cudaMemsetAsync(R->maxr.p, 0, sizeof(int), R->stream));
+        for (size_t k = 0; k < doms.size(); ++k)
+        {
+            const size_t nops = (k + 1 < doms.size() ? offs[k + 1] : all.size()) - offs[k];
+            // states must exist for every cell (ncells > 0 when the domain has >= 1 op)
+            if ((rc = R->emit.reserve(emit_guess))) return rc;
+            if (doms[k]->ncells == 0) continue;
+            if ((rc = doms[k]->state[doms[k]->cur ^ 1].reserve(doms[k]->ncells * (2 + (size_t) R->rcap)))) return rc;
+            if ((rc = launch_domain(R, *doms[k], offs[k], nops, 1))) return rc;
+        }
+        unsigned long long nemit = 0;
+        int maxr = 0;
+        XKB_CUDA_TRY(cudaMemcpyAsync(&nemit, R->counters.p, sizeof(nemit), cudaMemcpyDeviceToHost, R->stream));
+        XKB_CUDA_TRY(cudaMemcpyAsync(&maxr, R->maxr.p, sizeof(int), cudaMemcpyDeviceToHost, R->stream));
+        XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
+        if (maxr > R->rcap)
+        {
+            // a cell held more readers than the state keeps: widen the state and redo the batch
+            int newcap = R->rcap;
+            while (newcap < maxr) newcap *= 2;
+            if ((size_t) newcap * 64 * sizeof(int) > 200 * 1024)
+                return xkb_set_error(XKB_ERANGE, "resolver: %d concurrent readers of one cell exceed the supported maximum", maxr);
+            for (Domain * d : doms) {
+                // re-layout the current state with the wider stride
+                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
+                std::vector<int> h(ncells * so);
+                if (ncells) XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+                std::vector<int> g(ncells * sn, 0);
+                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
+                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
+                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
+                if (ncells) XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
+            }
+            for (auto & d : R->blas) if (d->ops.empty() && d->ncells) {
+                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
+                std::vector<int> h(ncells * so);
+                XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+                std::vector<int> g(ncells * sn, 0);
+                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
+                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
+                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
+                XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
+            }
+            if (R->interval.ops.empty() && R->interval.ncells) {
+                Domain * d = &R->interval;
+                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
+                std::vector<int> h(ncells * so);
+                XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+                std::vector<int> g(ncells * sn, 0);
+                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
+                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
+                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
+                XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
+            }
+            R->rcap = newcap;
+            continue;
+        }
+        if (nemit > R->emit.cap) { emit_guess = (size_t) nemit; continue; }
+
+        // success: unique the emitted pairs into the accumulated edge list
+        if (nemit)
+        {
+            size_t tcap = 1024;
+            while (tcap < 2 * nemit) tcap *= 2;
+            if ((rc = R->table.reserve(tcap))) return rc;
+            if ((rc = R->uniq.grow_keep(R->nuniq + nemit, R->nuniq, R->stream))) return rc;
+            XKB_CUDA_TRY(cudaMemsetAsync(R->table.p, 0xff, tcap * sizeof(unsigned long long), R->stream));
+            unsigned long long nu0 = R->nuniq;
+            XKB_CUDA_TRY(cudaMemcpyAsync(R->counters.p + 1, &nu0, sizeof(nu0), cudaMemcpyHostToDevice, R->stream));
+            dedupe_kernel<<<(unsigned) ((nemit + 255) / 256), 256, 0, R->stream>>>(R->emit.p, nemit, R->table.p, tcap - 1,
+                                                                                 R->uniq.p, R->counters.p + 1, R->uniq.cap);
+            XKB_CUDA_TRY(cudaGetLastError());
+            unsigned long long nu = 0;
+            XKB_CUDA_TRY(cudaMemcpyAsync(&nu, R->counters.p + 1, sizeof(nu), cudaMemcpyDeviceToHost, R->stream));
+            XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
+            R->nuniq = nu;
+        }
+        for (Domain * d : doms) { d->cur ^= 1; d->ops.clear(); }
+        return XKB_OK;
+    }
+    return xkb_set_error(XKB_ERANGE, "resolver: batch did not fit after resizing");
+}
+
+static int build_graph(xkb_resolver * R)
+{
+    int rc;
+    const size_t nt = R->ntasks, ne = R->nuniq;
+    if ((rc = R->succ_ptr.reserve(nt + 1))) return rc;
+    if ((rc = R->npred.reserve(nt + 1))) return rc;
+    if ((rc = R->succ.reserve(ne ? ne : 1))) return rc;
+    if ((rc = R->tmp.reserve(nt + 1 + (nt + 1) / SCAN_TILE + 2))) return rc;
+    cudaStream_t st = R->stream;
+    XKB_CUDA_TRY(cudaMemsetAsync(R->succ_ptr.p, 0, (nt + 1) * sizeof(uint32_t), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(R->npred.p, 0, (nt + 1) * sizeof(uint32_t), st));
+    if (ne) count_edges_kernel<<<(unsigned) ((ne + 255) / 256), 256, 0, st>>>(R->uniq.p, ne, R->succ_ptr.p, R->npred.p);
+    if ((rc = device_exclusive_scan(R->succ_ptr.p, R->succ_ptr.p, nt + 1, R->tmp.p + nt + 1, nullptr, st))) return rc;
+    XKB_CUDA_TRY(cudaMemcpyAsync(R->tmp.p, R->succ_ptr.p, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    if (ne) scatter_edges_kernel<<<(unsigned) ((ne + 255) / 256), 256, 0, st>>>(R->uniq.p, ne, R->tmp.p, R->succ.p);
+    if (nt) sort_segments_kernel<<<(unsigned) ((nt + 255) / 256), 256, 0, st>>>(R->succ_ptr.p, R->succ.p, (uint32_t) nt);
+    XKB_CUDA_TRY(cudaGetLastError());
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    R->graph_valid = true;
+    return XKB_OK;
+}
+
+} // namespace xkb
+
+extern "C" int xkb_resolver_create(xkb_resolver_t ** out, void * stream)
+{
+    if (!out) return xkb_set_error(XKB_EINVAL, "resolver_create: null output");
+    int dev;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    xkb_resolver * R = new (std::nothrow) xkb_resolver();
+    if (!R) return xkb_set_error(XKB_ENOMEM, "resolver_create: out of host memory");
+    R->interval.interval = true;
+    R->stream = (cudaStream_t) stream;
+    *out = R;
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_destroy(xkb_resolver_t * R)
+{
+    if (R) { cudaStreamSynchronize(R->stream); delete R; }
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * recs, size_t n)
+{
+    if (!R || (n && !recs)) return xkb_set_error(XKB_EINVAL, "resolver_add: bad arguments");
+    if (n == 0) return XKB_OK;
+    int rc = validate(recs, n, R->ntasks);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaEventRecord(e0, R->stream);
+    rc = resolve_batch(R, recs, n);
+    if (rc == XKB_OK) { R->ntasks = recs[n - 1].task + 1; R->graph_valid = false; }
+    cudaEventRecord(e1, R->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0; cudaEventElapsedTime(&ms, e0, e1);
+    R->last_device_ms = ms;
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    return rc;
+}
+
+extern "C" int xkb_resolver_graph(xkb_resolver_t * R, xkb_task_graph_t * g)
+{
+    if (!R || !g) return xkb_set_error(XKB_EINVAL, "resolver_graph: bad arguments");
+    if (!R->graph_valid) { int rc = build_graph(R); if (rc) return rc; }
+    g->ntasks = R->ntasks;
+    g->nedges = R->nuniq;
+    g->succ_ptr = R->succ_ptr.p;
+    g->succ = R->succ.p;
+    g->npred = R->npred.p;
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_edges(xkb_resolver_t * R, uint32_t * pairs, size_t cap_pairs, size_t * nedges)
+{
+    if (!R || !nedges) return xkb_set_error(XKB_EINVAL, "resolver_edges: bad arguments");
+    if (!R->graph_valid) { int rc = build_graph(R); if (rc) return rc; }
+    *nedges = R->nuniq;
+    if (R->nuniq > cap_pairs) return xkb_set_error(XKB_ERANGE, "resolver_edges: %zu pairs needed", R->nuniq);
+    if (!pairs || R->nuniq == 0) return XKB_OK;
+    std::vector<uint32_t> ptr(R->ntasks + 1), succ(R->nuniq);
+    XKB_CUDA_TRY(cudaMemcpy(ptr.data(), R->succ_ptr.p, ptr.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    XKB_CUDA_TRY(cudaMemcpy(succ.data(), R->succ.p, succ.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    size_t k = 0;
+    for (uint32_t t = 0; t < R->ntasks; ++t)
+        for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i) { pairs[2 * k] = t; pairs[2 * k + 1] = succ[i]; ++k; }
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_stats(xkb_resolver_t * R, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms)
+{
+    if (!R) return xkb_set_error(XKB_EINVAL, "resolver_stats: null resolver");
+    if (ntasks) *ntasks = R->ntasks;
+    if (nedges) *nedges = R->nuniq;
+    if (last_batch_ms) *last_batch_ms = R->last_device_ms;
+    return XKB_OK;
+}
