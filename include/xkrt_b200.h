@@ -115,6 +115,51 @@ XKB_API int xkb_resolver_edges(xkb_resolver_t * resolver, uint32_t * pairs, size
 /* Counters: tasks added, unique edges, device+host time of the last batch in ms. */
 XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms);
 
+/* ---- tasks and the device scheduler ------------------------------------------------------ */
+/* Built-in task bodies the device scheduler can run inline (the reference runs them as
+ * per-task kernel launches through a format's launcher, include/xkrt/driver/kernel-launcher.h:44-51). */
+#define XKB_TASK_NOOP      0   /* placement / first-touch task with no body (src/memory/distribute.cc:86-170) */
+#define XKB_TASK_HEAT_F64  1   /* heat tile, FP64 grids                                      */
+#define XKB_TASK_HEAT_F32  2   /* heat tile, FP32 storage with FP64 arithmetic               */
+#define XKB_TASK_AXPBY     3   /* y[lo:hi] = a*x[lo:hi] + b*y[lo:hi], FP64                    */
+
+/* 64-byte task descriptor. heat: whole grids src/dst (device pointers, column-major, ld),
+ * nx x ny, the tile's rows [x0,x1) x cols [y0,y1) (only interior cells are written), c.
+ * axpby: device vectors x, y, element range [lo, hi), scalars a, b. */
+typedef struct xkb_task_desc_t {
+    uint32_t kind;
+    uint32_t flags;
+    union {
+        struct { uint64_t src, dst; int64_t ld; int32_t nx, ny, x0, x1, y0, y1; double c; } heat;
+        struct { uint64_t x, y; int64_t lo, hi; double a, b; } axpby;
+        uint8_t raw[56];
+    } u;
+} xkb_task_desc_t;
+
+/* Execution forms of a resolved task graph. */
+#define XKB_FORM_PERSISTENT 0  /* one persistent kernel, device ready queue, inline task bodies   */
+#define XKB_FORM_PLAIN      1  /* one kernel launch per task in spawn order (the reference's path) */
+#define XKB_FORM_GRAPH      2  /* CUDA graph: one kernel node per task, one edge per dependency    */
+
+typedef struct xkb_sched xkb_sched_t;
+
+/* Scheduler bound to `stream`. Replaces the device threads' ready queues and launch loop
+ * (src/sched.cc:249-351, :413-505) and completion/successor release (src/task.cc:160-247). */
+XKB_API int xkb_sched_create(xkb_sched_t ** sched, void * stream);
+XKB_API int xkb_sched_destroy(xkb_sched_t * sched);
+/* Host array of task descriptors, in spawn order (task i of the graph = tasks[i]); copied. */
+XKB_API int xkb_sched_set_tasks(xkb_sched_t * sched, const xkb_task_desc_t * tasks, size_t ntasks);
+/* Longest time a persistent CTA waits for its next queue slot before it gives up and reports
+ * XKB_ETIMEDOUT (default 10 s). */
+XKB_API int xkb_sched_set_timeout(xkb_sched_t * sched, double seconds);
+/* CTAs of the persistent kernel (default: SMs x resident CTAs per SM). */
+XKB_API int xkb_sched_set_grid(xkb_sched_t * sched, int ctas);
+/* Enqueue one execution of the whole graph on the scheduler's stream (asynchronous). */
+XKB_API int xkb_sched_run(xkb_sched_t * sched, const xkb_task_graph_t * graph, int form);
+/* Wait for the stream; *executed = tasks the persistent kernel ran. Returns XKB_ETIMEDOUT if
+ * a device wait ran out of time (the kernel returned; the context stays usable). */
+XKB_API int xkb_sched_wait(xkb_sched_t * sched, uint64_t * executed);
+
 /* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
 /* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float
  * storage, every cell update computed in double and rounded once to float on store. */

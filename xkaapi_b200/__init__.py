@@ -19,6 +19,8 @@ XKB_ETIMEDOUT = -110
 XKB_ENODEV = -19
 XKB_ECUDA = -1000
 F64, F32 = 0, 1
+TASK_NOOP, TASK_HEAT_F64, TASK_HEAT_F32, TASK_AXPBY = 0, 1, 2, 3
+FORM_PERSISTENT, FORM_PLAIN, FORM_GRAPH = 0, 1, 2
 
 _lib = None
 
@@ -52,6 +54,13 @@ SIGNATURES = {
     "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step_cfg": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, ctypes.POINTER(HeatCfg), _vp]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
+    "xkb_sched_create": (_int, [ctypes.POINTER(_vp), _vp]),
+    "xkb_sched_destroy": (_int, [_vp]),
+    "xkb_sched_set_tasks": (_int, [_vp, _vp, ctypes.c_size_t]),
+    "xkb_sched_set_timeout": (_int, [_vp, _dbl]),
+    "xkb_sched_set_grid": (_int, [_vp, _int]),
+    "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
+    "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_resolver_destroy": (_int, [_vp]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
@@ -163,3 +172,76 @@ class Resolver:
             self.close()
         except Exception:
             pass
+
+
+def task_desc_dtype():
+    """numpy dtype of xkb_task_desc_t (64 bytes); heat and axpby views share the union bytes."""
+    import numpy as np
+    return np.dtype({"names": ["kind", "flags", "src", "dst", "ld", "nx", "ny", "x0", "x1", "y0", "y1", "c"],
+                     "formats": ["<u4", "<u4", "<u8", "<u8", "<i8", "<i4", "<i4", "<i4", "<i4", "<i4", "<i4", "<f8"],
+                     "offsets": [0, 4, 8, 16, 24, 32, 36, 40, 44, 48, 52, 56], "itemsize": 64})
+
+
+def axpby_desc_dtype():
+    import numpy as np
+    return np.dtype({"names": ["kind", "flags", "x", "y", "lo", "hi", "a", "b"],
+                     "formats": ["<u4", "<u4", "<u8", "<u8", "<i8", "<i8", "<f8", "<f8"],
+                     "offsets": [0, 4, 8, 16, 24, 32, 40, 48], "itemsize": 64})
+
+
+class Scheduler:
+    """Device scheduler (xkb_sched_t): runs a resolved task graph in one of three forms."""
+
+    def __init__(self, stream=None):
+        self._h = ctypes.c_void_p()
+        check(lib().xkb_sched_create(ctypes.byref(self._h), _stream(stream) if stream is not None else None))
+
+    def set_tasks(self, descs):
+        import numpy as np
+        descs = np.ascontiguousarray(descs)
+        assert descs.dtype.itemsize == 64
+        check(lib().xkb_sched_set_tasks(self._h, descs.ctypes.data, len(descs)))
+
+    def set_timeout(self, seconds):
+        check(lib().xkb_sched_set_timeout(self._h, seconds))
+
+    def set_grid(self, ctas):
+        check(lib().xkb_sched_set_grid(self._h, ctas))
+
+    def run(self, graph, form=FORM_PERSISTENT):
+        check(lib().xkb_sched_run(self._h, ctypes.byref(graph), form))
+
+    def wait(self):
+        n = ctypes.c_uint64()
+        check(lib().xkb_sched_wait(self._h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if self._h:
+            lib().xkb_sched_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def heat_task_descs(src_ptrs, nx, ny, ld, tsx, tsy, steps, c, f32=False):
+    """Descriptors of the heat-diffusion-2d tile tasks in spawn order
+    (examples/heat-diffusion-2d/src/main.cc:569-581: tile_x outer, tile_y inner, grids swap
+    every step). src_ptrs = (grid A device pointer, grid B device pointer)."""
+    import numpy as np
+    ntx, nty = -(-nx // tsx), -(-ny // tsy)
+    per = ntx * nty
+    d = np.zeros(per * steps, dtype=task_desc_dtype())
+    tx = np.repeat(np.arange(ntx), nty); ty = np.tile(np.arange(nty), ntx)
+    for s in range(steps):
+        blk = d[s * per:(s + 1) * per]
+        blk["kind"] = TASK_HEAT_F32 if f32 else TASK_HEAT_F64
+        blk["src"], blk["dst"] = (src_ptrs[0], src_ptrs[1]) if s % 2 == 0 else (src_ptrs[1], src_ptrs[0])
+        blk["ld"], blk["nx"], blk["ny"], blk["c"] = ld, nx, ny, c
+        blk["x0"] = tx * tsx; blk["x1"] = np.minimum(tx * tsx + tsx, nx)
+        blk["y0"] = ty * tsy; blk["y1"] = np.minimum(ty * tsy + tsy, ny)
+    return d

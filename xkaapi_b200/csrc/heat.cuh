@@ -197,15 +197,127 @@ __host__ __device__ __forceinline__ TileBox heat_tile_box(int64_t nx, int64_t ny
     return b;
 }
 
-// Strips a tile box splits into when `nwarps` warps share it: row groups of OUT written rows
-// (first base = rx0-1 rounded down to a multiple of VEC) times column groups.
+// Tile tasks use HALO strips: a strip based at rbase (multiple of VEC) writes the rows
+// [rbase, rbase + 32*VEC) it loads; lanes 0 and 31 fetch the north/south halo cell of each
+// column. A 128-row FP64 tile is then exactly two strips (overlapping strips would need three).
+template <typename T, int VEC, int PF, bool CG, bool FAST>
+__device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                                     int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
+                                                     int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t r = rbase + (int64_t) lane * VEC;
+    const int64_t rn = rbase - 1, rs = rbase + 32 * VEC;
+    const bool has_n = lane == 0 && rn >= 0, has_s = lane == 31 && rs < nx;
+    const bool lane_rows = (r + VEC > rx0) && (r < rx1);
+    const bool full_store = vec_ok && r >= rx0 && r + VEC <= rx1;
+    int64_t pf_rows = nx - rbase; if (pf_rows > 32 * VEC) pf_rows = 32 * VEC;
+    const uint32_t pf_bytes = (uint32_t) ((pf_rows * (int64_t) sizeof(T)) & ~(int64_t) 15);
+    const bool pf_on = pfd > 0 && vec_ok && pf_bytes > 0;
+    const T * __restrict__ sp = src + r;
+    T * __restrict__ dp = dst + r;
+    auto load = [&](int64_t j) -> Cells<T, VEC> {
+        if constexpr (FAST) {
+            Cells<T, VEC> q;
+            const T * p = sp + j * ld;
+            if constexpr (VEC == 2 && sizeof(T) == 8) {
+                double2 v = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
+                q.v[0] = v.x; q.v[1] = v.y;
+            } else {
+                float4 v = CG ? __ldcg((const float4 *) p) : __ldg((const float4 *) p);
+                q.v[0] = v.x; q.v[1] = v.y; q.v[2] = v.z; q.v[3] = v.w;
+            }
+            return q;
+        } else {
+            return ld_cells<T, VEC, CG>(src, ld, nx, r, j, vec_ok);
+        }
+    };
+    Cells<T, VEC> west = load(cy0 - 1);
+    Cells<T, VEC> cur  = load(cy0);
+    for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
+    {
+        if (pf_on && lane < PF)
+        {
+            const int64_t jp = j0 + pfd + lane;
+            if (jp <= cy1) l2_prefetch_bulk(src + jp * ld + rbase, pf_bytes);
+        }
+        Cells<T, VEC> nxt[PF];
+        T hn[PF], hs[PF];
+#pragma unroll
+        for (int k = 0; k < PF; ++k)
+        {
+            if (j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
+            const int64_t jc = j0 + k;
+            hn[k] = (has_n && jc < cy1) ? ld_scalar<CG>(src + jc * ld + rn) : T(0);
+            hs[k] = (has_s && jc < cy1) ? ld_scalar<CG>(src + jc * ld + rs) : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < PF; ++k)
+        {
+            const int64_t jc = j0 + k;
+            if (jc >= cy1) break;                        // warp-uniform
+            T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
+            T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
+            if (lane == 0)  north = hn[k];
+            if (lane == 31) south = hs[k];
+            if (lane_rows)
+            {
+                Cells<T, VEC> out;
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                {
+                    const double sv = (double) cur.v[e];
+                    const double up = (double) (e == 0 ? north : cur.v[e - 1]);
+                    const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
+                    out.v[e] = (T) heat_update(sv, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
+                }
+                T * q = dp + jc * ld;
+                if (full_store)
+                {
+                    if constexpr (VEC == 2 && sizeof(T) == 8) *(double2 *) q = make_double2(out.v[0], out.v[1]);
+                    else *(float4 *) q = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e)
+                        if (r + e >= rx0 && r + e < rx1) q[e] = out.v[e];
+                }
+            }
+            west = cur;
+            cur = nxt[k];
+        }
+    }
+}
+
+template <typename T, int VEC, int PF, bool CG>
+__device__ __noinline__ void heat_strip_halo_edge(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                                  int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
+                                                  int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
+{
+    heat_strip_halo_impl<T, VEC, 2, CG, false>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
+}
+
+template <typename T, int VEC, int PF, bool CG>
+__device__ __forceinline__ void heat_strip_halo(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
+                                                int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
+                                                int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
+{
+    if (vec_ok && rbase >= 0 && rbase + 32 * VEC <= nx)
+        heat_strip_halo_impl<T, VEC, PF, CG, true>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
+    else
+        heat_strip_halo_edge<T, VEC, PF, CG>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
+}
+
+// Strips a tile box splits into when `nwarps` warps share it: row groups of 32*VEC rows
+// (first base = rx0 rounded down to a multiple of VEC) times column groups.
 template <int VEC>
 __host__ __device__ __forceinline__ void heat_tile_split(const TileBox & b, int nwarps, int64_t & rbase0,
                                                          int & nrg, int & ncg, int64_t & cols_per)
 {
-    rbase0 = (b.rx0 - 1) - ((b.rx0 - 1) % VEC);
-    const int64_t rows = b.rx1 - (rbase0 + 1);
-    nrg = (int) ((rows + StripGeom<VEC>::OUT - 1) / StripGeom<VEC>::OUT);
+    rbase0 = b.rx0 - (b.rx0 % VEC);
+    const int64_t rows = b.rx1 - rbase0;
+    nrg = (int) ((rows + 32 * VEC - 1) / (32 * VEC));
     ncg = nwarps / (nrg > 0 ? nrg : 1);
     if (ncg < 1) ncg = 1;
     const int64_t cols = b.cy1 - b.cy0;
@@ -230,7 +342,7 @@ __device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld
         const int64_t cy0 = b.cy0 + cg * cols_per;
         int64_t cy1 = cy0 + cols_per; if (cy1 > b.cy1) cy1 = b.cy1;
         if (cy0 >= cy1) continue;
-        heat_strip<T, VEC, PF, CG>(src, dst, ld, nx, ny, rbase0 + (int64_t) rg * StripGeom<VEC>::OUT, b.rx0, b.rx1, cy0, cy1, c, vec_ok, pfd);
+        heat_strip_halo<T, VEC, PF, CG>(src, dst, ld, nx, rbase0 + (int64_t) rg * 32 * VEC, b.rx0, b.rx1, cy0, cy1, c, vec_ok, pfd);
     }
 }
 

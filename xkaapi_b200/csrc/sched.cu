@@ -1,0 +1,430 @@
+// Device-side ready-queue scheduler and the three execution forms of a resolved task graph.
+//
+// Reference behaviour replaced (XKRT, file:line): a task becomes ready when its wait counter
+// reaches 0 (include/xkrt/task/task.hpp:518-551), is queued (src/sched.cc:413-455), executed
+// by a device thread that launches its kernel (src/sched.cc:249-351, :469-505), and on
+// completion decrements each successor's counter, queueing those that reach 0
+// (src/task.cc:160-247).
+//
+//  * PERSISTENT: one kernel, one CTA per resident slot. CTA thread 0 takes the next queue
+//    slot (atomicAdd on head) and waits, with a time limit, for a task id to be published
+//    there; the CTA runs the built-in tile body; after a fence and a barrier, warp 0 decrements
+//    the successors' counters with acq_rel atomics and publishes every successor that reaches
+//    zero with a release store. Every queue slot is written exactly once (a task is pushed
+//    once), so the queue is a plain array of ntasks slots. Tile data written inside the kernel
+//    is read back with L1-bypassing loads.
+//  * PLAIN: the host launches one kernel per task in spawn order (a topological order) on one
+//    stream -- the reference's one-launch-per-task device path.
+//  * GRAPH: the task graph becomes a CUDA graph (one kernel node per task, one edge per
+//    dependency), instantiated once and replayed.
+#include "common.cuh"
+#include "heat.cuh"
+
+#include <new>
+#include <vector>
+
+namespace xkb {
+
+template <bool CG>
+__device__ __forceinline__ double axpby1(double a, double x, double b, double y) { return __dadd_rn(__dmul_rn(a, x), __dmul_rn(b, y)); }
+
+template <bool CG>
+__device__ __forceinline__ void axpby_cta(int64_t lo, int64_t hi, double a, const double * __restrict__ x,
+                                          double b, double * __restrict__ y)
+{
+    if (lo >= hi) return;
+    const int64_t tid = threadIdx.x, nth = blockDim.x;
+    const bool same_phase = (((uintptr_t) (x + lo)) & 15) == (((uintptr_t) (y + lo)) & 15);
+    int64_t head = lo;
+    if (same_phase && (((uintptr_t) (y + lo)) & 15)) head = lo + 1;
+    if (!same_phase) head = hi;
+    if (head > hi) head = hi;
+    for (int64_t i = lo + tid; i < head; i += nth)
+        y[i] = axpby1<CG>(a, CG ? __ldcg(x + i) : __ldg(x + i), b, CG ? __ldcg(y + i) : y[i]);
+    const int64_t nv = (hi - head) / 2;
+    const double2 * xv = (const double2 *) (x + head);
+    double2 * yv = (double2 *) (y + head);
+    for (int64_t v = tid; v < nv; v += nth)
+    {
+        const double2 xx = CG ? __ldcg(xv + v) : __ldg(xv + v);
+        const double2 yy = CG ? __ldcg(yv + v) : yv[v];
+        yv[v] = make_double2(axpby1<CG>(a, xx.x, b, yy.x), axpby1<CG>(a, xx.y, b, yy.y));
+    }
+    for (int64_t i = head + 2 * nv + tid; i < hi; i += nth)
+        y[i] = axpby1<CG>(a, CG ? __ldcg(x + i) : __ldg(x + i), b, CG ? __ldcg(y + i) : y[i]);
+}
+
+constexpr int SCHED_THREADS = 256;
+
+__device__ __forceinline__ void run_task_cta(const xkb_task_desc_t & d)
+{
+    switch (d.kind)
+    {
+        case XKB_TASK_HEAT_F64: {
+            const auto & h = d.u.heat;
+            const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
+            heat_tile_cta<double, 2, 4, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
+                                              h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+            break;
+        }
+        case XKB_TASK_HEAT_F32: {
+            const auto & h = d.u.heat;
+            const bool vok = (h.ld % 4 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
+            heat_tile_cta<float, 4, 4, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
+                                             h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+            break;
+        }
+        case XKB_TASK_AXPBY: {
+            const auto & a = d.u.axpby;
+            axpby_cta<true>(a.lo, a.hi, a.a, (const double *) a.x, a.b, (double *) a.y);
+            break;
+        }
+        default: break;   // XKB_TASK_NOOP (first-touch / placement tasks)
+    }
+}
+
+__device__ __forceinline__ int atom_add_acq_rel(int * p, int v)
+{
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+struct SchedArgs {
+    const xkb_task_desc_t * tasks;
+    uint32_t ntasks;
+    const uint32_t * succ_ptr;
+    const uint32_t * succ;
+    int * wc;
+    int * queue;
+    unsigned * ctr;            // [0] head, [1] tail, [2] status, [3] executed
+    uint64_t timeout_ns;
+};
+
+__global__ void sched_init_kernel(SchedArgs a, const uint32_t * npred)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ntasks) return;
+    a.queue[t] = -1;
+    const int n = (int) npred[t];
+    a.wc[t] = n;
+}
+
+__global__ void sched_seed_kernel(SchedArgs a, const uint32_t * npred)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ntasks || npred[t] != 0) return;
+    const unsigned pos = atomicAdd(a.ctr + 1, 1u);
+    a.queue[pos] = (int) t;
+}
+
+__global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(SchedArgs a)
+{
+    __shared__ int cur;
+    unsigned executed = 0;
+    for (;;)
+    {
+        if (threadIdx.x == 0)
+        {
+            int t = -1;
+            const unsigned slot = atomicAdd(a.ctr + 0, 1u);
+            if (slot < a.ntasks)
+            {
+                const uint64_t t0 = xkb_globaltimer();
+                uint32_t spins = 0;
+                while ((t = xkb_ld_acquire(a.queue + slot)) < 0)
+                {
+                    if (*(volatile unsigned *) (a.ctr + 2) != 0) { t = -2; break; }   // another CTA gave up
+                    if ((++spins & 63) == 0 && xkb_globaltimer() - t0 > a.timeout_ns)
+                    {
+                        atomicCAS(a.ctr + 2, 0u, (unsigned) -XKB_ETIMEDOUT);
+                        t = -2;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            cur = t;
+        }
+        __syncthreads();
+        const int t = cur;
+        if (t < 0) break;
+        run_task_cta(a.tasks[t]);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x < 32)
+        {
+            const uint32_t b = a.succ_ptr[t], e = a.succ_ptr[t + 1];
+            for (uint32_t i = b + threadIdx.x; i < e; i += 32)
+            {
+                const uint32_t s = a.succ[i];
+                if (atom_add_acq_rel(a.wc + s, -1) == 1)
+                {
+                    const unsigned pos = atomicAdd(a.ctr + 1, 1u);
+                    xkb_st_release(a.queue + pos, (int) s);
+                }
+            }
+        }
+        ++executed;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && executed) atomicAdd(a.ctr + 3, executed);
+}
+
+// per-task kernels (PLAIN and GRAPH forms)
+__global__ void __launch_bounds__(SCHED_THREADS, 2) task_kernel(xkb_task_desc_t d, int nslabs)
+{
+    // blockIdx.x selects a column slab of a heat tile / a chunk of an axpby range
+    if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
+    {
+        xkb_task_desc_t q = d;
+        const int64_t cols = (int64_t) d.u.heat.y1 - d.u.heat.y0;
+        const int64_t per = (cols + nslabs - 1) / nslabs;
+        q.u.heat.y0 = (int32_t) (d.u.heat.y0 + blockIdx.x * per);
+        { const int64_t e = (int64_t) q.u.heat.y0 + per; q.u.heat.y1 = (int32_t) (e < d.u.heat.y1 ? e : d.u.heat.y1); }
+        if (q.u.heat.y0 >= q.u.heat.y1) return;
+        if (d.kind == XKB_TASK_HEAT_F64) {
+            const auto & h = q.u.heat;
+            const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
+            heat_tile_cta<double, 2, 4, false>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny, h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+        } else {
+            const auto & h = q.u.heat;
+            const bool vok = (h.ld % 4 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
+            heat_tile_cta<float, 4, 4, false>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny, h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+        }
+    }
+    else if (d.kind == XKB_TASK_AXPBY)
+    {
+        const auto & a = d.u.axpby;
+        const int64_t n = a.hi - a.lo, per = ((n + nslabs - 1) / nslabs + 1) & ~(int64_t) 1;
+        const int64_t lo = a.lo + blockIdx.x * per;
+        const int64_t hi = (lo + per < a.hi) ? lo + per : a.hi;
+        axpby_cta<false>(lo, hi, a.a, (const double *) a.x, a.b, (double *) a.y);
+    }
+}
+
+static int task_slabs(const xkb_task_desc_t & d)
+{
+    if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
+    {
+        const int64_t cols = (int64_t) d.u.heat.y1 - d.u.heat.y0;
+        return (int) std::max<int64_t>(1, (cols + 31) / 32);
+    }
+    if (d.kind == XKB_TASK_AXPBY)
+    {
+        const int64_t n = d.u.axpby.hi - d.u.axpby.lo;
+        return (int) std::min<int64_t>(std::max<int64_t>(1, n / 4096), 1184);
+    }
+    return 1;
+}
+
+template <typename T>
+struct Dev {
+    T * p = nullptr; size_t cap = 0;
+    ~Dev() { if (p) cudaFree(p); }
+    int reserve(size_t n) {
+        if (n <= cap) return XKB_OK;
+        if (p) { cudaFree(p); p = nullptr; cap = 0; }
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        cap = n; return XKB_OK;
+    }
+};
+
+} // namespace xkb
+
+using namespace xkb;
+
+struct xkb_sched {
+    cudaStream_t stream = nullptr;
+    std::vector<xkb_task_desc_t> host_tasks;
+    Dev<xkb_task_desc_t> tasks;
+    Dev<int> wc, queue;
+    Dev<unsigned> ctr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    const void * graph_key = nullptr;
+    int last_form = -1;
+    int grid = 0;
+    uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
+    ~xkb_sched() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+static int check_tasks(const xkb_task_desc_t * t, size_t n)
+{
+    for (size_t i = 0; i < n; ++i)
+    {
+        const xkb_task_desc_t & d = t[i];
+        if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
+        {
+            const auto & h = d.u.heat;
+            if (!h.src || !h.dst || h.src == h.dst || h.ld < h.nx || h.nx < 0 || h.ny < 0 || h.x0 > h.x1 || h.y0 > h.y1)
+                return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad heat tile", i);
+        }
+        else if (d.kind == XKB_TASK_AXPBY)
+        {
+            const auto & a = d.u.axpby;
+            if (a.lo < 0 || a.lo > a.hi || (a.hi > a.lo && (!a.x || !a.y)))
+                return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad axpby range", i);
+        }
+        else if (d.kind != XKB_TASK_NOOP)
+            return xkb_set_error(XKB_EINVAL, "sched: task %zu: unknown kind %u", i, d.kind);
+    }
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_create(xkb_sched_t ** out, void * stream)
+{
+    if (!out) return xkb_set_error(XKB_EINVAL, "sched_create: null output");
+    int dev;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    xkb_sched * S = new (std::nothrow) xkb_sched();
+    if (!S) return xkb_set_error(XKB_ENOMEM, "sched_create: out of host memory");
+    S->stream = (cudaStream_t) stream;
+    int sms = 148, per = 2;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel, SCHED_THREADS, 0);
+    S->grid = sms * (per > 0 ? per : 1);
+    *out = S;
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_destroy(xkb_sched_t * S)
+{
+    if (S) { cudaStreamSynchronize(S->stream); delete S; }
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_set_tasks(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks)
+{
+    if (!S || (ntasks && !tasks)) return xkb_set_error(XKB_EINVAL, "sched_set_tasks: bad arguments");
+    int rc = check_tasks(tasks, ntasks);
+    if (rc) return rc;
+    S->host_tasks.assign(tasks, tasks + ntasks);
+    if ((rc = S->tasks.reserve(ntasks ? ntasks : 1))) return rc;
+    if (ntasks) XKB_CUDA_TRY(cudaMemcpyAsync(S->tasks.p, tasks, ntasks * sizeof(xkb_task_desc_t), cudaMemcpyHostToDevice, S->stream));
+    XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; }
+    if (S->graph) { cudaGraphDestroy(S->graph); S->graph = nullptr; }
+    S->graph_key = nullptr;
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_set_timeout(xkb_sched_t * S, double seconds)
+{
+    if (!S || !(seconds > 0)) return xkb_set_error(XKB_EINVAL, "sched_set_timeout: bad arguments");
+    S->timeout_ns = (uint64_t) (seconds * 1e9);
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_set_grid(xkb_sched_t * S, int ctas)
+{
+    if (!S || ctas <= 0) return xkb_set_error(XKB_EINVAL, "sched_set_grid: bad arguments");
+    S->grid = ctas;
+    return XKB_OK;
+}
+
+static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
+{
+    const uint32_t n = (uint32_t) g->ntasks;
+    int rc;
+    if ((rc = S->wc.reserve(n ? n : 1)) || (rc = S->queue.reserve(n ? n : 1)) || (rc = S->ctr.reserve(4))) return rc;
+    SchedArgs a;
+    a.tasks = S->tasks.p; a.ntasks = n; a.succ_ptr = g->succ_ptr; a.succ = g->succ;
+    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns;
+    XKB_CUDA_TRY(cudaMemsetAsync(S->ctr.p, 0, 4 * sizeof(unsigned), S->stream));
+    if (n)
+    {
+        sched_init_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
+        sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
+        sched_persistent_kernel<<<S->grid, SCHED_THREADS, 0, S->stream>>>(a);
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
+static int run_plain(xkb_sched * S)
+{
+    for (const xkb_task_desc_t & d : S->host_tasks)
+    {
+        if (d.kind == XKB_TASK_NOOP) continue;
+        task_kernel<<<task_slabs(d), SCHED_THREADS, 0, S->stream>>>(d, task_slabs(d));
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
+static int build_cuda_graph(xkb_sched * S, const xkb_task_graph_t * g)
+{
+    const size_t n = S->host_tasks.size();
+    std::vector<uint32_t> ptr(n + 1), succ(g->nedges);
+    XKB_CUDA_TRY(cudaMemcpy(ptr.data(), g->succ_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (g->nedges) XKB_CUDA_TRY(cudaMemcpy(succ.data(), g->succ, g->nedges * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaGraph_t graph;
+    XKB_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    std::vector<cudaGraphNode_t> nodes(n);
+    for (size_t i = 0; i < n; ++i)
+    {
+        xkb_task_desc_t d = S->host_tasks[i];
+        int slabs = task_slabs(d);
+        void * args[2] = {&d, &slabs};
+        cudaKernelNodeParams p = {};
+        p.func = (void *) task_kernel;
+        p.gridDim = dim3(d.kind == XKB_TASK_NOOP ? 1 : slabs);
+        p.blockDim = dim3(SCHED_THREADS);
+        p.kernelParams = args;
+        cudaError_t e = cudaGraphAddKernelNode(&nodes[i], graph, nullptr, 0, &p);
+        if (e != cudaSuccess) { cudaGraphDestroy(graph); return xkb_set_cuda_error(e); }
+    }
+    std::vector<cudaGraphNode_t> from, to;
+    from.reserve(g->nedges); to.reserve(g->nedges);
+    for (size_t t = 0; t < n; ++t)
+        for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i) { from.push_back(nodes[t]); to.push_back(nodes[succ[i]]); }
+    if (!from.empty())
+    {
+        cudaError_t e = cudaGraphAddDependencies(graph, from.data(), to.data(), from.size());
+        if (e != cudaSuccess) { cudaGraphDestroy(graph); return xkb_set_cuda_error(e); }
+    }
+    cudaGraphExec_t exec;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(graph); return xkb_set_cuda_error(e); }
+    if (S->gexec) cudaGraphExecDestroy(S->gexec);
+    if (S->graph) cudaGraphDestroy(S->graph);
+    S->graph = graph; S->gexec = exec; S->graph_key = g->succ;
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_run(xkb_sched_t * S, const xkb_task_graph_t * g, int form)
+{
+    if (!S || !g) return xkb_set_error(XKB_EINVAL, "sched_run: bad arguments");
+    if (g->ntasks != S->host_tasks.size())
+        return xkb_set_error(XKB_EINVAL, "sched_run: graph has %llu tasks, %zu descriptors set",
+                             (unsigned long long) g->ntasks, S->host_tasks.size());
+    S->last_form = form;
+    switch (form)
+    {
+        case XKB_FORM_PERSISTENT: return run_persistent(S, g);
+        case XKB_FORM_PLAIN: return run_plain(S);
+        case XKB_FORM_GRAPH:
+            if (!S->gexec || S->graph_key != g->succ) { int rc = build_cuda_graph(S, g); if (rc) return rc; }
+            XKB_CUDA_TRY(cudaGraphLaunch(S->gexec, S->stream));
+            return XKB_OK;
+        default: return xkb_set_error(XKB_EINVAL, "sched_run: unknown form %d", form);
+    }
+}
+
+extern "C" int xkb_sched_wait(xkb_sched_t * S, uint64_t * executed)
+{
+    if (!S) return xkb_set_error(XKB_EINVAL, "sched_wait: null scheduler");
+    XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    unsigned ctr[4] = {0, 0, 0, (unsigned) S->host_tasks.size()};
+    if (S->ctr.p && S->last_form == XKB_FORM_PERSISTENT) XKB_CUDA_TRY(cudaMemcpy(ctr, S->ctr.p, sizeof(ctr), cudaMemcpyDeviceToHost));
+    if (executed) *executed = ctr[3];
+    if (ctr[2] != 0)
+        return xkb_set_error(-(int) ctr[2], "sched: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], (unsigned) S->host_tasks.size());
+    return XKB_OK;
+}
