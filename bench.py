@@ -1,0 +1,413 @@
+"""Benchmark of the B200 dataflow hot path (one JSON line on rank 0).
+
+Workload (headline): the batched heat-diffusion-2d task graph -- a 16384 x 16384 FP64 grid,
+128 x 128 tile tasks (16384 per Jacobi step: R on the halo-expanded source tile, W on the
+destination tile), 500 double-buffered steps = 8,192,000 tile tasks -- dependencies resolved by
+the GPU resolver, executed by the persistent device scheduler. One bench "step" = one
+execution of the whole 500-step graph. Metric: tasks/s (whole job, all ranks).
+
+Beside it: the same graph's first two steps in the plain one-launch-per-task form and as a CUDA
+graph (the fused/plain ratio), the whole-step stencil kernel's HBM GB/s (FP64 and FP32
+storage), the resolver on the dependency microbench (65,536 tasks, 1-4 accesses on an 8192^2
+FP64 matrix), and the CPU baseline (the C restatement of the same tile bodies on the host's
+cores, a bounded sample).
+
+--impl reference times the reference's CPU implementation of the path (the oracle port of the
+tile bodies on all host threads) on bounded samples of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+NX = NY = 16384
+TS = 128
+STEPS = 500
+COEF = 0.2
+SEED = 42
+HBM_FALLBACK = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the persistent kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            return json.load(f).get("sched_persistent_kernel_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev, self.proc, self.f = dev, None, None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush(); self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) > 8:
+                for k, name in enumerate(names):
+                    if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0")); world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_heat_graph(xk, torch, a, b, nx, ny, ts, steps, stream, batch_steps=25):
+    res = xk.Resolver(stream)
+    t0 = time.perf_counter()
+    for s0 in range(0, steps, batch_steps):
+        res.add(xk.heat_access_records(nx, ny, ts, ts, s0, min(batch_steps, steps - s0), a.data_ptr(), b.data_ptr()))
+    g = res.graph()
+    torch.cuda.synchronize()
+    return res, g, time.perf_counter() - t0
+
+
+_CPU_GRIDS = {}
+
+
+def cpu_heat_sample(nthreads, steps=None, n=NX, target_s=10.0):
+    """C restatement of the heat tile bodies on the host: Jacobi steps of the n x n FP64 grid.
+    steps=None: run one step, then enough more to make about target_s seconds of CPU work."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import kernels_oracle as O
+    L = O.c_oracle()
+    if n not in _CPU_GRIDS:
+        g = O.heat_init(n, n, seed=SEED)
+        _CPU_GRIDS[n] = (g, g.copy())
+    a, b = _CPU_GRIDS[n]
+    done, t_all = 0, 0.0
+    plan = steps if steps is not None else 1
+    while True:
+        t0 = time.perf_counter()
+        for _ in range(plan):
+            L.xk_oracle_heat_step_f64(a.ctypes.data, b.ctypes.data, n, n, n, COEF, nthreads)
+            a, b = b, a
+        t_all += time.perf_counter() - t0
+        done += plan
+        if steps is not None or t_all >= target_s * 0.8:
+            break
+        plan = max(1, min(50, int(target_s / (t_all / done)) - done))
+    _CPU_GRIDS[n] = (a, b)
+    tasks = done * (-(-n // TS)) ** 2
+    return tasks / t_all, t_all, tasks
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = host_threads()
+    for _ in range(args.warmup):
+        cpu_heat_sample(cores, steps=1)
+    # each bench step: a bounded sample of the workload sized to a few seconds of CPU work
+    t0 = time.perf_counter(); tasks = 0
+    for _ in range(args.steps):
+        _, _, n = cpu_heat_sample(cores, steps=None, target_s=5.0)
+        tasks += n
+    dt = time.perf_counter() - t0
+    v = tasks / dt
+    print(json.dumps({
+        "impl": "reference", "metric": "tasks/s", "value": v, "unit": "tasks/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"batched heat-diffusion-2d: {NX}x{NY} FP64 grid, {TS}x{TS} tile tasks; each bench step "
+                               "times a bounded sample (about 5 s of Jacobi steps) on the host", "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "tasks/s", "cores": cores, "kind": "port",
+                         "sample": "Jacobi steps of the 16384^2 FP64 grid, about 5 s per bench step (C restatement of "
+                                   "the tile body, POSIX threads)"},
+        "e2e": {"value": v, "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def microbench_stream(ntasks, seed, n=8192, ld=8192, align=64, max_units=32, base=1 << 40):
+    """Dependency microbench: 1-4 accesses per task on an n x n FP64 matrix (LD = ld), rectangles
+    aligned to 64 elements with sides 64*U{1..32}, modes R 60% / W 20% / RW 20%."""
+    import xkaapi_b200 as xk
+    rng = np.random.default_rng(seed)
+    na = rng.integers(1, 5, ntasks)
+    tot = int(na.sum())
+    units = n // align
+    mu = rng.integers(1, max_units + 1, tot); nu = rng.integers(1, max_units + 1, tot)
+    xu = (rng.random(tot) * (units - mu + 1)).astype(np.int64); yu = (rng.random(tot) * (units - nu + 1)).astype(np.int64)
+    r = rng.integers(0, 10, tot)
+    recs = np.zeros(tot, dtype=xk.heat.ACCESS_REC)
+    recs["task"] = np.repeat(np.arange(ntasks, dtype=np.uint32), na)
+    recs["type"] = 2; recs["mode"] = np.where(r < 6, 1, np.where(r < 8, 2, 3))
+    recs["addr"] = base; recs["ld"] = ld; recs["sizeof_type"] = 8
+    recs["offset_m"] = xu * align; recs["offset_n"] = yu * align; recs["m"] = mu * align; recs["n"] = nu * align
+    return recs
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="smaller side studies (plain/graph/microbench)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import xkaapi_b200 as xk
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    hbm_peak, peak_kind = peaks()
+    extra = {}
+
+    # ---------------- headline: persistent scheduler over the whole 500-step graph ----------
+    host = torch.empty((NY, NX), dtype=torch.float64).pin_memory()
+    rng = np.random.default_rng(SEED + rank)
+    hv = host.numpy()
+    hv[:] = 0.0
+    hv[1:NY - 1, 1:NX - 1] = rng.random((NY - 2, NX - 2))
+    a = torch.empty((NY, NX), dtype=torch.float64, device="cuda")
+    b = torch.empty_like(a)
+    a.copy_(host); b.copy_(a)
+    torch.cuda.synchronize()
+    res, graph, t_resolve = build_heat_graph(xk, torch, a, b, NX, NY, TS, STEPS, stream)
+    ntasks = graph.ntasks
+    descs = xk.heat_task_descs((a.data_ptr(), b.data_ptr()), NX, NY, NX, TS, TS, STEPS, COEF)
+    sch = xk.Scheduler(stream)
+    sch.set_tasks(descs)
+    del descs
+    extra["graph_build"] = {"tasks": int(ntasks), "edges": int(graph.nedges), "resolve_s": round(t_resolve, 3),
+                            "resolve_tasks_per_s": round(ntasks / t_resolve)}
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            sch.run(graph); sch.wait()
+    barrier(world); torch.cuda.synchronize()
+    clocks = Clocks(dev); clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kms = []
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            sch.run(graph)
+            kms.append(None)
+        e1.record(stream)
+    stream.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    executed = sch.wait()
+    last_kernel_ms = sch.kernel_ms()
+    barrier(world)
+    ms_total = max_over_ranks(ms_total, world)
+    ms_step = ms_total / args.steps
+    value = world * ntasks * args.steps / (ms_total / 1e3)
+    assert executed == ntasks, (executed, ntasks)
+    cells = (NX - 2) * (NY - 2)
+    alg_bytes = 16.0 * cells * STEPS
+    achieved = alg_bytes / (last_kernel_ms / 1e3) / 1e9
+    traffic = profile_traffic()
+
+    # result check against the CPU restatement on a sample of rows after one more run is not
+    # possible at this size; the parity suite covers correctness. Keep a checksum instead.
+    res_grid = a if STEPS % 2 == 0 else b
+    checksum = float(res_grid.sum().item())
+
+    # ---------------- e2e through the C ABI with host buffers ---------------------------------
+    torch.cuda.synchronize()
+    out_host = torch.empty_like(host).pin_memory()
+    with torch.cuda.stream(stream):
+        sch.run(graph); sch.wait()
+    t0 = time.perf_counter()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        f0.record(stream)
+        for _ in range(args.steps):
+            a.copy_(host, non_blocking=True)
+            b.copy_(a, non_blocking=True)
+            sch.run(graph)
+            out_host.copy_(res_grid, non_blocking=True)
+        f1.record(stream)
+    stream.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), world)
+    e2e_value = world * ntasks * args.steps / (e2e_ms / 1e3)
+    bytes_grid = NX * NY * 8
+
+    # ---------------- forms at equal work: first two steps ------------------------------------
+    forms = {}
+    if rank == 0:
+        win = 2
+        res2, g2, _ = build_heat_graph(xk, torch, a, b, NX, NY, TS, win, stream)
+        d2 = xk.heat_task_descs((a.data_ptr(), b.data_ptr()), NX, NY, NX, TS, TS, win, COEF)
+        s2 = xk.Scheduler(stream)
+        s2.set_tasks(d2)
+        for name, form, reps in (("persistent", xk.FORM_PERSISTENT, 10), ("plain", xk.FORM_PLAIN, 2),
+                                 ("cuda_graph", xk.FORM_GRAPH, 5)):
+            t_build = time.perf_counter()
+            with torch.cuda.stream(stream):
+                s2.run(g2, form); s2.wait()
+            t_build = time.perf_counter() - t_build
+            h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                h0.record(stream)
+                for _ in range(reps):
+                    s2.run(g2, form)
+                h1.record(stream)
+            stream.synchronize(); s2.wait()
+            ms = h0.elapsed_time(h1) / reps
+            forms[name] = {"tasks": int(g2.ntasks), "ms": round(ms, 3), "tasks_per_s": round(g2.ntasks / (ms / 1e3)),
+                           "first_run_s": round(t_build, 3)}
+        forms["fused_vs_plain"] = round(forms["persistent"]["tasks_per_s"] / forms["plain"]["tasks_per_s"], 2)
+        forms["graph_vs_plain"] = round(forms["cuda_graph"]["tasks_per_s"] / forms["plain"]["tasks_per_s"], 2)
+        s2.close(); res2.close()
+
+        # whole-step stencil kernel (all tile tasks of a step fused into one launch)
+        sten = {}
+        for dt, name, esz in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
+            x = a if dt == torch.float64 else a.float()
+            y = torch.empty_like(x); y.copy_(x)
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    xk.heat_step(x, y, NX, NY, NX, COEF, stream=stream); x, y = y, x
+                q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                q0.record(stream)
+                for _ in range(10):
+                    xk.heat_step(x, y, NX, NY, NX, COEF, stream=stream); x, y = y, x
+                q1.record(stream)
+            stream.synchronize()
+            ms = q0.elapsed_time(q1) / 10
+            gbs = 2.0 * esz * cells / (ms / 1e3) / 1e9
+            sten[name] = {"ms_per_step": round(ms, 4), "GBps": round(gbs, 1), "frac_of_peak": round(gbs / hbm_peak, 3)}
+            del x, y
+        extra["stencil_whole_step"] = sten
+
+        # resolver microbench
+        mb_tasks = 16384 if args.quick else 65536
+        recs = microbench_stream(mb_tasks, 12345)
+        r3 = xk.Resolver(stream)
+        t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        extra["resolver_microbench"] = {"tasks": mb_tasks, "accesses": int(len(recs)), "unique_edges": int(g3.nedges),
+                                        "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt)}
+        r3.close()
+
+    # ---------------- CPU baseline (rank 0, N=1) ----------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1:
+        cores = host_threads()
+        v, secs, tasks = cpu_heat_sample(cores, steps=None, target_s=10.0)
+        cpu = {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "port",
+               "sample": f"{tasks // (NX // TS) ** 2} Jacobi steps of the 16384^2 FP64 grid ({tasks} tile tasks, "
+                         f"{secs:.1f} s), C restatement of the tile body on POSIX threads"}
+
+    if rank == 0:
+        line = {
+            "metric": "tasks/s", "value": round(value, 1), "unit": "tasks/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded U[0,1) interior, Dirichlet 0 boundary)",
+            "config": {"workload": f"batched heat-diffusion-2d: {NX}x{NY} FP64 grid, {TS}x{TS} tile tasks, {STEPS} steps "
+                                   f"({ntasks} tasks/step of the bench), dependencies from the GPU resolver, persistent "
+                                   "device scheduler", "l2": "inputs (2 x 2 GiB grids) larger than L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 3), "traffic": traffic,
+                         "kernel": "sched_persistent_kernel", "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": round(last_kernel_ms, 3)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 1), "unit": "tasks/s", "h2d_bytes_per_step": bytes_grid,
+                    "d2h_bytes_per_step": bytes_grid, "ms_per_step": round(e2e_ms / args.steps, 3)},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk,
+            "forms_first_2_steps": forms,
+            "checksum": checksum,
+        }
+        line.update(extra)
+        print(json.dumps(line))
+    sch.close(); res.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,6 +159,8 @@ XKB_API int xkb_sched_run(xkb_sched_t * sched, const xkb_task_graph_t * graph, i
 /* Wait for the stream; *executed = tasks the persistent kernel ran. Returns XKB_ETIMEDOUT if
  * a device wait ran out of time (the kernel returned; the context stays usable). */
 XKB_API int xkb_sched_wait(xkb_sched_t * sched, uint64_t * executed);
+/* Device time of the last run's persistent kernel (CUDA events on the scheduler's stream). */
+XKB_API int xkb_sched_kernel_ms(xkb_sched_t * sched, double * ms);
 
 /* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
 /* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float

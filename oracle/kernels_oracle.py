@@ -69,3 +69,16 @@ def heat_run(grid, nx, ny, steps, c, dtype=np.float64):
 
 def axpby(a, x, b, y):
     return (a * x) + (b * y)
+
+
+def c_oracle():
+    """ctypes handle on oracle/_bin/libheat_oracle.so (C restatement, POSIX threads)."""
+    import ctypes
+    import os
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_bin", "libheat_oracle.so")
+    L = ctypes.CDLL(p)
+    i64, vp, dbl, ci = ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    for name in ("xk_oracle_heat_step_f64", "xk_oracle_heat_step_f32"):
+        getattr(L, name).argtypes = [vp, vp, i64, i64, i64, dbl, ci]
+    L.xk_oracle_axpby.argtypes = [i64, dbl, vp, dbl, vp, ci]
+    return L

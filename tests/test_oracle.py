@@ -48,3 +48,17 @@ def test_heat_oracle_properties():
         for ty in range(3):
             O.heat_tile(g, t, 40, 30, tx, ty, 16, 11, 0.2)
     np.testing.assert_array_equal(t, ref)
+
+
+def test_c_oracle_equals_numpy_oracle():
+    import kernels_oracle as O
+    L = O.c_oracle()
+    for dt, fn in ((np.float64, L.xk_oracle_heat_step_f64), (np.float32, L.xk_oracle_heat_step_f32)):
+        g = O.heat_init(97, 61, 100, seed=2).astype(dt)
+        ref = O.heat_step(g, g.copy(), 97, 61, 0.2)
+        out = g.copy()
+        fn(g.ctypes.data, out.ctypes.data, 97, 61, 100, 0.2, 4)
+        np.testing.assert_array_equal(out, ref)
+    x = np.linspace(-1, 1, 1001); y = np.linspace(3, -2, 1001); ref = O.axpby(0.3, x, -1.7, y)
+    L.xk_oracle_axpby(1001, 0.3, x.ctypes.data, -1.7, y.ctypes.data, 2)
+    np.testing.assert_array_equal(y, ref)

@@ -61,6 +61,7 @@ SIGNATURES = {
     "xkb_sched_set_grid": (_int, [_vp, _int]),
     "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
     "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "xkb_sched_kernel_ms": (_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_resolver_destroy": (_int, [_vp]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
@@ -216,6 +217,11 @@ class Scheduler:
         check(lib().xkb_sched_wait(self._h, ctypes.byref(n)))
         return n.value
 
+    def kernel_ms(self):
+        ms = ctypes.c_double()
+        check(lib().xkb_sched_kernel_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
     def close(self):
         if self._h:
             lib().xkb_sched_destroy(self._h)
@@ -228,20 +234,4 @@ class Scheduler:
             pass
 
 
-def heat_task_descs(src_ptrs, nx, ny, ld, tsx, tsy, steps, c, f32=False):
-    """Descriptors of the heat-diffusion-2d tile tasks in spawn order
-    (examples/heat-diffusion-2d/src/main.cc:569-581: tile_x outer, tile_y inner, grids swap
-    every step). src_ptrs = (grid A device pointer, grid B device pointer)."""
-    import numpy as np
-    ntx, nty = -(-nx // tsx), -(-ny // tsy)
-    per = ntx * nty
-    d = np.zeros(per * steps, dtype=task_desc_dtype())
-    tx = np.repeat(np.arange(ntx), nty); ty = np.tile(np.arange(nty), ntx)
-    for s in range(steps):
-        blk = d[s * per:(s + 1) * per]
-        blk["kind"] = TASK_HEAT_F32 if f32 else TASK_HEAT_F64
-        blk["src"], blk["dst"] = (src_ptrs[0], src_ptrs[1]) if s % 2 == 0 else (src_ptrs[1], src_ptrs[0])
-        blk["ld"], blk["nx"], blk["ny"], blk["c"] = ld, nx, ny, c
-        blk["x0"] = tx * tsx; blk["x1"] = np.minimum(tx * tsx + tsx, nx)
-        blk["y0"] = ty * tsy; blk["y1"] = np.minimum(ty * tsy + tsy, ny)
-    return d
+from .heat import heat_task_descs, heat_access_records  # noqa: E402,F401

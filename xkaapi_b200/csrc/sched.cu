@@ -246,8 +246,11 @@ struct xkb_sched {
     const void * graph_key = nullptr;
     int last_form = -1;
     int grid = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
     ~xkb_sched() {
+        if (ev[0]) cudaEventDestroy(ev[0]);
+        if (ev[1]) cudaEventDestroy(ev[1]);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
     }
@@ -341,7 +344,10 @@ static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
     {
         sched_init_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
         sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
+        if (!S->ev[0]) { XKB_CUDA_TRY(cudaEventCreate(&S->ev[0])); XKB_CUDA_TRY(cudaEventCreate(&S->ev[1])); }
+        XKB_CUDA_TRY(cudaEventRecord(S->ev[0], S->stream));
         sched_persistent_kernel<<<S->grid, SCHED_THREADS, 0, S->stream>>>(a);
+        XKB_CUDA_TRY(cudaEventRecord(S->ev[1], S->stream));
     }
     XKB_CUDA_TRY(cudaGetLastError());
     return XKB_OK;
@@ -426,5 +432,17 @@ extern "C" int xkb_sched_wait(xkb_sched_t * S, uint64_t * executed)
     if (executed) *executed = ctr[3];
     if (ctr[2] != 0)
         return xkb_set_error(-(int) ctr[2], "sched: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], (unsigned) S->host_tasks.size());
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_kernel_ms(xkb_sched_t * S, double * ms)
+{
+    if (!S || !ms) return xkb_set_error(XKB_EINVAL, "sched_kernel_ms: bad arguments");
+    *ms = 0;
+    if (S->last_form != XKB_FORM_PERSISTENT || !S->ev[0]) return XKB_OK;
+    float f = 0;
+    XKB_CUDA_TRY(cudaEventSynchronize(S->ev[1]));
+    XKB_CUDA_TRY(cudaEventElapsedTime(&f, S->ev[0], S->ev[1]));
+    *ms = f;
     return XKB_OK;
 }
