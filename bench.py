@@ -271,14 +271,18 @@ def main():
     barrier(world); torch.cuda.synchronize()
     clocks = Clocks(dev); clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    run_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.nvtx.range_push("timed")
     with torch.cuda.stream(stream):
         e0.record(stream)
-        for _ in range(args.steps):
+        for k in range(args.steps):
+            run_ev[k][0].record(stream)
             sch.run(graph)
+            run_ev[k][1].record(stream)
         e1.record(stream)
     stream.synchronize()
     torch.cuda.nvtx.range_pop()
+    runs_ms = [round(x.elapsed_time(y), 3) for x, y in run_ev]
     ms_total = e0.elapsed_time(e1)
     clk = clocks.stop()
     executed = sch.wait()
@@ -366,6 +370,12 @@ def main():
             del x, y
         extra["stencil_whole_step"] = sten
 
+        # autotuner: tile shape x warps per task on a short graph of the same grid
+        from xkaapi_b200.autotune import autotune_heat
+        best, cands = autotune_heat(a, b, NX, NY, steps=4, stream=stream)
+        extra["autotune"] = {"best": best, "candidates": len(cands),
+                             "tile128_best": max((r for r in cands if r["tile"] == 128), key=lambda r: r["GBps"])}
+
         # resolver microbench
         mb_tasks = 16384 if args.quick else 65536
         recs = microbench_stream(mb_tasks, 12345)
@@ -405,6 +415,7 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clk,
             "forms_first_2_steps": forms,
+            "runs_ms": runs_ms,
             "checksum": checksum,
         }
         line.update(extra)

@@ -154,6 +154,10 @@ XKB_API int xkb_sched_set_tasks(xkb_sched_t * sched, const xkb_task_desc_t * tas
 XKB_API int xkb_sched_set_timeout(xkb_sched_t * sched, double seconds);
 /* CTAs of the persistent kernel (default: SMs x resident CTAs per SM). */
 XKB_API int xkb_sched_set_grid(xkb_sched_t * sched, int ctas);
+/* Warps that execute one task in the persistent kernel (1, 2, 4 or 8; default 2): each CTA
+ * of 8 warps runs 8 / warps_per_task tasks at a time, each team taking and releasing tasks on
+ * its own. */
+XKB_API int xkb_sched_set_team(xkb_sched_t * sched, int warps_per_task);
 /* Enqueue one execution of the whole graph on the scheduler's stream (asynchronous). */
 XKB_API int xkb_sched_run(xkb_sched_t * sched, const xkb_task_graph_t * graph, int form);
 /* Wait for the stream; *executed = tasks the persistent kernel ran. Returns XKB_ETIMEDOUT if

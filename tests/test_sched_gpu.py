@@ -120,3 +120,21 @@ def test_timeout_returns_error_and_context_survives(torch_cuda):
     g2, a, b, res, d2 = heat_graph(torch, 128, 128, 64, 4)
     sch.set_tasks(d2); sch.run(res.graph()); sch.wait()
     np.testing.assert_array_equal(a.cpu().numpy(), O.heat_run(g2, 128, 128, 4, C))
+
+
+@pytest.mark.parametrize("team", [1, 2, 4, 8])
+def test_heat_persistent_team_sizes(torch_cuda, team):
+    torch = torch_cuda
+    g, a, b, res, descs = heat_graph(torch, 300, 200, 64, 9)
+    sch = xk.Scheduler(); sch.set_team(team); sch.set_tasks(descs); sch.run(res.graph())
+    assert sch.wait() == len(descs)
+    np.testing.assert_array_equal(b.cpu().numpy(), O.heat_run(g, 300, 200, 9, C))
+
+
+@pytest.mark.parametrize("team", [1, 8])
+def test_axpby_chains_team_sizes(torch_cuda, team):
+    torch = torch_cuda
+    recs, descs, dy, ref = axpby_chain(torch, 50_001, 6, 3)
+    res = xk.Resolver(); res.add(recs)
+    sch = xk.Scheduler(); sch.set_team(team); sch.set_tasks(descs); sch.run(res.graph()); sch.wait()
+    np.testing.assert_array_equal(dy.cpu().numpy(), ref)

@@ -325,15 +325,15 @@ __host__ __device__ __forceinline__ void heat_tile_split(const TileBox & b, int 
     cols_per = (cols + ncg - 1) / ncg;
 }
 
-// A whole CTA executes one tile task: the warps take the tile's strips round-robin.
+// A team of `nwarps` warps (warp index `warp` within the team) executes one tile task: the
+// warps take the tile's strips round-robin.
 template <typename T, int VEC, int PF, bool CG>
-__device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld, int64_t nx, int64_t ny,
-                                              int64_t x0, int64_t x1, int64_t y0, int64_t y1, double c, bool vec_ok,
-                                              int pfd = 0)
+__device__ __forceinline__ void heat_tile_team(const T * src, T * dst, int64_t ld, int64_t nx, int64_t ny,
+                                               int64_t x0, int64_t x1, int64_t y0, int64_t y1, double c, bool vec_ok,
+                                               int pfd, int warp, int nwarps)
 {
     const TileBox b = heat_tile_box(nx, ny, x0, x1, y0, y1);
     if (b.rx0 >= b.rx1 || b.cy0 >= b.cy1) return;
-    const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5;
     int64_t rbase0, cols_per; int nrg, ncg;
     heat_tile_split<VEC>(b, nwarps, rbase0, nrg, ncg, cols_per);
     for (int s = warp; s < nrg * ncg; s += nwarps)
@@ -344,6 +344,15 @@ __device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld
         if (cy0 >= cy1) continue;
         heat_strip_halo<T, VEC, PF, CG>(src, dst, ld, nx, rbase0 + (int64_t) rg * 32 * VEC, b.rx0, b.rx1, cy0, cy1, c, vec_ok, pfd);
     }
+}
+
+// A whole CTA executes one tile task.
+template <typename T, int VEC, int PF, bool CG>
+__device__ __forceinline__ void heat_tile_cta(const T * src, T * dst, int64_t ld, int64_t nx, int64_t ny,
+                                              int64_t x0, int64_t x1, int64_t y0, int64_t y1, double c, bool vec_ok,
+                                              int pfd = 0)
+{
+    heat_tile_team<T, VEC, PF, CG>(src, dst, ld, nx, ny, x0, x1, y0, y1, c, vec_ok, pfd, threadIdx.x >> 5, blockDim.x >> 5);
 }
 
 } // namespace xkb

@@ -29,11 +29,10 @@ template <bool CG>
 __device__ __forceinline__ double axpby1(double a, double x, double b, double y) { return __dadd_rn(__dmul_rn(a, x), __dmul_rn(b, y)); }
 
 template <bool CG>
-__device__ __forceinline__ void axpby_cta(int64_t lo, int64_t hi, double a, const double * __restrict__ x,
-                                          double b, double * __restrict__ y)
+__device__ __forceinline__ void axpby_team(int64_t lo, int64_t hi, double a, const double * __restrict__ x,
+                                           double b, double * __restrict__ y, int64_t tid, int64_t nth)
 {
     if (lo >= hi) return;
-    const int64_t tid = threadIdx.x, nth = blockDim.x;
     const bool same_phase = (((uintptr_t) (x + lo)) & 15) == (((uintptr_t) (y + lo)) & 15);
     int64_t head = lo;
     if (same_phase && (((uintptr_t) (y + lo)) & 15)) head = lo + 1;
@@ -56,27 +55,29 @@ __device__ __forceinline__ void axpby_cta(int64_t lo, int64_t hi, double a, cons
 
 constexpr int SCHED_THREADS = 256;
 
-__device__ __forceinline__ void run_task_cta(const xkb_task_desc_t & d)
+// Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
+__device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps)
 {
     switch (d.kind)
     {
         case XKB_TASK_HEAT_F64: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
-            heat_tile_cta<double, 2, 4, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
-                                              h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+            heat_tile_team<double, 2, 4, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
+                                               h.x0, h.x1, h.y0, h.y1, h.c, vok, 8, warp, nwarps);
             break;
         }
         case XKB_TASK_HEAT_F32: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 4 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
-            heat_tile_cta<float, 4, 4, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
-                                             h.x0, h.x1, h.y0, h.y1, h.c, vok, 8);
+            heat_tile_team<float, 4, 4, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
+                                              h.x0, h.x1, h.y0, h.y1, h.c, vok, 8, warp, nwarps);
             break;
         }
         case XKB_TASK_AXPBY: {
             const auto & a = d.u.axpby;
-            axpby_cta<true>(a.lo, a.hi, a.a, (const double *) a.x, a.b, (double *) a.y);
+            axpby_team<true>(a.lo, a.hi, a.a, (const double *) a.x, a.b, (double *) a.y,
+                             (int64_t) warp * 32 + (threadIdx.x & 31), (int64_t) nwarps * 32);
             break;
         }
         default: break;   // XKB_TASK_NOOP (first-touch / placement tasks)
@@ -118,13 +119,29 @@ __global__ void sched_seed_kernel(SchedArgs a, const uint32_t * npred)
     a.queue[pos] = (int) t;
 }
 
+__device__ __forceinline__ void team_sync(int id, int nthreads)
+{
+    if (nthreads == SCHED_THREADS) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
+}
+
+// Each CTA holds 8 / TEAM_WARPS independent TEAMS of TEAM_WARPS warps. A team's first
+// thread takes the next queue slot and waits for it; the team runs the task, fences, syncs
+// on its own named barrier, and its first warp releases the successors. Teams never wait for
+// one another, so while one team takes or releases a task the others keep HBM busy.
+template <int TEAM_WARPS>
 __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(SchedArgs a)
 {
-    __shared__ int cur;
+    constexpr int NTEAMS = (SCHED_THREADS / 32) / TEAM_WARPS;
+    constexpr int TEAM_THREADS = TEAM_WARPS * 32;
+    __shared__ int cur[NTEAMS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int team = warp / TEAM_WARPS, twarp = warp % TEAM_WARPS;
+    const int bar = 1 + team;
     unsigned executed = 0;
     for (;;)
     {
-        if (threadIdx.x == 0)
+        if (twarp == 0 && lane == 0)
         {
             int t = -1;
             const unsigned slot = atomicAdd(a.ctr + 0, 1u);
@@ -134,7 +151,7 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
                 uint32_t spins = 0;
                 while ((t = xkb_ld_acquire(a.queue + slot)) < 0)
                 {
-                    if (*(volatile unsigned *) (a.ctr + 2) != 0) { t = -2; break; }   // another CTA gave up
+                    if (*(volatile unsigned *) (a.ctr + 2) != 0) { t = -2; break; }   // another team gave up
                     if ((++spins & 63) == 0 && xkb_globaltimer() - t0 > a.timeout_ns)
                     {
                         atomicCAS(a.ctr + 2, 0u, (unsigned) -XKB_ETIMEDOUT);
@@ -144,18 +161,18 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
                     __nanosleep(64);
                 }
             }
-            cur = t;
+            cur[team] = t;
         }
-        __syncthreads();
-        const int t = cur;
+        team_sync(bar, TEAM_THREADS);
+        const int t = cur[team];
         if (t < 0) break;
-        run_task_cta(a.tasks[t]);
+        run_task_team(a.tasks[t], twarp, TEAM_WARPS);
         __threadfence();
-        __syncthreads();
-        if (threadIdx.x < 32)
+        team_sync(bar, TEAM_THREADS);
+        if (twarp == 0)
         {
             const uint32_t b = a.succ_ptr[t], e = a.succ_ptr[t + 1];
-            for (uint32_t i = b + threadIdx.x; i < e; i += 32)
+            for (uint32_t i = b + lane; i < e; i += 32)
             {
                 const uint32_t s = a.succ[i];
                 if (atom_add_acq_rel(a.wc + s, -1) == 1)
@@ -164,11 +181,10 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
                     xkb_st_release(a.queue + pos, (int) s);
                 }
             }
+            ++executed;
         }
-        ++executed;
-        __syncthreads();
     }
-    if (threadIdx.x == 0 && executed) atomicAdd(a.ctr + 3, executed);
+    if (twarp == 0 && lane == 0 && executed) atomicAdd(a.ctr + 3, executed);
 }
 
 // per-task kernels (PLAIN and GRAPH forms)
@@ -199,7 +215,7 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) task_kernel(xkb_task_desc_t 
         const int64_t n = a.hi - a.lo, per = ((n + nslabs - 1) / nslabs + 1) & ~(int64_t) 1;
         const int64_t lo = a.lo + blockIdx.x * per;
         const int64_t hi = (lo + per < a.hi) ? lo + per : a.hi;
-        axpby_cta<false>(lo, hi, a.a, (const double *) a.x, a.b, (double *) a.y);
+        axpby_team<false>(lo, hi, a.a, (const double *) a.x, a.b, (double *) a.y, threadIdx.x, blockDim.x);
     }
 }
 
@@ -246,6 +262,7 @@ struct xkb_sched {
     const void * graph_key = nullptr;
     int last_form = -1;
     int grid = 0;
+    int team_warps = 2;
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
     ~xkb_sched() {
@@ -290,7 +307,8 @@ extern "C" int xkb_sched_create(xkb_sched_t ** out, void * stream)
     S->stream = (cudaStream_t) stream;
     int sms = 148, per = 2;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel, SCHED_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel<2>, SCHED_THREADS, 0);
+    // (all team variants share the register budget fixed by __launch_bounds__(256, 2))
     S->grid = sms * (per > 0 ? per : 1);
     *out = S;
     return XKB_OK;
@@ -331,6 +349,14 @@ extern "C" int xkb_sched_set_grid(xkb_sched_t * S, int ctas)
     return XKB_OK;
 }
 
+extern "C" int xkb_sched_set_team(xkb_sched_t * S, int warps_per_task)
+{
+    if (!S || (warps_per_task != 1 && warps_per_task != 2 && warps_per_task != 4 && warps_per_task != 8))
+        return xkb_set_error(XKB_EINVAL, "sched_set_team: warps per task must be 1, 2, 4 or 8");
+    S->team_warps = warps_per_task;
+    return XKB_OK;
+}
+
 static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
 {
     const uint32_t n = (uint32_t) g->ntasks;
@@ -346,7 +372,13 @@ static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
         sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
         if (!S->ev[0]) { XKB_CUDA_TRY(cudaEventCreate(&S->ev[0])); XKB_CUDA_TRY(cudaEventCreate(&S->ev[1])); }
         XKB_CUDA_TRY(cudaEventRecord(S->ev[0], S->stream));
-        sched_persistent_kernel<<<S->grid, SCHED_THREADS, 0, S->stream>>>(a);
+        switch (S->team_warps)
+        {
+            case 1: sched_persistent_kernel<1><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+            case 2: sched_persistent_kernel<2><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+            case 4: sched_persistent_kernel<4><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+            default: sched_persistent_kernel<8><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+        }
         XKB_CUDA_TRY(cudaEventRecord(S->ev[1], S->stream));
     }
     XKB_CUDA_TRY(cudaGetLastError());
