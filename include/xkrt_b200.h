@@ -115,6 +115,44 @@ XKB_API int xkb_resolver_edges(xkb_resolver_t * resolver, uint32_t * pairs, size
 /* Counters: tasks added, unique edges, device+host time of the last batch in ms. */
 XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms);
 
+/* ---- coherency and transfer planning (1 host + 1 GPU) ------------------------------------ */
+/* A planner decides, for each access fetched to the GPU (device 1) or back to the host
+ * (device 0), which device allocation holds it and which copies make it coherent -- the
+ * decisions of the reference's coherency controller, KBLASMemoryTree::fetch
+ * (include/xkrt/memory/access/blas/memory-tree.hpp:1805-1874; fetch_list_to_device :1738-1802,
+ * fetch_list_to_host :1185-1215), with every fetch's copies completed before the next fetch.
+ * Device addresses are reported as (allocation ordinal, byte offset); host addresses as raw
+ * byte addresses. Matrix tiles that wrap the leading dimension are rejected (XKB_EINVAL); a
+ * block needing a 9th allocation view returns XKB_ERANGE where the reference aborts. */
+typedef struct xkb_planner xkb_planner_t;
+
+#define XKB_COPY_H2D 0
+#define XKB_COPY_D2H 1
+#define XKB_COPY_D2D 2
+
+typedef struct xkb_copy_t {
+    int64_t task, access, kind;            /* issuing access; XKB_COPY_*                        */
+    int64_t src_dev, src_alloc, src_off, src_ld;
+    int64_t dst_dev, dst_alloc, dst_off, dst_ld;
+    int64_t m, n, sizeof_type;             /* m x n elements (segments: m bytes, n = 1, size 1) */
+} xkb_copy_t;
+
+typedef struct xkb_view_t { int64_t alloc, off, ld; } xkb_view_t;   /* an access's device view */
+
+XKB_API int xkb_planner_create(xkb_planner_t ** planner);
+XKB_API int xkb_planner_destroy(xkb_planner_t * planner);
+/* Fetch one access (record of task `access->task`, index `access_index` in that task) to
+ * `device`; appends its copies; *view receives the device view the task body uses. */
+XKB_API int xkb_planner_fetch(xkb_planner_t * planner, const xkb_access_rec_t * access, uint32_t access_index,
+                              int device, xkb_view_t * view);
+/* Fetch every access of a stream in order to `device`; views[i] (optional) for access i. */
+XKB_API int xkb_planner_plan(xkb_planner_t * planner, const xkb_access_rec_t * accesses, size_t n, int device,
+                             xkb_view_t * views);
+/* Copies planned so far (*n = count; out may be NULL to query); take != 0 clears the list. */
+XKB_API int xkb_planner_copies(xkb_planner_t * planner, xkb_copy_t * out, size_t cap, size_t * n, int take);
+/* Byte size of every device allocation made so far, in allocation order. */
+XKB_API int xkb_planner_allocations(xkb_planner_t * planner, uint64_t * sizes, size_t cap, size_t * n);
+
 /* ---- tasks and the device scheduler ------------------------------------------------------ */
 /* Built-in task bodies the device scheduler can run inline (the reference runs them as
  * per-task kernel launches through a format's launcher, include/xkrt/driver/kernel-launcher.h:44-51). */

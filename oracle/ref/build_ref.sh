@@ -142,3 +142,8 @@ CXXFLAGS="-std=c++20 -O2 -DNDEBUG -D_Static_assert=static_assert -include list -
 "$CXX" $CXXFLAGS -o "$OUT/ref_deps" \
     "$HERE/ref_deps.cc" "$HERE/seams.cc" "$REF/src/task/task.cc" "$REF/src/logger/logger.cc" -lpthread
 echo "built $OUT/ref_deps"
+
+# ---- transfer-plan oracle: reference memory tree under the canonical schedule ----------------
+"$CXX" $CXXFLAGS -include array -o "$OUT/ref_plan" \
+    "$HERE/ref_plan.cc" "$HERE/seams.cc" "$REF/src/task/task.cc" "$REF/src/logger/logger.cc" -lpthread
+echo "built $OUT/ref_plan"

@@ -1,4 +1,5 @@
-"""Regenerates tests/golden/deps_golden.npz from the REFERENCE's own dependency trees.
+"""Regenerates tests/golden/deps_golden.npz from the REFERENCE's own dependency trees and
+tests/golden/plan_golden.npz from the reference's own coherency controller (memory tree).
 
 Each case is a seeded access stream (tests/streams.py) run through oracle/_ref/ref_deps,
 which drives the reference's KBLASDependencyTree / IntervalDependencyTree via
@@ -9,7 +10,11 @@ fixtures pin the oracle restatement and the GPU resolver without the reference p
 Known-answer cases restate the reference's own ordering tests:
   tests/task-dependency-interval.cc:86-121         W/R/RW chain on overlapping intervals
   tests/task-dependency-interval-matrix.cc:84-160  interval W -> matrix W -> interval W
-Run: python tests/golden/make_golden.py   (needs oracle/_ref/ref_deps; see oracle/ref/build_ref.sh)
+Plan fixtures: oracle/_ref/ref_plan drives KBLASMemoryTree::fetch
+(include/xkrt/memory/access/blas/memory-tree.hpp:1805-1874) under the canonical schedule (fetches in
+spawn order, each fetch's copies completed before the next); allocations, device views and the
+sorted copy records are stored.
+Run: python tests/golden/make_golden.py   (needs oracle/_ref/ref_deps and ref_plan; see oracle/ref/build_ref.sh)
 """
 import os, subprocess, sys, tempfile
 import numpy as np
@@ -66,6 +71,47 @@ def cases():
             yield f"mixed_{kind}_{seed}", mixed(kind, seed)
 
 
+def ref_plan(recs):
+    """The reference memory tree's plan (oracle/_ref/ref_plan), canonical schedule. Copy records
+    are sorted (a task's copies have no order among themselves in the reference's fetch list)."""
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "s.bin")
+        S.write_stream(p, recs)
+        subprocess.run([os.path.join(REPO, "oracle/_ref/ref_plan"), p, os.path.join(d, "o")],
+                       check=True, capture_output=True)
+        plan = np.fromfile(os.path.join(d, "o.plan"), dtype="<i8").reshape(-1, 14)
+        allocs = np.fromfile(os.path.join(d, "o.allocs"), dtype="<i8")
+        views = np.fromfile(os.path.join(d, "o.views"), dtype="<i8").reshape(-1, 5)
+    if len(plan):
+        plan = plan[np.lexsort(tuple(plan[:, k] for k in range(13, -1, -1)))]
+    return plan, allocs, views
+
+
+def plan_cases():
+    """Streams for the transfer-plan fixtures. Record field `reserved` bit 0 = fetch to the host."""
+    heat = S.heat_stream(1024, 1024, 128, 128, 4, base_src=1 << 30, base_dst=(1 << 30) + (1 << 24))
+    yield "plan_heat_1024_t128_s4", heat
+    small = S.heat_stream(256, 256, 64, 64, 5, base_src=1 << 20, base_dst=1 << 21)
+    export = S.from_tuples([[("m", S.R, 1 << 21, 256, 0, 0, 256, 256, 8)]])
+    export["task"] = small["task"].max() + 1
+    export["reserved"] = 1
+    yield "plan_heat_256_export", np.concatenate([small, export])
+    for seed in range(4):
+        recs = S.microbench_stream(7, seed, n=256, ld=256, align=16, max_side_units=6)
+        rng = np.random.default_rng(seed + 1000)
+        recs["reserved"] = (rng.random(len(recs)) < 0.25).astype(np.uint16)
+        yield f"plan_mat_wb_{seed}", recs
+    for seed in range(3):
+        rng = np.random.default_rng(seed)
+        rows = []
+        for t in range(8):
+            for _ in range(int(rng.integers(1, 3))):
+                a = 4096 + int(rng.integers(0, 512)) * 8
+                b = a + int(rng.integers(1, 64)) * 8
+                rows.append((t, S.SEGMENT, [S.R, S.W, S.RW][int(rng.integers(0, 3))], int(rng.random() < 0.2), a, b, 0, 0, 0, 0, 0))
+        yield f"plan_seg_{seed}", np.array(rows, dtype=S.REC)
+
+
 def main():
     out = {}
     for name, recs in cases():
@@ -74,6 +120,15 @@ def main():
         out[name + "__edges"] = e
         print(f"{name}: {len(recs)} accesses, {len(e)} unique edges")
     np.savez_compressed(os.path.join(HERE, "deps_golden.npz"), **out)
+    out = {}
+    for name, recs in plan_cases():
+        plan, allocs, views = ref_plan(recs)
+        out[name + "__stream"] = recs
+        out[name + "__plan"] = plan
+        out[name + "__allocs"] = allocs
+        out[name + "__views"] = views
+        print(f"{name}: {len(recs)} accesses, {len(plan)} copies, {len(allocs)} allocations")
+    np.savez_compressed(os.path.join(HERE, "plan_golden.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,68 @@
+"""Transfer planner (host code, no GPU): bit-exact against the reference's own memory tree
+(golden plans from tests/golden/make_golden.py) -- allocation sizes and order, every copy
+(kind, source and destination allocation/offset/ld, shape) and every access's device view."""
+import os
+
+import numpy as np
+import pytest
+
+import xkaapi_b200 as xk
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+G = np.load(os.path.join(REPO, "tests", "golden", "plan_golden.npz"))
+CASES = sorted(k[:-len("__stream")] for k in G.files if k.endswith("__stream"))
+
+
+def plan_of(recs):
+    P = xk.Planner()
+    views = []
+    first = 0
+    for i in range(len(recs)):
+        if i == 0 or recs[i]["task"] != recs[i - 1]["task"]:
+            first = i
+        views.append(P.fetch(recs[i], i - first, 0 if recs[i]["reserved"] & 1 else 1))
+    q = P.copies()
+    if len(q):
+        q = q[np.lexsort(tuple(q[:, k] for k in range(13, -1, -1)))]
+    return q, P.allocations(), np.array(views)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_plan_matches_reference(case):
+    recs = G[case + "__stream"]
+    q, allocs, views = plan_of(recs)
+    np.testing.assert_array_equal(q, G[case + "__plan"])
+    np.testing.assert_array_equal(allocs.astype(np.int64), G[case + "__allocs"])
+    dev = (recs["reserved"] & 1) == 0
+    np.testing.assert_array_equal(views[dev], G[case + "__views"][dev][:, 2:])
+
+
+def test_heat_plan_counts_per_step():
+    """1024^2 FP64, 128^2 tiles: step 0 allocates 128 buffers and issues 127 H2D + 427 D2D copies;
+    step 1 issues 60 H2D + 1184 D2D; from step 2 the pattern alternates 812 / 1296 D2D."""
+    recs = G["plan_heat_1024_t128_s4__stream"]
+    q, allocs, _ = plan_of(recs)
+    per = []
+    for s in range(4):
+        sel = (q[:, 0] >= 64 * s) & (q[:, 0] < 64 * (s + 1))
+        per.append((int((q[sel, 2] == 0).sum()), int((q[sel, 2] == 2).sum())))
+    assert per == [(127, 427), (60, 1184), (0, 812), (0, 1296)]
+
+
+def test_planner_rejects_wrapping_tiles_and_view_overflow():
+    import streams as S
+    P = xk.Planner()
+    wrap = S.from_tuples([[("m", S.R, 4096, 64, 60, 0, 8, 2, 8)]])          # rows 60..67 wrap ld 64
+    with pytest.raises(xk.XkbError) as e:
+        P.fetch(wrap[0], 0, 1)
+    assert e.value.code == xk.XKB_EINVAL
+    # nine differently shaped reads of one block: the 9th needs a 9th allocation view
+    P = xk.Planner()
+    for k in range(9):
+        r = S.from_tuples([[("m", S.R, 1 << 20, 64, 0, 0, 8 + k, 4, 8)]])[0]
+        if k < 8:
+            P.fetch(r, 0, 1)
+        else:
+            with pytest.raises(xk.XkbError) as e:
+                P.fetch(r, 0, 1)
+            assert e.value.code == xk.XKB_ERANGE

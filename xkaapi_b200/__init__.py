@@ -63,6 +63,12 @@ SIGNATURES = {
     "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
     "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_sched_kernel_ms": (_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "xkb_planner_create": (_int, [ctypes.POINTER(_vp)]),
+    "xkb_planner_destroy": (_int, [_vp]),
+    "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),
+    "xkb_planner_plan": (_int, [_vp, _vp, ctypes.c_size_t, _int, _vp]),
+    "xkb_planner_copies": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _int]),
+    "xkb_planner_allocations": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_resolver_destroy": (_int, [_vp]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
@@ -239,3 +245,54 @@ class Scheduler:
 
 
 from .heat import heat_task_descs, heat_access_records  # noqa: E402,F401
+
+
+class Planner:
+    """Coherency/transfer planner (xkb_planner_t, host code: no GPU needed). Copies come back as
+    an (n, 14) int64 array: task, access, kind, src_dev, src_alloc, src_off, src_ld, dst_dev,
+    dst_alloc, dst_off, dst_ld, m, n, sizeof."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        check(lib().xkb_planner_create(ctypes.byref(self._h)))
+
+    def plan(self, recs, device=1):
+        import numpy as np
+        recs = np.ascontiguousarray(recs)
+        views = np.zeros((len(recs), 3), dtype=np.int64)
+        check(lib().xkb_planner_plan(self._h, recs.ctypes.data, len(recs), device, views.ctypes.data))
+        return views
+
+    def fetch(self, rec, access_index, device=1):
+        import numpy as np
+        rec = np.ascontiguousarray(rec).reshape(1)
+        v = np.zeros(3, dtype=np.int64)
+        check(lib().xkb_planner_fetch(self._h, rec.ctypes.data, access_index, device, v.ctypes.data))
+        return v
+
+    def copies(self, take=False):
+        import numpy as np
+        n = ctypes.c_size_t()
+        check(lib().xkb_planner_copies(self._h, None, 0, ctypes.byref(n), 0))
+        out = np.zeros((n.value, 14), dtype=np.int64)
+        check(lib().xkb_planner_copies(self._h, out.ctypes.data, n.value, ctypes.byref(n), 1 if take else 0))
+        return out
+
+    def allocations(self):
+        import numpy as np
+        n = ctypes.c_size_t()
+        check(lib().xkb_planner_allocations(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=np.uint64)
+        check(lib().xkb_planner_allocations(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().xkb_planner_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,343 @@
+// Coherency and transfer planner for one host (device 0) and one GPU (device 1).
+//
+// Computes the same allocations, device views and copies as the reference's coherency
+// controller, KBLASMemoryTree::fetch (include/xkrt/memory/access/blas/memory-tree.hpp:1805-1874),
+// under the canonical schedule: accesses fetched one at a time in spawn/declaration order, each
+// fetch's copies completed before the next fetch (so no block is ever "being fetched" when a
+// fetch starts, and no access has to await another's copy).
+//
+// Model (my own data structures; the decisions are the reference's):
+//  * Block partition of a (ld, sizeof) frame. The reference's tree is a partition of every rect
+//    inserted so far into blocks; that partition is canonical: the x-slabs are the elementary
+//    intervals of every x-boundary inserted so far, and within a slab the y-cuts are the
+//    boundaries of every inserted rect covering that slab. A block never merges. Here: an
+//    ordered map of slabs, each an ordered map of blocks. Inserting a rect splits the slabs
+//    straddling its x-boundaries (both halves keep every block), creates slabs over x-gaps,
+//    and in each slab it covers splits the blocks straddling its y-boundaries and creates
+//    fresh blocks over y-gaps (fetch_list_to_device step 1, memory-tree.hpp:1765-1770).
+//  * Block state: up to 8 allocation views (MEMORY_REPLICATE_ALLOCATION_VIEWS_MAX,
+//    memory-tree.hpp:91), a coherent-view bitmask on the GPU, and the per-device coherent bits
+//    (host = bit 0, GPU = bit 1). A view is (allocation, origin x, origin y, ld): the byte of
+//    frame point p lives at alloc + (p.x - ox) + (p.y - oy) * ld * sizeof. With views stored by
+//    origin, the reference's offset adjustment on split (memory_block_init, :284-339) is a copy.
+//  * Device fetch: reuse the oldest allocation on which every block of the access has a view
+//    (:1396-1450), else allocate m*n*sizeof bytes and give every block a view with origin at the
+//    access corner and ld = m (:1326-1372); the access's device view is its corner's view
+//    (:1452-1469). R: per block, nothing if that view is coherent; D2D from the block's first
+//    coherent GPU view if the GPU holds it; else H2D from the host (:1471-1631). W: that view
+//    becomes the only coherent copy anywhere (:1633-1667). Completion marks the fetched view
+//    coherent and the GPU bit set (:2067-2105).
+//  * Host fetch (write-back): no copy if no device holds the block, or the host already does;
+//    else D2H from the view on the LARGEST allocation of the block (first one of maximal size,
+//    coherent or not -- as the reference selects it, :1110-1160); completion sets the host bit.
+#include "common.cuh"
+
+#include <cstring>
+#include <iterator>
+#include <map>
+#include <memory>
+#include <new>
+#include <vector>
+
+namespace {
+
+constexpr int MAX_VIEWS = 8;
+constexpr uint8_t DEV_HOST = 1, DEV_GPU = 2;
+
+struct View { int32_t alloc; uint64_t ox, oy, ld; };
+struct State {
+    uint8_t nviews = 0;
+    View views[MAX_VIEWS];
+    uint8_t coh = 0;        // coherent GPU views (bit per view index)
+    uint8_t dev = 0;        // coherent devices: DEV_HOST | DEV_GPU
+};
+struct Block { uint64_t y1; State st; };
+struct Slab { uint64_t x1; std::map<uint64_t, Block> blocks; };
+struct Frame {
+    uint64_t ld, s;
+    bool any = false;
+    std::map<uint64_t, Slab> slabs;
+};
+struct Rect { uint64_t x0, x1, y0, y1; };
+struct Partite { uint64_t x0, x1, y0, y1; State * st; };
+
+void split_x(Frame & f, uint64_t x)
+{
+    auto it = f.slabs.upper_bound(x);
+    if (it == f.slabs.begin()) return;
+    --it;
+    if (it->first < x && x < it->second.x1)
+    {
+        Slab right;
+        right.x1 = it->second.x1;
+        right.blocks = it->second.blocks;
+        it->second.x1 = x;
+        f.slabs.emplace(x, std::move(right));
+    }
+}
+
+void split_y(Slab & sl, uint64_t y)
+{
+    auto it = sl.blocks.upper_bound(y);
+    if (it == sl.blocks.begin()) return;
+    --it;
+    if (it->first < y && y < it->second.y1)
+    {
+        Block right = it->second;
+        it->second.y1 = y;
+        sl.blocks.emplace(y, right);
+    }
+}
+
+void insert(Frame & f, const Rect & r)
+{
+    split_x(f, r.x0);
+    split_x(f, r.x1);
+    // slabs over the x-gaps of [x0, x1)
+    uint64_t x = r.x0;
+    auto it = f.slabs.lower_bound(r.x0);
+    while (x < r.x1)
+    {
+        if (it != f.slabs.end() && it->first == x) { x = it->second.x1; ++it; continue; }
+        const uint64_t end = (it != f.slabs.end() && it->first < r.x1) ? it->first : r.x1;
+        Slab s; s.x1 = end;
+        it = std::next(f.slabs.emplace(x, std::move(s)).first);
+        x = end;
+    }
+    for (auto sit = f.slabs.lower_bound(r.x0); sit != f.slabs.end() && sit->first < r.x1; ++sit)
+    {
+        Slab & sl = sit->second;
+        split_y(sl, r.y0);
+        split_y(sl, r.y1);
+        uint64_t y = r.y0;
+        auto bit = sl.blocks.lower_bound(r.y0);
+        while (y < r.y1)
+        {
+            if (bit != sl.blocks.end() && bit->first == y) { y = bit->second.y1; ++bit; continue; }
+            const uint64_t end = (bit != sl.blocks.end() && bit->first < r.y1) ? bit->first : r.y1;
+            Block b; b.y1 = end;
+            bit = std::next(sl.blocks.emplace(y, b).first);
+            y = end;
+        }
+    }
+    f.any = true;
+}
+
+void partites(Frame & f, const Rect & r, std::vector<Partite> & out)
+{
+    out.clear();
+    for (auto sit = f.slabs.lower_bound(r.x0); sit != f.slabs.end() && sit->first < r.x1; ++sit)
+        for (auto bit = sit->second.blocks.lower_bound(r.y0); bit != sit->second.blocks.end() && bit->first < r.y1; ++bit)
+            out.push_back({sit->first, sit->second.x1, bit->first, bit->second.y1, &bit->second.st});
+}
+
+inline int64_t view_off(const View & v, uint64_t x, uint64_t y, uint64_t s)
+{
+    return (int64_t) (x - v.ox) + (int64_t) (y - v.oy) * (int64_t) v.ld * (int64_t) s;
+}
+
+} // namespace
+
+struct xkb_planner {
+    std::map<std::pair<uint64_t, uint64_t>, std::unique_ptr<Frame>> frames;
+    std::vector<uint64_t> allocs;
+    std::vector<xkb_copy_t> copies;
+    std::vector<Partite> scratch;
+};
+
+static int frame_rect(const xkb_access_rec_t & a, uint64_t & ld, uint64_t & s, Rect & r)
+{
+    if (a.type == XKB_ACCESS_TYPE_SEGMENT)
+    {
+        if (a.ld <= a.addr) return xkb_set_error(XKB_EINVAL, "planner: empty segment");
+        ld = ~0ull; s = 1;                          // segments: frame ld = SIZE_MAX, sizeof = 1
+        r = {a.addr, a.ld, 0, 1};
+        return XKB_OK;
+    }
+    if (a.type != XKB_ACCESS_TYPE_BLAS_MATRIX || !a.ld || !a.sizeof_type || !a.m || !a.n || a.m > a.ld)
+        return xkb_set_error(XKB_EINVAL, "planner: bad access");
+    ld = a.ld; s = a.sizeof_type;
+    const uint64_t LDs = ld * s, A = a.addr + (a.offset_n * ld + a.offset_m) * s;
+    const uint64_t x0 = A % LDs, y0 = A / LDs;
+    if (x0 + a.m * s > LDs)
+        return xkb_set_error(XKB_EINVAL, "planner: matrix tiles that wrap the leading dimension are not supported");
+    r = {x0, x0 + a.m * s, y0, y0 + a.n};
+    return XKB_OK;
+}
+
+static void push_copy(xkb_planner * P, int64_t task, int64_t access, int kind, const Partite & p, uint64_t ld, uint64_t s,
+                      int64_t src_alloc, int64_t src_off, int64_t src_ld, int64_t dst_alloc, int64_t dst_off, int64_t dst_ld)
+{
+    xkb_copy_t c;
+    c.task = task; c.access = access; c.kind = kind;
+    c.src_dev = kind == XKB_COPY_H2D ? 0 : 1;
+    c.src_alloc = src_alloc; c.src_off = src_off; c.src_ld = src_ld;
+    c.dst_dev = kind == XKB_COPY_D2H ? 0 : 1;
+    c.dst_alloc = dst_alloc; c.dst_off = dst_off; c.dst_ld = dst_ld;
+    if (ld == ~0ull) { c.m = (int64_t) (p.x1 - p.x0); c.n = 1; c.sizeof_type = 1; c.src_ld = c.src_ld ? c.src_ld : 0; }
+    else { c.m = (int64_t) ((p.x1 - p.x0) / s); c.n = (int64_t) (p.y1 - p.y0); c.sizeof_type = (int64_t) s; }
+    P->copies.push_back(c);
+}
+
+static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access_index, int device, xkb_view_t * view)
+{
+    uint64_t ld, s; Rect r;
+    int rc = frame_rect(a, ld, s, r);
+    if (rc) return rc;
+    std::unique_ptr<Frame> & fp = P->frames[{ld, s}];
+    if (!fp) { fp.reset(new (std::nothrow) Frame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); fp->ld = ld; fp->s = s; }
+    Frame & f = *fp;
+    const bool seg = ld == ~0ull;
+    const uint64_t host_stride = seg ? 0 : ld * s;
+    auto host_addr = [&](const Partite & p) -> int64_t { return (int64_t) (p.x0 + p.y0 * host_stride); };
+
+    if (device == 0)
+    {
+        if (view) { view->alloc = -1; view->off = (int64_t) a.addr; view->ld = (int64_t) a.ld; }
+        if (!f.any) return XKB_OK;                 // no device access yet: nothing to write back
+        insert(f, r);
+        partites(f, r, P->scratch);
+        for (const Partite & p : P->scratch)
+        {
+            State & st = *p.st;
+            if (st.dev == 0 || (st.dev & DEV_HOST)) continue;
+            int src = 0;
+            for (int i = 1; i < st.nviews; ++i)
+                if (P->allocs[st.views[src].alloc] < P->allocs[st.views[i].alloc]) src = i;
+            const View & v = st.views[src];
+            push_copy(P, a.task, access_index, XKB_COPY_D2H, p, ld, s, v.alloc, view_off(v, p.x0, p.y0, s),
+                      seg ? 0 : (int64_t) v.ld, -1, host_addr(p), seg ? 0 : (int64_t) ld);
+        }
+        for (const Partite & p : P->scratch)
+            if (p.st->dev != 0 && !(p.st->dev & DEV_HOST)) p.st->dev |= DEV_HOST;   // completion
+        return XKB_OK;
+    }
+    if (device != 1) return xkb_set_error(XKB_EINVAL, "planner: device must be 0 (host) or 1 (GPU)");
+
+    insert(f, r);
+    partites(f, r, P->scratch);
+    std::vector<Partite> & parts = P->scratch;
+    // (3) oldest allocation with a view in every block, else a new one
+    int32_t alloc = -1;
+    {
+        const State & s0 = *parts[0].st;
+        for (int j = 0; j < s0.nviews && alloc < 0; ++j)
+        {
+            const int32_t c = s0.views[j].alloc;
+            bool all = true;
+            for (size_t k = 1; k < parts.size() && all; ++k)
+            {
+                bool has = false;
+                for (int q = 0; q < parts[k].st->nviews; ++q) if (parts[k].st->views[q].alloc == c) { has = true; break; }
+                all = has;
+            }
+            if (all) alloc = c;
+        }
+    }
+    const uint64_t m_el = seg ? (r.x1 - r.x0) : a.m;
+    if (alloc < 0)
+    {
+        for (const Partite & p : parts)
+            if (p.st->nviews >= MAX_VIEWS)
+                return xkb_set_error(XKB_ERANGE, "planner: a block would need more than %d allocations on the device "
+                                                 "(the reference stops here too)", MAX_VIEWS);
+        alloc = (int32_t) P->allocs.size();
+        P->allocs.push_back(seg ? (r.x1 - r.x0) : a.m * a.n * a.sizeof_type);
+        for (const Partite & p : parts)
+        {
+            State & st = *p.st;
+            st.views[st.nviews++] = View{alloc, r.x0, r.y0, m_el};
+        }
+    }
+    auto view_idx = [&](const State & st) { for (int q = 0; q < st.nviews; ++q) if (st.views[q].alloc == alloc) return q; return -1; };
+    // (4) the access's device view: its corner block's view
+    for (const Partite & p : parts)
+        if (p.x0 == r.x0 && p.y0 == r.y0)
+        {
+            const View & v = p.st->views[view_idx(*p.st)];
+            if (view) { view->alloc = alloc; view->off = view_off(v, r.x0, r.y0, s); view->ld = (int64_t) v.ld; }
+        }
+    // (5) reads: copies
+    std::vector<std::pair<State *, int>> done;
+    if (a.mode & XKB_ACCESS_MODE_R)
+    {
+        for (const Partite & p : parts)
+        {
+            State & st = *p.st;
+            const int vi = view_idx(st);
+            if (st.coh & (1u << vi)) continue;
+            const View & dv = st.views[vi];
+            if (st.dev & DEV_GPU)
+            {
+                int si = 0; while (!(st.coh & (1u << si))) ++si;
+                const View & sv = st.views[si];
+                push_copy(P, a.task, access_index, XKB_COPY_D2D, p, ld, s, sv.alloc, view_off(sv, p.x0, p.y0, s),
+                          seg ? 0 : (int64_t) sv.ld, alloc, view_off(dv, p.x0, p.y0, s), seg ? 0 : (int64_t) dv.ld);
+            }
+            else
+                push_copy(P, a.task, access_index, XKB_COPY_H2D, p, ld, s, -1, host_addr(p), seg ? 0 : (int64_t) ld,
+                          alloc, view_off(dv, p.x0, p.y0, s), seg ? 0 : (int64_t) dv.ld);
+            done.push_back({&st, vi});
+        }
+    }
+    // (6) writes: the written view becomes the only coherent copy
+    if (a.mode & XKB_ACCESS_MODE_W)
+        for (const Partite & p : parts) { p.st->coh = (uint8_t) (1u << view_idx(*p.st)); p.st->dev = DEV_GPU; }
+    // completion of the copies
+    for (auto & d : done) { d.first->coh |= (uint8_t) (1u << d.second); d.first->dev |= DEV_GPU; }
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_create(xkb_planner_t ** out)
+{
+    if (!out) return xkb_set_error(XKB_EINVAL, "planner_create: null output");
+    *out = new (std::nothrow) xkb_planner();
+    return *out ? XKB_OK : xkb_set_error(XKB_ENOMEM, "planner_create: out of memory");
+}
+
+extern "C" int xkb_planner_destroy(xkb_planner_t * P)
+{
+    delete P;
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_fetch(xkb_planner_t * P, const xkb_access_rec_t * access, uint32_t access_index, int device,
+                                 xkb_view_t * view)
+{
+    if (!P || !access) return xkb_set_error(XKB_EINVAL, "planner_fetch: bad arguments");
+    return fetch_one(P, *access, access_index, device, view);
+}
+
+extern "C" int xkb_planner_plan(xkb_planner_t * P, const xkb_access_rec_t * recs, size_t n, int device, xkb_view_t * views)
+{
+    if (!P || (n && !recs)) return xkb_set_error(XKB_EINVAL, "planner_plan: bad arguments");
+    size_t first = 0;
+    for (size_t i = 0; i < n; ++i)
+    {
+        if (i == 0 || recs[i].task != recs[i - 1].task) first = i;
+        int rc = fetch_one(P, recs[i], (int64_t) (i - first), device, views ? views + i : nullptr);
+        if (rc) return rc;
+    }
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_copies(xkb_planner_t * P, xkb_copy_t * out, size_t cap, size_t * n, int take)
+{
+    if (!P || !n) return xkb_set_error(XKB_EINVAL, "planner_copies: bad arguments");
+    *n = P->copies.size();
+    if (!out) return XKB_OK;
+    if (cap < P->copies.size()) return xkb_set_error(XKB_ERANGE, "planner_copies: %zu records needed", P->copies.size());
+    if (!P->copies.empty()) memcpy(out, P->copies.data(), P->copies.size() * sizeof(xkb_copy_t));
+    if (take) P->copies.clear();
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_allocations(xkb_planner_t * P, uint64_t * sizes, size_t cap, size_t * n)
+{
+    if (!P || !n) return xkb_set_error(XKB_EINVAL, "planner_allocations: bad arguments");
+    *n = P->allocs.size();
+    if (!sizes) return XKB_OK;
+    if (cap < P->allocs.size()) return xkb_set_error(XKB_ERANGE, "planner_allocations: %zu entries needed", P->allocs.size());
+    if (!P->allocs.empty()) memcpy(sizes, P->allocs.data(), P->allocs.size() * sizeof(uint64_t));
+    return XKB_OK;
+}
