@@ -153,6 +153,22 @@ XKB_API int xkb_planner_copies(xkb_planner_t * planner, xkb_copy_t * out, size_t
 /* Byte size of every device allocation made so far, in allocation order. */
 XKB_API int xkb_planner_allocations(xkb_planner_t * planner, uint64_t * sizes, size_t cap, size_t * n);
 
+/* Run planned copies in order on `stream`: H2D and D2H with cudaMemcpy2DAsync, the D2D copies
+ * of each access as one gather kernel (one CTA per copy). alloc_ptrs[k] is the device
+ * memory backing allocation ordinal k (at least xkb_planner_allocations' size). Host addresses
+ * in the records must be valid host memory (pinned memory makes the copies asynchronous).
+ * Replaces the copy commands the reference queues per planned copy (runtime_t::copy,
+ * src/memory/copy.cc:65-105, executed by src/driver/driver_cu.cc:616-767). */
+XKB_API int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, void * stream);
+
+/* The reference tile body's contract on per-access replicas (diffusion_cuda,
+ * examples/heat-diffusion-2d/src/kernels/diffusion.cu:130-154): src and dst are the replicas'
+ * device views re-based to the tile origin as the example's launcher does
+ * (examples/heat-diffusion-2d/src/main.cc:214-219), each with its own leading dimension;
+ * nx, ny, c and the storage type are run-time arguments instead of compile-time constants. */
+XKB_API int xkb_diffusion_views(int dtype, void * stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
+                                int64_t tile_x, int64_t tile_y, int64_t tsx, int64_t tsy, int64_t nx, int64_t ny, double c);
+
 /* ---- tasks and the device scheduler ------------------------------------------------------ */
 /* Built-in task bodies the device scheduler can run inline (the reference runs them as
  * per-task kernel launches through a format's launcher, include/xkrt/driver/kernel-launcher.h:44-51). */

@@ -69,6 +69,8 @@ SIGNATURES = {
     "xkb_planner_plan": (_int, [_vp, _vp, ctypes.c_size_t, _int, _vp]),
     "xkb_planner_copies": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _int]),
     "xkb_planner_allocations": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "xkb_plan_execute": (_int, [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]),
+    "xkb_diffusion_views": (_int, [_int, _vp, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _dbl]),
     "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_resolver_destroy": (_int, [_vp]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
@@ -296,3 +298,11 @@ class Planner:
             self.close()
         except Exception:
             pass
+
+
+def plan_execute(copies, alloc_ptrs, stream=None):
+    """Execute planned copies ((n, 14) int64 array) with the given allocation base pointers."""
+    import numpy as np
+    copies = np.ascontiguousarray(copies, dtype=np.int64)
+    ptrs = (ctypes.c_void_p * max(1, len(alloc_ptrs)))(*alloc_ptrs)
+    check(lib().xkb_plan_execute(copies.ctypes.data, len(copies), ptrs, len(alloc_ptrs), _stream(stream)))

@@ -1,0 +1,160 @@
+// Execution of a transfer plan and the replica-layout heat tile body.
+//
+// xkb_plan_execute runs a list of planned copies in order on one stream: host<->device copies
+// with cudaMemcpy2DAsync (the reference issues one cuMemcpy2DAsync per copy command,
+// src/driver/driver_cu.cc:671-761), and the device-to-device copies one access issues as ONE
+// gather kernel launch -- one CTA per copy, 16-, 8- or 1-byte moves depending on alignment --
+// instead of one copy command each. The copies of one access never alias one another: they
+// fill distinct blocks of the access, from views that were coherent before the access. Copies
+// of different accesses may (a later access can read what an earlier copy wrote), so a batch
+// never spans two accesses.
+//
+// xkb_diffusion_views is the reference's tile body contract (diffusion_cuda,
+// examples/heat-diffusion-2d/src/kernels/diffusion.cu:107-154) on per-access replicas:
+// src/dst point at the tile origin after the launcher's re-basing (main.cc:214-219), with their
+// own leading dimensions.
+#include "common.cuh"
+
+#include <vector>
+
+namespace xkb {
+
+struct D2D { const uint8_t * src; uint8_t * dst; int64_t src_pitch, dst_pitch, row_bytes, rows; };
+
+__global__ void __launch_bounds__(256) d2d_gather_kernel(const D2D * __restrict__ ops)
+{
+    const D2D o = ops[blockIdx.x];
+    const bool a16 = ((((uintptr_t) o.src) | ((uintptr_t) o.dst) | o.src_pitch | o.dst_pitch | o.row_bytes) & 15) == 0;
+    const bool a8 = ((((uintptr_t) o.src) | ((uintptr_t) o.dst) | o.src_pitch | o.dst_pitch | o.row_bytes) & 7) == 0;
+    if (a16)
+    {
+        const int64_t w = o.row_bytes / 16, total = w * o.rows;
+        for (int64_t k = threadIdx.x; k < total; k += blockDim.x)
+        {
+            const int64_t r = k / w, c = k % w;
+            *(uint4 *) (o.dst + r * o.dst_pitch + c * 16) = *(const uint4 *) (o.src + r * o.src_pitch + c * 16);
+        }
+    }
+    else if (a8)
+    {
+        const int64_t w = o.row_bytes / 8, total = w * o.rows;
+        for (int64_t k = threadIdx.x; k < total; k += blockDim.x)
+        {
+            const int64_t r = k / w, c = k % w;
+            *(uint2 *) (o.dst + r * o.dst_pitch + c * 8) = *(const uint2 *) (o.src + r * o.src_pitch + c * 8);
+        }
+    }
+    else
+    {
+        const int64_t total = o.row_bytes * o.rows;
+        for (int64_t k = threadIdx.x; k < total; k += blockDim.x)
+        {
+            const int64_t r = k / o.row_bytes, c = k % o.row_bytes;
+            o.dst[r * o.dst_pitch + c] = o.src[r * o.src_pitch + c];
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) diffusion_views_kernel(const T * __restrict__ src, int64_t ld_src, T * __restrict__ dst,
+                                                              int64_t ld_dst, int64_t i0, int64_t j0, int64_t tsx, int64_t tsy,
+                                                              int64_t nx, int64_t ny, double c)
+{
+    const int64_t li = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t lj = blockIdx.y; lj < tsy; lj += gridDim.y)
+    {
+        const int64_t i = i0 + li, j = j0 + lj;
+        if (li >= tsx || !(i > 0 && i < nx - 1 && j > 0 && j < ny - 1)) continue;
+        const T * s = src + lj * ld_src + li;
+        const double sv = (double) s[0];
+        const double s2 = __dmul_rn(2.0, sv);
+        const double a = __dadd_rn(__dsub_rn((double) s[1], s2), (double) s[-1]);
+        const double b = __dadd_rn(__dsub_rn((double) s[ld_src], s2), (double) s[-ld_src]);
+        dst[lj * ld_dst + li] = (T) __dadd_rn(sv, __dmul_rn(c, __dadd_rn(a, b)));
+    }
+}
+
+} // namespace xkb
+
+using namespace xkb;
+
+extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, void * stream)
+{
+    if (n && (!copies || !alloc_ptrs)) return xkb_set_error(XKB_EINVAL, "plan_execute: bad arguments");
+    cudaStream_t st = xkb_stream(stream);
+    auto dev_ptr = [&](int64_t alloc, int64_t off) -> uint8_t * {
+        return (alloc >= 0 && (size_t) alloc < nallocs) ? (uint8_t *) alloc_ptrs[alloc] + off : nullptr;
+    };
+    std::vector<D2D> batch;
+    D2D * dbatch = nullptr;
+    size_t dcap = 0;
+    auto flush = [&]() -> int {
+        if (batch.empty()) return XKB_OK;
+        if (batch.size() > dcap)
+        {
+            if (dbatch) { cudaStreamSynchronize(st); cudaFree(dbatch); }
+            dcap = batch.size() * 2;
+            cudaError_t e = cudaMalloc(&dbatch, dcap * sizeof(D2D));
+            if (e != cudaSuccess) { dbatch = nullptr; return xkb_set_cuda_error(e); }
+        }
+        else cudaStreamSynchronize(st);   // the previous batch must have been consumed
+        cudaError_t e = cudaMemcpyAsync(dbatch, batch.data(), batch.size() * sizeof(D2D), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        d2d_gather_kernel<<<(unsigned) batch.size(), 256, 0, st>>>(dbatch);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        cudaStreamSynchronize(st);         // `batch` (pageable) is reused after this
+        batch.clear();
+        return XKB_OK;
+    };
+    int rc = XKB_OK;
+    for (size_t i = 0; i < n && rc == XKB_OK; ++i)
+    {
+        const xkb_copy_t & c = copies[i];
+        const int64_t row_bytes = c.m * c.sizeof_type;
+        const int64_t sp = c.src_ld ? c.src_ld * c.sizeof_type : row_bytes, dp = c.dst_ld ? c.dst_ld * c.sizeof_type : row_bytes;
+        if (c.kind == XKB_COPY_D2D)
+        {
+            if (i > 0 && (copies[i - 1].task != c.task || copies[i - 1].access != c.access) && (rc = flush())) break;
+            uint8_t * s = dev_ptr(c.src_alloc, c.src_off), * d = dev_ptr(c.dst_alloc, c.dst_off);
+            if (!s || !d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
+            batch.push_back({s, d, sp, dp, row_bytes, c.n});
+            continue;
+        }
+        if ((rc = flush())) break;
+        cudaError_t e;
+        if (c.kind == XKB_COPY_H2D)
+        {
+            uint8_t * d = dev_ptr(c.dst_alloc, c.dst_off);
+            if (!d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
+            e = cudaMemcpy2DAsync(d, dp, (const void *) (uintptr_t) c.src_off, sp, row_bytes, c.n, cudaMemcpyHostToDevice, st);
+        }
+        else if (c.kind == XKB_COPY_D2H)
+        {
+            const uint8_t * s = dev_ptr(c.src_alloc, c.src_off);
+            if (!s) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
+            e = cudaMemcpy2DAsync((void *) (uintptr_t) c.dst_off, dp, s, sp, row_bytes, c.n, cudaMemcpyDeviceToHost, st);
+        }
+        else { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu has an unknown kind", i); break; }
+        if (e != cudaSuccess) rc = xkb_set_cuda_error(e);
+    }
+    if (rc == XKB_OK) rc = flush();
+    if (dbatch) { cudaStreamSynchronize(st); cudaFree(dbatch); }
+    return rc;
+}
+
+extern "C" int xkb_diffusion_views(int dtype, void * stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
+                                   int64_t tile_x, int64_t tile_y, int64_t tsx, int64_t tsy, int64_t nx, int64_t ny, double c)
+{
+    if ((dtype != XKB_F64 && dtype != XKB_F32) || !src || !dst || tsx <= 0 || tsy <= 0)
+        return xkb_set_error(XKB_EINVAL, "diffusion_views: bad arguments");
+    const dim3 block(256), grid((unsigned) ((tsx + 255) / 256), (unsigned) (tsy < 1024 ? tsy : 1024));
+    if (dtype == XKB_F64)
+        diffusion_views_kernel<double><<<grid, block, 0, xkb_stream(stream)>>>((const double *) src, ld_src, (double *) dst, ld_dst,
+                                                                             tile_x * tsx, tile_y * tsy, tsx, tsy, nx, ny, c);
+    else
+        diffusion_views_kernel<float><<<grid, block, 0, xkb_stream(stream)>>>((const float *) src, ld_src, (float *) dst, ld_dst,
+                                                                            tile_x * tsx, tile_y * tsy, tsx, tsy, nx, ny, c);
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
