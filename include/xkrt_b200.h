@@ -220,6 +220,23 @@ XKB_API int xkb_sched_wait(xkb_sched_t * sched, uint64_t * executed);
 /* Device time of the last run's persistent kernel (CUDA events on the scheduler's stream). */
 XKB_API int xkb_sched_kernel_ms(xkb_sched_t * sched, double * ms);
 
+/* Persistent run of a graph that allocates nothing. This entry point has no counterpart in the
+ * reference. It is for callers that cannot allocate device memory at the time they run a graph:
+ * a runtime that reserved most of the GPU's memory for its own allocator at start-up (XKRT
+ * reserves 90 % of HBM), a serving loop whose memory is already split into fixed pools, or a
+ * latency-critical loop where cudaMalloc/cudaFree would synchronise the device. The wait
+ * counters and queue live in one fixed array of the library (8 MiB + 256 B on every GPU that
+ * loads it, held until the process exits), so a graph may have at most XKB_NOALLOC_MAX_TASKS
+ * tasks; larger graphs get XKB_ERANGE. `tasks` is a DEVICE array of descriptors, `graph` the
+ * resolver's device CSR. The call waits for the run to finish and returns XKB_ETIMEDOUT if a
+ * device wait gave up after timeout_s seconds; *executed (optional) = tasks run. The first call
+ * on each device looks up the array's device address (do it before any stream capture). Every
+ * call shares the array: calls whose runs overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+#define XKB_NOALLOC_MAX_TASKS (1u << 20)
+XKB_API int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_task_graph_t * graph, int warps_per_task,
+                                  double timeout_s, void * stream, uint64_t * executed);
+
 /* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
 /* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float
  * storage, every cell update computed in double and rounded once to float on store. */

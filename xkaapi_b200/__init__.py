@@ -63,6 +63,7 @@ SIGNATURES = {
     "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
     "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_sched_kernel_ms": (_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "xkb_sched_run_noalloc": (_int, [_vp, ctypes.POINTER(TaskGraph), _int, _dbl, _vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_planner_create": (_int, [ctypes.POINTER(_vp)]),
     "xkb_planner_destroy": (_int, [_vp]),
     "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),

@@ -478,3 +478,87 @@ extern "C" int xkb_sched_kernel_ms(xkb_sched_t * S, double * ms)
     *ms = f;
     return XKB_OK;
 }
+
+// ------------------------------------------------------------------------------------------
+// Persistent run without any allocation.
+//
+// Some callers cannot allocate device memory when they run a graph: a task runtime that has
+// reserved most of the GPU's memory for its own allocator at start-up (XKRT reserves 90 % of
+// HBM for its device memory areas), or a serving loop whose device memory is already carved
+// into fixed pools, gets a failed or competing cudaMalloc; and cudaMalloc/cudaFree can
+// synchronise the device in the middle of a latency-critical loop. This entry point keeps the
+// scheduler's working set -- wait counters, queue slots and four counters -- in the file-scope
+// array below instead, sized for at most XKB_NOALLOC_MAX_TASKS tasks (8 MiB + 256 B held by
+// every GPU that loads the library, until the process exits).
+static __device__ __align__(256) int g_sched_noalloc_scratch[2 * XKB_NOALLOC_MAX_TASKS + 64];
+
+// Device address of the scratch array for the current device. In host code the array's name
+// only stands for it; its device address is looked up once per device, with that device
+// current, on the first call made on that device.
+static int noalloc_scratch(int ** out)
+{
+    static int * cache[256] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    if (dev < 0 || dev >= 256) return xkb_set_error(XKB_ENODEV, "sched_run_noalloc: device %d out of range", dev);
+    if (!cache[dev])
+    {
+        void * p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_sched_noalloc_scratch);
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        cache[dev] = (int *) p;
+    }
+    *out = cache[dev];
+    return XKB_OK;
+}
+
+extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_task_graph_t * graph, int warps_per_task,
+                                     double timeout_s, void * stream, uint64_t * executed)
+{
+    if (!graph || (graph->ntasks && (!tasks || !graph->succ_ptr || !graph->npred)) || !(timeout_s > 0))
+        return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: bad arguments");
+    if (warps_per_task != 1 && warps_per_task != 2 && warps_per_task != 4 && warps_per_task != 8)
+        return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: warps per task must be 1, 2, 4 or 8");
+    if (graph->ntasks > XKB_NOALLOC_MAX_TASKS)
+        return xkb_set_error(XKB_ERANGE, "sched_run_noalloc: %llu tasks exceed the fixed capacity of %u tasks",
+                             (unsigned long long) graph->ntasks, (unsigned) XKB_NOALLOC_MAX_TASKS);
+    int * scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = xkb_stream(stream);
+    const uint32_t n = (uint32_t) graph->ntasks;
+    SchedArgs a;
+    a.tasks = tasks; a.ntasks = n; a.succ_ptr = graph->succ_ptr; a.succ = graph->succ;
+    a.wc = scratch; a.queue = scratch + XKB_NOALLOC_MAX_TASKS;
+    a.ctr = (unsigned *) (scratch + 2 * XKB_NOALLOC_MAX_TASKS);
+    a.timeout_ns = (uint64_t) (timeout_s * 1e9);
+    // the array keeps the previous call's contents: the counters are zeroed here, and the init
+    // kernel rewrites every wait counter and queue slot this run uses
+    XKB_CUDA_TRY(cudaMemsetAsync(a.ctr, 0, 4 * sizeof(unsigned), st));
+    if (n)
+    {
+        int dev = 0, sms = 148, per = 2;
+        XKB_CUDA_TRY(cudaGetDevice(&dev));
+        XKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        XKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel<2>, SCHED_THREADS, 0));
+        const unsigned grid = (unsigned) (sms * (per > 0 ? per : 1));
+        sched_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, graph->npred);
+        sched_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, graph->npred);
+        switch (warps_per_task)
+        {
+            case 1: sched_persistent_kernel<1><<<grid, SCHED_THREADS, 0, st>>>(a); break;
+            case 2: sched_persistent_kernel<2><<<grid, SCHED_THREADS, 0, st>>>(a); break;
+            case 4: sched_persistent_kernel<4><<<grid, SCHED_THREADS, 0, st>>>(a); break;
+            default: sched_persistent_kernel<8><<<grid, SCHED_THREADS, 0, st>>>(a); break;
+        }
+        XKB_CUDA_TRY(cudaGetLastError());
+    }
+    unsigned ctr[4] = {0, 0, 0, 0};
+    XKB_CUDA_TRY(cudaMemcpyAsync(ctr, a.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (executed) *executed = ctr[3];
+    if (ctr[2] != 0)
+        return xkb_set_error(-(int) ctr[2], "sched_run_noalloc: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], n);
+    return XKB_OK;
+}
