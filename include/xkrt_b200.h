@@ -122,8 +122,8 @@ XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uin
  * (include/xkrt/memory/access/blas/memory-tree.hpp:1805-1874; fetch_list_to_device :1738-1802,
  * fetch_list_to_host :1185-1215), with every fetch's copies completed before the next fetch.
  * Device addresses are reported as (allocation ordinal, byte offset); host addresses as raw
- * byte addresses. Matrix tiles that wrap the leading dimension are rejected (XKB_EINVAL); a
- * block needing a 9th allocation view returns XKB_ERANGE where the reference aborts. */
+ * byte addresses. A block needing a 9th allocation view returns XKB_ERANGE where the reference
+ * aborts (MEMORY_REPLICATE_ALLOCATION_VIEWS_MAX, memory-tree.hpp:91,1364-1365). */
 typedef struct xkb_planner xkb_planner_t;
 
 #define XKB_COPY_H2D 0

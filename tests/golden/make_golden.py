@@ -66,6 +66,9 @@ def cases():
     yield "heat_1024_t128_s3", S.heat_stream(1024, 1024, 128, 128, 3)
     yield "heat_200x136_t64x48_s3", S.heat_stream(200, 136, 64, 48, 3)
     yield "microbench_1024_2000", S.microbench_stream(2000, 7, n=1024, ld=1024)
+    # grids not aligned to ld*sizeof: every tile wraps the leading dimension in the address frame
+    yield "heat_1024_t128_s3_unaligned", S.heat_stream(1024, 1024, 128, 128, 3, base_src=(1 << 20) + 4096,
+                                                       base_dst=(1 << 24) + 8)
     for kind in ("mat", "seg", "segmat"):
         for seed in range(3):
             yield f"mixed_{kind}_{seed}", mixed(kind, seed)
@@ -101,6 +104,17 @@ def plan_cases():
         rng = np.random.default_rng(seed + 1000)
         recs["reserved"] = (rng.random(len(recs)) < 0.25).astype(np.uint16)
         yield f"plan_mat_wb_{seed}", recs
+    # bases not aligned to ld*sizeof: tiles wrap the leading dimension in the address frame
+    yield "plan_heat_256_unaligned", S.heat_stream(256, 256, 64, 64, 4, base_src=(1 << 20) + 1024, base_dst=(1 << 22) + 512)
+    for seed in range(3):
+        rng = np.random.default_rng(seed)
+        rows = []
+        for t in range(8):
+            for _ in range(int(rng.integers(1, 3))):
+                m = int(rng.integers(1, 33)); om = int(rng.integers(0, 64)); nn = int(rng.integers(1, 6))
+                on = int(rng.integers(0, 8)); mode = [S.R, S.W, S.RW][int(rng.integers(0, 3))]
+                rows.append((t, S.MATRIX, mode, int(rng.random() < 0.2), 4096 + 8 * 24, 64, om, on, m, nn, 8))
+        yield f"plan_mat_wrap_{seed}", np.array(rows, dtype=S.REC)
     for seed in range(3):
         rng = np.random.default_rng(seed)
         rows = []

@@ -49,14 +49,10 @@ def test_heat_plan_counts_per_step():
     assert per == [(127, 427), (60, 1184), (0, 812), (0, 1296)]
 
 
-def test_planner_rejects_wrapping_tiles_and_view_overflow():
+def test_planner_rejects_view_overflow():
     import streams as S
-    P = xk.Planner()
-    wrap = S.from_tuples([[("m", S.R, 4096, 64, 60, 0, 8, 2, 8)]])          # rows 60..67 wrap ld 64
-    with pytest.raises(xk.XkbError) as e:
-        P.fetch(wrap[0], 0, 1)
-    assert e.value.code == xk.XKB_EINVAL
-    # nine differently shaped reads of one block: the 9th needs a 9th allocation view
+    # nine differently shaped reads of one block: the 9th needs a 9th allocation view, where the
+    # reference stops with a fatal error
     P = xk.Planner()
     for k in range(9):
         r = S.from_tuples([[("m", S.R, 1 << 20, 64, 0, 0, 8 + k, 4, 8)]])[0]
@@ -66,3 +62,14 @@ def test_planner_rejects_wrapping_tiles_and_view_overflow():
             with pytest.raises(xk.XkbError) as e:
                 P.fetch(r, 0, 1)
             assert e.value.code == xk.XKB_ERANGE
+
+
+def test_wrapped_tile_view_is_contiguous():
+    import streams as S
+    # an 8 x 2 tile whose rows wrap the leading dimension (ld 64, rows 60..67): one allocation of
+    # 8*2*8 bytes, device view at its start with ld 8
+    P = xk.Planner()
+    v = P.fetch(S.from_tuples([[("m", S.RW, 4096, 64, 60, 0, 8, 2, 8)]])[0], 0, 1)
+    assert list(P.allocations()) == [128] and list(v) == [0, 0, 8]
+    c = P.copies()
+    assert len(c) == 2 and set(c[:, 2]) == {xk.COPY_H2D}          # one H2D per rect of the tile

@@ -21,6 +21,7 @@ XKB_ECUDA = -1000
 F64, F32 = 0, 1
 TASK_NOOP, TASK_HEAT_F64, TASK_HEAT_F32, TASK_AXPBY = 0, 1, 2, 3
 FORM_PERSISTENT, FORM_PLAIN, FORM_GRAPH = 0, 1, 2
+COPY_H2D, COPY_D2H, COPY_D2D = 0, 1, 2
 
 _lib = None
 

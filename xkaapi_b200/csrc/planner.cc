@@ -44,7 +44,7 @@ namespace {
 constexpr int MAX_VIEWS = 8;
 constexpr uint8_t DEV_HOST = 1, DEV_GPU = 2;
 
-struct View { int32_t alloc; uint64_t ox, oy, ld; };
+struct View { int32_t alloc; int64_t ox, oy; uint64_t ld; };
 struct State {
     uint8_t nviews = 0;
     View views[MAX_VIEWS];
@@ -125,7 +125,6 @@ void insert(Frame & f, const Rect & r)
 
 void partites(Frame & f, const Rect & r, std::vector<Partite> & out)
 {
-    out.clear();
     for (auto sit = f.slabs.lower_bound(r.x0); sit != f.slabs.end() && sit->first < r.x1; ++sit)
         for (auto bit = sit->second.blocks.lower_bound(r.y0); bit != sit->second.blocks.end() && bit->first < r.y1; ++bit)
             out.push_back({sit->first, sit->second.x1, bit->first, bit->second.y1, &bit->second.st});
@@ -133,7 +132,7 @@ void partites(Frame & f, const Rect & r, std::vector<Partite> & out)
 
 inline int64_t view_off(const View & v, uint64_t x, uint64_t y, uint64_t s)
 {
-    return (int64_t) (x - v.ox) + (int64_t) (y - v.oy) * (int64_t) v.ld * (int64_t) s;
+    return ((int64_t) x - v.ox) + ((int64_t) y - v.oy) * (int64_t) v.ld * (int64_t) s;
 }
 
 } // namespace
@@ -145,13 +144,19 @@ struct xkb_planner {
     std::vector<Partite> scratch;
 };
 
-static int frame_rect(const xkb_access_rec_t & a, uint64_t & ld, uint64_t & s, Rect & r)
+// The access's rects in its (ld, sizeof) frame (access.hpp:204-287): one rect, or two when the
+// tile wraps the leading dimension; `origin` is where each rect's view origin lies so that
+// consecutive bytes of the access stay consecutive in a device allocation of ld = m
+// (the wrap adjustment of fetch_access_create_allocation_views, memory-tree.hpp:1341-1347).
+static int frame_rects(const xkb_access_rec_t & a, uint64_t & ld, uint64_t & s, Rect r[2], int64_t origin[2][2], int & nr)
 {
     if (a.type == XKB_ACCESS_TYPE_SEGMENT)
     {
         if (a.ld <= a.addr) return xkb_set_error(XKB_EINVAL, "planner: empty segment");
         ld = ~0ull; s = 1;                          // segments: frame ld = SIZE_MAX, sizeof = 1
-        r = {a.addr, a.ld, 0, 1};
+        r[0] = {a.addr, a.ld, 0, 1};
+        origin[0][0] = (int64_t) a.addr; origin[0][1] = 0;
+        nr = 1;
         return XKB_OK;
     }
     if (a.type != XKB_ACCESS_TYPE_BLAS_MATRIX || !a.ld || !a.sizeof_type || !a.m || !a.n || a.m > a.ld)
@@ -159,9 +164,12 @@ static int frame_rect(const xkb_access_rec_t & a, uint64_t & ld, uint64_t & s, R
     ld = a.ld; s = a.sizeof_type;
     const uint64_t LDs = ld * s, A = a.addr + (a.offset_n * ld + a.offset_m) * s;
     const uint64_t x0 = A % LDs, y0 = A / LDs;
-    if (x0 + a.m * s > LDs)
-        return xkb_set_error(XKB_EINVAL, "planner: matrix tiles that wrap the leading dimension are not supported");
-    r = {x0, x0 + a.m * s, y0, y0 + a.n};
+    origin[0][0] = (int64_t) x0; origin[0][1] = (int64_t) y0;
+    if (x0 + a.m * s <= LDs) { r[0] = {x0, x0 + a.m * s, y0, y0 + a.n}; nr = 1; return XKB_OK; }
+    r[0] = {x0, LDs, y0, y0 + a.n};
+    r[1] = {0, a.m * s - (LDs - x0), y0 + 1, y0 + a.n + 1};
+    origin[1][0] = (int64_t) x0 - (int64_t) LDs; origin[1][1] = (int64_t) y0 + 1;
+    nr = 2;
     return XKB_OK;
 }
 
@@ -181,9 +189,10 @@ static void push_copy(xkb_planner * P, int64_t task, int64_t access, int kind, c
 
 static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access_index, int device, xkb_view_t * view)
 {
-    uint64_t ld, s; Rect r;
-    int rc = frame_rect(a, ld, s, r);
+    uint64_t ld, s; Rect rr[2]; int64_t origin[2][2]; int nr = 0;
+    int rc = frame_rects(a, ld, s, rr, origin, nr);
     if (rc) return rc;
+    const Rect & r = rr[0];
     std::unique_ptr<Frame> & fp = P->frames[{ld, s}];
     if (!fp) { fp.reset(new (std::nothrow) Frame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); fp->ld = ld; fp->s = s; }
     Frame & f = *fp;
@@ -195,8 +204,9 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
     {
         if (view) { view->alloc = -1; view->off = (int64_t) a.addr; view->ld = (int64_t) a.ld; }
         if (!f.any) return XKB_OK;                 // no device access yet: nothing to write back
-        insert(f, r);
-        partites(f, r, P->scratch);
+        for (int k = 0; k < nr; ++k) insert(f, rr[k]);
+        P->scratch.clear();
+        for (int k = 0; k < nr; ++k) partites(f, rr[k], P->scratch);
         for (const Partite & p : P->scratch)
         {
             State & st = *p.st;
@@ -214,8 +224,16 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
     }
     if (device != 1) return xkb_set_error(XKB_EINVAL, "planner: device must be 0 (host) or 1 (GPU)");
 
-    insert(f, r);
-    partites(f, r, P->scratch);
+    for (int k = 0; k < nr; ++k) insert(f, rr[k]);
+    P->scratch.clear();
+    std::vector<int> part_rect;
+    for (int k = 0; k < nr; ++k)
+    {
+        const size_t before = P->scratch.size();
+        partites(f, rr[k], P->scratch);
+        part_rect.resize(P->scratch.size(), k);
+        (void) before;
+    }
     std::vector<Partite> & parts = P->scratch;
     // (3) oldest allocation with a view in every block, else a new one
     int32_t alloc = -1;
@@ -243,10 +261,10 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
                                                  "(the reference stops here too)", MAX_VIEWS);
         alloc = (int32_t) P->allocs.size();
         P->allocs.push_back(seg ? (r.x1 - r.x0) : a.m * a.n * a.sizeof_type);
-        for (const Partite & p : parts)
+        for (size_t k = 0; k < parts.size(); ++k)
         {
-            State & st = *p.st;
-            st.views[st.nviews++] = View{alloc, r.x0, r.y0, m_el};
+            State & st = *parts[k].st;
+            st.views[st.nviews++] = View{alloc, origin[part_rect[k]][0], origin[part_rect[k]][1], m_el};
         }
     }
     auto view_idx = [&](const State & st) { for (int q = 0; q < st.nviews; ++q) if (st.views[q].alloc == alloc) return q; return -1; };
