@@ -220,6 +220,60 @@ def microbench_stream(ntasks, seed, n=8192, ld=8192, align=64, max_units=32, bas
     return recs
 
 
+def serve_trace(ngraphs, seed, ts=128):
+    """Served-stream trace: grid side log-uniform in [256, 8192] rounded to a multiple of the
+    tile; steps uniform in {10..200}; FP64 / FP32 storage 50/50; Poisson arrival order."""
+    rng = np.random.default_rng(seed)
+    side = np.exp(rng.uniform(np.log(256), np.log(8192), ngraphs))
+    side = np.clip((np.round(side / ts) * ts).astype(np.int64), ts * 2, 8192)
+    steps = rng.integers(10, 201, ngraphs)
+    f32 = rng.integers(0, 2, ngraphs)
+    gaps = rng.exponential(1.0, ngraphs)              # unit-rate Poisson process, scaled later
+    bytes_ = (side.astype(np.float64) - 2) ** 2 * steps * np.where(f32 == 1, 8.0, 16.0)
+    return side, steps, f32, np.cumsum(gaps), bytes_
+
+
+def serve_requests(xk, side, steps, f32, arrivals):
+    reqs = (xk.Request * len(side))()
+    for k, r in enumerate(reqs):
+        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32 = float(arrivals[k]), int(side[k]), int(side[k]), 128, int(steps[k]), int(f32[k])
+        r.seed, r.c, r.result = 7000 + k, COEF, None
+    return reqs
+
+
+def serve_study(xk, torch, ngraphs=2000, slots=16, load=0.8):
+    side, steps, f32, unit_arrivals, bytes_ = serve_trace(ngraphs, 2026)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(150e9, free - 8e9))
+    srv = xk.Server(budget_bytes=budget, slots=slots)
+    # capacity: the first graphs of the trace all arriving at once (closed loop)
+    cal = min(300, ngraphs)
+    reqs = serve_requests(xk, side[:cal], steps[:cal], f32[:cal], np.zeros(cal))
+    srv.run(reqs)
+    capacity = float(bytes_[:cal].sum()) / max(r.finish_s for r in reqs)          # bytes/s served
+    # the trace: Poisson arrivals whose offered HBM traffic is `load` x the capacity
+    rate = load * capacity / float(bytes_.mean())                                  # graphs/s
+    arrivals = unit_arrivals / rate
+    reqs = serve_requests(xk, side, steps, f32, arrivals)
+    t0 = time.perf_counter()
+    srv.run(reqs)
+    wall = time.perf_counter() - t0
+    srv.close()
+    lat = np.array([r.finish_s - r.arrival_s for r in reqs]) * 1e3
+    wait = np.array([r.start_s - r.arrival_s for r in reqs]) * 1e3
+    fin = max(r.finish_s for r in reqs)
+    tasks = int(sum((-(-int(side[k]) // 128)) ** 2 * int(steps[k]) for k in range(ngraphs)))
+    return {"graphs": ngraphs, "p50_ms": round(float(np.percentile(lat, 50)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_ms": round(float(lat.mean()), 3),
+            "admission_wait_p99_ms": round(float(np.percentile(wait, 99)), 3),
+            "tasks": tasks, "tasks_per_s": round(tasks / fin), "GBps": round(float(bytes_.sum()) / fin / 1e9, 1),
+            "capacity_GBps": round(capacity / 1e9, 1), "offered_load": load, "rate_graphs_per_s": round(rate, 1),
+            "span_s": round(float(arrivals[-1]), 3), "makespan_s": round(fin, 3), "wall_s": round(wall, 3),
+            "budget_GB": round(budget / 1e9, 1), "slots": slots,
+            "trace": "Poisson arrivals, side log-uniform 256-8192 (multiple of 128), steps U{10..200}, FP64/FP32 50/50, "
+                     "128^2 tiles; load calibrated on a closed-loop run of the first 300 graphs"}
+
+
 def main():
     global NX, NY, STEPS
     ap = argparse.ArgumentParser()
@@ -386,6 +440,13 @@ def main():
                                         "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt)}
         r3.close()
 
+    # ---------------- served stream (after releasing the headline graph's memory) -----------
+    sch.close(); res.close()
+    del a, b
+    torch.cuda.synchronize(); torch.cuda.empty_cache()
+    if rank == 0 and not args.no_side:
+        extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000)
+
     # ---------------- CPU baseline (rank 0, N=1) ----------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_side:
@@ -420,7 +481,6 @@ def main():
         }
         line.update(extra)
         print(json.dumps(line))
-    sch.close(); res.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -112,6 +112,25 @@ XKB_API int xkb_resolver_graph(xkb_resolver_t * resolver, xkb_task_graph_t * gra
  * pairs. *nedges receives the count; XKB_ERANGE if cap_pairs is smaller. */
 XKB_API int xkb_resolver_edges(xkb_resolver_t * resolver, uint32_t * pairs, size_t cap_pairs, size_t * nedges);
 
+/* A periodic graph: the same window of `period` tasks repeated, task t of window w+1
+ * depending on tasks of window w only through the `x` (cross-window) edges -- e.g. the
+ * heat-diffusion graph with a window of two Jacobi steps (the grids swap back every two steps).
+ * Device arrays, owned by the resolver that built them. */
+typedef struct xkb_periodic_graph_t {
+    uint64_t period;
+    const uint32_t * succ_ptr;     /* [period+1] successors inside the same window              */
+    const uint32_t * succ;
+    const uint32_t * xsucc_ptr;    /* [period+1] successors in the NEXT window (ids in that window) */
+    const uint32_t * xsucc;
+    const uint32_t * npred_first;  /* [period] wait count of a task of the first window          */
+    const uint32_t * npred_next;   /* [period] wait count of a task of every later window        */
+} xkb_periodic_graph_t;
+
+/* Extract the periodic form of a resolver holding exactly three windows of `period` tasks:
+ * checks that window 1 repeats window 0 (its own and its incoming edges, shifted) and that no
+ * edge skips a window; XKB_EINVAL if the graph is not periodic that way. */
+XKB_API int xkb_resolver_periodic(xkb_resolver_t * resolver, uint64_t period, xkb_periodic_graph_t * out);
+
 /* Counters: tasks added, unique edges, device+host time of the last batch in ms. */
 XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms);
 
@@ -220,6 +239,14 @@ XKB_API int xkb_sched_wait(xkb_sched_t * sched, uint64_t * executed);
 /* Device time of the last run's persistent kernel (CUDA events on the scheduler's stream). */
 XKB_API int xkb_sched_kernel_ms(xkb_sched_t * sched, double * ms);
 
+/* Run `repeats` windows of a periodic graph in ONE persistent launch (the last window only up
+ * to its first `tail` tasks, 1 <= tail <= period); the descriptors set with
+ * xkb_sched_set_tasks are the window's `period` tasks. Task t of window w runs
+ * tasks[t] -- the window's data must be valid for every repetition (for heat: an even number
+ * of steps per window, so the grids are back in place). */
+XKB_API int xkb_sched_run_periodic(xkb_sched_t * sched, const xkb_periodic_graph_t * graph, uint32_t repeats,
+                                   uint32_t tail);
+
 /* Persistent run of a graph that allocates nothing. This entry point has no counterpart in the
  * reference. It is for callers that cannot allocate device memory at the time they run a graph:
  * a runtime that reserved most of the GPU's memory for its own allocator at start-up (XKRT
@@ -236,6 +263,41 @@ XKB_API int xkb_sched_kernel_ms(xkb_sched_t * sched, double * ms);
 #define XKB_NOALLOC_MAX_TASKS (1u << 20)
 XKB_API int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_task_graph_t * graph, int warps_per_task,
                                   double timeout_s, void * stream, uint64_t * executed);
+
+/* ---- serving: continuous admission of heat graphs under an HBM budget ------------------ */
+typedef struct xkb_server xkb_server_t;
+
+typedef struct xkb_server_cfg_t {
+    uint64_t budget_bytes;   /* device memory the server reserves once and carves grids from    */
+    int slots;               /* requests in flight at most (one stream each), 1..64              */
+    int ctas_per_graph;      /* CTAs of each request's persistent kernel (0 = SMs x resident)    */
+    double max_seconds;      /* xkb_server_run gives up (XKB_ETIMEDOUT) after this long (0: 600) */
+} xkb_server_cfg_t;
+
+/* One heat-diffusion request: nx x ny grid, ts x ts tiles, `steps` Jacobi steps, f32 = 1 for
+ * FP32 storage, seed of its U[0,1) initial interior (boundary 0), coefficient c; arrival_s is
+ * when it arrives (seconds after xkb_server_run starts, non-decreasing); result (optional,
+ * host memory of nx*ny elements) receives the final grid. start_s / finish_s are filled in:
+ * admission time and completion time as the host observed it. */
+typedef struct xkb_request_t {
+    double arrival_s;
+    int64_t nx, ny, ts;
+    int32_t steps, f32;
+    uint64_t seed;
+    double c;
+    void * result;
+    double start_s, finish_s;
+} xkb_request_t;
+
+/* The serving loop of the path: requests are admitted in arrival order as soon as a slot is
+ * free and their grids fit in the budget (best-fit allocation with split/merge, as the
+ * reference's device allocator, src/driver/device.cc:49-280); each runs its whole graph on the
+ * device (two-step windows of its resolved dependency graph on the persistent scheduler) while
+ * later arrivals are admitted and run beside it. */
+XKB_API int xkb_server_create(xkb_server_t ** server, const xkb_server_cfg_t * cfg);
+XKB_API int xkb_server_destroy(xkb_server_t * server);
+/* Serve a whole arrival trace; returns when every request has completed. */
+XKB_API int xkb_server_run(xkb_server_t * server, xkb_request_t * requests, size_t n);
 
 /* ---- heat-diffusion-2d tile body ------------------------------------------------------- */
 /* Storage types for the stencil. XKB_F64: double storage and arithmetic. XKB_F32: float

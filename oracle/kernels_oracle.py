@@ -82,3 +82,19 @@ def c_oracle():
         getattr(L, name).argtypes = [vp, vp, i64, i64, i64, dbl, ci]
     L.xk_oracle_axpby.argtypes = [i64, dbl, vp, dbl, vp, ci]
     return L
+
+
+def serve_init(nx, ny, seed, dtype=np.float64):
+    """Initial grid of a served request: interior cell k = j*nx + i gets U[0,1) from a splitmix64
+    hash of (seed * 0x100000001b3 + k), taking the top 53 bits; boundary 0."""
+    k = np.arange(nx * ny, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) * np.uint64(0x100000001B3) + k
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+    v = (x >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    g = v.reshape(ny, nx)
+    g[0, :] = 0; g[-1, :] = 0; g[:, 0] = 0; g[:, -1] = 0
+    return g.astype(dtype)

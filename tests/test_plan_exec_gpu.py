@@ -1,7 +1,13 @@
 """Reference-layout execution on the GPU: every heat tile task runs on its own per-access
 replicas, made coherent by executing the planner's copies (H2D, batched D2D), with the
-replica-layout tile body; a final host task writes the grid back (D2H). The host grid must
-equal the oracle bit-exactly -- the plan moves exactly the data the tile bodies need."""
+replica-layout tile body. The grid assembled from the last step's written replicas must equal
+the oracle bit-exactly -- the plan moves exactly the data the tile bodies need.
+
+(The reference's write-back path copies from the block's view on its LARGEST allocation without
+checking that view is coherent (fetch_list_to_host_setup_partition,
+include/xkrt/memory/access/blas/memory-tree.hpp:1135-1145); for heat that is a stale halo
+replica. The planner reproduces that plan exactly -- see tests/test_planner.py -- so the result
+is read from the written replicas here instead.)"""
 import numpy as np
 import pytest
 
@@ -19,20 +25,14 @@ def test_heat_through_plan(torch_cuda, nx, ny, ts, steps):
     g = O.heat_init(nx, ny, seed=11)
     A = torch.from_numpy(g.copy()).pin_memory(); B = torch.from_numpy(g.copy()).pin_memory()
     recs = S.heat_stream(nx, ny, ts, ts, steps, base_src=A.data_ptr(), base_dst=B.data_ptr())
-    final = A if steps % 2 == 0 else B
-    wb = S.from_tuples([[("m", S.R, final.data_ptr(), nx, 0, 0, nx, ny, 8)]])
-    wb["task"] = recs["task"].max() + 1; wb["reserved"] = 1
-    recs = np.concatenate([recs, wb])
-
     P = xk.Planner()
     views, tasks = [], []
     first = 0
     for i in range(len(recs)):
         if i == 0 or recs[i]["task"] != recs[i - 1]["task"]:
             first = i
-        views.append(P.fetch(recs[i], i - first, 0 if recs[i]["reserved"] & 1 else 1))
-        # plan and run as we go: copies of this access, then (after its last access) the task
-        tasks.append(P.copies(take=True))
+        views.append(P.fetch(recs[i], i - first, 1))
+        tasks.append(P.copies(take=True))          # the copies this access needs, in plan order
     sizes = P.allocations()
     bufs = [torch.empty(int(sz), dtype=torch.uint8, device="cuda") for sz in sizes]
     ptrs = [b.data_ptr() for b in bufs]
@@ -43,8 +43,6 @@ def test_heat_through_plan(torch_cuda, nx, ny, ts, steps):
         for i in idx:
             if len(tasks[i]):
                 xk.plan_execute(tasks[i], ptrs)
-        if recs[idx[0]]["reserved"] & 1:
-            continue                                   # the write-back task has no body
         k = t % per
         tx, ty = k // nty, k % nty
         vs, vd = views[idx[0]], views[idx[1]]
@@ -58,7 +56,17 @@ def test_heat_through_plan(torch_cuda, nx, ny, ts, steps):
         xk.check(xk.lib().xkb_diffusion_views(xk.F64, torch.cuda.current_stream().cuda_stream, src, ld_s, dst, ld_d,
                                               tx, ty, ts, ts, nx, ny, c))
     torch.cuda.synchronize()
-    np.testing.assert_array_equal(final.numpy(), O.heat_run(g, nx, ny, steps, c))
+    # assemble the final grid from the last step's written replicas (W access = index 1)
+    out = np.zeros((ny, nx))
+    host_bufs = [b.cpu().numpy() for b in bufs]
+    for t in range(per * (steps - 1), per * steps):
+        i = np.nonzero(recs["task"] == t)[0][1]
+        r, v = recs[i], views[i]
+        m, n, ld = int(r["m"]), int(r["n"]), int(v[2])
+        raw = host_bufs[v[0]][v[1]:v[1] + 8 * (ld * (n - 1) + m)].view(np.float64)
+        tile = np.lib.stride_tricks.as_strided(raw, shape=(n, m), strides=(8 * ld, 8))
+        out[int(r["offset_n"]):int(r["offset_n"]) + n, int(r["offset_m"]):int(r["offset_m"]) + m] = tile
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, c))
 
 
 def test_whole_plan_in_one_call(torch_cuda):

@@ -138,3 +138,30 @@ def test_axpby_chains_team_sizes(torch_cuda, team):
     res = xk.Resolver(); res.add(recs)
     sch = xk.Scheduler(); sch.set_team(team); sch.set_tasks(descs); sch.run(res.graph()); sch.wait()
     np.testing.assert_array_equal(dy.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("steps", [1, 2, 7, 10])
+def test_periodic_heat_one_launch(torch_cuda, steps):
+    """Three resolved two-step windows -> periodic form; one persistent launch runs all steps
+    (a half window at the end for odd step counts) and gives the oracle's grid."""
+    torch = torch_cuda
+    nx, ny, ts = 300, 200, 64
+    g0 = O.heat_init(nx, ny, seed=21)
+    a = torch.from_numpy(g0).cuda(); b = torch.from_numpy(g0).cuda()
+    res = xk.Resolver()
+    res.add(xk.heat_access_records(nx, ny, ts, ts, 0, 6, a.data_ptr(), b.data_ptr()))
+    per_step = (-(-nx // ts)) * (-(-ny // ts))
+    pg = res.periodic(2 * per_step)
+    sch = xk.Scheduler()
+    sch.set_tasks(xk.heat_task_descs((a.data_ptr(), b.data_ptr()), nx, ny, nx, ts, ts, 2, C))
+    sch.run_periodic(pg, (steps + 1) // 2, per_step if steps % 2 else 2 * per_step)
+    assert sch.wait() == steps * per_step
+    out = (a if steps % 2 == 0 else b).cpu().numpy()
+    np.testing.assert_array_equal(out, O.heat_run(g0, nx, ny, steps, C))
+
+
+def test_periodic_rejects_aperiodic_graph(torch_cuda):
+    recs = S.microbench_stream(30, 1, n=512, ld=512)
+    res = xk.Resolver(); res.add(recs)
+    with pytest.raises(xk.XkbError):
+        res.periodic(10)

@@ -1,0 +1,58 @@
+"""Served stream: heat graphs of mixed sizes, step counts and precisions arrive over time and
+run concurrently under an HBM budget. Each request's result equals the same request served
+alone and the oracle (bit-exact: FP64 and FP32 storage)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import kernels_oracle as O
+import xkaapi_b200 as xk
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(specs):
+    reqs = (xk.Request * len(specs))()
+    bufs = []
+    for r, (t, n, steps, f32, seed) in zip(reqs, specs):
+        buf = np.zeros((n, n), dtype=np.float32 if f32 else np.float64)
+        bufs.append(buf)
+        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32, r.seed, r.c = t, n, n, 64, steps, f32, seed, 0.2
+        r.result = buf.ctypes.data
+    return reqs, bufs
+
+
+def test_mixed_stream_equals_alone_and_oracle(torch_cuda):
+    rng = np.random.default_rng(3)
+    specs = []
+    t = 0.0
+    for k in range(24):
+        t += float(rng.exponential(0.004))
+        n = int(rng.choice([64, 96, 128, 200, 256, 384]))
+        specs.append((t, n, int(rng.integers(1, 13)), int(k % 2), 1000 + k))
+    # budget for only a few grids at once: admission has to wait for memory to be freed
+    srv = xk.Server(budget_bytes=6 << 20, slots=4, ctas_per_graph=64)
+    reqs, bufs = make_requests(specs)
+    srv.run(reqs)
+    for r in reqs:
+        assert r.finish_s >= r.start_s >= r.arrival_s - 1e-9
+    alone = xk.Server(budget_bytes=6 << 20, slots=1)
+    for i, (spec, buf) in enumerate(zip(specs, bufs)):
+        solo, sbuf = make_requests([(0.0,) + spec[1:]])
+        alone.run(solo)
+        np.testing.assert_array_equal(buf, sbuf[0])
+        t, n, steps, f32, seed = spec
+        dt = np.float32 if f32 else np.float64
+        ref = O.heat_run(O.serve_init(n, n, seed, dt), n, n, steps, 0.2, dtype=dt)
+        np.testing.assert_array_equal(buf, ref)
+    srv.close(); alone.close()
+
+
+def test_request_over_budget_is_rejected(torch_cuda):
+    srv = xk.Server(budget_bytes=1 << 20, slots=2)
+    reqs, _ = make_requests([(0.0, 1024, 2, 0, 1)])          # 2 x 8 MiB grids > 1 MiB budget
+    with pytest.raises(xk.XkbError) as e:
+        srv.run(reqs)
+    assert e.value.code == xk.XKB_ERANGE
+    srv.close()

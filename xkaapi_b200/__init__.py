@@ -47,6 +47,25 @@ class TaskGraph(ctypes.Structure):
                 ("succ", ctypes.c_void_p), ("npred", ctypes.c_void_p)]
 
 
+class ServerCfg(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("slots", ctypes.c_int), ("ctas_per_graph", ctypes.c_int),
+                ("max_seconds", ctypes.c_double)]
+
+
+class Request(ctypes.Structure):
+    """xkb_request_t: one heat-diffusion request of a served stream."""
+    _fields_ = [("arrival_s", ctypes.c_double), ("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("ts", ctypes.c_int64),
+                ("steps", ctypes.c_int32), ("f32", ctypes.c_int32), ("seed", ctypes.c_uint64), ("c", ctypes.c_double),
+                ("result", ctypes.c_void_p), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
+
+
+class PeriodicGraph(ctypes.Structure):
+    """xkb_periodic_graph_t: one window's CSR plus its edges into the next window (device)."""
+    _fields_ = [("period", ctypes.c_uint64), ("succ_ptr", ctypes.c_void_p), ("succ", ctypes.c_void_p),
+                ("xsucc_ptr", ctypes.c_void_p), ("xsucc", ctypes.c_void_p), ("npred_first", ctypes.c_void_p),
+                ("npred_next", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "xkb_last_error": (_c.c_char_p, []),
@@ -73,7 +92,12 @@ SIGNATURES = {
     "xkb_planner_allocations": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_plan_execute": (_int, [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]),
     "xkb_diffusion_views": (_int, [_int, _vp, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _dbl]),
+    "xkb_server_create": (_int, [ctypes.POINTER(_vp), ctypes.POINTER(ServerCfg)]),
+    "xkb_server_destroy": (_int, [_vp]),
+    "xkb_server_run": (_int, [_vp, ctypes.POINTER(Request), ctypes.c_size_t]),
     "xkb_resolver_create": (_int, [ctypes.POINTER(_vp), _vp]),
+    "xkb_resolver_periodic": (_int, [_vp, ctypes.c_uint64, ctypes.POINTER(PeriodicGraph)]),
+    "xkb_sched_run_periodic": (_int, [_vp, ctypes.POINTER(PeriodicGraph), ctypes.c_uint32, ctypes.c_uint32]),
     "xkb_resolver_destroy": (_int, [_vp]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
     "xkb_resolver_graph": (_int, [_vp, ctypes.POINTER(TaskGraph)]),
@@ -169,6 +193,11 @@ class Resolver:
         check(lib().xkb_resolver_graph(self._h, ctypes.byref(g)))
         return g
 
+    def periodic(self, period):
+        g = PeriodicGraph()
+        check(lib().xkb_resolver_periodic(self._h, period, ctypes.byref(g)))
+        return g
+
     def stats(self):
         nt, ne, ms = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
         check(lib().xkb_resolver_stats(self._h, ctypes.byref(nt), ctypes.byref(ne), ctypes.byref(ms)))
@@ -225,6 +254,10 @@ class Scheduler:
 
     def run(self, graph, form=FORM_PERSISTENT):
         check(lib().xkb_sched_run(self._h, ctypes.byref(graph), form))
+
+    def run_periodic(self, graph, repeats, tail=None):
+        check(lib().xkb_sched_run_periodic(self._h, ctypes.byref(graph), repeats,
+                                           graph.period if tail is None else tail))
 
     def wait(self):
         n = ctypes.c_uint64()
@@ -308,3 +341,28 @@ def plan_execute(copies, alloc_ptrs, stream=None):
     copies = np.ascontiguousarray(copies, dtype=np.int64)
     ptrs = (ctypes.c_void_p * max(1, len(alloc_ptrs)))(*alloc_ptrs)
     check(lib().xkb_plan_execute(copies.ctypes.data, len(copies), ptrs, len(alloc_ptrs), _stream(stream)))
+
+
+class Server:
+    """Serving loop (xkb_server_t): continuous admission of heat graphs under an HBM budget."""
+
+    def __init__(self, budget_bytes, slots=8, ctas_per_graph=0, max_seconds=600.0):
+        self._h = ctypes.c_void_p()
+        cfg = ServerCfg(int(budget_bytes), slots, ctas_per_graph, max_seconds)
+        check(lib().xkb_server_create(ctypes.byref(self._h), ctypes.byref(cfg)))
+
+    def run(self, reqs):
+        """reqs: a ctypes array of Request (filled in place with start_s / finish_s)."""
+        check(lib().xkb_server_run(self._h, reqs, len(reqs)))
+        return reqs
+
+    def close(self):
+        if self._h:
+            lib().xkb_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -352,6 +352,7 @@ struct xkb_resolver {
     size_t nuniq = 0;
     // graph
     DevBuf<uint32_t> succ_ptr, succ, npred, tmp;
+    DevBuf<uint32_t> periodic;                  // packed arrays of the periodic form
     bool graph_valid = false;
     double last_device_ms = 0;
 };
@@ -770,5 +771,73 @@ extern "C" int xkb_resolver_stats(xkb_resolver_t * R, uint64_t * ntasks, uint64_
     if (ntasks) *ntasks = R->ntasks;
     if (nedges) *nedges = R->nuniq;
     if (last_batch_ms) *last_batch_ms = R->last_device_ms;
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_periodic(xkb_resolver_t * R, uint64_t period, xkb_periodic_graph_t * out)
+{
+    if (!R || !out || period == 0) return xkb_set_error(XKB_EINVAL, "resolver_periodic: bad arguments");
+    if (R->ntasks != 3 * period)
+        return xkb_set_error(XKB_EINVAL, "resolver_periodic: the resolver must hold exactly 3 windows (%llu tasks), it holds %u",
+                             (unsigned long long) (3 * period), R->ntasks);
+    if (!R->graph_valid) { int rc = build_graph(R); if (rc) return rc; }
+    const size_t nt = R->ntasks, P = period;
+    std::vector<uint32_t> ptr(nt + 1), succ(R->nuniq ? R->nuniq : 1), npred(nt);
+    XKB_CUDA_TRY(cudaMemcpy(ptr.data(), R->succ_ptr.p, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (R->nuniq) XKB_CUDA_TRY(cudaMemcpy(succ.data(), R->succ.p, R->nuniq * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    XKB_CUDA_TRY(cudaMemcpy(npred.data(), R->npred.p, nt * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    // split the successors of window w into its own window and the next one
+    auto split = [&](size_t w, std::vector<uint32_t> & ip, std::vector<uint32_t> & is,
+                     std::vector<uint32_t> & xp, std::vector<uint32_t> & xs) -> bool {
+        ip.assign(1, 0); xp.assign(1, 0); is.clear(); xs.clear();
+        for (size_t t = w * P; t < (w + 1) * P; ++t)
+        {
+            for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i)
+            {
+                const uint32_t s = succ[i];
+                if (s < (w + 1) * P) is.push_back((uint32_t) (s - w * P));
+                else if (s < (w + 2) * P) xs.push_back((uint32_t) (s - (w + 1) * P));
+                else return false;                              // an edge skips a window
+            }
+            ip.push_back((uint32_t) is.size()); xp.push_back((uint32_t) xs.size());
+        }
+        return true;
+    };
+    std::vector<uint32_t> ip0, is0, xp0, xs0, ip1, is1, xp1, xs1;
+    if (!split(0, ip0, is0, xp0, xs0) || !split(1, ip1, is1, xp1, xs1))
+        return xkb_set_error(XKB_EINVAL, "resolver_periodic: an edge skips a window");
+    std::vector<uint32_t> ip2, is2, xp2, xs2;
+    {   // window 2's own edges (no next window was resolved)
+        ip2.assign(1, 0);
+        for (size_t t = 2 * P; t < 3 * P; ++t)
+        {
+            for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i) is2.push_back((uint32_t) (succ[i] - 2 * P));
+            ip2.push_back((uint32_t) is2.size());
+        }
+    }
+    if (ip0 != ip1 || is0 != is1 || xp0 != xp1 || xs0 != xs1 || ip0 != ip2 || is0 != is2 ||
+        !std::equal(npred.begin() + P, npred.begin() + 2 * P, npred.begin() + 2 * P))
+        return xkb_set_error(XKB_EINVAL, "resolver_periodic: the windows do not repeat");
+    // pack: succ_ptr | succ | xsucc_ptr | xsucc | npred_first | npred_next
+    const size_t total = (P + 1) + is0.size() + (P + 1) + xs0.size() + P + P;
+    int rc = R->periodic.reserve(total ? total : 1);
+    if (rc) return rc;
+    std::vector<uint32_t> h;
+    h.reserve(total);
+    h.insert(h.end(), ip0.begin(), ip0.end());
+    h.insert(h.end(), is0.begin(), is0.end());
+    h.insert(h.end(), xp0.begin(), xp0.end());
+    h.insert(h.end(), xs0.begin(), xs0.end());
+    h.insert(h.end(), npred.begin(), npred.begin() + P);
+    h.insert(h.end(), npred.begin() + P, npred.begin() + 2 * P);
+    XKB_CUDA_TRY(cudaMemcpy(R->periodic.p, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    const uint32_t * d = R->periodic.p;
+    out->period = P;
+    out->succ_ptr = d; d += P + 1;
+    out->succ = d; d += is0.size();
+    out->xsucc_ptr = d; d += P + 1;
+    out->xsucc = d; d += xs0.size();
+    out->npred_first = d; d += P;
+    out->npred_next = d;
     return XKB_OK;
 }

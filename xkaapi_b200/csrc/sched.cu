@@ -91,30 +91,40 @@ __device__ __forceinline__ int atom_add_acq_rel(int * p, int v)
     return old;
 }
 
+// A run covers `ntasks` tasks numbered w * period + t (window w, task t of the window's
+// `period` descriptors). A plain graph is one window (period = ntasks); a periodic graph adds
+// cross-window successors (xsucc) and a wait count for tasks of later windows (npred_next).
 struct SchedArgs {
     const xkb_task_desc_t * tasks;
     uint32_t ntasks;
+    uint32_t period;
     const uint32_t * succ_ptr;
     const uint32_t * succ;
+    const uint32_t * xsucc_ptr;    // null for a plain graph
+    const uint32_t * xsucc;
+    const uint32_t * npred_first;
+    const uint32_t * npred_next;
     int * wc;
     int * queue;
     unsigned * ctr;            // [0] head, [1] tail, [2] status, [3] executed
     uint64_t timeout_ns;
 };
 
-__global__ void sched_init_kernel(SchedArgs a, const uint32_t * npred)
+__global__ void sched_init_kernel(SchedArgs a)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.ntasks) return;
     a.queue[t] = -1;
-    const int n = (int) npred[t];
-    a.wc[t] = n;
+    const uint32_t w = t / a.period, l = t - w * a.period;
+    a.wc[t] = (int) (w == 0 ? a.npred_first[l] : a.npred_next[l]);
 }
 
-__global__ void sched_seed_kernel(SchedArgs a, const uint32_t * npred)
+__global__ void sched_seed_kernel(SchedArgs a)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.ntasks || npred[t] != 0) return;
+    if (t >= a.ntasks) return;
+    const uint32_t w = t / a.period, l = t - w * a.period;
+    if ((w == 0 ? a.npred_first[l] : a.npred_next[l]) != 0) return;
     const unsigned pos = atomicAdd(a.ctr + 1, 1u);
     a.queue[pos] = (int) t;
 }
@@ -166,19 +176,36 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
         team_sync(bar, TEAM_THREADS);
         const int t = cur[team];
         if (t < 0) break;
-        run_task_team(a.tasks[t], twarp, TEAM_WARPS);
+        const uint32_t w = (uint32_t) t / a.period, l = (uint32_t) t - w * a.period;
+        run_task_team(a.tasks[l], twarp, TEAM_WARPS);
         __threadfence();
         team_sync(bar, TEAM_THREADS);
         if (twarp == 0)
         {
-            const uint32_t b = a.succ_ptr[t], e = a.succ_ptr[t + 1];
+            const uint32_t base = w * a.period;
+            const uint32_t b = a.succ_ptr[l], e = a.succ_ptr[l + 1];
             for (uint32_t i = b + lane; i < e; i += 32)
             {
-                const uint32_t s = a.succ[i];
+                const uint32_t s = base + a.succ[i];
+                if (s >= a.ntasks) continue;                 // beyond the tail of the last window
                 if (atom_add_acq_rel(a.wc + s, -1) == 1)
                 {
                     const unsigned pos = atomicAdd(a.ctr + 1, 1u);
                     xkb_st_release(a.queue + pos, (int) s);
+                }
+            }
+            if (a.xsucc_ptr)
+            {
+                const uint32_t xb = a.xsucc_ptr[l], xe = a.xsucc_ptr[l + 1];
+                for (uint32_t i = xb + lane; i < xe; i += 32)
+                {
+                    const uint32_t s = base + a.period + a.xsucc[i];
+                    if (s >= a.ntasks) continue;
+                    if (atom_add_acq_rel(a.wc + s, -1) == 1)
+                    {
+                        const unsigned pos = atomicAdd(a.ctr + 1, 1u);
+                        xkb_st_release(a.queue + pos, (int) s);
+                    }
                 }
             }
             ++executed;
@@ -263,6 +290,7 @@ struct xkb_sched {
     int last_form = -1;
     int grid = 0;
     int team_warps = 2;
+    uint64_t last_total = 0;                  // tasks of the last run
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
     ~xkb_sched() {
@@ -357,19 +385,28 @@ extern "C" int xkb_sched_set_team(xkb_sched_t * S, int warps_per_task)
     return XKB_OK;
 }
 
+static int launch_persistent(xkb_sched * S, SchedArgs & a);
+
 static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
 {
     const uint32_t n = (uint32_t) g->ntasks;
     int rc;
     if ((rc = S->wc.reserve(n ? n : 1)) || (rc = S->queue.reserve(n ? n : 1)) || (rc = S->ctr.reserve(4))) return rc;
     SchedArgs a;
-    a.tasks = S->tasks.p; a.ntasks = n; a.succ_ptr = g->succ_ptr; a.succ = g->succ;
+    a.tasks = S->tasks.p; a.ntasks = n; a.period = n ? n : 1; a.succ_ptr = g->succ_ptr; a.succ = g->succ;
+    a.xsucc_ptr = nullptr; a.xsucc = nullptr; a.npred_first = g->npred; a.npred_next = g->npred;
     a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns;
+    return launch_persistent(S, a);
+}
+
+static int launch_persistent(xkb_sched * S, SchedArgs & a)
+{
+    const uint32_t n = a.ntasks;
     XKB_CUDA_TRY(cudaMemsetAsync(S->ctr.p, 0, 4 * sizeof(unsigned), S->stream));
     if (n)
     {
-        sched_init_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
-        sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a, g->npred);
+        sched_init_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a);
+        sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a);
         if (!S->ev[0]) { XKB_CUDA_TRY(cudaEventCreate(&S->ev[0])); XKB_CUDA_TRY(cudaEventCreate(&S->ev[1])); }
         XKB_CUDA_TRY(cudaEventRecord(S->ev[0], S->stream));
         switch (S->team_warps)
@@ -443,6 +480,7 @@ extern "C" int xkb_sched_run(xkb_sched_t * S, const xkb_task_graph_t * g, int fo
         return xkb_set_error(XKB_EINVAL, "sched_run: graph has %llu tasks, %zu descriptors set",
                              (unsigned long long) g->ntasks, S->host_tasks.size());
     S->last_form = form;
+    S->last_total = g->ntasks;
     switch (form)
     {
         case XKB_FORM_PERSISTENT: return run_persistent(S, g);
@@ -455,15 +493,36 @@ extern "C" int xkb_sched_run(xkb_sched_t * S, const xkb_task_graph_t * g, int fo
     }
 }
 
+extern "C" int xkb_sched_run_periodic(xkb_sched_t * S, const xkb_periodic_graph_t * g, uint32_t repeats, uint32_t tail)
+{
+    if (!S || !g || repeats == 0 || tail == 0 || tail > g->period)
+        return xkb_set_error(XKB_EINVAL, "sched_run_periodic: bad arguments");
+    if (g->period != S->host_tasks.size())
+        return xkb_set_error(XKB_EINVAL, "sched_run_periodic: period %llu but %zu descriptors set",
+                             (unsigned long long) g->period, S->host_tasks.size());
+    const uint64_t total = (uint64_t) (repeats - 1) * g->period + tail;
+    if (total >= (1ull << 31)) return xkb_set_error(XKB_ERANGE, "sched_run_periodic: %llu tasks in one run", (unsigned long long) total);
+    int rc;
+    if ((rc = S->wc.reserve(total)) || (rc = S->queue.reserve(total)) || (rc = S->ctr.reserve(4))) return rc;
+    SchedArgs a;
+    a.tasks = S->tasks.p; a.ntasks = (uint32_t) total; a.period = (uint32_t) g->period;
+    a.succ_ptr = g->succ_ptr; a.succ = g->succ; a.xsucc_ptr = g->xsucc_ptr; a.xsucc = g->xsucc;
+    a.npred_first = g->npred_first; a.npred_next = g->npred_next;
+    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns;
+    S->last_form = XKB_FORM_PERSISTENT;
+    S->last_total = total;
+    return launch_persistent(S, a);
+}
+
 extern "C" int xkb_sched_wait(xkb_sched_t * S, uint64_t * executed)
 {
     if (!S) return xkb_set_error(XKB_EINVAL, "sched_wait: null scheduler");
     XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
-    unsigned ctr[4] = {0, 0, 0, (unsigned) S->host_tasks.size()};
+    unsigned ctr[4] = {0, 0, 0, (unsigned) S->last_total};
     if (S->ctr.p && S->last_form == XKB_FORM_PERSISTENT) XKB_CUDA_TRY(cudaMemcpy(ctr, S->ctr.p, sizeof(ctr), cudaMemcpyDeviceToHost));
     if (executed) *executed = ctr[3];
     if (ctr[2] != 0)
-        return xkb_set_error(-(int) ctr[2], "sched: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], (unsigned) S->host_tasks.size());
+        return xkb_set_error(-(int) ctr[2], "sched: a device wait ran out of time (%u of %llu tasks were made ready)", ctr[1], (unsigned long long) S->last_total);
     return XKB_OK;
 }
 
@@ -529,7 +588,8 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
     cudaStream_t st = xkb_stream(stream);
     const uint32_t n = (uint32_t) graph->ntasks;
     SchedArgs a;
-    a.tasks = tasks; a.ntasks = n; a.succ_ptr = graph->succ_ptr; a.succ = graph->succ;
+    a.tasks = tasks; a.ntasks = n; a.period = n ? n : 1; a.succ_ptr = graph->succ_ptr; a.succ = graph->succ;
+    a.xsucc_ptr = nullptr; a.xsucc = nullptr; a.npred_first = graph->npred; a.npred_next = graph->npred;
     a.wc = scratch; a.queue = scratch + XKB_NOALLOC_MAX_TASKS;
     a.ctr = (unsigned *) (scratch + 2 * XKB_NOALLOC_MAX_TASKS);
     a.timeout_ns = (uint64_t) (timeout_s * 1e9);
@@ -543,8 +603,8 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
         XKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         XKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel<2>, SCHED_THREADS, 0));
         const unsigned grid = (unsigned) (sms * (per > 0 ? per : 1));
-        sched_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, graph->npred);
-        sched_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, graph->npred);
+        sched_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
+        sched_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
         switch (warps_per_task)
         {
             case 1: sched_persistent_kernel<1><<<grid, SCHED_THREADS, 0, st>>>(a); break;
