@@ -172,6 +172,14 @@ XKB_API int xkb_planner_copies(xkb_planner_t * planner, xkb_copy_t * out, size_t
 /* Byte size of every device allocation made so far, in allocation order. */
 XKB_API int xkb_planner_allocations(xkb_planner_t * planner, uint64_t * sizes, size_t cap, size_t * n);
 
+/* Resident mode (the B200 layout): every host region registered with xkb_planner_add_region
+ * has ONE device mirror with the host layout (allocation ordinal = region index, byte offset =
+ * offset in the region). A fetch to the GPU copies (H2D) only the blocks of the access the
+ * mirror lacks; a fetch to the host copies back (D2H) only blocks the host lacks; a write makes
+ * the writer's copy the only coherent one. Blocks are the same canonical partition as above. */
+XKB_API int xkb_planner_create_resident(xkb_planner_t ** planner);
+XKB_API int xkb_planner_add_region(xkb_planner_t * planner, uint64_t host_base, uint64_t size, int32_t * region);
+
 /* Run planned copies in order on `stream`: H2D and D2H with cudaMemcpy2DAsync, the D2D copies
  * of each access as one gather kernel (one CTA per copy). alloc_ptrs[k] is the device
  * memory backing allocation ordinal k (at least xkb_planner_allocations' size). Host addresses

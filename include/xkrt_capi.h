@@ -1,0 +1,209 @@
+/* XKRT C API (task spawn / access / wait) implemented on libxkb200.
+ *
+ * The names, enum values, typedefs and the xkrt_access_t layout are those of the reference's C
+ * API (api/c/include/xkrt/xkrt.h:61-566 and the headers it includes: memory/access/mode.h,
+ * concurrency.h, scope.h, type.h, blas/matrix-storage.h, task/flag.h, task/format.h,
+ * driver/driver-type.h, consts.h), so a C program written against that API compiles against
+ * this header and links against libxkb200.so. Only the part of the API on the dataflow path is
+ * provided: runtime init/deinit, task formats, task spawn with segment and matrix accesses,
+ * task wait, task argument/access accessors, host memory allocation and registration.
+ *
+ * Execution model: spawned tasks are buffered; xkrt_task_wait resolves their dependencies on the
+ * GPU (xkb_resolver), makes the data each task touches coherent where it runs (resident
+ * planner: one device mirror per registered host region, H2D/D2H only for blocks the target
+ * lacks), runs the tasks -- every task on the device scheduler's persistent kernel when all are
+ * built-in device bodies, else one by one in spawn order (host bodies on the calling thread) --
+ * and leaves host memory coherent when it returns. Handle accesses and moldable tasks are not
+ * supported. Functions that return void in the reference record failures instead; read them
+ * with xkb_runtime_status().
+ */
+#ifndef XKRT_B200_CAPI_H
+#define XKRT_B200_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "xkrt_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void * xkrt_runtime_t;
+typedef void * xkrt_task_t;
+typedef void * xkrt_team_t;
+typedef void * xkrt_driver_t;
+typedef void * xkrt_device_t;
+
+typedef uint8_t  xkrt_device_global_id_t;
+typedef uint8_t  xkrt_device_driver_id_t;
+typedef uint16_t xkrt_task_wait_counter_type_t;
+typedef uint16_t xkrt_task_access_counter_type_t;
+typedef uint8_t  xkrt_task_flag_bitfield_t;
+typedef uint8_t  xkrt_task_format_id_t;
+
+#define HOST_DEVICE_GLOBAL_ID        ((xkrt_device_global_id_t) 0)
+#define XKRT_DEVICES_MAX             (16)
+#define UNSPECIFIED_DEVICE_GLOBAL_ID (XKRT_DEVICES_MAX)
+#define TASK_MAX_ACCESSES            (1024)
+#define UNSPECIFIED_TASK_ACCESS      ((xkrt_task_access_counter_type_t) TASK_MAX_ACCESSES)
+#define XKRT_TASK_FORMAT_NULL        0
+
+typedef enum xkrt_access_concurrency_t {
+    ACCESS_CONCURRENCY_SEQUENTIAL  = 0x1,
+    ACCESS_CONCURRENCY_COMMUTATIVE = 0x2,
+    ACCESS_CONCURRENCY_CONCURRENT  = 0x4
+} xkrt_access_concurrency_t;
+
+typedef enum xkrt_access_mode_t {
+    ACCESS_MODE_R  = 0x1,
+    ACCESS_MODE_W  = 0x2,
+    ACCESS_MODE_RW = 0x3,
+    ACCESS_MODE_V  = 0x4,
+    ACCESS_MODE_VW = 0x6,
+    ACCESS_MODE_VR = 0x5,
+    ACCESS_MODE_D  = 0x8
+} xkrt_access_mode_t;
+
+typedef enum xkrt_access_scope_t {
+    ACCESS_SCOPE_NONUNIFIED = 0,
+    ACCESS_SCOPE_UNIFIED    = 1
+} xkrt_access_scope_t;
+
+typedef enum xkrt_access_type_t {
+    ACCESS_TYPE_HANDLE      = 0,
+    ACCESS_TYPE_SEGMENT     = 1,
+    ACCESS_TYPE_BLAS_MATRIX = 2,
+    ACCESS_TYPE_NULL        = 3,
+    ACCESS_TYPE_MAX         = 4
+} xkrt_access_type_t;
+
+typedef enum xkrt_matrix_storage_t {
+    MATRIX_ROWMAJOR,
+    MATRIX_COLMAJOR
+} xkrt_matrix_storage_t;
+
+typedef enum xkrt_task_flags_t {
+    TASK_FLAG_ZERO       = 0,
+    TASK_FLAG_DEPENDENT  = 1 << 0,
+    TASK_FLAG_DETACHABLE = 1 << 1,
+    TASK_FLAG_DEVICE     = 1 << 2,
+    TASK_FLAG_DOMAIN     = 1 << 3,
+    TASK_FLAG_MOLDABLE   = 1 << 4,
+    TASK_FLAG_REQUEUE    = 1 << 7,
+    TASK_FLAG_MAX        = 1 << 8
+} xkrt_task_flags_t;
+
+typedef enum xkrt_task_format_target_t {
+    XKRT_TASK_FORMAT_TARGET_HOST = 0,
+    XKRT_TASK_FORMAT_TARGET_CUDA = 1,
+    XKRT_TASK_FORMAT_TARGET_ZE   = 2,
+    XKRT_TASK_FORMAT_TARGET_CL   = 3,
+    XKRT_TASK_FORMAT_TARGET_HIP  = 4,
+    XKRT_TASK_FORMAT_TARGET_SYCL = 5,
+    XKRT_TASK_FORMAT_TARGET_MAX  = 6
+} xkrt_task_format_target_t;
+
+typedef enum xkrt_driver_type_t {
+    XKRT_DRIVER_TYPE_HOST = 0,
+    XKRT_DRIVER_TYPE_CUDA = 1,
+    XKRT_DRIVER_TYPE_ZE   = 2,
+    XKRT_DRIVER_TYPE_CL   = 3,
+    XKRT_DRIVER_TYPE_HIP  = 4,
+    XKRT_DRIVER_TYPE_SYCL = 5,
+    XKRT_DRIVER_TYPE_MAX  = 6
+} xkrt_driver_type_t;
+
+/* format bodies are called as f(runtime, device, task) (the reference's task_execute) */
+typedef void (*xkrt_task_format_func_t)();
+typedef void (*xkrt_task_func_t)(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_task_t * task, void * user_data);
+
+typedef struct xkrt_access_t {
+    xkrt_access_concurrency_t concurrency;
+    xkrt_access_mode_t        mode;
+    xkrt_access_scope_t       scope;
+    xkrt_access_type_t        type;
+    union xkrt_region_t {
+        struct xkrt_handle_t { void * addr; } handle;
+        struct xkrt_segment_t { void * a; void * b; } segment;
+        struct xkrt_matrix_t {
+            xkrt_matrix_storage_t storage;
+            void * addr;
+            unsigned long ld;
+            unsigned long offset_m;
+            unsigned long offset_n;
+            unsigned long m;
+            unsigned long n;
+            unsigned long sizeof_type;
+        } matrix;
+    } region;
+} xkrt_access_t;
+
+/* runtime (api/c/include/xkrt/xkrt.h:105-108) */
+XKB_API int  xkrt_init(xkrt_runtime_t ** runtime);
+XKB_API int  xkrt_deinit(xkrt_runtime_t * runtime);
+XKB_API void xkrt_reset(xkrt_runtime_t * runtime);
+
+/* memory (xkrt.h:110-124): host allocations and registrations are the regions that get device
+ * mirrors; data a device task touches must lie in one of them */
+XKB_API int    xkrt_memory_register(xkrt_runtime_t * runtime, void * ptr, size_t size);
+XKB_API int    xkrt_memory_unregister(xkrt_runtime_t * runtime, void * ptr, size_t size);
+XKB_API void * xkrt_memory_host_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size);
+XKB_API void   xkrt_memory_host_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * ptr, size_t size);
+
+/* devices (xkrt.h:134-135): the host is device 0, the GPU device 1 */
+XKB_API unsigned int xkrt_get_ndevices(xkrt_runtime_t * runtime);
+
+/* tasking (xkrt.h:138-163) */
+XKB_API void xkrt_task_wait(xkrt_runtime_t * runtime);
+XKB_API void * xkrt_task_args(xkrt_task_t * task);
+XKB_API xkrt_access_t * xkrt_task_accesses(xkrt_task_t * task);
+XKB_API xkrt_access_t * xkrt_task_access(xkrt_task_t * task, xkrt_task_access_counter_type_t access_id);
+XKB_API void * xkrt_task_access_replica(xkrt_task_t * task, xkrt_task_access_counter_type_t access_id);
+
+/* spawn (xkrt.h:160-196) */
+XKB_API void xkrt_task_spawn_generic(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
+                                     const xkrt_task_flag_bitfield_t flags, const xkrt_task_format_id_t fmtid,
+                                     const void * args, const size_t args_size, const xkrt_access_t * accesses,
+                                     const xkrt_task_access_counter_type_t naccesses,
+                                     const xkrt_task_access_counter_type_t ocr_access,
+                                     const xkrt_task_wait_counter_type_t detachable_counter_initial);
+XKB_API void xkrt_task_spawn_with_format(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
+                                         const xkrt_task_format_id_t fmtid, const void * args, const size_t args_size);
+XKB_API void xkrt_task_spawn_with_format_with_accesses(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
+                                                       const xkrt_task_format_id_t fmtid, const void * args,
+                                                       const size_t args_size, const xkrt_access_t * accesses,
+                                                       const int naccesses);
+XKB_API void xkrt_task_spawn(xkrt_runtime_t * runtime, xkrt_task_func_t func, void * user_data);
+
+/* teams (xkrt.h:206-226): one host team */
+XKB_API xkrt_team_t * xkrt_team_driver_device_get(xkrt_runtime_t * runtime, xkrt_driver_type_t type,
+                                                  xkrt_device_driver_id_t device_driver_id);
+XKB_API void xkrt_team_task_spawn(xkrt_runtime_t * runtime, xkrt_team_t * team, xkrt_task_func_t func, void * user_data);
+XKB_API void xkrt_team_task_spawn_with_accesses(xkrt_runtime_t * runtime, xkrt_team_t * team, xkrt_task_func_t func,
+                                                void * user_data, const xkrt_access_t * accesses, const int naccesses);
+
+/* formats (xkrt.h:228-229) */
+XKB_API xkrt_task_format_id_t xkrt_task_format_put(xkrt_runtime_t * runtime, const char * label);
+XKB_API int xkrt_task_format_set(xkrt_runtime_t * runtime, xkrt_task_format_id_t fmtid, xkrt_task_format_target_t target,
+                                 xkrt_task_format_func_t func);
+
+/* ---- additions of this library (no counterpart in the reference API) --------------------- */
+/* A format whose device body is one of the library's built-in tile bodies (XKB_TASK_HEAT_F64,
+ * XKB_TASK_HEAT_F32, XKB_TASK_AXPBY): the task's args are an xkb_task_desc_t whose grid / vector
+ * pointers are HOST addresses inside registered regions; the runtime points them at the
+ * device mirrors. Batches made only of such tasks run on the persistent scheduler. */
+XKB_API xkrt_task_format_id_t xkb_task_format_builtin(xkrt_runtime_t * runtime, int kind);
+/* First failure recorded since the last call (XKB_OK if none); clears it. */
+XKB_API int xkb_runtime_status(xkrt_runtime_t * runtime);
+/* The CUDA stream CUDA-target format bodies launch on (cudaStream_t as void *). */
+XKB_API void * xkb_runtime_stream(xkrt_runtime_t * runtime);
+/* Counters of the last xkrt_task_wait: tasks run, unique edges, copies H2D / D2H, and whether the
+ * persistent scheduler ran the batch (1) or the tasks ran one by one (0). */
+XKB_API int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks, uint64_t * edges, uint64_t * h2d,
+                                  uint64_t * d2h, int * fused);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XKRT_B200_CAPI_H */

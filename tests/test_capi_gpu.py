@@ -1,0 +1,51 @@
+"""The XKRT C API over libxkb200, exercised by C programs compiled against include/xkrt_capi.h
+(gcc) and linked to the library: the reference's ordering tests, and the heat example --
+fused (device tasks only) and mixed with host export tasks -- checked against the oracle."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import kernels_oracle as O
+
+pytestmark = pytest.mark.gpu
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def build(name, tmp_path):
+    exe = str(tmp_path / name)
+    lib = os.path.join(REPO, "xkaapi_b200")
+    subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "capi", name + ".c"), "-o", exe, "-L", lib, "-lxkb200",
+                    "-Wl,-rpath," + lib], check=True)
+    return exe
+
+
+def test_ordering_programs(torch_cuda, tmp_path):
+    r = subprocess.run([build("order_capi", tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    assert out["tasks"] == 6 and out["edges"] >= 4
+
+
+@pytest.mark.parametrize("every", [0, 3])
+def test_heat_example(torch_cuda, tmp_path, every):
+    nx, ny, ts, steps = 200, 136, 64, 7
+    g = O.heat_init(nx, ny, seed=4)
+    g.tofile(tmp_path / "init.bin")
+    exe = build("heat_capi", tmp_path)
+    r = subprocess.run([exe, str(nx), str(ny), str(ts), str(steps), str(every), str(tmp_path / "init.bin"),
+                        str(tmp_path / "out.bin"), str(tmp_path / "sums.txt")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    stats = json.loads(r.stdout)
+    out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2))
+    assert stats["fused"] == (1 if every == 0 else 0)
+    assert stats["h2d"] > 0 and stats["d2h"] > 0
+    if every:
+        for line in open(tmp_path / "sums.txt"):
+            s, v = line.split()
+            # the export body sums in memory order, one add at a time: cumsum does the same
+            assert float(v) == np.cumsum(O.heat_run(g, nx, ny, int(s), 0.2).ravel())[-1]

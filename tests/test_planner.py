@@ -73,3 +73,29 @@ def test_wrapped_tile_view_is_contiguous():
     assert list(P.allocations()) == [128] and list(v) == [0, 0, 8]
     c = P.copies()
     assert len(c) == 2 and set(c[:, 2]) == {xk.COPY_H2D}          # one H2D per rect of the tile
+
+
+def test_resident_mode_moves_each_byte_once():
+    """Resident layout: heat on one mirror per grid. Step 0 copies grid A in once (every cell);
+    step 1 copies in only grid B's boundary ring, which no task writes; no later step copies
+    anything; a host read of the final grid copies back exactly the interior the tasks wrote."""
+    import streams as S
+    nx, ts, steps = 256, 64, 4
+    A, B = 1 << 30, 1 << 31
+    recs = S.heat_stream(nx, nx, ts, ts, steps, base_src=A, base_dst=B)
+    P = xk.Planner(resident=True)
+    ra, rb = P.add_region(A, nx * nx * 8), P.add_region(B, nx * nx * 8)
+    P.plan(recs, 1)
+    c = P.copies(take=True)
+    assert set(c[:, 2]) == {xk.COPY_H2D}
+    cells = c[:, 11] * c[:, 12]
+    assert int(cells[c[:, 8] == ra].sum()) == nx * nx               # every cell of A exactly once
+    assert int(cells[c[:, 8] == rb].sum()) == 4 * nx - 4            # B's boundary ring
+    assert c[c[:, 8] == rb, 0].min() >= (nx // ts) ** 2             # ... first needed at step 1
+    final = A if steps % 2 == 0 else B
+    P.fetch(S.from_tuples([[("m", S.R, final, nx, 0, 0, nx, nx, 8)]])[0], 0, 0)
+    c = P.copies(take=True)
+    assert set(c[:, 2]) == {xk.COPY_D2H}
+    assert int((c[:, 11] * c[:, 12]).sum()) == (nx - 2) ** 2       # the interior the tasks wrote
+    with pytest.raises(xk.XkbError):                                # outside every region
+        P.fetch(S.from_tuples([[("m", S.R, 1 << 20, nx, 0, 0, 8, 8, 8)]])[0], 0, 1)

@@ -86,6 +86,8 @@ SIGNATURES = {
     "xkb_sched_run_noalloc": (_int, [_vp, ctypes.POINTER(TaskGraph), _int, _dbl, _vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_planner_create": (_int, [ctypes.POINTER(_vp)]),
     "xkb_planner_destroy": (_int, [_vp]),
+    "xkb_planner_create_resident": (_int, [ctypes.POINTER(_vp)]),
+    "xkb_planner_add_region": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
     "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),
     "xkb_planner_plan": (_int, [_vp, _vp, ctypes.c_size_t, _int, _vp]),
     "xkb_planner_copies": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _int]),
@@ -289,9 +291,17 @@ class Planner:
     an (n, 14) int64 array: task, access, kind, src_dev, src_alloc, src_off, src_ld, dst_dev,
     dst_alloc, dst_off, dst_ld, m, n, sizeof."""
 
-    def __init__(self):
+    def __init__(self, resident=False):
         self._h = ctypes.c_void_p()
-        check(lib().xkb_planner_create(ctypes.byref(self._h)))
+        if resident:
+            check(lib().xkb_planner_create_resident(ctypes.byref(self._h)))
+        else:
+            check(lib().xkb_planner_create(ctypes.byref(self._h)))
+
+    def add_region(self, base, size):
+        r = ctypes.c_int32()
+        check(lib().xkb_planner_add_region(self._h, base, size, ctypes.byref(r)))
+        return r.value
 
     def plan(self, recs, device=1):
         import numpy as np

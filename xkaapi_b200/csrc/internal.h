@@ -1,0 +1,8 @@
+// Library-internal entry points shared between translation units (not exported).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/xkrt_b200.h"
+
+// Launch one task descriptor as its own kernel (the plain per-task form) on `stream`.
+int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream);

@@ -142,6 +142,9 @@ struct xkb_planner {
     std::vector<uint64_t> allocs;
     std::vector<xkb_copy_t> copies;
     std::vector<Partite> scratch;
+    // resident mode: one device mirror per registered host region (base -> (size, index))
+    bool resident = false;
+    std::map<uint64_t, std::pair<uint64_t, int32_t>> regions;
 };
 
 // The access's rects in its (ld, sizeof) frame (access.hpp:204-287): one rect, or two when the
@@ -187,8 +190,60 @@ static void push_copy(xkb_planner * P, int64_t task, int64_t access, int kind, c
     P->copies.push_back(c);
 }
 
+// Resident mode: every registered host region has one device mirror with the host layout
+// (byte at host address h lives at mirror + (h - region base)). A block is coherent on the host
+// when no device bit is set or the host bit is; on the GPU when the GPU bit is. Reads copy the
+// blocks the target lacks (H2D / D2H, whole blocks, pitched like the host matrix); writes leave
+// the target as the only coherent copy.
+static int resident_fetch(xkb_planner * P, const xkb_access_rec_t & a, int64_t access_index, int device, xkb_view_t * view)
+{
+    uint64_t ld, s; Rect rr[2]; int64_t origin[2][2]; int nr = 0;
+    int rc = frame_rects(a, ld, s, rr, origin, nr);
+    if (rc) return rc;
+    const bool seg = ld == ~0ull;
+    const uint64_t stride = seg ? 0 : ld * s;
+    const uint64_t begin = seg ? a.addr : a.addr + (a.offset_n * a.ld + a.offset_m) * a.sizeof_type;
+    auto rit = P->regions.upper_bound(begin);
+    if (rit == P->regions.begin()) return xkb_set_error(XKB_EINVAL, "planner: access at %#llx is in no registered region", (unsigned long long) begin);
+    --rit;
+    const uint64_t rbase = rit->first, rsize = rit->second.first;
+    const int32_t region = rit->second.second;
+    const uint64_t end = seg ? a.ld : begin + ((a.n - 1) * a.ld + a.m) * a.sizeof_type;
+    if (begin < rbase || end > rbase + rsize) return xkb_set_error(XKB_EINVAL, "planner: access crosses the end of its region");
+    if (view) { view->alloc = region; view->off = (int64_t) (begin - rbase); view->ld = seg ? (int64_t) (a.ld - a.addr) : (int64_t) a.ld; }
+    std::unique_ptr<Frame> & fp = P->frames[{ld, s}];
+    if (!fp) { fp.reset(new (std::nothrow) Frame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); fp->ld = ld; fp->s = s; }
+    for (int k = 0; k < nr; ++k) insert(*fp, rr[k]);
+    P->scratch.clear();
+    for (int k = 0; k < nr; ++k) partites(*fp, rr[k], P->scratch);
+    const uint8_t me = device == 0 ? DEV_HOST : DEV_GPU;
+    for (const Partite & p : P->scratch)
+    {
+        State & st = *p.st;
+        const bool host_ok = st.dev == 0 || (st.dev & DEV_HOST), gpu_ok = st.dev & DEV_GPU;
+        if (a.mode & XKB_ACCESS_MODE_R && !(a.mode & XKB_ACCESS_MODE_V) && !(me == DEV_HOST ? host_ok : gpu_ok))
+        {
+            const uint64_t h = p.x0 + p.y0 * stride;
+            xkb_copy_t c;
+            c.task = a.task; c.access = access_index; c.kind = me == DEV_GPU ? XKB_COPY_H2D : XKB_COPY_D2H;
+            c.src_dev = me == DEV_GPU ? 0 : 1; c.dst_dev = me == DEV_GPU ? 1 : 0;
+            c.src_alloc = me == DEV_GPU ? -1 : region; c.dst_alloc = me == DEV_GPU ? region : -1;
+            c.src_off = me == DEV_GPU ? (int64_t) h : (int64_t) (h - rbase);
+            c.dst_off = me == DEV_GPU ? (int64_t) (h - rbase) : (int64_t) h;
+            c.src_ld = c.dst_ld = seg ? 0 : (int64_t) ld;
+            if (seg) { c.m = (int64_t) (p.x1 - p.x0); c.n = 1; c.sizeof_type = 1; }
+            else { c.m = (int64_t) ((p.x1 - p.x0) / s); c.n = (int64_t) (p.y1 - p.y0); c.sizeof_type = (int64_t) s; }
+            P->copies.push_back(c);
+            st.dev |= (st.dev == 0 ? DEV_HOST : 0) | me;
+        }
+        if (a.mode & XKB_ACCESS_MODE_W && !(a.mode & XKB_ACCESS_MODE_V)) st.dev = me;
+    }
+    return XKB_OK;
+}
+
 static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access_index, int device, xkb_view_t * view)
 {
+    if (P->resident) return resident_fetch(P, a, access_index, device, view);
     uint64_t ld, s; Rect rr[2]; int64_t origin[2][2]; int nr = 0;
     int rc = frame_rects(a, ld, s, rr, origin, nr);
     if (rc) return rc;
@@ -357,5 +412,25 @@ extern "C" int xkb_planner_allocations(xkb_planner_t * P, uint64_t * sizes, size
     if (!sizes) return XKB_OK;
     if (cap < P->allocs.size()) return xkb_set_error(XKB_ERANGE, "planner_allocations: %zu entries needed", P->allocs.size());
     if (!P->allocs.empty()) memcpy(sizes, P->allocs.data(), P->allocs.size() * sizeof(uint64_t));
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_create_resident(xkb_planner_t ** out)
+{
+    int rc = xkb_planner_create(out);
+    if (rc == XKB_OK) (*out)->resident = true;
+    return rc;
+}
+
+extern "C" int xkb_planner_add_region(xkb_planner_t * P, uint64_t host_base, uint64_t size, int32_t * region)
+{
+    if (!P || !P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_add_region: needs a resident planner and a size");
+    auto it = P->regions.upper_bound(host_base);
+    if (it != P->regions.end() && it->first < host_base + size) return xkb_set_error(XKB_EINVAL, "planner_add_region: overlaps a region");
+    if (it != P->regions.begin()) { --it; if (it->first + it->second.first > host_base) return xkb_set_error(XKB_EINVAL, "planner_add_region: overlaps a region"); }
+    const int32_t id = (int32_t) P->allocs.size();
+    P->allocs.push_back(size);
+    P->regions[host_base] = {size, id};
+    if (region) *region = id;
     return XKB_OK;
 }

@@ -19,6 +19,7 @@
 //    dependency), instantiated once and replayed.
 #include "common.cuh"
 #include "heat.cuh"
+#include "internal.h"
 
 #include <new>
 #include <vector>
@@ -620,5 +621,14 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
     if (executed) *executed = ctr[3];
     if (ctr[2] != 0)
         return xkb_set_error(-(int) ctr[2], "sched_run_noalloc: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], n);
+    return XKB_OK;
+}
+
+int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream)
+{
+    if (d->kind == XKB_TASK_NOOP) return XKB_OK;
+    const int slabs = task_slabs(*d);
+    task_kernel<<<slabs, SCHED_THREADS, 0, stream>>>(*d, slabs);
+    XKB_CUDA_TRY(cudaGetLastError());
     return XKB_OK;
 }
