@@ -457,11 +457,13 @@ static int wait_batch(xkb_runtime * R)
             const bool dev = is_device(R, T);
             for (; k < recs.size() && rec_of[k].first == t; ++k)
             {
-                xkb_view_t v;
-                if ((rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) rec_of[k].second, dev ? 1 : 0, &v))) break;
                 const uint64_t begin = recs[k].type == XKB_ACCESS_TYPE_SEGMENT ? recs[k].addr
                                      : recs[k].addr + (recs[k].offset_n * recs[k].ld + recs[k].offset_m) * recs[k].sizeof_type;
                 T.replica[rec_of[k].second] = dev ? mirror_of(R, begin) : (void *) begin;
+                // a host task on memory no region covers: that memory never has a device copy
+                if (!dev && !mirror_of(R, begin)) continue;
+                xkb_view_t v;
+                if ((rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) rec_of[k].second, dev ? 1 : 0, &v))) break;
             }
             if (rc) break;
             if ((rc = run_copies(R))) break;
