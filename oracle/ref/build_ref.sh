@@ -12,7 +12,8 @@
 #   P2 blas/dependency-tree.hpp, blas/memory-tree.hpp: constructors spelled `Node<K>(` -> `Node(`.
 #   P3 task/task.hpp: `void (*F)(Args..., task_t *)` is non-deducible in g++ -> generic `FN F`.
 #   P4 thread/thread.h: non-template `commit` overloads for the two callback shapes used.
-#   flags: -std=c++20 -D_Static_assert=static_assert -include list -DNDEBUG
+#   flags: -std=c++20 (c++23 for the runtime sources, whose <stdatomic.h> needs it in g++ 13)
+#          -D_Static_assert=static_assert -include list -DNDEBUG
 #   generated: support.h (CMake defaults, every vendor driver off), version.h, an hwloc shim.
 #
 # Usage: oracle/ref/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
@@ -113,7 +114,7 @@ typedef hwloc_bitmap_t hwloc_cpuset_t;
 typedef const struct hwloc_bitmap_s * hwloc_const_cpuset_t;
 typedef enum { HWLOC_OBJ_MACHINE, HWLOC_OBJ_PACKAGE, HWLOC_OBJ_CORE, HWLOC_OBJ_PU, HWLOC_OBJ_L1CACHE,
                HWLOC_OBJ_L2CACHE, HWLOC_OBJ_L3CACHE, HWLOC_OBJ_NUMANODE } hwloc_obj_type_t;
-typedef struct hwloc_obj { hwloc_cpuset_t cpuset; unsigned logical_index; unsigned os_index; } * hwloc_obj_t;
+typedef struct hwloc_obj { hwloc_cpuset_t cpuset; unsigned logical_index; unsigned os_index; char * name; } * hwloc_obj_t;
 static inline int hwloc_topology_init(hwloc_topology_t * t) { *t = 0; return 0; }
 static inline int hwloc_topology_load(hwloc_topology_t) { return 0; }
 static inline void hwloc_topology_destroy(hwloc_topology_t) {}
@@ -135,7 +136,7 @@ static inline int hwloc_cpuset_to_glibc_sched_affinity(hwloc_topology_t, hwloc_c
 #endif
 H
 
-CXX="${CXX:-g++}"
+CXX="${XK_ORACLE_CXX:-g++}"   # the g++ on PATH (g++ 13.3); a CXX from the environment may lack C++23 <stdatomic.h>
 CXXFLAGS="-std=c++20 -O2 -DNDEBUG -D_Static_assert=static_assert -include list -w -I$OUT/include -I$OUT/shim -I$REF/api/c/include"
 
 # ---- dependency oracle: reference trees driven by src/task/task.cc --------------------------
@@ -147,3 +148,21 @@ echo "built $OUT/ref_deps"
 "$CXX" $CXXFLAGS -include array -o "$OUT/ref_plan" \
     "$HERE/ref_plan.cc" "$HERE/seams.cc" "$REF/src/task/task.cc" "$REF/src/logger/logger.cc" -lpthread
 echo "built $OUT/ref_plan"
+
+# ---- host-only runtime (CPU baseline): the reference's runtime sources + its host driver ------
+OBJ="$OUT/obj"
+mkdir -p "$OBJ"
+RT_SRCS="src/memory/access.cc src/conf/conf.cc src/debug/cairo.cc src/distribution/distribution.cc src/driver.cc
+ src/driver/device.cc src/driver/driver.cc src/driver/queue.cc src/driver/driver_host.cc src/file/readwrite.cc
+ src/logger/logger.cc src/logger/metric.cc src/memory.cc src/memory/coherent.cc src/memory/copy.cc
+ src/memory/distribute.cc src/memory/invalidate.cc src/memory/register.cc src/power.cc src/runtime.cc src/sched.cc
+ src/stats/stats.cc src/task.cc src/task/format.cc src/task/task.cc src/thread/deque.cc src/thread/thread.cc"
+OBJS=""
+for s in $RT_SRCS; do
+    o="$OBJ/$(echo "$s" | tr '/' '_').o"
+    "$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -c "$REF/$s" -o "$o" &
+    OBJS="$OBJS $o"
+done
+wait
+"$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_heat" "$HERE/ref_heat.cc" $OBJS -lpthread -ldl
+echo "built $OUT/ref_heat"

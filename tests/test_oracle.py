@@ -62,3 +62,20 @@ def test_c_oracle_equals_numpy_oracle():
     x = np.linspace(-1, 1, 1001); y = np.linspace(3, -2, 1001); ref = O.axpby(0.3, x, -1.7, y)
     L.xk_oracle_axpby(1001, 0.3, x.ctypes.data, -1.7, y.ctypes.data, 2)
     np.testing.assert_array_equal(y, ref)
+
+
+def test_reference_runtime_heat_equals_oracle(tmp_path):
+    """The reference's own host-only runtime (oracle/_ref/ref_heat, built from its sources)
+    running the heat example's task graph produces the oracle's grid bit for bit."""
+    import kernels_oracle as O
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_heat")
+    if not os.path.exists(exe):
+        pytest.skip("reference runtime not built (oracle/ref/build_ref.sh)")
+    nx, ny, ts, steps = 300, 200, 64, 9
+    g = O.heat_init(nx, ny, seed=3)
+    g.tofile(tmp_path / "init.bin")
+    env = dict(os.environ, DRIVERS="host,4", XKRT_DRIVERS="host,4")
+    subprocess.run([exe, str(nx), str(ny), str(ts), str(steps), str(tmp_path / "init.bin"), str(tmp_path / "out.bin")],
+                   env=env, check=True, capture_output=True, cwd=str(tmp_path), timeout=120)
+    out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2))
