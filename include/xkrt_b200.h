@@ -239,6 +239,8 @@ XKB_API int xkb_sched_set_grid(xkb_sched_t * sched, int ctas);
  * of 8 warps runs 8 / warps_per_task tasks at a time, each team taking and releasing tasks on
  * its own. */
 XKB_API int xkb_sched_set_team(xkb_sched_t * sched, int warps_per_task);
+/* Distance, in columns, of the L2 bulk prefetch ahead of a heat tile's sweep (0 = off; default 8). */
+XKB_API int xkb_sched_set_prefetch(xkb_sched_t * sched, int columns);
 /* Enqueue one execution of the whole graph on the scheduler's stream (asynchronous). */
 XKB_API int xkb_sched_run(xkb_sched_t * sched, const xkb_task_graph_t * graph, int form);
 /* Wait for the stream; *executed = tasks the persistent kernel ran. Returns XKB_ETIMEDOUT if

@@ -80,6 +80,7 @@ SIGNATURES = {
     "xkb_sched_set_timeout": (_int, [_vp, _dbl]),
     "xkb_sched_set_grid": (_int, [_vp, _int]),
     "xkb_sched_set_team": (_int, [_vp, _int]),
+    "xkb_sched_set_prefetch": (_int, [_vp, _int]),
     "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
     "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_sched_kernel_ms": (_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
@@ -253,6 +254,9 @@ class Scheduler:
 
     def set_team(self, warps_per_task):
         check(lib().xkb_sched_set_team(self._h, warps_per_task))
+
+    def set_prefetch(self, columns):
+        check(lib().xkb_sched_set_prefetch(self._h, columns))
 
     def run(self, graph, form=FORM_PERSISTENT):
         check(lib().xkb_sched_run(self._h, ctypes.byref(graph), form))

@@ -57,7 +57,7 @@ __device__ __forceinline__ void axpby_team(int64_t lo, int64_t hi, double a, con
 constexpr int SCHED_THREADS = 256;
 
 // Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
-__device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps)
+__device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps, int pfd)
 {
     switch (d.kind)
     {
@@ -65,14 +65,14 @@ __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int war
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
             heat_tile_team<double, 2, 4, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
-                                               h.x0, h.x1, h.y0, h.y1, h.c, vok, 8, warp, nwarps);
+                                               h.x0, h.x1, h.y0, h.y1, h.c, vok, pfd, warp, nwarps);
             break;
         }
         case XKB_TASK_HEAT_F32: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 4 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
             heat_tile_team<float, 4, 4, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
-                                              h.x0, h.x1, h.y0, h.y1, h.c, vok, 8, warp, nwarps);
+                                              h.x0, h.x1, h.y0, h.y1, h.c, vok, pfd, warp, nwarps);
             break;
         }
         case XKB_TASK_AXPBY: {
@@ -109,6 +109,7 @@ struct SchedArgs {
     int * queue;
     unsigned * ctr;            // [0] head, [1] tail, [2] status, [3] executed
     uint64_t timeout_ns;
+    int pfd;                   // L2 prefetch distance of the tile bodies, in columns
 };
 
 __global__ void sched_init_kernel(SchedArgs a)
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
         const int t = cur[team];
         if (t < 0) break;
         const uint32_t w = (uint32_t) t / a.period, l = (uint32_t) t - w * a.period;
-        run_task_team(a.tasks[l], twarp, TEAM_WARPS);
+        run_task_team(a.tasks[l], twarp, TEAM_WARPS, a.pfd);
         __threadfence();
         team_sync(bar, TEAM_THREADS);
         if (twarp == 0)
@@ -291,6 +292,7 @@ struct xkb_sched {
     int last_form = -1;
     int grid = 0;
     int team_warps = 2;
+    int pfd = 8;
     uint64_t last_total = 0;                  // tasks of the last run
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
@@ -378,6 +380,13 @@ extern "C" int xkb_sched_set_grid(xkb_sched_t * S, int ctas)
     return XKB_OK;
 }
 
+extern "C" int xkb_sched_set_prefetch(xkb_sched_t * S, int columns)
+{
+    if (!S || columns < 0 || columns > 256) return xkb_set_error(XKB_EINVAL, "sched_set_prefetch: 0..256 columns");
+    S->pfd = columns;
+    return XKB_OK;
+}
+
 extern "C" int xkb_sched_set_team(xkb_sched_t * S, int warps_per_task)
 {
     if (!S || (warps_per_task != 1 && warps_per_task != 2 && warps_per_task != 4 && warps_per_task != 8))
@@ -396,7 +405,7 @@ static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
     SchedArgs a;
     a.tasks = S->tasks.p; a.ntasks = n; a.period = n ? n : 1; a.succ_ptr = g->succ_ptr; a.succ = g->succ;
     a.xsucc_ptr = nullptr; a.xsucc = nullptr; a.npred_first = g->npred; a.npred_next = g->npred;
-    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns;
+    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns; a.pfd = S->pfd;
     return launch_persistent(S, a);
 }
 
@@ -509,7 +518,7 @@ extern "C" int xkb_sched_run_periodic(xkb_sched_t * S, const xkb_periodic_graph_
     a.tasks = S->tasks.p; a.ntasks = (uint32_t) total; a.period = (uint32_t) g->period;
     a.succ_ptr = g->succ_ptr; a.succ = g->succ; a.xsucc_ptr = g->xsucc_ptr; a.xsucc = g->xsucc;
     a.npred_first = g->npred_first; a.npred_next = g->npred_next;
-    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns;
+    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns; a.pfd = S->pfd;
     S->last_form = XKB_FORM_PERSISTENT;
     S->last_total = total;
     return launch_persistent(S, a);
@@ -594,6 +603,7 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
     a.wc = scratch; a.queue = scratch + XKB_NOALLOC_MAX_TASKS;
     a.ctr = (unsigned *) (scratch + 2 * XKB_NOALLOC_MAX_TASKS);
     a.timeout_ns = (uint64_t) (timeout_s * 1e9);
+    a.pfd = 8;
     // the array keeps the previous call's contents: the counters are zeroed here, and the init
     // kernel rewrites every wait counter and queue slot this run uses
     XKB_CUDA_TRY(cudaMemsetAsync(a.ctr, 0, 4 * sizeof(unsigned), st));
