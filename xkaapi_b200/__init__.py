@@ -107,6 +107,8 @@ SIGNATURES = {
     "xkb_resolver_edges": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_resolver_stats": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                   ctypes.POINTER(ctypes.c_double)]),
+    "xkb_resolver_timing": (_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]),
 }
 
 
@@ -205,6 +207,12 @@ class Resolver:
         nt, ne, ms = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
         check(lib().xkb_resolver_stats(self._h, ctypes.byref(nt), ctypes.byref(ne), ctypes.byref(ms)))
         return nt.value, ne.value, ms.value
+
+    def timing(self):
+        """(ops_ms, compress_ms, batch_ms) of the last batch."""
+        o, c, b = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().xkb_resolver_timing(self._h, ctypes.byref(o), ctypes.byref(c), ctypes.byref(b)))
+        return o.value, c.value, b.value
 
     def close(self):
         if self._h:

@@ -28,6 +28,7 @@
 #include "scan.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -62,9 +63,11 @@ struct ResolveArgs {
     int * max_readers;        // largest reader count seen (overflow when > rcap)
 };
 
-template <int RX, int RY>
+// BINNED: the CTA's ops come from its region's list (op indices in op order, built by the
+// binning kernels below) instead of a scan of every op of the batch.
+template <int RX, int RY, bool BINNED>
 __global__ void __launch_bounds__(RX * RY)
-resolve_region_kernel(ResolveArgs a)
+resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const int * __restrict__ rlist)
 {
     constexpr int NT = RX * RY;
     constexpr int NW = NT / 32;
@@ -92,8 +95,18 @@ resolve_region_kernel(ResolveArgs a)
         maxnr = nr;
     }
 
-    for (int base = 0; base < a.nops; base += CHUNK)
+    const int lo = BINNED ? (int) roff[blockIdx.x] : 0, hi = BINNED ? (int) roff[blockIdx.x + 1] : a.nops;
+    for (int base = lo; base < hi; base += CHUNK)
     {
+        if constexpr (BINNED)
+        {
+            // ---- gather the next CHUNK ops of this region's list (already in op order) -----
+            for (int j = tid; j < CHUNK && base + j < hi; j += NT) list[j] = a.ops[rlist[base + j]];
+            if (tid == 0) nlist_s = min(CHUNK, hi - base);
+            __syncthreads();
+        }
+        else
+        {
         // ---- compact the ops of this chunk that overlap the region, in op order ----------
         if (tid == 0) nlist_s = 0;
         __syncthreads();
@@ -116,6 +129,7 @@ resolve_region_kernel(ResolveArgs a)
             __syncthreads();
             if (tid == 0) { int t = 0; for (int w = 0; w < NW; ++w) t += wcount[w]; nlist_s += t; }
             __syncthreads();
+        }
         }
         const int nlist = nlist_s;
 
@@ -167,6 +181,68 @@ resolve_region_kernel(ResolveArgs a)
         for (int k = 0; k < nr && k < a.rcap; ++k) st[2 + k] = rd[k * NT + tid];
     }
     if (maxnr > a.rcap) atomicMax(a.max_readers, maxnr);
+}
+
+// ---- binning of ops to regions ----------------------------------------------------------------
+// The regions of an op: the RX x RY cell blocks its cell rect overlaps.
+__global__ void bin_count_kernel(const DOp * __restrict__ ops, int nops, int RX, int RY, int nrx, unsigned * rcount)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nops) return;
+    const DOp o = ops[i];
+    if (o.cx0 >= o.cx1 || o.cy0 >= o.cy1) return;
+    for (int ry = o.cy0 / RY; ry <= (o.cy1 - 1) / RY; ++ry)
+        for (int rx = o.cx0 / RX; rx <= (o.cx1 - 1) / RX; ++rx)
+            atomicAdd(rcount + ry * nrx + rx, 1u);
+}
+
+__global__ void bin_fill_kernel(const DOp * __restrict__ ops, int nops, int RX, int RY, int nrx, const unsigned * __restrict__ roff,
+                                unsigned * cursor, int * list)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nops) return;
+    const DOp o = ops[i];
+    if (o.cx0 >= o.cx1 || o.cy0 >= o.cy1) return;
+    for (int ry = o.cy0 / RY; ry <= (o.cy1 - 1) / RY; ++ry)
+        for (int rx = o.cx0 / RX; rx <= (o.cx1 - 1) / RX; ++rx)
+        {
+            const int r = ry * nrx + rx;
+            list[roff[r] + atomicAdd(cursor + r, 1u)] = i;
+        }
+}
+
+constexpr int BIN_SORT_THREADS = 1024;
+constexpr int BIN_SORT_CAP = 16384;          // ops of one region sortable in one CTA (64 KB of shared memory)
+
+// Put each region's list back in op order (the fill appends in arbitrary order): bitonic sort of
+// the region's segment in shared memory. A region holding more than BIN_SORT_CAP ops sets
+// *too_long and the batch falls back to the unbinned scan.
+__global__ void __launch_bounds__(BIN_SORT_THREADS) bin_sort_kernel(const unsigned * __restrict__ roff, int * list, int * too_long)
+{
+    extern __shared__ int keys[];
+    const unsigned b = roff[blockIdx.x], e = roff[blockIdx.x + 1];
+    const int n = (int) (e - b);
+    if (n <= 1) return;
+    if (n > BIN_SORT_CAP) { if (threadIdx.x == 0) atomicExch(too_long, 1); return; }
+    int p2 = 1;
+    while (p2 < n) p2 <<= 1;
+    for (int i = threadIdx.x; i < p2; i += blockDim.x) keys[i] = i < n ? list[b + i] : 0x7fffffff;
+    __syncthreads();
+    for (int k = 2; k <= p2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            for (int i = threadIdx.x; i < p2; i += blockDim.x)
+            {
+                const int l = i ^ j;
+                if (l > i)
+                {
+                    const int x = keys[i], y = keys[l];
+                    if (((i & k) == 0) == (x > y)) { keys[i] = y; keys[l] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) list[b + i] = keys[i];
 }
 
 // New compression refines the old one: every new cell lies inside exactly one old cell (or
@@ -291,35 +367,66 @@ struct DevBuf {
     }
 };
 
-// Sorted unique values with a fast path for heavily repeated inputs.
-static void unique_sorted(std::vector<uint64_t> & v)
+// ---- coordinate compression on the device ----------------------------------------------------
+// Every op's rect boundaries go into two open-addressing hash sets (x and y); each first insert
+// appends the key to a compact list, so the host only sorts the distinct boundaries of the batch.
+// The tables hold at least twice as many slots as keys can be inserted, so a probe always ends at
+// an empty slot. Slots only ever change from empty to a key, so a stale read sees empty at worst
+// and the CAS settles it. The key ~0 (the empty marker) is reported through a flag bit instead.
+constexpr uint64_t KEY_EMPTY = ~0ull;
+
+__device__ __forceinline__ void hset_insert(uint64_t * tab, uint32_t mask, uint64_t key, uint64_t * out, unsigned * count,
+                                            unsigned * flags, unsigned max_bit)
 {
-    if (v.empty()) return;
-    // linear-probing pre-filter: boundaries repeat massively (tile grids), so keep each value once
-    size_t cap = 1024;
-    std::vector<uint64_t> table(cap, ~0ull);
-    std::vector<uint64_t> out;
-    size_t used = 0;
-    for (uint64_t x : v)
+    if (key == KEY_EMPTY) { atomicOr(flags, max_bit); return; }
+    uint32_t h = (uint32_t) ((key * 0x9e3779b97f4a7c15ull) >> 32) & mask;
+    for (;;)
     {
-        if (x == ~0ull) { out.push_back(x); continue; }
-        if (used * 2 >= cap)
+        const uint64_t v = *(volatile uint64_t *) (tab + h);
+        if (v == key) return;
+        if (v == KEY_EMPTY)
         {
-            std::vector<uint64_t> t2(cap * 2, ~0ull);
-            for (uint64_t y : table) if (y != ~0ull) {
-                size_t h = (y * 0x9e3779b97f4a7c15ull) >> 20 & (cap * 2 - 1);
-                while (t2[h] != ~0ull) h = (h + 1) & (cap * 2 - 1);
-                t2[h] = y;
-            }
-            table.swap(t2); cap *= 2;
+            const uint64_t prev = atomicCAS((unsigned long long *) (tab + h), (unsigned long long) KEY_EMPTY,
+                                            (unsigned long long) key);
+            if (prev == KEY_EMPTY) { out[atomicAdd(count, 1u)] = key; return; }
+            if (prev == key) return;
         }
-        size_t h = (x * 0x9e3779b97f4a7c15ull) >> 20 & (cap - 1);
-        while (table[h] != ~0ull && table[h] != x) h = (h + 1) & (cap - 1);
-        if (table[h] == ~0ull) { table[h] = x; out.push_back(x); ++used; }
+        h = (h + 1) & mask;
     }
-    std::sort(out.begin(), out.end());
-    out.erase(std::unique(out.begin(), out.end()), out.end());
-    v.swap(out);
+}
+
+// counts[0] / counts[1]: distinct x / y keys appended; counts[2]: bit 1 / 2 when ~0 was an x / y key
+__global__ void collect_bounds_kernel(const HOp * __restrict__ ops, int n, uint64_t * tx, uint64_t * ty, uint32_t mask,
+                                      uint64_t * ux, uint64_t * uy, unsigned * counts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const HRect r = ops[i].r;
+    hset_insert(tx, mask, r.x0, ux, counts + 0, counts + 2, 1u);
+    hset_insert(tx, mask, r.x1, ux, counts + 0, counts + 2, 1u);
+    hset_insert(ty, mask, r.y0, uy, counts + 1, counts + 2, 2u);
+    hset_insert(ty, mask, r.y1, uy, counts + 1, counts + 2, 2u);
+}
+
+__device__ __forceinline__ int32_t lower_index(const uint64_t * __restrict__ v, int n, uint64_t key)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (__ldg(v + mid) < key) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+
+// Ops in cell coordinates: each boundary's index in the domain's sorted boundary lists.
+__global__ void map_ops_kernel(const HOp * __restrict__ ops, int n, const uint64_t * __restrict__ xs, int nxs,
+                               const uint64_t * __restrict__ ys, int nys, DOp * out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const HOp o = ops[i];
+    DOp q;
+    q.task = (int32_t) o.task; q.link = o.link; q.mode = o.mode; q.pad = 0;
+    q.cx0 = lower_index(xs, nxs, o.r.x0); q.cx1 = lower_index(xs, nxs, o.r.x1);
+    q.cy0 = lower_index(ys, nys, o.r.y0); q.cy1 = lower_index(ys, nys, o.r.y1);
+    out[i] = q;
 }
 
 struct Domain {
@@ -346,6 +453,9 @@ struct xkb_resolver {
     uint32_t ntasks = 0;
     // device work buffers
     DevBuf<DOp> dops;
+    DevBuf<HOp> hops;                           // the batch's ops in byte coordinates
+    DevBuf<uint64_t> hset, ukeys, bounds;       // compression: hash sets, distinct keys, sorted boundaries
+    DevBuf<unsigned> ucount;
     DevBuf<unsigned long long> emit, table, uniq;
     DevBuf<unsigned long long> counters;        // [0] emit count, [1] unique count
     DevBuf<int> maxr;
@@ -353,8 +463,11 @@ struct xkb_resolver {
     // graph
     DevBuf<uint32_t> succ_ptr, succ, npred, tmp;
     DevBuf<uint32_t> periodic;                  // packed arrays of the periodic form
+    DevBuf<unsigned> bin_off, bin_cur;          // ops binned to regions: offsets, fill cursors
+    DevBuf<int> bin_list, bin_flag;             // op indices per region; region-too-long flag
     bool graph_valid = false;
     double last_device_ms = 0;
+    double last_ops_ms = 0, last_compress_ms = 0;   // host phases of the last batch
 };
 
 namespace xkb {
@@ -471,12 +584,8 @@ static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 
 // Extend the domain's compression with the batch's boundaries; remap the device state when
 // the cell grid changes.
-static int refine_domain(xkb_resolver * R, Domain & d)
+static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & xs, std::vector<uint64_t> & ys)
 {
-    std::vector<uint64_t> xs = d.xs, ys = d.ys;
-    xs.reserve(xs.size() + 2 * d.ops.size()); ys.reserve(ys.size() + 2 * d.ops.size());
-    for (const HOp & o : d.ops) { xs.push_back(o.r.x0); xs.push_back(o.r.x1); ys.push_back(o.r.y0); ys.push_back(o.r.y1); }
-    unique_sorted(xs); unique_sorted(ys);
     if (xs.size() < 2 || ys.size() < 2) { d.xs = xs; d.ys = ys; return XKB_OK; }
     const bool same = xs == d.xs && ys == d.ys;
     const size_t ncx = xs.size() - 1, ncy = ys.size() - 1, ncells = ncx * ncy;
@@ -517,9 +626,56 @@ static int refine_domain(xkb_resolver * R, Domain & d)
     return XKB_OK;
 }
 
-static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t nops, int rcap_smem_ok)
+// Bin the batch's ops to regions (counts, offsets, fill, per-region sort) and run the region
+// kernel over each region's own list; a region too crowded to sort falls back to the kernel that
+// scans every op of the batch.
+template <int RX, int RY>
+static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
 {
-    (void) rcap_smem_ok;
+    const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
+    cudaStream_t st = R->stream;
+    const size_t nb = (size_t) nregions + 1;
+    int rc;
+    if ((rc = R->bin_off.reserve(nb)) || (rc = R->bin_cur.reserve(nb)) ||
+        (rc = R->tmp.reserve(nb / SCAN_TILE + 2)) || (rc = R->bin_flag.reserve(1)))
+        return rc;
+    XKB_CUDA_TRY(cudaMemsetAsync(R->bin_off.p, 0, nb * sizeof(unsigned), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(R->bin_cur.p, 0, nb * sizeof(unsigned), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(R->bin_flag.p, 0, sizeof(int), st));
+    const unsigned g = (unsigned) ((a.nops + 255) / 256);
+    bin_count_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p);
+    if ((rc = device_exclusive_scan(R->bin_off.p, R->bin_off.p, nb, R->tmp.p, nullptr, st))) return rc;
+    unsigned total = 0;
+    XKB_CUDA_TRY(cudaMemcpyAsync(&total, R->bin_off.p + nregions, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    bool binned = total > 0;
+    if (binned)
+    {
+        if ((rc = R->bin_list.reserve(total))) return rc;
+        bin_fill_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p, R->bin_cur.p, R->bin_list.p);
+        XKB_CUDA_TRY(cudaFuncSetAttribute(bin_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BIN_SORT_CAP * (int) sizeof(int)));
+        bin_sort_kernel<<<(unsigned) nregions, BIN_SORT_THREADS, BIN_SORT_CAP * sizeof(int), st>>>(R->bin_off.p, R->bin_list.p, R->bin_flag.p);
+        int too_long = 0;
+        XKB_CUDA_TRY(cudaMemcpyAsync(&too_long, R->bin_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        XKB_CUDA_TRY(cudaStreamSynchronize(st));
+        binned = !too_long;
+    }
+    if (binned)
+    {
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        resolve_region_kernel<RX, RY, true><<<(unsigned) nregions, RX * RY, smem, st>>>(a, R->bin_off.p, R->bin_list.p);
+    }
+    else
+    {
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        resolve_region_kernel<RX, RY, false><<<(unsigned) nregions, RX * RY, smem, st>>>(a, nullptr, nullptr);
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
+static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t nops)
+{
     const int ncx = (int) d.xs.size() - 1, ncy = (int) d.ys.size() - 1;
     ResolveArgs a;
     a.ops = R->dops.p + op_offset; a.nops = (int) nops;
@@ -532,59 +688,82 @@ static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t 
     {
         constexpr int RX = 64, RY = 1;
         a.nrx = (ncx + RX - 1) / RX;
-        const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
-        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        resolve_region_kernel<RX, RY><<<(unsigned) a.nrx, RX * RY, smem, R->stream>>>(a);
+        return launch_region<RX, RY>(R, a, a.nrx);
     }
-    else
-    {
-        constexpr int RX = 8, RY = 8;
-        a.nrx = (ncx + RX - 1) / RX;
-        const int nry = (ncy + RY - 1) / RY;
-        const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
-        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        resolve_region_kernel<RX, RY><<<(unsigned) (a.nrx * nry), RX * RY, smem, R->stream>>>(a);
-    }
-    XKB_CUDA_TRY(cudaGetLastError());
-    return XKB_OK;
+    constexpr int RX = 8, RY = 8;
+    a.nrx = (ncx + RX - 1) / RX;
+    const int nry = (ncy + RY - 1) / RY;
+    return launch_region<RX, RY>(R, a, a.nrx * nry);
 }
 
-static int map_ops(Domain & d, std::vector<DOp> & out)
+// Compress the domain's coordinates with the batch's boundaries (found on the device, merged with
+// the domain's earlier ones on the host), refine the cell state, and write the batch's ops in cell
+// coordinates to dops. hops / dops: this domain's nops ops on the device.
+static int compress_domain(xkb_resolver * R, Domain & d, const HOp * hops, DOp * dops, size_t nops)
 {
-    for (const HOp & o : d.ops)
+    cudaStream_t st = R->stream;
+    size_t cap = 1024;
+    while (cap < 4 * nops) cap *= 2;
+    int rc;
+    if ((rc = R->hset.reserve(2 * cap)) || (rc = R->ukeys.reserve(4 * nops)) || (rc = R->ucount.reserve(3))) return rc;
+    XKB_CUDA_TRY(cudaMemsetAsync(R->hset.p, 0xff, 2 * cap * sizeof(uint64_t), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(R->ucount.p, 0, 3 * sizeof(unsigned), st));
+    const unsigned g = (unsigned) ((nops + 255) / 256);
+    collect_bounds_kernel<<<g, 256, 0, st>>>(hops, (int) nops, R->hset.p, R->hset.p + cap, (uint32_t) (cap - 1),
+                                             R->ukeys.p, R->ukeys.p + 2 * nops, R->ucount.p);
+    XKB_CUDA_TRY(cudaGetLastError());
+    unsigned cnt[3];
+    XKB_CUDA_TRY(cudaMemcpyAsync(cnt, R->ucount.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<uint64_t> xs(d.xs.size() + cnt[0] + 1), ys(d.ys.size() + cnt[1] + 1);
+    std::copy(d.xs.begin(), d.xs.end(), xs.begin());
+    std::copy(d.ys.begin(), d.ys.end(), ys.begin());
+    if (cnt[0]) XKB_CUDA_TRY(cudaMemcpyAsync(xs.data() + d.xs.size(), R->ukeys.p, cnt[0] * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    if (cnt[1]) XKB_CUDA_TRY(cudaMemcpyAsync(ys.data() + d.ys.size(), R->ukeys.p + 2 * nops, cnt[1] * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (cnt[2] & 1u) xs.back() = KEY_EMPTY; else xs.pop_back();
+    if (cnt[2] & 2u) ys.back() = KEY_EMPTY; else ys.pop_back();
+    for (std::vector<uint64_t> * v : {&xs, &ys})
     {
-        DOp q;
-        q.task = (int32_t) o.task; q.link = o.link; q.mode = o.mode; q.pad = 0;
-        q.cx0 = (int32_t) (std::lower_bound(d.xs.begin(), d.xs.end(), o.r.x0) - d.xs.begin());
-        q.cx1 = (int32_t) (std::lower_bound(d.xs.begin(), d.xs.end(), o.r.x1) - d.xs.begin());
-        q.cy0 = (int32_t) (std::lower_bound(d.ys.begin(), d.ys.end(), o.r.y0) - d.ys.begin());
-        q.cy1 = (int32_t) (std::lower_bound(d.ys.begin(), d.ys.end(), o.r.y1) - d.ys.begin());
-        out.push_back(q);
+        std::sort(v->begin(), v->end());
+        v->erase(std::unique(v->begin(), v->end()), v->end());
     }
+    if ((rc = refine_domain(R, d, xs, ys))) return rc;
+    if ((rc = R->bounds.reserve(d.xs.size() + d.ys.size()))) return rc;
+    XKB_CUDA_TRY(cudaMemcpyAsync(R->bounds.p, d.xs.data(), d.xs.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    XKB_CUDA_TRY(cudaMemcpyAsync(R->bounds.p + d.xs.size(), d.ys.data(), d.ys.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    map_ops_kernel<<<g, 256, 0, st>>>(hops, (int) nops, R->bounds.p, (int) d.xs.size(), R->bounds.p + d.xs.size(),
+                                      (int) d.ys.size(), dops);
+    XKB_CUDA_TRY(cudaGetLastError());
+    // the host vectors above die on return: the copies out of them must be done
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
     return XKB_OK;
 }
 
 static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 {
     int rc;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     build_ops(R, recs, n);
+    const auto t1 = clk::now();
     std::vector<Domain *> doms;
     if (!R->interval.ops.empty()) doms.push_back(&R->interval);
     for (auto & d : R->blas) if (!d->ops.empty()) doms.push_back(d.get());
 
-    std::vector<DOp> all;
     std::vector<size_t> offs;
-    for (Domain * d : doms)
-    {
-        if ((rc = refine_domain(R, *d))) return rc;
-        offs.push_back(all.size());
-        map_ops(*d, all);
-    }
-    if ((rc = R->dops.reserve(all.size() ? all.size() : 1))) return rc;
-    if (!all.empty())
-        XKB_CUDA_TRY(cudaMemcpyAsync(R->dops.p, all.data(), all.size() * sizeof(DOp), cudaMemcpyHostToDevice, R->stream));
+    size_t total = 0;
+    for (Domain * d : doms) { offs.push_back(total); total += d->ops.size(); }
+    if ((rc = R->hops.reserve(total ? total : 1)) || (rc = R->dops.reserve(total ? total : 1))) return rc;
+    for (size_t k = 0; k < doms.size(); ++k)
+        XKB_CUDA_TRY(cudaMemcpyAsync(R->hops.p + offs[k], doms[k]->ops.data(), doms[k]->ops.size() * sizeof(HOp),
+                                     cudaMemcpyHostToDevice, R->stream));
+    for (size_t k = 0; k < doms.size(); ++k)
+        if ((rc = compress_domain(R, *doms[k], R->hops.p + offs[k], R->dops.p + offs[k], doms[k]->ops.size()))) return rc;
+    R->last_ops_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    R->last_compress_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
 
-    size_t emit_guess = std::max<size_t>(1 << 16, all.size() * 2);
+    size_t emit_guess = std::max<size_t>(1 << 16, total * 2);
     for (int attempt = 0; attempt < 6; ++attempt)
     {
         if ((rc = R->emit.reserve(emit_guess))) return rc;
@@ -594,12 +773,12 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
         XKB_CUDA_TRY(cudaMemsetAsync(R->maxr.p, 0, sizeof(int), R->stream));
         for (size_t k = 0; k < doms.size(); ++k)
         {
-            const size_t nops = (k + 1 < doms.size() ? offs[k + 1] : all.size()) - offs[k];
+            const size_t nops = doms[k]->ops.size();
             // states must exist for every cell (ncells > 0 when the domain has >= 1 op)
             if ((rc = R->emit.reserve(emit_guess))) return rc;
             if (doms[k]->ncells == 0) continue;
             if ((rc = doms[k]->state[doms[k]->cur ^ 1].reserve(doms[k]->ncells * (2 + (size_t) R->rcap)))) return rc;
-            if ((rc = launch_domain(R, *doms[k], offs[k], nops, 1))) return rc;
+            if ((rc = launch_domain(R, *doms[k], offs[k], nops))) return rc;
         }
         unsigned long long nemit = 0;
         int maxr = 0;
@@ -771,6 +950,15 @@ extern "C" int xkb_resolver_stats(xkb_resolver_t * R, uint64_t * ntasks, uint64_
     if (ntasks) *ntasks = R->ntasks;
     if (nedges) *nedges = R->nuniq;
     if (last_batch_ms) *last_batch_ms = R->last_device_ms;
+    return XKB_OK;
+}
+
+extern "C" int xkb_resolver_timing(xkb_resolver_t * R, double * ops_ms, double * compress_ms, double * batch_ms)
+{
+    if (!R) return xkb_set_error(XKB_EINVAL, "resolver_timing: null resolver");
+    if (ops_ms) *ops_ms = R->last_ops_ms;
+    if (compress_ms) *compress_ms = R->last_compress_ms;
+    if (batch_ms) *batch_ms = R->last_device_ms;
     return XKB_OK;
 }
 
