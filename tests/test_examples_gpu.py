@@ -1,0 +1,53 @@
+"""examples/heat_xkrt: the heat example through the XKRT C API (spawn -> xkrt_task_wait), the
+program the C-API end-to-end measurement runs. Its output grids are checked against the oracle:
+bit-exact for FP64, and for FP32 storage bit-exact against the oracle's FP32-storage run (FP64
+arithmetic, one rounding to float per cell and step) and within 1e-5 relative of FP64."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import kernels_oracle as O
+
+pytestmark = pytest.mark.gpu
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(REPO, "xkaapi_b200", "examples", "heat_xkrt")
+
+
+def run(args):
+    r = subprocess.run([EXE] + [str(a) for a in args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return [json.loads(l) for l in r.stdout.strip().splitlines()]
+
+
+@pytest.mark.parametrize("nx,ny,ts,steps", [(256, 256, 64, 6), (300, 170, 64, 5), (129, 65, 32, 4)])
+def test_heat_xkrt_f64(torch_cuda, tmp_path, nx, ny, ts, steps):
+    g = O.heat_init(nx, ny, seed=7)
+    g.tofile(tmp_path / "init.bin")
+    lines = run([nx, ny, ts, steps, 2, 0, tmp_path / "init.bin", tmp_path / "out.bin"])
+    ntasks = -(-nx // ts) * -(-ny // ts) * steps
+    assert len(lines) == 2
+    for ln in lines:
+        assert ln["tasks"] == ntasks and ln["fused"] == 1 and ln["h2d"] > 0 and ln["d2h"] > 0
+    assert lines[0]["edges"] == lines[1]["edges"] and lines[0]["checksum"] == lines[1]["checksum"]
+    out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2))
+
+
+def test_heat_xkrt_f32(torch_cuda, tmp_path):
+    nx, ny, ts, steps = 320, 200, 64, 8
+    g = O.heat_init(nx, ny, seed=11)
+    g.tofile(tmp_path / "init.bin")
+    run([nx, ny, ts, steps, 1, 1, tmp_path / "init.bin", tmp_path / "out.bin"])
+    out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2, dtype=np.float32).astype(np.float64))
+    ref = O.heat_run(g, nx, ny, steps, 0.2)
+    assert np.max(np.abs(out - ref)) <= 1e-5 * np.max(np.abs(ref))
+
+
+def test_heat_xkrt_seeded_default(torch_cuda):
+    """Without an init file the program fills the grid itself; two repetitions agree."""
+    lines = run([512, 384, 128, 3, 2])
+    assert lines[0]["checksum"] == lines[1]["checksum"] and lines[0]["checksum"] > 0

@@ -52,7 +52,20 @@ def test_heat_graph_100_steps_vs_oracle(torch_cuda):
     np.testing.assert_array_equal(gpu_edges(recs, batches=5), U.oracle_edges(recs))
 
 
-def test_many_readers_grow_reader_capacity(torch_cuda):
+@pytest.mark.parametrize("which", ["microbench_32k", "heat_4096_t64_s10"])
+def test_large_matrix_batches_vs_oracle(torch_cuda, which):
+    # a small first batch creates the domain; the large second batch (tens of thousands of
+    # matrix records on existing domains) is split over host threads when building ops
+    recs = S.microbench_stream(32768, 777) if which == "microbench_32k" else S.heat_stream(4096, 4096, 64, 64, 10)
+    cut = int(np.searchsorted(recs["task"], 500))
+    r = xk.Resolver()
+    r.add(recs[:cut]); r.add(recs[cut:])
+    e = r.edges()
+    r.close()
+    np.testing.assert_array_equal(e, U.oracle_edges(recs))
+
+
+def test_many_readers(torch_cuda):
     # 150 readers of the same rows, then a writer: the writer depends on all 150 readers
     tasks = [[("m", S.W, 1 << 20, 256, 0, 0, 64, 8, 8)]]
     tasks += [[("m", S.R, 1 << 20, 256, 0, 0, 64, 8, 8)] for _ in range(150)]
@@ -61,6 +74,37 @@ def test_many_readers_grow_reader_capacity(torch_cuda):
     e = gpu_edges(recs)
     np.testing.assert_array_equal(e, U.oracle_edges(recs))
     assert sum(1 for p, s in e if s == 151) == 150
+
+
+@pytest.mark.parametrize("nreaders,batches", [(5000, 1), (3000, 9)])
+def test_thousands_of_readers_spill(torch_cuda, nreaders, batches):
+    # far more readers of one region than a cell keeps inline (they spill to chained chunks,
+    # across batches too); then two writers, each over part of it, depend on every reader
+    tasks = [[("m", S.W, 1 << 20, 256, 0, 0, 64, 8, 8)]]
+    tasks += [[("m", S.R, 1 << 20, 256, 0, 0, 64, 8, 8)] for _ in range(nreaders)]
+    tasks += [[("m", S.W, 1 << 20, 256, 16, 2, 8, 2, 8)], [("m", S.W, 1 << 20, 256, 40, 5, 4, 1, 8)]]
+    recs = S.from_tuples(tasks)
+    e = gpu_edges(recs, batches, seed=3)
+    np.testing.assert_array_equal(e, U.oracle_edges(recs))
+    assert sum(1 for p, s in e if s == nreaders + 1) == nreaders
+
+
+def test_spilled_readers_survive_refinement(torch_cuda):
+    # readers spill in a first batch; the second batch brings new boundaries that split the
+    # cells (each piece copies the spilled readers), appends readers to some pieces, and then
+    # writes each piece separately
+    ld, base = 512, 1 << 22
+    first = [[("m", S.W, base, ld, 0, 0, 256, 16, 8)]]
+    first += [[("m", S.R, base, ld, 0, 0, 256, 16, 8)] for _ in range(200)]
+    second = [[("m", S.R, base, ld, 64, 4, 32, 4, 8)] for _ in range(40)]
+    second += [[("m", S.W, base, ld, x, y, 16, 3, 8)] for x in (0, 60, 100, 200) for y in (0, 5, 12)]
+    recs = S.from_tuples(first + second)
+    cut = int(np.searchsorted(recs["task"], len(first)))
+    r = xk.Resolver()
+    r.add(recs[:cut]); r.add(recs[cut:])
+    e = r.edges()
+    r.close()
+    np.testing.assert_array_equal(e, U.oracle_edges(recs))
 
 
 class _DevView:

@@ -72,7 +72,33 @@ def build(verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_examples(verbose)
     return LIB
+
+
+EXAMPLES = os.path.join(PKG, "examples")
+
+
+def build_examples(verbose=False):
+    """C programs under examples/ (the reference's examples written against include/xkrt_capi.h),
+    linked to libxkb200.so with an $ORIGIN-relative rpath so the tree can move."""
+    out = []
+    for f in sorted(os.listdir(EXAMPLES)):
+        if not f.endswith(".c"):
+            continue
+        src, exe = os.path.join(EXAMPLES, f), os.path.join(EXAMPLES, f[:-2])
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), os.path.getmtime(LIB)):
+            out.append(exe)
+            continue
+        cmd = ["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-D_POSIX_C_SOURCE=200809L", "-I" + os.path.join(REPO, "include"),
+               src, "-o", exe, "-L" + PKG, "-lxkb200", "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"gcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+        out.append(exe)
+    return out
 
 
 if __name__ == "__main__":

@@ -6,3 +6,6 @@
 
 // Launch one task descriptor as its own kernel (the plain per-task form) on `stream`.
 int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream);
+
+// Set a scheduler's descriptors on the device only (persistent forms only; no host copy).
+int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks);

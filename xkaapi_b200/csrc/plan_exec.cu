@@ -9,12 +9,19 @@
 // of different accesses may (a later access can read what an earlier copy wrote), so a batch
 // never spans two accesses.
 //
+// Host copies are coalesced first: within a run of consecutive copies of one direction (all H2D
+// or all D2H) no copy reads what another writes, so their order is free, and blocks that are
+// side by side in both address spaces merge into one wider copy, then copies stacked at the
+// same pitch merge into one taller copy. A canonical block partition cuts a tile's data into
+// many small blocks; merged, a whole band of tiles moves as one cudaMemcpy2DAsync.
+//
 // xkb_diffusion_views is the reference's tile body contract (diffusion_cuda,
 // examples/heat-diffusion-2d/src/kernels/diffusion.cu:107-154) on per-access replicas:
 // src/dst point at the tile origin after the launcher's re-basing (main.cc:214-219), with their
 // own leading dimensions.
 #include "common.cuh"
 
+#include <algorithm>
 #include <vector>
 
 namespace xkb {
@@ -78,6 +85,67 @@ __global__ void __launch_bounds__(256) diffusion_views_kernel(const T * __restri
 
 using namespace xkb;
 
+// One host copy: rows x width bytes from src (pitch sp) to dst (pitch dp).
+struct HostCopy { uintptr_t src, dst; int64_t sp, dp, width, rows; };
+
+static size_t coalesce(std::vector<HostCopy> & v)
+{
+    if (v.size() < 2) return v.size();
+    // side by side: same rows and pitches, each continuing the previous one in both spaces
+    std::sort(v.begin(), v.end(), [](const HostCopy & a, const HostCopy & b) {
+        if (a.sp != b.sp) return a.sp < b.sp;
+        if (a.dp != b.dp) return a.dp < b.dp;
+        if (a.rows != b.rows) return a.rows < b.rows;
+        return a.src < b.src;
+    });
+    size_t k = 0;
+    for (size_t i = 1; i < v.size(); ++i)
+    {
+        HostCopy & a = v[k];
+        const HostCopy & b = v[i];
+        if (a.sp == b.sp && a.dp == b.dp && a.rows == b.rows && b.src == a.src + (uintptr_t) a.width &&
+            b.dst == a.dst + (uintptr_t) a.width && (a.rows == 1 || a.width + b.width <= std::min(a.sp, a.dp)))
+        {
+            a.width += b.width;
+            if (a.rows == 1) { a.sp = std::max(a.sp, a.width); a.dp = std::max(a.dp, a.width); }
+        }
+        else v[++k] = b;
+    }
+    v.resize(k + 1);
+    // stacked: same width and pitches, each starting one pitch x rows below the previous one
+    std::sort(v.begin(), v.end(), [](const HostCopy & a, const HostCopy & b) {
+        if (a.sp != b.sp) return a.sp < b.sp;
+        if (a.dp != b.dp) return a.dp < b.dp;
+        if (a.width != b.width) return a.width < b.width;
+        return a.src < b.src;
+    });
+    k = 0;
+    for (size_t i = 1; i < v.size(); ++i)
+    {
+        HostCopy & a = v[k];
+        const HostCopy & b = v[i];
+        if (a.sp == b.sp && a.dp == b.dp && a.width == b.width && a.width <= std::min(a.sp, a.dp) &&
+            b.src == a.src + (uintptr_t) (a.rows * a.sp) && b.dst == a.dst + (uintptr_t) (a.rows * a.dp))
+            a.rows += b.rows;
+        else v[++k] = b;
+    }
+    v.resize(k + 1);
+    return v.size();
+}
+
+static int issue_host_copies(std::vector<HostCopy> & v, cudaMemcpyKind kind, cudaStream_t st)
+{
+    coalesce(v);
+    for (const HostCopy & c : v)
+    {
+        cudaError_t e = cudaMemcpy2DAsync((void *) c.dst, (size_t) c.dp, (const void *) c.src, (size_t) c.sp, (size_t) c.width,
+                                          (size_t) c.rows, kind, st);
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    }
+    v.clear();
+    return XKB_OK;
+}
+
 extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, void * stream)
 {
     if (n && (!copies || !alloc_ptrs)) return xkb_set_error(XKB_EINVAL, "plan_execute: bad arguments");
@@ -107,37 +175,45 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
         batch.clear();
         return XKB_OK;
     };
+    std::vector<HostCopy> hrun;          // pending run of host copies, all of kind hkind
+    int64_t hkind = -1;
     int rc = XKB_OK;
     for (size_t i = 0; i < n && rc == XKB_OK; ++i)
     {
         const xkb_copy_t & c = copies[i];
         const int64_t row_bytes = c.m * c.sizeof_type;
         const int64_t sp = c.src_ld ? c.src_ld * c.sizeof_type : row_bytes, dp = c.dst_ld ? c.dst_ld * c.sizeof_type : row_bytes;
+        if (c.kind != hkind && !hrun.empty() &&
+            (rc = issue_host_copies(hrun, hkind == XKB_COPY_H2D ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, st)))
+            break;
         if (c.kind == XKB_COPY_D2D)
         {
             if (i > 0 && (copies[i - 1].task != c.task || copies[i - 1].access != c.access) && (rc = flush())) break;
             uint8_t * s = dev_ptr(c.src_alloc, c.src_off), * d = dev_ptr(c.dst_alloc, c.dst_off);
             if (!s || !d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
             batch.push_back({s, d, sp, dp, row_bytes, c.n});
+            hkind = c.kind;
             continue;
         }
         if ((rc = flush())) break;
-        cudaError_t e;
+        if (row_bytes <= 0 || c.n <= 0) { hkind = c.kind; continue; }   // nothing to move
         if (c.kind == XKB_COPY_H2D)
         {
             uint8_t * d = dev_ptr(c.dst_alloc, c.dst_off);
             if (!d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
-            e = cudaMemcpy2DAsync(d, dp, (const void *) (uintptr_t) c.src_off, sp, row_bytes, c.n, cudaMemcpyHostToDevice, st);
+            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, sp, dp, row_bytes, c.n});
         }
         else if (c.kind == XKB_COPY_D2H)
         {
             const uint8_t * s = dev_ptr(c.src_alloc, c.src_off);
             if (!s) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
-            e = cudaMemcpy2DAsync((void *) (uintptr_t) c.dst_off, dp, s, sp, row_bytes, c.n, cudaMemcpyDeviceToHost, st);
+            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, sp, dp, row_bytes, c.n});
         }
         else { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu has an unknown kind", i); break; }
-        if (e != cudaSuccess) rc = xkb_set_cuda_error(e);
+        hkind = c.kind;
     }
+    if (rc == XKB_OK && !hrun.empty())
+        rc = issue_host_copies(hrun, hkind == XKB_COPY_H2D ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, st);
     if (rc == XKB_OK) rc = flush();
     if (dbatch) { cudaStreamSynchronize(st); cudaFree(dbatch); }
     return rc;

@@ -1,0 +1,82 @@
+// PoolArray<T>: a growable array of trivially copyable T in anonymous memory, for the runtime's
+// per-batch pools (spawned tasks, their arguments and accesses, the access records). Growing
+// remaps the pages (mremap) instead of copying them, and the range is marked for transparent
+// huge pages, so filling millions of entries costs one page fault per 2 MB rather than per 4 KB
+// and no copy at all. Element addresses change when the array grows; they are stable while it
+// does not.
+#pragma once
+
+#include <sys/mman.h>
+
+#include <cstddef>
+#include <cstring>
+#include <type_traits>
+
+namespace xkb {
+
+template <typename T>
+class PoolArray {
+    static_assert(std::is_trivially_copyable<T>::value, "PoolArray holds trivially copyable elements");
+
+public:
+    PoolArray() = default;
+    PoolArray(const PoolArray &) = delete;
+    PoolArray & operator=(const PoolArray &) = delete;
+    ~PoolArray() { release(); }
+
+    size_t size() const { return n_; }
+    bool empty() const { return n_ == 0; }
+    T * data() { return p_; }
+    const T * data() const { return p_; }
+    T & operator[](size_t i) { return p_[i]; }
+    const T & operator[](size_t i) const { return p_[i]; }
+    T & back() { return p_[n_ - 1]; }
+    size_t capacity_bytes() const { return bytes_; }
+
+    // n elements; new elements are NOT initialised (callers write them). false: out of memory.
+    bool resize(size_t n)
+    {
+        if (n * sizeof(T) > bytes_ && !grow(n * sizeof(T))) return false;
+        n_ = n;
+        return true;
+    }
+    bool push_back(const T & v)
+    {
+        if (!resize(n_ + 1)) return false;
+        p_[n_ - 1] = v;
+        return true;
+    }
+    bool append(const T * v, size_t k)
+    {
+        const size_t at = n_;
+        if (!resize(n_ + k)) return false;
+        if (k) memcpy(p_ + at, v, k * sizeof(T));
+        return true;
+    }
+    void clear() { n_ = 0; }
+    void release()
+    {
+        if (p_) munmap(p_, bytes_);
+        p_ = nullptr; n_ = 0; bytes_ = 0;
+    }
+
+private:
+    bool grow(size_t need)
+    {
+        constexpr size_t HUGE = size_t(2) << 20;
+        size_t nb = bytes_ ? 2 * bytes_ : size_t(32) << 20;
+        while (nb < need) nb *= 2;
+        nb = (nb + HUGE - 1) & ~(HUGE - 1);
+        void * q = p_ ? mremap(p_, bytes_, nb, MREMAP_MAYMOVE)
+                      : mmap(nullptr, nb, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        if (q == MAP_FAILED) return false;
+        madvise(q, nb, MADV_HUGEPAGE);
+        p_ = (T *) q; bytes_ = nb;
+        return true;
+    }
+
+    T * p_ = nullptr;
+    size_t n_ = 0, bytes_ = 0;
+};
+
+} // namespace xkb

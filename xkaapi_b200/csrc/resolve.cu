@@ -29,10 +29,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <new>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -50,18 +53,40 @@ struct DOp {            // one op in cell coordinates (24 bytes)
     int32_t cx0, cx1, cy0, cy1;
 };
 
+// Cell state: writer, number of readers since that write, head and tail of the reader spill
+// chain, and the first RCAP readers. Readers past RCAP go to chains of SPILL-int chunks
+// (next chunk, then SPILL - 1 readers) drawn from one pool per resolver, so a cell can collect
+// any number of readers (a region that is read every step and never written) while the state
+// and the region kernel's shared memory stay small. Chunks of a chain that a write clears are
+// not reused.
+constexpr int RCAP = 32;
+constexpr int SHDR = 4;
+constexpr int STRIDE = SHDR + RCAP;
+constexpr int SPILL = 32;
+constexpr int SPILL_R = SPILL - 1;
+
 struct ResolveArgs {
     const DOp * ops;
     int nops;
     int ncx, ncy, nrx;
-    const int * state_in;     // per cell: writer, nreaders, readers[rcap]
+    const int * state_in;     // STRIDE ints per cell
     int * state_out;
-    int rcap;
     unsigned long long * emit;
     unsigned long long * emit_count;
     unsigned long long emit_cap;
-    int * max_readers;        // largest reader count seen (overflow when > rcap)
+    int * spill;              // chunk pool
+    unsigned * spill_ctr;     // [0] chunks handed out, [1] set when the pool ran out
+    unsigned spill_cap;       // chunks in the pool
 };
+
+// A fresh spill chunk (its next link cleared), or -1 with the out-of-pool flag set.
+__device__ __forceinline__ int spill_alloc(int * spill, unsigned * ctr, unsigned cap)
+{
+    const unsigned c = atomicAdd(ctr, 1u);
+    if (c >= cap) { atomicExch(ctr + 1, 1u); return -1; }
+    spill[(size_t) c * SPILL] = -1;
+    return (int) c;
+}
 
 // BINNED: the CTA's ops come from its region's list (op indices in op order, built by the
 // binning kernels below) instead of a scan of every op of the batch.
@@ -84,15 +109,13 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
     const int cx = gx0 + tid % RX, cy = gy0 + tid / RX;
     const bool valid = cx < a.ncx && cy < a.ncy;
     const size_t cell = valid ? (size_t) cy * a.ncx + cx : 0;
-    const size_t stride = 2 + (size_t) a.rcap;
 
-    int writer = -1, nr = 0, maxnr = 0;
+    int writer = -1, nr = 0, head = -1, tail = -1;
     if (valid)
     {
-        const int * st = a.state_in + cell * stride;
-        writer = st[0]; nr = st[1];
-        for (int k = 0; k < nr && k < a.rcap; ++k) rd[k * NT + tid] = st[2 + k];
-        maxnr = nr;
+        const int * st = a.state_in + cell * STRIDE;
+        writer = st[0]; nr = st[1]; head = st[2]; tail = st[3];
+        for (int k = 0; k < nr && k < RCAP; ++k) rd[k * NT + tid] = st[SHDR + k];
     }
 
     const int lo = BINNED ? (int) roff[blockIdx.x] : 0, hi = BINNED ? (int) roff[blockIdx.x + 1] : a.nops;
@@ -141,11 +164,23 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
             if (op.link)
             {
                 const bool from_readers = in && (op.mode & M_W) && nr > 0;
-                const int cnt = from_readers ? min(nr, a.rcap) : ((in && writer >= 0) ? 1 : 0);
+                const int cnt = from_readers ? nr : ((in && writer >= 0) ? 1 : 0);
                 const int maxcnt = __reduce_max_sync(0xffffffffu, cnt);
+                int chunk = head, ci = 0;                // walk of the spill chain past RCAP
                 for (int q = 0; q < maxcnt; ++q)
                 {
-                    const int p = q < cnt ? (from_readers ? rd[q * NT + tid] : writer) : -1;
+                    int p = -1;
+                    if (q < cnt)
+                    {
+                        if (!from_readers) p = writer;
+                        else if (q < RCAP) p = rd[q * NT + tid];
+                        else
+                        {
+                            if (ci == SPILL_R) { chunk = chunk >= 0 ? a.spill[(size_t) chunk * SPILL] : -1; ci = 0; }
+                            p = chunk >= 0 ? a.spill[(size_t) chunk * SPILL + 1 + ci] : -1;   // -1: pool ran out, batch redone
+                            ++ci;
+                        }
+                    }
                     const unsigned peers = __match_any_sync(0xffffffffu, p);
                     const bool leader = p >= 0 && lane == __ffs(peers) - 1;
                     const unsigned em = __ballot_sync(0xffffffffu, leader);
@@ -162,12 +197,22 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
             }
             else if (in)
             {
-                if (op.mode & M_W) { writer = op.task; nr = 0; }
+                if (op.mode & M_W) { writer = op.task; nr = 0; head = tail = -1; }
                 else if (op.mode == M_R)
                 {
-                    if (nr < a.rcap) rd[nr * NT + tid] = op.task;
+                    if (nr < RCAP) rd[nr * NT + tid] = op.task;
+                    else
+                    {
+                        const int slot = (nr - RCAP) % SPILL_R;
+                        if (slot == 0)
+                        {
+                            const int c = spill_alloc(a.spill, a.spill_ctr, a.spill_cap);
+                            if (c >= 0) { if (tail >= 0) a.spill[(size_t) tail * SPILL] = c; else head = c; }
+                            tail = c;
+                        }
+                        if (tail >= 0) a.spill[(size_t) tail * SPILL + 1 + slot] = op.task;
+                    }
                     ++nr;
-                    maxnr = max(maxnr, nr);
                 }
             }
         }
@@ -176,11 +221,10 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
 
     if (valid)
     {
-        int * st = a.state_out + cell * stride;
-        st[0] = writer; st[1] = min(nr, a.rcap);
-        for (int k = 0; k < nr && k < a.rcap; ++k) st[2 + k] = rd[k * NT + tid];
+        int * st = a.state_out + cell * STRIDE;
+        st[0] = writer; st[1] = nr; st[2] = head; st[3] = tail;
+        for (int k = 0; k < nr && k < RCAP; ++k) st[SHDR + k] = rd[k * NT + tid];
     }
-    if (maxnr > a.rcap) atomicMax(a.max_readers, maxnr);
 }
 
 // ---- binning of ops to regions ----------------------------------------------------------------
@@ -247,25 +291,40 @@ __global__ void __launch_bounds__(BIN_SORT_THREADS) bin_sort_kernel(const unsign
 
 // New compression refines the old one: every new cell lies inside exactly one old cell (or
 // outside the old domain, where the state is empty).
-__global__ void refine_state_kernel(const int * __restrict__ old_state, int * __restrict__ new_state, size_t stride,
-                                    const int * __restrict__ map_x, const int * __restrict__ map_y, int ncx, int ncy, int old_ncx)
+// Every new cell takes the state of the old cell it lies in; a spill chain is copied into fresh
+// chunks, since several new cells can come from one old cell and each appends on its own.
+__global__ void refine_state_kernel(const int * __restrict__ old_state, int * __restrict__ new_state,
+                                    const int * __restrict__ map_x, const int * __restrict__ map_y, int ncx, int ncy, int old_ncx,
+                                    int * spill, unsigned * spill_ctr, unsigned spill_cap)
 {
     const size_t cell = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= (size_t) ncx * ncy) return;
     const int cx = (int) (cell % ncx), cy = (int) (cell / ncx);
     const int ox = map_x[cx], oy = map_y[cy];
-    int * dst = new_state + cell * stride;
-    if (ox < 0 || oy < 0) { dst[0] = -1; dst[1] = 0; return; }
-    const int * src = old_state + ((size_t) oy * old_ncx + ox) * stride;
+    int * dst = new_state + cell * STRIDE;
+    if (ox < 0 || oy < 0) { dst[0] = -1; dst[1] = 0; dst[2] = -1; dst[3] = -1; return; }
+    const int * src = old_state + ((size_t) oy * old_ncx + ox) * STRIDE;
     const int n = src[1];
     dst[0] = src[0]; dst[1] = n;
-    for (int k = 0; k < n; ++k) dst[2 + k] = src[2 + k];
+    for (int k = 0; k < n && k < RCAP; ++k) dst[SHDR + k] = src[SHDR + k];
+    int head = -1, tail = -1;
+    int from = src[2];
+    for (int left = n - RCAP; left > 0 && from >= 0; left -= SPILL_R)
+    {
+        const int c = spill_alloc(spill, spill_ctr, spill_cap);
+        if (c < 0) { head = tail = -1; break; }                 // pool ran out: redone after growing
+        for (int k = 1; k < SPILL; ++k) spill[(size_t) c * SPILL + k] = spill[(size_t) from * SPILL + k];
+        if (tail >= 0) spill[(size_t) tail * SPILL] = c; else head = c;
+        tail = c;
+        from = spill[(size_t) from * SPILL];
+    }
+    dst[2] = head; dst[3] = tail;
 }
 
-__global__ void init_state_kernel(int * state, size_t ncells, size_t stride)
+__global__ void init_state_kernel(int * state, size_t ncells)
 {
     const size_t cell = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell < ncells) { state[cell * stride] = -1; state[cell * stride + 1] = 0; }
+    if (cell < ncells) { int * st = state + cell * STRIDE; st[0] = -1; st[1] = 0; st[2] = -1; st[3] = -1; }
 }
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long k)
@@ -335,6 +394,8 @@ __global__ void sort_segments_kernel(const uint32_t * __restrict__ ptr, uint32_t
 struct HRect { uint64_t x0, x1, y0, y1; };
 struct HOp { uint32_t task; uint8_t link; uint8_t mode; HRect r; };
 
+static size_t g_realloc_bytes = 0;               // device bytes allocated by reserve (trace)
+
 template <typename T>
 struct DevBuf {
     T * p = nullptr;
@@ -346,22 +407,10 @@ struct DevBuf {
         size_t c = cap ? cap : 1024;
         while (c < n) c *= 2;
         T * q = nullptr;
+        g_realloc_bytes += c * sizeof(T);
         cudaError_t e = cudaMalloc(&q, c * sizeof(T));
         if (e != cudaSuccess) return xkb_set_cuda_error(e);
         if (p) cudaFree(p);
-        p = q; cap = c;
-        return XKB_OK;
-    }
-    int grow_keep(size_t n, size_t used, cudaStream_t st)
-    {
-        if (n <= cap) return XKB_OK;
-        size_t c = cap ? cap : 1024;
-        while (c < n) c *= 2;
-        T * q = nullptr;
-        cudaError_t e = cudaMalloc(&q, c * sizeof(T));
-        if (e != cudaSuccess) return xkb_set_cuda_error(e);
-        if (p && used) { e = cudaMemcpyAsync(q, p, used * sizeof(T), cudaMemcpyDeviceToDevice, st); if (e != cudaSuccess) { cudaFree(q); return xkb_set_cuda_error(e); } }
-        if (p) { cudaStreamSynchronize(st); cudaFree(p); }
         p = q; cap = c;
         return XKB_OK;
     }
@@ -444,7 +493,6 @@ struct Domain {
 using namespace xkb;
 
 struct xkb_resolver {
-    int rcap = 64;
     cudaStream_t stream = nullptr;
     Domain interval;
     std::vector<std::unique_ptr<Domain>> blas;
@@ -456,9 +504,17 @@ struct xkb_resolver {
     DevBuf<HOp> hops;                           // the batch's ops in byte coordinates
     DevBuf<uint64_t> hset, ukeys, bounds;       // compression: hash sets, distinct keys, sorted boundaries
     DevBuf<unsigned> ucount;
-    DevBuf<unsigned long long> emit, table, uniq;
+    DevBuf<unsigned long long> emit, table;
+    // unique edges, appended batch by batch into segments (a batch's edges all end in the
+    // batch's own tasks, so batches never repeat each other's pairs); a new segment starts when
+    // the last one cannot take a batch's worst case, so stored edges are never moved
+    std::vector<std::unique_ptr<DevBuf<unsigned long long>>> useg;
+    std::vector<size_t> useg_n;
     DevBuf<unsigned long long> counters;        // [0] emit count, [1] unique count
-    DevBuf<int> maxr;
+    DevBuf<int> spill;                          // reader spill chunks (SPILL ints each)
+    DevBuf<unsigned> spill_ctr;                 // [0] chunks handed out, [1] ran-out flag
+    size_t spill_chunks = 0;                    // pool capacity in chunks
+    unsigned spill_used = 0;                    // chunks in use after the last completed step
     size_t nuniq = 0;
     // graph
     DevBuf<uint32_t> succ_ptr, succ, npred, tmp;
@@ -536,9 +592,84 @@ static int validate(const xkb_access_rec_t * recs, size_t n, uint32_t first_task
     return XKB_OK;
 }
 
+// Matrix-only batches whose every (ld, sizeof) already has a domain: each record's ops go to its
+// own domain only (LINK ops of a task's records, then their PUT ops), so chunks of whole tasks
+// can be built on several host threads and appended in chunk order. Returns false (nothing
+// built) when the batch needs the sequential path: a segment, or a matrix key seen for the first
+// time (a new domain replays earlier segments at that point of the stream).
+static bool build_ops_parallel(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nthreads = std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 32768));
+    if (nthreads < 2) return false;
+    std::vector<uint32_t> dom(n);
+    {
+        uint64_t lk = ~0ull, ls = ~0ull;
+        uint32_t li = 0;
+        for (size_t i = 0; i < n; ++i)
+        {
+            const xkb_access_rec_t & r = recs[i];
+            if (r.type != XKB_ACCESS_TYPE_BLAS_MATRIX) return false;
+            if (r.ld != lk || r.sizeof_type != ls)
+            {
+                auto it = R->blas_index.find(std::make_pair(r.ld, r.sizeof_type));
+                if (it == R->blas_index.end()) return false;
+                lk = r.ld; ls = r.sizeof_type; li = (uint32_t) it->second;
+            }
+            dom[i] = li;
+        }
+    }
+    const size_t nd = R->blas.size();
+    std::vector<size_t> cut(nthreads + 1, n);
+    cut[0] = 0;
+    for (size_t t = 1; t < nthreads; ++t)
+    {
+        size_t c = std::max(cut[t - 1], n * t / nthreads);
+        while (c > cut[t - 1] && c < n && recs[c].task == recs[c - 1].task) ++c;     // whole tasks per chunk
+        cut[t] = c;
+    }
+    std::vector<std::vector<Domain>> local(nthreads);
+    auto work = [&](size_t t) {
+        std::vector<Domain> & L = local[t];
+        L.resize(nd);
+        for (size_t k = 0; k < nd; ++k) { L[k].ld = R->blas[k]->ld; L[k].s = R->blas[k]->s; }
+        for (size_t i = cut[t]; i < cut[t + 1];)
+        {
+            size_t j = i;
+            while (j < cut[t + 1] && recs[j].task == recs[i].task) ++j;
+            for (size_t a = i; a < j; ++a) push_ops(L[dom[a]], true, recs[a]);
+            for (size_t a = i; a < j; ++a) push_ops(L[dom[a]], false, recs[a]);
+            i = j;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto & th : pool) th.join();
+    pool.clear();
+    // append in chunk order: offsets per (domain, chunk), then parallel copies
+    std::vector<size_t> off(nd * nthreads);
+    for (size_t k = 0; k < nd; ++k)
+    {
+        size_t o = R->blas[k]->ops.size();
+        for (size_t t = 0; t < nthreads; ++t) { off[k * nthreads + t] = o; o += local[t][k].ops.size(); }
+        R->blas[k]->ops.resize(o);
+    }
+    auto copy = [&](size_t t) {
+        for (size_t k = 0; k < nd; ++k)
+            if (!local[t][k].ops.empty())
+                memcpy(R->blas[k]->ops.data() + off[k * nthreads + t], local[t][k].ops.data(), local[t][k].ops.size() * sizeof(HOp));
+    };
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(copy, t);
+    copy(0);
+    for (auto & th : pool) th.join();
+    return true;
+}
+
 // Build every domain's op list for the batch, in the order the reference performs them.
 static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 {
+    if (build_ops_parallel(R, recs, n)) return;
     for (size_t i = 0; i < n;)
     {
         size_t j = i;
@@ -584,19 +715,68 @@ static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 
 // Extend the domain's compression with the batch's boundaries; remap the device state when
 // the cell grid changes.
+// The spill pool: created on first use; grown keeping its chunks (cell states name them by
+// index). reset_spill() rewinds the hand-out counter to the last completed step before a kernel
+// that may run out of chunks and be redone.
+static int spill_reserve(xkb_resolver * R, size_t chunks)
+{
+    if (!R->spill_ctr.p)
+    {
+        int rc = R->spill_ctr.reserve(2);
+        if (rc) return rc;
+        XKB_CUDA_TRY(cudaMemsetAsync(R->spill_ctr.p, 0, 2 * sizeof(unsigned), R->stream));
+    }
+    if (chunks <= R->spill_chunks) return XKB_OK;
+    size_t c = R->spill_chunks ? R->spill_chunks : 65536;
+    while (c < chunks) c *= 2;
+    if (c > 0xffffffffu / 2) return xkb_set_error(XKB_ERANGE, "resolver: reader spill pool exceeds 2^31 chunks");
+    int * q = nullptr;
+    cudaError_t e = cudaMalloc(&q, c * SPILL * sizeof(int));
+    if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    if (R->spill.p && R->spill_used)
+    {
+        e = cudaMemcpyAsync(q, R->spill.p, (size_t) R->spill_used * SPILL * sizeof(int), cudaMemcpyDeviceToDevice, R->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(R->stream);
+        if (e != cudaSuccess) { cudaFree(q); return xkb_set_cuda_error(e); }
+    }
+    if (R->spill.p) cudaFree(R->spill.p);
+    R->spill.p = q; R->spill.cap = c * SPILL; R->spill_chunks = c;
+    return XKB_OK;
+}
+
+static int reset_spill(xkb_resolver * R)
+{
+    const unsigned v[2] = {R->spill_used, 0u};
+    XKB_CUDA_TRY(cudaMemcpyAsync(R->spill_ctr.p, v, sizeof(v), cudaMemcpyHostToDevice, R->stream));
+    XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));   // v is on this stack frame
+    return XKB_OK;
+}
+
+// After a kernel that draws chunks: true (and the pool grown) if it ran out and must be redone;
+// else the chunks it drew become part of the kept state.
+static int spill_check(xkb_resolver * R, bool & redo)
+{
+    unsigned v[2];
+    XKB_CUDA_TRY(cudaMemcpyAsync(v, R->spill_ctr.p, sizeof(v), cudaMemcpyDeviceToHost, R->stream));
+    XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
+    redo = v[1] != 0;
+    if (redo) return spill_reserve(R, (size_t) v[0] + 1);
+    R->spill_used = v[0];
+    return XKB_OK;
+}
+
 static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & xs, std::vector<uint64_t> & ys)
 {
     if (xs.size() < 2 || ys.size() < 2) { d.xs = xs; d.ys = ys; return XKB_OK; }
     const bool same = xs == d.xs && ys == d.ys;
     const size_t ncx = xs.size() - 1, ncy = ys.size() - 1, ncells = ncx * ncy;
-    const size_t stride = 2 + (size_t) R->rcap;
     if (same && d.ncells == ncells) return XKB_OK;
     int rc;
     DevBuf<int> & out = d.state[d.cur ^ 1];
-    if ((rc = out.reserve(ncells * stride))) return rc;
+    if ((rc = out.reserve(ncells * STRIDE))) return rc;
     if (d.ncells == 0)
     {
-        init_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(out.p, ncells, stride);
+        init_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(out.p, ncells);
     }
     else
     {
@@ -616,9 +796,16 @@ static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & x
         if ((rc = dm.reserve(ncx + ncy))) return rc;
         XKB_CUDA_TRY(cudaMemcpyAsync(dm.p, mx.data(), ncx * sizeof(int), cudaMemcpyHostToDevice, R->stream));
         XKB_CUDA_TRY(cudaMemcpyAsync(dm.p + ncx, my.data(), ncy * sizeof(int), cudaMemcpyHostToDevice, R->stream));
-        refine_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(
-            d.state[d.cur].p, out.p, stride, dm.p, dm.p + ncx, (int) ncx, (int) ncy, (int) old_ncx);
-        XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));   // dm is freed on return
+        if ((rc = spill_reserve(R, 1))) return rc;
+        for (bool redo = true; redo;)
+        {
+            if ((rc = reset_spill(R))) return rc;
+            refine_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(
+                d.state[d.cur].p, out.p, dm.p, dm.p + ncx, (int) ncx, (int) ncy, (int) old_ncx, R->spill.p, R->spill_ctr.p,
+                (unsigned) R->spill_chunks);
+            XKB_CUDA_TRY(cudaGetLastError());
+            if ((rc = spill_check(R, redo))) return rc;   // synchronises: dm is freed on return
+        }
     }
     XKB_CUDA_TRY(cudaGetLastError());
     d.cur ^= 1;
@@ -632,7 +819,7 @@ static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & x
 template <int RX, int RY>
 static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
 {
-    const size_t smem = (size_t) R->rcap * RX * RY * sizeof(int);
+    const size_t smem = (size_t) RCAP * RX * RY * sizeof(int);
     cudaStream_t st = R->stream;
     const size_t nb = (size_t) nregions + 1;
     int rc;
@@ -681,9 +868,8 @@ static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t 
     a.ops = R->dops.p + op_offset; a.nops = (int) nops;
     a.ncx = ncx; a.ncy = ncy;
     a.state_in = d.state[d.cur].p; a.state_out = d.state[d.cur ^ 1].p;
-    a.rcap = R->rcap;
     a.emit = R->emit.p; a.emit_count = R->counters.p; a.emit_cap = R->emit.cap;
-    a.max_readers = R->maxr.p;
+    a.spill = R->spill.p; a.spill_ctr = R->spill_ctr.p; a.spill_cap = (unsigned) R->spill_chunks;
     if (ncy == 1)
     {
         constexpr int RX = 64, RY = 1;
@@ -763,71 +949,39 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
     R->last_ops_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     R->last_compress_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
 
-    size_t emit_guess = std::max<size_t>(1 << 16, total * 2);
-    for (int attempt = 0; attempt < 6; ++attempt)
+    static const bool trace = getenv("XKB_TRACE_RESOLVE") != nullptr;
+    const size_t realloc0 = g_realloc_bytes;
+    size_t emit_guess = std::max<size_t>(1 << 16, total * 8);
+    for (int attempt = 0; attempt < 16; ++attempt)
     {
+        const auto ta = clk::now();
         if ((rc = R->emit.reserve(emit_guess))) return rc;
         if ((rc = R->counters.reserve(2))) return rc;
-        if ((rc = R->maxr.reserve(1))) return rc;
+        if ((rc = spill_reserve(R, 1)) || (rc = reset_spill(R))) return rc;
         XKB_CUDA_TRY(cudaMemsetAsync(R->counters.p, 0, 2 * sizeof(unsigned long long), R->stream));
-        XKB_CUDA_TRY(cudaMemsetAsync(R->maxr.p, 0, sizeof(int), R->stream));
         for (size_t k = 0; k < doms.size(); ++k)
         {
             const size_t nops = doms[k]->ops.size();
             // states must exist for every cell (ncells > 0 when the domain has >= 1 op)
             if ((rc = R->emit.reserve(emit_guess))) return rc;
             if (doms[k]->ncells == 0) continue;
-            if ((rc = doms[k]->state[doms[k]->cur ^ 1].reserve(doms[k]->ncells * (2 + (size_t) R->rcap)))) return rc;
+            if ((rc = doms[k]->state[doms[k]->cur ^ 1].reserve(doms[k]->ncells * STRIDE))) return rc;
             if ((rc = launch_domain(R, *doms[k], offs[k], nops))) return rc;
         }
         unsigned long long nemit = 0;
-        int maxr = 0;
+        unsigned sp[2] = {0, 0};
         XKB_CUDA_TRY(cudaMemcpyAsync(&nemit, R->counters.p, sizeof(nemit), cudaMemcpyDeviceToHost, R->stream));
-        XKB_CUDA_TRY(cudaMemcpyAsync(&maxr, R->maxr.p, sizeof(int), cudaMemcpyDeviceToHost, R->stream));
+        XKB_CUDA_TRY(cudaMemcpyAsync(sp, R->spill_ctr.p, sizeof(sp), cudaMemcpyDeviceToHost, R->stream));
         XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
-        if (maxr > R->rcap)
+        if (sp[1])
         {
-            // a cell held more readers than the state keeps: widen the state and redo the batch
-            int newcap = R->rcap;
-            while (newcap < maxr) newcap *= 2;
-            if ((size_t) newcap * 64 * sizeof(int) > 200 * 1024)
-                return xkb_set_error(XKB_ERANGE, "resolver: %d concurrent readers of one cell exceed the supported maximum", maxr);
-            for (Domain * d : doms) {
-                // re-layout the current state with the wider stride
-                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
-                std::vector<int> h(ncells * so);
-                if (ncells) XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
-                std::vector<int> g(ncells * sn, 0);
-                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
-                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
-                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
-                if (ncells) XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
-            }
-            for (auto & d : R->blas) if (d->ops.empty() && d->ncells) {
-                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
-                std::vector<int> h(ncells * so);
-                XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
-                std::vector<int> g(ncells * sn, 0);
-                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
-                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
-                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
-                XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
-            }
-            if (R->interval.ops.empty() && R->interval.ncells) {
-                Domain * d = &R->interval;
-                const size_t ncells = d->ncells, so = 2 + (size_t) R->rcap, sn = 2 + (size_t) newcap;
-                std::vector<int> h(ncells * so);
-                XKB_CUDA_TRY(cudaMemcpy(h.data(), d->state[d->cur].p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
-                std::vector<int> g(ncells * sn, 0);
-                for (size_t c = 0; c < ncells; ++c) memcpy(&g[c * sn], &h[c * so], so * sizeof(int));
-                if ((rc = d->state[d->cur].reserve(g.size()))) return rc;
-                if ((rc = d->state[d->cur ^ 1].reserve(g.size()))) return rc;
-                XKB_CUDA_TRY(cudaMemcpy(d->state[d->cur].p, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
-            }
-            R->rcap = newcap;
+            // the reader spill pool ran out: grow it (keeping its chunks) and redo the batch
+            if ((rc = spill_reserve(R, (size_t) sp[0] + 1))) return rc;
             continue;
         }
+        const auto tb = clk::now();
         if (nemit > R->emit.cap) { emit_guess = (size_t) nemit; continue; }
+        R->spill_used = sp[0];
 
         // success: unique the emitted pairs into the accumulated edge list
         if (nemit)
@@ -835,19 +989,32 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
             size_t tcap = 1024;
             while (tcap < 2 * nemit) tcap *= 2;
             if ((rc = R->table.reserve(tcap))) return rc;
-            if ((rc = R->uniq.grow_keep(R->nuniq + nemit, R->nuniq, R->stream))) return rc;
+            if (R->useg.empty() || R->useg.back()->cap - R->useg_n.back() < nemit)
+            {
+                std::unique_ptr<DevBuf<unsigned long long>> seg(new (std::nothrow) DevBuf<unsigned long long>());
+                if (!seg) return xkb_set_error(XKB_ENOMEM, "resolver: out of host memory");
+                if ((rc = seg->reserve(std::max<size_t>((size_t) nemit, size_t(1) << 24)))) return rc;
+                R->useg.push_back(std::move(seg));
+                R->useg_n.push_back(0);
+            }
+            DevBuf<unsigned long long> & seg = *R->useg.back();
             XKB_CUDA_TRY(cudaMemsetAsync(R->table.p, 0xff, tcap * sizeof(unsigned long long), R->stream));
-            unsigned long long nu0 = R->nuniq;
+            unsigned long long nu0 = R->useg_n.back();
             XKB_CUDA_TRY(cudaMemcpyAsync(R->counters.p + 1, &nu0, sizeof(nu0), cudaMemcpyHostToDevice, R->stream));
             dedupe_kernel<<<(unsigned) ((nemit + 255) / 256), 256, 0, R->stream>>>(R->emit.p, nemit, R->table.p, tcap - 1,
-                                                                                 R->uniq.p, R->counters.p + 1, R->uniq.cap);
+                                                                                 seg.p, R->counters.p + 1, seg.cap);
             XKB_CUDA_TRY(cudaGetLastError());
             unsigned long long nu = 0;
             XKB_CUDA_TRY(cudaMemcpyAsync(&nu, R->counters.p + 1, sizeof(nu), cudaMemcpyDeviceToHost, R->stream));
             XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
-            R->nuniq = nu;
+            R->nuniq += nu - nu0;
+            R->useg_n.back() = nu;
         }
         for (Domain * d : doms) { d->cur ^= 1; d->ops.clear(); }
+        if (trace)
+            fprintf(stderr, "resolver batch: %zu ops, attempt %d, regions %.1f ms, dedupe %.1f ms, %llu emitted, %.1f MB allocated\n",
+                    total, attempt, std::chrono::duration<double, std::milli>(tb - ta).count(),
+                    std::chrono::duration<double, std::milli>(clk::now() - tb).count(), nemit, (g_realloc_bytes - realloc0) / 1e6);
         return XKB_OK;
     }
     return xkb_set_error(XKB_ERANGE, "resolver: batch did not fit after resizing");
@@ -864,10 +1031,16 @@ static int build_graph(xkb_resolver * R)
     cudaStream_t st = R->stream;
     XKB_CUDA_TRY(cudaMemsetAsync(R->succ_ptr.p, 0, (nt + 1) * sizeof(uint32_t), st));
     XKB_CUDA_TRY(cudaMemsetAsync(R->npred.p, 0, (nt + 1) * sizeof(uint32_t), st));
-    if (ne) count_edges_kernel<<<(unsigned) ((ne + 255) / 256), 256, 0, st>>>(R->uniq.p, ne, R->succ_ptr.p, R->npred.p);
+    for (size_t k = 0; k < R->useg.size(); ++k)
+        if (R->useg_n[k])
+            count_edges_kernel<<<(unsigned) ((R->useg_n[k] + 255) / 256), 256, 0, st>>>(R->useg[k]->p, R->useg_n[k], R->succ_ptr.p,
+                                                                                       R->npred.p);
     if ((rc = device_exclusive_scan(R->succ_ptr.p, R->succ_ptr.p, nt + 1, R->tmp.p + nt + 1, nullptr, st))) return rc;
     XKB_CUDA_TRY(cudaMemcpyAsync(R->tmp.p, R->succ_ptr.p, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    if (ne) scatter_edges_kernel<<<(unsigned) ((ne + 255) / 256), 256, 0, st>>>(R->uniq.p, ne, R->tmp.p, R->succ.p);
+    for (size_t k = 0; k < R->useg.size(); ++k)
+        if (R->useg_n[k])
+            scatter_edges_kernel<<<(unsigned) ((R->useg_n[k] + 255) / 256), 256, 0, st>>>(R->useg[k]->p, R->useg_n[k], R->tmp.p,
+                                                                                         R->succ.p);
     if (nt) sort_segments_kernel<<<(unsigned) ((nt + 255) / 256), 256, 0, st>>>(R->succ_ptr.p, R->succ.p, (uint32_t) nt);
     XKB_CUDA_TRY(cudaGetLastError());
     XKB_CUDA_TRY(cudaStreamSynchronize(st));

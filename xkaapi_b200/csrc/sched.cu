@@ -282,7 +282,8 @@ using namespace xkb;
 
 struct xkb_sched {
     cudaStream_t stream = nullptr;
-    std::vector<xkb_task_desc_t> host_tasks;
+    std::vector<xkb_task_desc_t> host_tasks;  // host copy for the per-task forms (empty: device only)
+    size_t ntasks = 0;                        // descriptors set
     Dev<xkb_task_desc_t> tasks;
     Dev<int> wc, queue;
     Dev<unsigned> ctr;
@@ -357,6 +358,25 @@ extern "C" int xkb_sched_set_tasks(xkb_sched_t * S, const xkb_task_desc_t * task
     int rc = check_tasks(tasks, ntasks);
     if (rc) return rc;
     S->host_tasks.assign(tasks, tasks + ntasks);
+    S->ntasks = ntasks;
+    if ((rc = S->tasks.reserve(ntasks ? ntasks : 1))) return rc;
+    if (ntasks) XKB_CUDA_TRY(cudaMemcpyAsync(S->tasks.p, tasks, ntasks * sizeof(xkb_task_desc_t), cudaMemcpyHostToDevice, S->stream));
+    XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    if (S->gexec) { cudaGraphExecDestroy(S->gexec); S->gexec = nullptr; }
+    if (S->graph) { cudaGraphDestroy(S->graph); S->graph = nullptr; }
+    S->graph_key = nullptr;
+    return XKB_OK;
+}
+
+// Library-internal: the descriptors go to the device only (no host copy, so only the persistent
+// forms can run them); for callers that hand over millions of descriptors for one run.
+int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks)
+{
+    if (!S || (ntasks && !tasks)) return xkb_set_error(XKB_EINVAL, "sched_set_tasks: bad arguments");
+    int rc = check_tasks(tasks, ntasks);
+    if (rc) return rc;
+    S->host_tasks.clear(); S->host_tasks.shrink_to_fit();
+    S->ntasks = ntasks;
     if ((rc = S->tasks.reserve(ntasks ? ntasks : 1))) return rc;
     if (ntasks) XKB_CUDA_TRY(cudaMemcpyAsync(S->tasks.p, tasks, ntasks * sizeof(xkb_task_desc_t), cudaMemcpyHostToDevice, S->stream));
     XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
@@ -486,9 +506,11 @@ static int build_cuda_graph(xkb_sched * S, const xkb_task_graph_t * g)
 extern "C" int xkb_sched_run(xkb_sched_t * S, const xkb_task_graph_t * g, int form)
 {
     if (!S || !g) return xkb_set_error(XKB_EINVAL, "sched_run: bad arguments");
-    if (g->ntasks != S->host_tasks.size())
+    if (g->ntasks != S->ntasks)
         return xkb_set_error(XKB_EINVAL, "sched_run: graph has %llu tasks, %zu descriptors set",
-                             (unsigned long long) g->ntasks, S->host_tasks.size());
+                             (unsigned long long) g->ntasks, S->ntasks);
+    if (form != XKB_FORM_PERSISTENT && S->host_tasks.size() != S->ntasks)
+        return xkb_set_error(XKB_EINVAL, "sched_run: the descriptors were set for the persistent form only");
     S->last_form = form;
     S->last_total = g->ntasks;
     switch (form)
@@ -507,9 +529,9 @@ extern "C" int xkb_sched_run_periodic(xkb_sched_t * S, const xkb_periodic_graph_
 {
     if (!S || !g || repeats == 0 || tail == 0 || tail > g->period)
         return xkb_set_error(XKB_EINVAL, "sched_run_periodic: bad arguments");
-    if (g->period != S->host_tasks.size())
+    if (g->period != S->ntasks)
         return xkb_set_error(XKB_EINVAL, "sched_run_periodic: period %llu but %zu descriptors set",
-                             (unsigned long long) g->period, S->host_tasks.size());
+                             (unsigned long long) g->period, S->ntasks);
     const uint64_t total = (uint64_t) (repeats - 1) * g->period + tail;
     if (total >= (1ull << 31)) return xkb_set_error(XKB_ERANGE, "sched_run_periodic: %llu tasks in one run", (unsigned long long) total);
     int rc;

@@ -12,14 +12,23 @@
 // (a topological order). Host memory is coherent again when xkrt_task_wait returns.
 #include "common.cuh"
 #include "internal.h"
+#include "pool.h"
 #include "../../include/xkrt_capi.h"
 
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <new>
+#include <thread>
 #include <string>
 #include <vector>
+
+struct xkb_runtime;
 
 namespace {
 
@@ -30,12 +39,15 @@ struct Format {
     int builtin = -1;                     // XKB_TASK_* for built-in device bodies
 };
 
+// A spawned task. Tasks, their arguments, accesses and replica pointers live in the runtime's
+// pools (one mapping per pool, not one allocation per task); the pools only grow during spawns,
+// so their addresses are stable while bodies run.
 struct Task {
+    ::xkb_runtime * rt = nullptr;
     uint8_t fmtid = 0, flags = 0;
     xkrt_device_global_id_t device = 0;
-    std::vector<uint8_t> args;
-    std::vector<xkrt_access_t> acc;
-    std::vector<void *> replica;
+    uint32_t nargs = 0, nacc = 0;
+    size_t args_off = 0, acc_off = 0;
     xkrt_task_func_t func = nullptr;      // team / plain function spawns
     void * user_data = nullptr;
 };
@@ -47,7 +59,14 @@ struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; };
 struct xkb_runtime {
     Format formats[256];
     int next_fmtid = 1;
-    std::vector<std::unique_ptr<Task>> pending;
+    xkb::PoolArray<Task> pending;                     // bodies get Task *
+    xkb::PoolArray<uint8_t> args_pool;                // argument bytes, 16-byte aligned per task
+    xkb::PoolArray<xkrt_access_t> acc_pool;
+    xkb::PoolArray<void *> replica_pool;              // sized to acc_pool at wait
+    xkb::PoolArray<xkb_access_rec_t> recs;            // one record per access, same index (wait)
+    bool in_wait = false;
+    uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
+    uint8_t * last_mirror = nullptr;
     std::map<uint64_t, Region> regions;               // host base -> region
     xkb_planner_t * planner = nullptr;
     xkb_sched_t * sched = nullptr;
@@ -56,6 +75,7 @@ struct xkb_runtime {
     int status = XKB_OK;
     uint64_t last_tasks = 0, last_edges = 0, last_h2d = 0, last_d2h = 0;
     int last_fused = 0;
+    double last_ms[4] = {0, 0, 0, 0};                 // resolve, coherency + launch prep, run, write-back
     int dummy_team = 0;
 };
 
@@ -106,7 +126,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
 extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
-    if (R) R->pending.clear();
+    if (R) { R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear(); }
 }
 
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned)
@@ -233,14 +253,21 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
     for (size_t i = 0; i < nacc; ++i)
         if (acc[i].type == ACCESS_TYPE_HANDLE)
         { fail(R, xkb_set_error(XKB_EINVAL, "spawn: handle accesses are not supported")); return; }
-    std::unique_ptr<Task> t(new (std::nothrow) Task());
-    if (!t) { fail(R, XKB_ENOMEM); return; }
-    t->fmtid = fmtid; t->flags = flags; t->device = device;
-    if (args_size) t->args.assign((const uint8_t *) args, (const uint8_t *) args + args_size);
-    t->acc.assign(acc, acc + nacc);
-    t->replica.assign(nacc, nullptr);
-    t->func = func; t->user_data = ud;
-    R->pending.push_back(std::move(t));
+    if (args_size && !args) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null arguments")); return; }
+    if (R->in_wait) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: spawning from a task body during xkrt_task_wait is not supported")); return; }
+    Task t;
+    t.rt = R; t.fmtid = fmtid; t.flags = flags; t.device = device;
+    t.nargs = (uint32_t) args_size; t.nacc = (uint32_t) nacc;
+    t.args_off = (R->args_pool.size() + 15) & ~(size_t) 15;
+    t.acc_off = R->acc_pool.size();
+    t.func = func; t.user_data = ud;
+    const size_t args_end = args_size ? t.args_off + args_size : R->args_pool.size();
+    if (!R->args_pool.resize(args_end) || !R->acc_pool.append(acc, nacc) || !R->pending.push_back(t))
+    {
+        fail(R, xkb_set_error(XKB_ENOMEM, "spawn: out of host memory"));
+        return;
+    }
+    if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
 }
 
 extern "C" void xkrt_task_spawn_generic(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
@@ -299,17 +326,25 @@ extern "C" void xkrt_team_task_spawn_with_accesses(xkrt_runtime_t * runtime, xkr
 
 // ---- task accessors --------------------------------------------------------------------------
 
-extern "C" void * xkrt_task_args(xkrt_task_t * task) { Task * t = (Task *) task; return t && !t->args.empty() ? t->args.data() : nullptr; }
-extern "C" xkrt_access_t * xkrt_task_accesses(xkrt_task_t * task) { Task * t = (Task *) task; return t && !t->acc.empty() ? t->acc.data() : nullptr; }
+extern "C" void * xkrt_task_args(xkrt_task_t * task)
+{
+    Task * t = (Task *) task;
+    return t && t->nargs ? t->rt->args_pool.data() + t->args_off : nullptr;
+}
+extern "C" xkrt_access_t * xkrt_task_accesses(xkrt_task_t * task)
+{
+    Task * t = (Task *) task;
+    return t && t->nacc ? t->rt->acc_pool.data() + t->acc_off : nullptr;
+}
 extern "C" xkrt_access_t * xkrt_task_access(xkrt_task_t * task, xkrt_task_access_counter_type_t i)
 {
     Task * t = (Task *) task;
-    return t && i < t->acc.size() ? &t->acc[i] : nullptr;
+    return t && i < t->nacc ? t->rt->acc_pool.data() + t->acc_off + i : nullptr;
 }
 extern "C" void * xkrt_task_access_replica(xkrt_task_t * task, xkrt_task_access_counter_type_t i)
 {
     Task * t = (Task *) task;
-    return t && i < t->replica.size() ? t->replica[i] : nullptr;
+    return t && i < t->nacc && t->acc_off + i < t->rt->replica_pool.size() ? t->rt->replica_pool[t->acc_off + i] : nullptr;
 }
 
 // ---- wait --------------------------------------------------------------------------------------
@@ -342,10 +377,12 @@ static bool is_device(const xkb_runtime * R, const Task & t)
 
 static void * mirror_of(xkb_runtime * R, uint64_t host)
 {
+    if (host >= R->last_base && host < R->last_end) return R->last_mirror + (host - R->last_base);   // same region as last time
     auto it = R->regions.upper_bound(host);
     if (it == R->regions.begin()) return nullptr;
     --it;
     if (host >= it->first + it->second.size || !it->second.mirror) return nullptr;
+    R->last_base = it->first; R->last_end = it->first + it->second.size; R->last_mirror = (uint8_t *) it->second.mirror;
     return (uint8_t *) it->second.mirror + (host - it->first);
 }
 
@@ -380,90 +417,255 @@ static int translate(xkb_runtime * R, xkb_task_desc_t & d)
     return XKB_OK;
 }
 
+constexpr uint8_t REC_NONE = 0xff;                     // record type of an untracked access
+
+// fn(begin, end) over [0, n) in contiguous chunks on up to 16 host threads (inline when small)
+template <typename F>
+static void parallel_chunks(size_t n, F fn)
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nth = std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536));
+    if (nth < 2) { fn(0, n); return; }
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < nth; ++k) pool.emplace_back(fn, n * k / nth, n * (k + 1) / nth);
+    fn(0, n / nth);
+    for (auto & th : pool) th.join();
+}
+
+// Records that name the same bytes in the same mode: fetching them again to the same device is a
+// no-op (a device fetch never invalidates the device's copy of other data), so batches whose
+// fetches all go one way fetch each distinct record once. The set grows with the number of
+// DISTINCT records (a few per tile for a stencil), so it stays in cache however long the batch.
+class RecordSet {
+public:
+    RecordSet() : slot_(1024, UINT32_MAX) {}
+    // true if r (task id ignored) was not in the set; it is now
+    bool insert(const xkb_access_rec_t * recs, uint32_t i)
+    {
+        if (2 * (used_ + 1) > slot_.size()) rehash(recs);
+        const size_t mask = slot_.size() - 1;
+        size_t h = key_hash(recs[i]) & mask;
+        while (slot_[h] != UINT32_MAX)
+        {
+            if (same(recs[slot_[h]], recs[i])) return false;
+            h = (h + 1) & mask;
+        }
+        slot_[h] = i;
+        ++used_;
+        return true;
+    }
+private:
+    void rehash(const xkb_access_rec_t * recs)
+    {
+        std::vector<uint32_t> old(2 * slot_.size(), UINT32_MAX);
+        old.swap(slot_);
+        const size_t mask = slot_.size() - 1;
+        for (uint32_t i : old)
+            if (i != UINT32_MAX)
+            {
+                size_t h = key_hash(recs[i]) & mask;
+                while (slot_[h] != UINT32_MAX) h = (h + 1) & mask;
+                slot_[h] = i;
+            }
+    }
+    static uint64_t mix(uint64_t h, uint64_t v) { h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2); return h; }
+    static uint64_t key_hash(const xkb_access_rec_t & r)
+    {
+        uint64_t h = ((uint64_t) r.type << 8) | r.mode;
+        for (uint64_t v : {r.addr, r.ld, r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type}) h = mix(h, v);
+        return h * 0xff51afd7ed558ccdull;
+    }
+    static bool same(const xkb_access_rec_t & a, const xkb_access_rec_t & b)
+    {
+        return a.type == b.type && a.mode == b.mode && a.addr == b.addr && a.ld == b.ld && a.offset_m == b.offset_m &&
+               a.offset_n == b.offset_n && a.m == b.m && a.n == b.n && a.sizeof_type == b.sizeof_type;
+    }
+    std::vector<uint32_t> slot_;
+    size_t used_ = 0;
+};
+
+// Indices of the first occurrence of every distinct record among those `keep` accepts, in
+// record order. Chunks of records are scanned on host threads, each keeping its own first
+// occurrences; merging the chunks' lists in chunk order keeps the global first occurrences.
+template <typename Keep>
+static std::vector<uint32_t> distinct_records(const xkb_access_rec_t * recs, size_t n, Keep keep)
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nth = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536)));
+    std::vector<std::vector<uint32_t>> firsts(nth);
+    auto scan = [&](size_t k) {
+        RecordSet seen;
+        for (size_t i = n * k / nth; i < n * (k + 1) / nth; ++i)
+            if (keep(i) && seen.insert(recs, (uint32_t) i)) firsts[k].push_back((uint32_t) i);
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < nth; ++k) pool.emplace_back(scan, k);
+    scan(0);
+    for (auto & th : pool) th.join();
+    if (nth == 1) return std::move(firsts[0]);
+    std::vector<uint32_t> out;
+    RecordSet seen;
+    for (auto & f : firsts)
+        for (uint32_t i : f)
+            if (seen.insert(recs, i)) out.push_back(i);
+    return out;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Records per resolver batch: the resolver's working set grows with the batch, and batches of
+// about a million accesses keep it small while amortising each batch's fixed costs.
+constexpr size_t RESOLVE_CHUNK = size_t(1) << 20;
+
 static int wait_batch(xkb_runtime * R)
 {
     R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
+    for (double & m : R->last_ms) m = 0;
     if (R->pending.empty()) return XKB_OK;
     if (!R->gpu) return xkb_set_error(XKB_ENODEV, "xkrt_task_wait: dependency resolution runs on the GPU and none is visible");
-    // (1) dependencies
-    std::vector<xkb_access_rec_t> recs;
-    std::vector<std::pair<size_t, size_t>> rec_of;      // (task, access) of every record
-    for (size_t t = 0; t < R->pending.size(); ++t)
-        for (size_t a = 0; a < R->pending[t]->acc.size(); ++a)
+    auto t0 = std::chrono::steady_clock::now();
+    // (1) dependencies. One record per access, at the access's own index (type REC_NONE when
+    // the access names nothing the runtime tracks). The resolver is fed these records directly
+    // when every task has one; otherwise a compacted copy where a task without any gets a
+    // one-byte virtual read of its own Task object (nothing else touches it), so that the task
+    // numbering stays dense.
+    const size_t nacc = R->acc_pool.size(), ntasks = R->pending.size();
+    if (!R->replica_pool.resize(nacc) || !R->recs.resize(nacc)) return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
+    if (nacc) memset(R->replica_pool.data(), 0, nacc * sizeof(void *));
+    xkb_access_rec_t * recs = R->recs.data();
+    std::atomic<bool> dense(true);
+    parallel_chunks(ntasks, [&](size_t b, size_t e) {
+        bool d = true;
+        for (size_t t = b; t < e; ++t)
         {
-            xkb_access_rec_t r;
-            if (to_rec(R->pending[t]->acc[a], (uint32_t) t, r)) { recs.push_back(r); rec_of.push_back({t, a}); }
-        }
-    xkb_resolver_t * res = nullptr;
-    int rc = xkb_resolver_create(&res, R->stream);
-    if (rc) return rc;
-    // every task needs a record for the task numbering to stay dense: a task without data
-    // accesses gets a zero-byte stand-in? -- no: give it a one-byte virtual read of its own
-    // descriptor, which nothing else touches
-    std::vector<xkb_access_rec_t> all;
-    {
-        size_t k = 0;
-        for (size_t t = 0; t < R->pending.size(); ++t)
-        {
+            const Task & T = R->pending[t];
             bool any = false;
-            while (k < recs.size() && recs[k].task == t) { all.push_back(recs[k++]); any = true; }
+            for (uint32_t a = 0; a < T.nacc; ++a)
+            {
+                xkb_access_rec_t & r = recs[T.acc_off + a];
+                if (to_rec(R->acc_pool[T.acc_off + a], (uint32_t) t, r)) any = true;
+                else { r.type = REC_NONE; d = false; }
+            }
+            d = d && any;
+        }
+        if (!d) dense = false;
+    });
+    std::vector<xkb_access_rec_t> all;
+    if (!dense)
+    {
+        all.reserve(nacc + 16);
+        for (size_t t = 0; t < ntasks; ++t)
+        {
+            const Task & T = R->pending[t];
+            bool any = false;
+            for (uint32_t a = 0; a < T.nacc; ++a)
+                if (recs[T.acc_off + a].type != REC_NONE) { all.push_back(recs[T.acc_off + a]); any = true; }
             if (!any)
             {
                 xkb_access_rec_t r;
                 memset(&r, 0, sizeof(r));
                 r.task = (uint32_t) t; r.type = XKB_ACCESS_TYPE_SEGMENT; r.mode = XKB_ACCESS_MODE_R | XKB_ACCESS_MODE_V;
-                r.addr = (uint64_t) R->pending[t].get(); r.ld = r.addr + 1;
+                r.addr = (uint64_t) &R->pending[t]; r.ld = r.addr + 1;
                 all.push_back(r);
             }
         }
     }
-    rc = xkb_resolver_add(res, all.data(), all.size());
+    const xkb_access_rec_t * feed = dense ? recs : all.data();
+    const size_t nfeed = dense ? nacc : all.size();
+    const double records_ms = ms_since(t0);
+    xkb_resolver_t * res = nullptr;
+    int rc = xkb_resolver_create(&res, R->stream);
+    if (rc) return rc;
+    for (size_t b = 0; b < nfeed && rc == XKB_OK;)
+    {
+        size_t e = std::min(nfeed, b + RESOLVE_CHUNK);
+        while (e < nfeed && feed[e].task == feed[e - 1].task) ++e;     // whole tasks per batch
+        rc = xkb_resolver_add(res, feed + b, e - b);
+        b = e;
+    }
+    all.clear(); all.shrink_to_fit();
     xkb_task_graph_t g;
     if (rc == XKB_OK) rc = xkb_resolver_graph(res, &g);
     if (rc) { xkb_resolver_destroy(res); return rc; }
     R->last_edges = g.nedges;
+    R->last_ms[0] = ms_since(t0);
+    if (getenv("XKB_TRACE_WAIT"))
+        fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms\n", nacc, records_ms, R->last_ms[0] - records_ms);
 
     bool fused = true;
-    for (auto & t : R->pending) if (!is_device(R, *t) || R->formats[t->fmtid].builtin < 0) { fused = false; break; }
+    for (size_t t = 0; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
 
     if (fused)
     {
         // (2) every access made coherent on the device up front: with no host task in the batch
         // the host data cannot change meanwhile, so the first-touch copies can all go first
-        for (size_t k = 0; k < recs.size(); ++k)
-            if ((rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) rec_of[k].second, 1, nullptr))) break;
-        if (rc == XKB_OK) rc = run_copies(R);
-        std::vector<xkb_task_desc_t> descs(R->pending.size());
-        for (size_t t = 0; t < R->pending.size() && rc == XKB_OK; ++t)
+        t0 = std::chrono::steady_clock::now();
         {
-            if (R->pending[t]->args.size() < sizeof(xkb_task_desc_t)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
-            memcpy(&descs[t], R->pending[t]->args.data(), sizeof(xkb_task_desc_t));
-            descs[t].kind = (uint32_t) R->formats[R->pending[t]->fmtid].builtin;
+            const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) { return recs[k].type != REC_NONE; });
+            for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j)
+            {
+                const uint32_t k = first[j];
+                rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
+            }
+        }
+        if (rc == XKB_OK) rc = run_copies(R);
+        const double fetch_ms = ms_since(t0);
+        // the descriptors: when every task's args are exactly one descriptor, the args pool is
+        // already the descriptor array (16-byte aligned 64-byte entries back to back) and is
+        // rewritten in place (nothing reads these args after a fused batch)
+        const size_t nt = R->pending.size();
+        bool dense_args = true;
+        for (size_t t = 0; t < nt && dense_args; ++t)
+            dense_args = R->pending[t].nargs == sizeof(xkb_task_desc_t) && R->pending[t].args_off == t * sizeof(xkb_task_desc_t);
+        std::vector<xkb_task_desc_t> copy;
+        xkb_task_desc_t * descs = (xkb_task_desc_t *) R->args_pool.data();
+        if (!dense_args) { copy.resize(nt); descs = copy.data(); }
+        for (size_t t = 0; t < nt && rc == XKB_OK; ++t)
+        {
+            const Task & T = R->pending[t];
+            if (!dense_args)
+            {
+                if (T.nargs < sizeof(xkb_task_desc_t)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
+                memcpy(&descs[t], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
+            }
+            descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
             rc = translate(R, descs[t]);
         }
-        if (rc == XKB_OK) rc = xkb_sched_set_tasks(R->sched, descs.data(), descs.size());
+        const double desc_ms = ms_since(t0) - fetch_ms;
+        if (rc == XKB_OK) rc = xkb_internal_sched_set_tasks_device(R->sched, descs, nt);
+        if (getenv("XKB_TRACE_WAIT"))
+            fprintf(stderr, "xkrt_task_wait: fetches + copies %.1f ms, descriptors %.1f ms, upload %.1f ms\n", fetch_ms, desc_ms,
+                    ms_since(t0) - fetch_ms - desc_ms);
+        if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
+        R->last_ms[1] = ms_since(t0);
+        t0 = std::chrono::steady_clock::now();
         if (rc == XKB_OK) rc = xkb_sched_run(R->sched, &g, XKB_FORM_PERSISTENT);
         uint64_t ran = 0;
         if (rc == XKB_OK) rc = xkb_sched_wait(R->sched, &ran);
+        R->last_ms[2] = ms_since(t0);
         R->last_fused = 1;
     }
     else
     {
         // (3) task by task in spawn order
-        size_t k = 0;
+        t0 = std::chrono::steady_clock::now();
         for (size_t t = 0; t < R->pending.size() && rc == XKB_OK; ++t)
         {
-            Task & T = *R->pending[t];
+            Task & T = R->pending[t];
             const bool dev = is_device(R, T);
-            for (; k < recs.size() && rec_of[k].first == t; ++k)
+            for (uint32_t a = 0; a < T.nacc; ++a)
             {
-                const uint64_t begin = recs[k].type == XKB_ACCESS_TYPE_SEGMENT ? recs[k].addr
-                                     : recs[k].addr + (recs[k].offset_n * recs[k].ld + recs[k].offset_m) * recs[k].sizeof_type;
-                T.replica[rec_of[k].second] = dev ? mirror_of(R, begin) : (void *) begin;
+                const xkb_access_rec_t & r = recs[T.acc_off + a];
+                if (r.type == REC_NONE) continue;
+                const uint64_t begin = r.type == XKB_ACCESS_TYPE_SEGMENT ? r.addr : r.addr + (r.offset_n * r.ld + r.offset_m) * r.sizeof_type;
+                R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
                 // a host task on memory no region covers: that memory never has a device copy
                 if (!dev && !mirror_of(R, begin)) continue;
                 xkb_view_t v;
-                if ((rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) rec_of[k].second, dev ? 1 : 0, &v))) break;
+                if ((rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v))) break;
             }
             if (rc) break;
             if ((rc = run_copies(R))) break;
@@ -473,8 +675,8 @@ static int wait_batch(xkb_runtime * R)
                 if (f.builtin >= 0)
                 {
                     xkb_task_desc_t d;
-                    if (T.args.size() < sizeof(d)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
-                    memcpy(&d, T.args.data(), sizeof(d));
+                    if (T.nargs < sizeof(d)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
+                    memcpy(&d, R->args_pool.data() + T.args_off, sizeof(d));
                     d.kind = (uint32_t) f.builtin;
                     if ((rc = translate(R, d)) || (rc = xkb_internal_launch_task(&d, R->stream))) break;
                 }
@@ -492,28 +694,50 @@ static int wait_batch(xkb_runtime * R)
                 else if (T.fmtid) { rc = xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t); break; }
             }
         }
+        if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
+        R->last_ms[2] = ms_since(t0);
     }
-    // (4) host memory coherent again: read back every block a device task wrote
+    // (4) host memory coherent again: read back every block a device task wrote (every fetch
+    // here goes to the host, so each distinct record is fetched once)
     if (rc == XKB_OK)
     {
-        for (size_t k = 0; k < recs.size() && rc == XKB_OK; ++k)
-            if ((recs[k].mode & XKB_ACCESS_MODE_W) && is_device(R, *R->pending[rec_of[k].first]))
-            {
-                xkb_access_rec_t r = recs[k];
-                r.mode = XKB_ACCESS_MODE_R;
-                rc = xkb_planner_fetch(R->planner, &r, 0, 0, nullptr);
-            }
+        t0 = std::chrono::steady_clock::now();
+        // the blocks device tasks wrote, as reads (records rewritten in place: unused after this)
+        const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
+            if (recs[k].type == REC_NONE || !(recs[k].mode & XKB_ACCESS_MODE_W) || !is_device(R, R->pending[recs[k].task])) return false;
+            recs[k].mode = XKB_ACCESS_MODE_R;
+            return true;
+        });
+        for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j) rc = xkb_planner_fetch(R->planner, &recs[first[j]], 0, 0, nullptr);
+        const double fetch_ms = ms_since(t0);
         if (rc == XKB_OK) rc = run_copies(R);
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
+        R->last_ms[3] = ms_since(t0);
+        if (getenv("XKB_TRACE_WAIT"))
+            fprintf(stderr, "xkrt_task_wait: write-back fetches %.1f ms, copies %.1f ms\n", fetch_ms, R->last_ms[3] - fetch_ms);
     }
     xkb_resolver_destroy(res);
     return rc;
+}
+
+extern "C" int xkb_runtime_last_wait_times(xkrt_runtime_t * runtime, double * resolve_ms, double * coherency_ms, double * run_ms,
+                                           double * writeback_ms)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R) return xkb_set_error(XKB_EINVAL, "xkb_runtime_last_wait_times: null runtime");
+    if (resolve_ms) *resolve_ms = R->last_ms[0];
+    if (coherency_ms) *coherency_ms = R->last_ms[1];
+    if (run_ms) *run_ms = R->last_ms[2];
+    if (writeback_ms) *writeback_ms = R->last_ms[3];
+    return XKB_OK;
 }
 
 extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
     if (!R) return;
+    R->in_wait = true;
     fail(R, wait_batch(R));
-    R->pending.clear();
+    R->in_wait = false;
+    R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
 }
