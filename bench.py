@@ -6,6 +6,11 @@ destination tile), 500 double-buffered steps = 8,192,000 tile tasks -- dependenc
 the GPU resolver, executed by the persistent device scheduler. One bench "step" = one
 execution of the whole 500-step graph. Metric: tasks/s (whole job, all ranks).
 
+e2e: the same graph through the drop-in XKRT C API (xkaapi_b200/examples/heat_xkrt): every bench
+step spawns the 8,192,000 tasks with their accesses and calls xkrt_task_wait, which resolves the
+dependencies on the GPU, copies both grids in from pinned host memory, runs the graph and copies
+the written blocks back -- timed spawn -> wait, as the reference's runtime is timed.
+
 Beside it: the same graph's first two steps in the plain one-launch-per-task form and as a CUDA
 graph (the fused/plain ratio), the whole-step stencil kernel's HBM GB/s (FP64 and FP32
 storage), the resolver on the dependency microbench (65,536 tasks, 1-4 accesses on an 8192^2
@@ -187,7 +192,8 @@ def ref_heat_sample(nthreads, steps, n=NX):
         r = subprocess.run([REF_HEAT, str(n), str(n), str(TS), str(steps)], env=env, cwd=d, capture_output=True,
                            text=True, timeout=600)
     if r.returncode != 0:
-        raise RuntimeError(f"reference heat run failed: {r.stderr[-400:]}")
+        tail = [l for l in r.stderr.splitlines() if "[LOGGER]" not in l][-5:]
+        raise RuntimeError(f"reference heat run exited {r.returncode}: {' | '.join(tail)}")
     out = json.loads(r.stdout.strip().splitlines()[-1])
     return out["tasks_per_s"], out["seconds"], out["tasks"]
 
@@ -196,17 +202,28 @@ def cpu_baseline_sample(target_s=10.0):
     """CPU baseline on this host: the reference runtime when it was built, else the C
     restatement of the tile body. About target_s seconds of CPU work."""
     cores = host_threads()
+    why = None
     if os.path.exists(REF_HEAT):
-        v, secs, tasks = ref_heat_sample(cores, 1)
-        steps = max(1, min(200, int(target_s / max(secs, 1e-3))))
-        v, secs, tasks = ref_heat_sample(cores, steps)
-        return {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "reference",
-                "sample": f"{steps} Jacobi steps of the {NX}^2 FP64 heat graph ({tasks} tile tasks of {TS}^2, {secs:.1f} s): "
-                          f"the reference's own host-only runtime (DRIVERS=host,{cores}) with a host-format tile body"}
+        try:
+            return _ref_baseline(cores, target_s)
+        except Exception as ex:              # keep the bench line; say why the port stands in
+            why = str(ex)[:300]
     v, secs, tasks = cpu_heat_sample(cores, steps=None, target_s=target_s)
-    return {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "port",
-            "sample": f"{tasks // (NX // TS) ** 2} Jacobi steps of the {NX}^2 FP64 grid ({tasks} tile tasks, {secs:.1f} s), "
-                      "C restatement of the tile body on POSIX threads"}
+    out = {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "port",
+           "sample": f"{tasks // (NX // TS) ** 2} Jacobi steps of the {NX}^2 FP64 grid ({tasks} tile tasks, {secs:.1f} s), "
+                     "C restatement of the tile body on POSIX threads"}
+    if why:
+        out["reference_failed"] = why
+    return out
+
+
+def _ref_baseline(cores, target_s):
+    v, secs, tasks = ref_heat_sample(cores, 1)
+    steps = max(1, min(200, int(target_s / max(secs, 1e-3))))
+    v, secs, tasks = ref_heat_sample(cores, steps)
+    return {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "reference",
+            "sample": f"{steps} Jacobi steps of the {NX}^2 FP64 heat graph ({tasks} tile tasks of {TS}^2, {secs:.1f} s): "
+                      f"the reference's own host-only runtime (DRIVERS=host,{cores}) with a host-format tile body"}
 
 
 def run_reference(args):
@@ -243,6 +260,36 @@ def run_reference(args):
         "e2e": {"value": round(v, 1), "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
+
+
+HEAT_XKRT = os.path.join(HERE, "xkaapi_b200", "examples", "heat_xkrt")
+
+
+def capi_e2e(reps, world, local, warm=1):
+    """End to end through the XKRT C API (xkaapi_b200/examples/heat_xkrt, the heat example
+    written against include/xkrt_capi.h): per repetition, spawn every tile task of the graph
+    with its R/W accesses, then xkrt_task_wait -- GPU dependency resolution, H2D of both grids
+    from pinned host memory, the persistent-scheduler run, D2H of the written blocks -- timed
+    from the first spawn to the return of the wait, as the reference's runtime is timed on the
+    same graph. `warm` untimed repetitions first. Returns the e2e object (whole job over ranks)."""
+    env = dict(os.environ)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = vis.split(",")[local] if vis else str(local)
+    r = subprocess.run([HEAT_XKRT, str(NX), str(NY), str(TS), str(STEPS), str(warm + reps)], env=env,
+                       capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(f"heat_xkrt failed: {r.stderr[-600:]}")
+    lines = [json.loads(l) for l in r.stdout.strip().splitlines()][warm:]
+    secs = max_over_ranks(sum(l["seconds"] for l in lines), world)
+    tasks = sum(l["tasks"] for l in lines)
+    phases = {k: round(statistics.median(l[k] for l in lines), 1)
+              for k in ("resolve_ms", "coherency_ms", "run_ms", "writeback_ms")}
+    phases["spawn_ms"] = round(statistics.median(l["spawn_s"] for l in lines) * 1e3, 1)
+    return {"value": round(world * tasks / secs, 1), "unit": "tasks/s",
+            "h2d_bytes_per_step": int(lines[-1]["h2d_bytes"]), "d2h_bytes_per_step": int(lines[-1]["d2h_bytes"]),
+            "ms_per_step": round(secs / len(lines) * 1e3, 3), "steps": len(lines), "phases_ms": phases,
+            "api": "XKRT C API (xkrt_task_spawn_with_format_with_accesses x tasks, xkrt_task_wait), fresh runtime per step",
+            "checksum": lines[-1]["checksum"]}
 
 
 def microbench_stream(ntasks, seed, n=8192, ld=8192, align=64, max_units=32, base=1 << 40):
@@ -400,7 +447,7 @@ def main():
     res_grid = a if STEPS % 2 == 0 else b
     checksum = float(res_grid.sum().item())
 
-    # ---------------- e2e through the C ABI with host buffers ---------------------------------
+    # ---------------- e2e replay: the resolved graph re-run with host grids copied in and out --
     torch.cuda.synchronize()
     out_host = torch.empty_like(host).pin_memory()
     with torch.cuda.stream(stream):
@@ -488,6 +535,9 @@ def main():
     sch.close(); res.close()
     del a, b
     torch.cuda.synchronize(); torch.cuda.empty_cache()
+
+    # ---------------- e2e: the drop-in C API, spawn -> wait, resolution included ------------
+    e2e = capi_e2e(max(2, min(args.steps, 3)), world, local)
     if rank == 0 and not args.no_side:
         extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000)
 
@@ -511,8 +561,11 @@ def main():
                          "kernel": "sched_persistent_kernel", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": round(last_kernel_ms, 3)},
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e_value, 1), "unit": "tasks/s", "h2d_bytes_per_step": bytes_grid,
-                    "d2h_bytes_per_step": bytes_grid, "ms_per_step": round(e2e_ms / args.steps, 3)},
+            "e2e": e2e,
+            "e2e_replay": {"value": round(e2e_value, 1), "unit": "tasks/s", "h2d_bytes_per_step": bytes_grid,
+                           "d2h_bytes_per_step": bytes_grid, "ms_per_step": round(e2e_ms / args.steps, 3),
+                           "what": "the resolved graph re-run by xkb_sched_run, the grid copied in from pinned host memory "
+                                   "and the result copied out every step"},
             "gpu_launches": 3 * args.steps,
             "clocks": clk,
             "forms_first_2_steps": forms,

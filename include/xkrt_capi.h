@@ -202,6 +202,8 @@ XKB_API void * xkb_runtime_stream(xkrt_runtime_t * runtime);
  * persistent scheduler ran the batch (1) or the tasks ran one by one (0). */
 XKB_API int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks, uint64_t * edges, uint64_t * h2d,
                                   uint64_t * d2h, int * fused);
+/* Bytes the last xkrt_task_wait copied host -> device and device -> host. */
+XKB_API int xkb_runtime_last_wait_bytes(xkrt_runtime_t * runtime, uint64_t * h2d_bytes, uint64_t * d2h_bytes);
 /* Wall time of the phases of the last xkrt_task_wait, in ms: dependency resolution (records,
  * resolver batches, successor graph), coherency (planner fetches, H2D copies, descriptor upload;
  * fused batches only), execution, and the write-back of device-written blocks to the host. */

@@ -30,7 +30,8 @@ def test_python_signatures_cover_header():
     # the xkb_* library API is bound in Python; the xkrt_* C API is for C programs
     xkb = {n for n in declared_symbols() if n.startswith("xkb_")}
     assert xkb - set(xk.SIGNATURES) <= {"xkb_task_format_builtin", "xkb_runtime_status", "xkb_runtime_stream",
-                                        "xkb_runtime_last_wait", "xkb_runtime_last_wait_times"}, xkb - set(xk.SIGNATURES)
+                                        "xkb_runtime_last_wait", "xkb_runtime_last_wait_times",
+                                        "xkb_runtime_last_wait_bytes"}, xkb - set(xk.SIGNATURES)
 
 
 def test_c_api_symbols_exported():

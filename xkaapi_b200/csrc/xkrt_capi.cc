@@ -73,7 +73,7 @@ struct xkb_runtime {
     cudaStream_t stream = nullptr;
     bool gpu = false;
     int status = XKB_OK;
-    uint64_t last_tasks = 0, last_edges = 0, last_h2d = 0, last_d2h = 0;
+    uint64_t last_tasks = 0, last_edges = 0, last_h2d = 0, last_d2h = 0, last_h2d_bytes = 0, last_d2h_bytes = 0;
     int last_fused = 0;
     double last_ms[4] = {0, 0, 0, 0};                 // resolve, coherency + launch prep, run, write-back
     int dummy_team = 0;
@@ -395,7 +395,11 @@ static int run_copies(xkb_runtime * R)
     if ((rc = xkb_planner_copies(R->planner, c.data(), n, &n, 1))) return rc;
     std::vector<void *> ptrs(R->regions.size(), nullptr);
     for (auto & kv : R->regions) ptrs[kv.second.id] = kv.second.mirror;
-    for (const xkb_copy_t & k : c) (k.kind == XKB_COPY_H2D ? R->last_h2d : R->last_d2h) += 1;
+    for (const xkb_copy_t & k : c)
+    {
+        (k.kind == XKB_COPY_H2D ? R->last_h2d : R->last_d2h) += 1;
+        (k.kind == XKB_COPY_H2D ? R->last_h2d_bytes : R->last_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
+    }
     return xkb_plan_execute(c.data(), n, ptrs.data(), ptrs.size(), R->stream);
 }
 
@@ -523,6 +527,7 @@ constexpr size_t RESOLVE_CHUNK = size_t(1) << 20;
 static int wait_batch(xkb_runtime * R)
 {
     R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
+    R->last_h2d_bytes = R->last_d2h_bytes = 0;
     for (double & m : R->last_ms) m = 0;
     if (R->pending.empty()) return XKB_OK;
     if (!R->gpu) return xkb_set_error(XKB_ENODEV, "xkrt_task_wait: dependency resolution runs on the GPU and none is visible");
@@ -718,6 +723,15 @@ static int wait_batch(xkb_runtime * R)
     }
     xkb_resolver_destroy(res);
     return rc;
+}
+
+extern "C" int xkb_runtime_last_wait_bytes(xkrt_runtime_t * runtime, uint64_t * h2d_bytes, uint64_t * d2h_bytes)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R) return xkb_set_error(XKB_EINVAL, "xkb_runtime_last_wait_bytes: null runtime");
+    if (h2d_bytes) *h2d_bytes = R->last_h2d_bytes;
+    if (d2h_bytes) *d2h_bytes = R->last_d2h_bytes;
+    return XKB_OK;
 }
 
 extern "C" int xkb_runtime_last_wait_times(xkrt_runtime_t * runtime, double * resolve_ms, double * coherency_ms, double * run_ms,
