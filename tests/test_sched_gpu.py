@@ -165,3 +165,23 @@ def test_periodic_rejects_aperiodic_graph(torch_cuda):
     res = xk.Resolver(); res.add(recs)
     with pytest.raises(xk.XkbError):
         res.periodic(10)
+
+
+@pytest.mark.parametrize("nx,ny,ts,steps,f32,team", [
+    (1024, 768, 128, 12, False, 2), (300, 200, 64, 9, False, 1), (300, 200, 100, 9, False, 8),
+    (301, 203, 64, 6, False, 2),                       # rows not 16-byte aligned: register body
+    (516, 260, 128, 10, True, 2), (514, 130, 64, 6, True, 4), (1000, 1000, 96, 8, True, 1)])
+def test_bulk_staged_body_matches_register_body(torch_cuda, nx, ny, ts, steps, f32, team):
+    """The bulk-staged tile body (default) and the register body give the oracle's grid bit for
+    bit, for FP64 and FP32 storage, tiles that are not a multiple of the strip, and grids whose
+    rows cannot be staged (odd FP64 / non-multiple-of-4 FP32 widths fall back)."""
+    torch = torch_cuda
+    dt = np.float32 if f32 else np.float64
+    want = O.heat_run(O.heat_init(nx, ny, seed=5), nx, ny, steps, C, dtype=dt)
+    for bulk in (True, False):
+        g, a, b, res, descs = heat_graph(torch, nx, ny, ts, steps, f32=f32, seed=5)
+        sch = xk.Scheduler(); sch.set_team(team); sch.set_staging(bulk); sch.set_tasks(descs)
+        sch.run(res.graph())
+        assert sch.wait() == len(descs)
+        np.testing.assert_array_equal((a if steps % 2 == 0 else b).cpu().numpy(), want)
+        sch.close(); res.close()

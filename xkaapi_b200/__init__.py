@@ -81,6 +81,7 @@ SIGNATURES = {
     "xkb_sched_set_grid": (_int, [_vp, _int]),
     "xkb_sched_set_team": (_int, [_vp, _int]),
     "xkb_sched_set_prefetch": (_int, [_vp, _int]),
+    "xkb_sched_set_staging": (_int, [_vp, _int]),
     "xkb_sched_run": (_int, [_vp, ctypes.POINTER(TaskGraph), _int]),
     "xkb_sched_wait": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_sched_kernel_ms": (_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
@@ -265,6 +266,10 @@ class Scheduler:
 
     def set_prefetch(self, columns):
         check(lib().xkb_sched_set_prefetch(self._h, columns))
+
+    def set_staging(self, bulk):
+        """Heat tile body of the persistent kernel: False = register body (default), True = bulk-staged."""
+        check(lib().xkb_sched_set_staging(self._h, 1 if bulk else 0))
 
     def run(self, graph, form=FORM_PERSISTENT):
         check(lib().xkb_sched_run(self._h, ctypes.byref(graph), form))

@@ -19,6 +19,7 @@
 //    dependency), instantiated once and replayed.
 #include "common.cuh"
 #include "heat.cuh"
+#include "heat_bulk.cuh"
 #include "internal.h"
 
 #include <new>
@@ -55,6 +56,8 @@ __device__ __forceinline__ void axpby_team(int64_t lo, int64_t hi, double a, con
 }
 
 constexpr int SCHED_THREADS = 256;
+
+constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (bulk tile body)
 
 // Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
 __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps, int pfd)
@@ -141,16 +144,32 @@ __device__ __forceinline__ void team_sync(int id, int nthreads)
 // thread takes the next queue slot and waits for it; the team runs the task, fences, syncs
 // on its own named barrier, and its first warp releases the successors. Teams never wait for
 // one another, so while one team takes or releases a task the others keep HBM busy.
-template <int TEAM_WARPS>
+//
+// BULK: heat tiles whose layout allows it run the bulk-staged body (heat_bulk.cuh): each warp
+// streams its strips' columns through its own ring of shared-memory slots; other tasks run the
+// register body.
+// Dynamic shared memory of the BULK variant with NBUF slots per warp: the slots, then the mbarriers.
+constexpr size_t bulk_smem_bytes(int nbuf) { return (size_t) (SCHED_THREADS / 32) * nbuf * (BULK_SLOT_BYTES + 8); }
+
+template <int TEAM_WARPS, bool BULK = false, int NBUF = SCHED_BULK_NBUF>
 __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(SchedArgs a)
 {
     constexpr int NTEAMS = (SCHED_THREADS / 32) / TEAM_WARPS;
     constexpr int TEAM_THREADS = TEAM_WARPS * 32;
+    constexpr int NWARPS = SCHED_THREADS / 32;
     __shared__ int cur[NTEAMS];
+    extern __shared__ __align__(128) unsigned char bulk_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int team = warp / TEAM_WARPS, twarp = warp % TEAM_WARPS;
     const int bar = 1 + team;
     unsigned executed = 0;
+    BulkRing<NBUF> ring;
+    if constexpr (BULK)
+    {
+        ring.slots = bulk_smem + (size_t) warp * NBUF * BULK_SLOT_BYTES;
+        ring.bars = (uint64_t *) (bulk_smem + (size_t) NWARPS * NBUF * BULK_SLOT_BYTES) + warp * NBUF;
+        bulk_ring_init(ring);
+    }
     for (;;)
     {
         if (twarp == 0 && lane == 0)
@@ -179,7 +198,30 @@ __global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(Sche
         const int t = cur[team];
         if (t < 0) break;
         const uint32_t w = (uint32_t) t / a.period, l = (uint32_t) t - w * a.period;
-        run_task_team(a.tasks[l], twarp, TEAM_WARPS, a.pfd);
+        if constexpr (BULK)
+        {
+            const xkb_task_desc_t & d = a.tasks[l];
+            const auto & h = d.u.heat;
+            // once a wait has run out anywhere, the remaining tasks are passed over quickly
+            bool done = *(volatile unsigned *) (a.ctr + 2) != 0;
+            if (d.kind == XKB_TASK_HEAT_F64 && bulk_ok<double, 2>((const double *) h.src, h.ld, h.nx) && h.dst % 16 == 0)
+            {
+                done = true;
+                if (!heat_tile_team_bulk<double, 2, NBUF>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny, h.x0, h.x1,
+                                                          h.y0, h.y1, h.c, twarp, TEAM_WARPS, ring, xkb_globaltimer() + a.timeout_ns))
+                    atomicCAS(a.ctr + 2, 0u, (unsigned) -XKB_ETIMEDOUT);
+            }
+            else if (d.kind == XKB_TASK_HEAT_F32 && bulk_ok<float, 4>((const float *) h.src, h.ld, h.nx) && h.dst % 16 == 0)
+            {
+                done = true;
+                if (!heat_tile_team_bulk<float, 4, NBUF>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny, h.x0, h.x1,
+                                                         h.y0, h.y1, h.c, twarp, TEAM_WARPS, ring, xkb_globaltimer() + a.timeout_ns))
+                    atomicCAS(a.ctr + 2, 0u, (unsigned) -XKB_ETIMEDOUT);
+            }
+            if (!done) run_task_team(d, twarp, TEAM_WARPS, a.pfd);
+        }
+        else
+            run_task_team(a.tasks[l], twarp, TEAM_WARPS, a.pfd);
         __threadfence();
         team_sync(bar, TEAM_THREADS);
         if (twarp == 0)
@@ -293,6 +335,7 @@ struct xkb_sched {
     int last_form = -1;
     int grid = 0;
     int team_warps = 2;
+    int bulk = 0;                             // 1: bulk-staged heat tile body (measured slower; opt-in)
     int pfd = 8;
     uint64_t last_total = 0;                  // tasks of the last run
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
@@ -415,7 +458,34 @@ extern "C" int xkb_sched_set_team(xkb_sched_t * S, int warps_per_task)
     return XKB_OK;
 }
 
+extern "C" int xkb_sched_set_staging(xkb_sched_t * S, int bulk)
+{
+    if (!S || bulk < 0 || bulk > 1) return xkb_set_error(XKB_EINVAL, "sched_set_staging: 0 (register body) or 1 (bulk-staged body)");
+    S->bulk = bulk;
+    return XKB_OK;
+}
+
 static int launch_persistent(xkb_sched * S, SchedArgs & a);
+
+template <int TEAM, int NBUF>
+static int launch_bulk_n(xkb_sched * S, SchedArgs & a)
+{
+    const size_t smem = bulk_smem_bytes(NBUF);
+    XKB_CUDA_TRY(cudaFuncSetAttribute(sched_persistent_kernel<TEAM, true, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    sched_persistent_kernel<TEAM, true, NBUF><<<S->grid, SCHED_THREADS, smem, S->stream>>>(a);
+    return XKB_OK;
+}
+
+static int launch_bulk(xkb_sched * S, SchedArgs & a)
+{
+    switch (S->team_warps)
+    {
+        case 1: return launch_bulk_n<1, SCHED_BULK_NBUF>(S, a);
+        case 2: return launch_bulk_n<2, SCHED_BULK_NBUF>(S, a);
+        case 4: return launch_bulk_n<4, SCHED_BULK_NBUF>(S, a);
+        default: return launch_bulk_n<8, SCHED_BULK_NBUF>(S, a);
+    }
+}
 
 static int run_persistent(xkb_sched * S, const xkb_task_graph_t * g)
 {
@@ -439,13 +509,19 @@ static int launch_persistent(xkb_sched * S, SchedArgs & a)
         sched_seed_kernel<<<(n + 255) / 256, 256, 0, S->stream>>>(a);
         if (!S->ev[0]) { XKB_CUDA_TRY(cudaEventCreate(&S->ev[0])); XKB_CUDA_TRY(cudaEventCreate(&S->ev[1])); }
         XKB_CUDA_TRY(cudaEventRecord(S->ev[0], S->stream));
-        switch (S->team_warps)
+        if (S->bulk)
         {
-            case 1: sched_persistent_kernel<1><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
-            case 2: sched_persistent_kernel<2><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
-            case 4: sched_persistent_kernel<4><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
-            default: sched_persistent_kernel<8><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+            int rc = launch_bulk(S, a);
+            if (rc) return rc;
         }
+        else
+            switch (S->team_warps)
+            {
+                case 1: sched_persistent_kernel<1><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+                case 2: sched_persistent_kernel<2><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+                case 4: sched_persistent_kernel<4><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+                default: sched_persistent_kernel<8><<<S->grid, SCHED_THREADS, 0, S->stream>>>(a); break;
+            }
         XKB_CUDA_TRY(cudaEventRecord(S->ev[1], S->stream));
     }
     XKB_CUDA_TRY(cudaGetLastError());
