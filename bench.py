@@ -292,6 +292,74 @@ def capi_e2e(reps, world, local, warm=1):
             "checksum": lines[-1]["checksum"]}
 
 
+AXPBY_XKRT = os.path.join(HERE, "xkaapi_b200", "examples", "axpby_xkrt")
+REF_AXPBY = os.path.join(HERE, "oracle", "_ref", "ref_axpby")
+AXPBY_N, AXPBY_PASSES, AXPBY_SEED, AXPBY_CMIN, AXPBY_CMAX = 1 << 28, 10, 2026, 65536, 16 << 20
+
+
+def axpby_study(local):
+    """axpby task chains (2^28 FP64, 10 passes, seeded chunks of 64 KiB-16 MiB whose boundaries
+    move between passes) through the C API with host-resident x and y: one warm-up and one timed
+    repetition of spawn -> xkrt_task_wait. Beside it the reference's own host runtime on the same
+    graph (same generator) with all host threads."""
+    env = dict(os.environ)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = vis.split(",")[local] if vis else str(local)
+    args = [str(AXPBY_N), str(AXPBY_PASSES), str(AXPBY_SEED)]
+    r = subprocess.run([AXPBY_XKRT] + args + ["2", str(AXPBY_CMIN), str(AXPBY_CMAX)], env=env, capture_output=True,
+                       text=True, timeout=900)
+    if r.returncode != 0:
+        return {"failed": r.stderr[-300:]}
+    ln = json.loads(r.stdout.strip().splitlines()[-1])
+    dev_bytes = 24.0 * AXPBY_N * AXPBY_PASSES
+    out = {"tasks": ln["tasks"], "edges": ln["edges"], "seconds": round(ln["seconds"], 4),
+           "tasks_per_s": round(ln["tasks_per_s"], 1),
+           "phases_ms": {k: round(ln[k], 1) for k in ("resolve_ms", "coherency_ms", "run_ms", "writeback_ms")},
+           "spawn_ms": round(ln["spawn_s"] * 1e3, 1), "h2d_bytes": ln["h2d_bytes"], "d2h_bytes": ln["d2h_bytes"],
+           "run_GBps": round(dev_bytes / (ln["run_ms"] / 1e3) / 1e9, 1),
+           "workload": f"y = a*x + b*y on 2^28 FP64, {AXPBY_PASSES} passes, chunks log-uniform {AXPBY_CMIN} B-{AXPBY_CMAX >> 20} MiB "
+                       "(moving boundaries), segment accesses R x / RW y, host-resident inputs; run_GBps = 24 B x elements x "
+                       "passes / run_ms", "checksum": ln["checksum"]}
+    if os.path.exists(REF_AXPBY):
+        cores = host_threads()
+        renv = dict(os.environ, DRIVERS=f"host,{cores}", XKRT_DRIVERS=f"host,{cores}")
+        with tempfile.TemporaryDirectory() as d:
+            rr = subprocess.run([REF_AXPBY] + args + [str(AXPBY_CMIN), str(AXPBY_CMAX)], env=renv, cwd=d,
+                                capture_output=True, text=True, timeout=900)
+        if rr.returncode == 0:
+            rl = json.loads(rr.stdout.strip().splitlines()[-1])
+            out["reference_cpu"] = {"tasks_per_s": rl["tasks_per_s"], "seconds": rl["seconds"], "cores": cores,
+                                    "same_result": rl["checksum"] == ln["checksum"],
+                                    "what": "the reference's host-only runtime (oracle/_ref/ref_axpby), same graph, spawn -> task_wait"}
+    return out
+
+
+REF_DEPS = os.path.join(HERE, "oracle", "_ref", "ref_deps")
+STREAM_MAGIC = 0x314D525453424B58
+
+
+def ref_deps_time(recs):
+    """The reference's own dependency trees (oracle/_ref/ref_deps: KBLASDependencyTree driven by
+    task_dependency_resolve, one producer thread as in the reference) on the same stream."""
+    if not os.path.exists(REF_DEPS):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "s.bin")
+        with open(p, "wb") as f:
+            np.array([STREAM_MAGIC, len(recs)], dtype="<u8").tofile(f)
+            recs.tofile(f)
+        try:
+            r = subprocess.run([REF_DEPS, p, os.path.join(d, "o")], capture_output=True, text=True, timeout=300)
+        except subprocess.TimeoutExpired:
+            return {"failed": "timed out after 300 s"}
+    if r.returncode != 0:
+        return {"failed": r.stderr[-200:]}
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"tasks_per_s": round(out["ntasks"] / out["resolve_s"], 1), "seconds": out["resolve_s"], "cores": 1,
+            "unique_edges": out["unique_edges"],
+            "what": "the reference's KBLASDependencyTree via task_dependency_resolve on the same stream, one thread"}
+
+
 def microbench_stream(ntasks, seed, n=8192, ld=8192, align=64, max_units=32, base=1 << 40):
     """Dependency microbench: 1-4 accesses per task on an n x n FP64 matrix (LD = ld), rectangles
     aligned to 64 elements with sides 64*U{1..32}, modes R 60% / W 20% / RW 20%."""
@@ -530,6 +598,10 @@ def main():
         extra["resolver_microbench"] = {"tasks": mb_tasks, "accesses": int(len(recs)), "unique_edges": int(g3.nedges),
                                         "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt)}
         r3.close()
+        ref = ref_deps_time(recs)
+        if ref:
+            ref["same_unique_edges"] = ref.pop("unique_edges") == int(g3.nedges)
+            extra["resolver_microbench"]["reference_cpu"] = ref
 
     # ---------------- served stream (after releasing the headline graph's memory) -----------
     sch.close(); res.close()
@@ -538,6 +610,8 @@ def main():
 
     # ---------------- e2e: the drop-in C API, spawn -> wait, resolution included ------------
     e2e = capi_e2e(max(2, min(args.steps, 3)), world, local)
+    if rank == 0 and not args.no_side:
+        extra["axpby_chains"] = axpby_study(local)
     if rank == 0 and not args.no_side:
         extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000)
 

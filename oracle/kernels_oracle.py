@@ -98,3 +98,60 @@ def serve_init(nx, ny, seed, dtype=np.float64):
     g = v.reshape(ny, nx)
     g[0, :] = 0; g[-1, :] = 0; g[:, 0] = 0; g[:, -1] = 0
     return g.astype(dtype)
+
+
+_GAMMA = 0x9E3779B97F4A7C15
+_M64 = (1 << 64) - 1
+
+
+def _mix64(z):
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def axpby_chain(n, passes, seed, cmin, cmax):
+    """The seeded axpby task-chain workload (the draw sequence of the reference-runtime driver
+    oracle/ref/ref_axpby.cc and the example xkaapi_b200/examples/axpby_xkrt.c): a splitmix64
+    stream s += gamma; x[i], then y[i] = 2u - 1 (u = top 53 bits / 2^53); per pass a, b = 4u - 2,
+    then chunk lengths floor(exp(log cmin + (log cmax - log cmin) u) / 8) elements (at least 1),
+    the first one of a pass shortened to 1 + floor(u * len). Returns (x, y, chunks) with chunks a
+    list of (lo, hi, a, b) in spawn order."""
+    import math
+    k = np.arange(1, 2 * n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + k * np.uint64(_GAMMA)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    x, y = 2.0 * u[:n] - 1.0, 2.0 * u[n:] - 1.0
+    s = (seed + 2 * n * _GAMMA) & _M64
+
+    def unit():
+        nonlocal s
+        s = (s + _GAMMA) & _M64
+        return (_mix64(s) >> 11) * (1.0 / 9007199254740992.0)
+
+    lmin, lmax = math.log(cmin), math.log(cmax)
+    chunks = []
+    for _ in range(passes):
+        a = 4.0 * unit() - 2.0
+        b = 4.0 * unit() - 2.0
+        at, first = 0, True
+        while at < n:
+            ln = max(int(math.exp(lmin + (lmax - lmin) * unit()) / 8.0), 1)
+            if first:
+                ln, first = 1 + int(unit() * ln), False
+            hi = min(at + ln, n)
+            chunks.append((at, hi, a, b))
+            at = hi
+    return x, y, chunks
+
+
+def axpby_chain_run(x, y, chunks):
+    """y after every chunk task in spawn order (each element once per pass)."""
+    y = y.copy()
+    for lo, hi, a, b in chunks:
+        y[lo:hi] = axpby(a, x[lo:hi], b, y[lo:hi])
+    return y

@@ -166,3 +166,5 @@ done
 wait
 "$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_heat" "$HERE/ref_heat.cc" $OBJS -lpthread -ldl
 echo "built $OUT/ref_heat"
+"$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_axpby" "$HERE/ref_axpby.cc" $OBJS -lpthread -ldl
+echo "built $OUT/ref_axpby"

@@ -14,7 +14,11 @@ Plan fixtures: oracle/_ref/ref_plan drives KBLASMemoryTree::fetch
 (include/xkrt/memory/access/blas/memory-tree.hpp:1805-1874) under the canonical schedule (fetches in
 spawn order, each fetch's copies completed before the next); allocations, device views and the
 sorted copy records are stored.
-Run: python tests/golden/make_golden.py   (needs oracle/_ref/ref_deps and ref_plan; see oracle/ref/build_ref.sh)
+axpby fixtures: oracle/_ref/ref_axpby (the reference's host-only runtime running the seeded
+axpby task chains with segment accesses, oracle/ref/ref_axpby.cc); the final y of each case is
+stored with its parameters, pinning the oracle's restatement of the chain generator and update.
+Run: python tests/golden/make_golden.py [deps] [plan] [axpby]   (default: all; needs the binaries
+of oracle/ref/build_ref.sh)
 """
 import os, subprocess, sys, tempfile
 import numpy as np
@@ -126,14 +130,45 @@ def plan_cases():
         yield f"plan_seg_{seed}", np.array(rows, dtype=S.REC)
 
 
+AXPBY_CASES = [  # name, n, passes, seed, cmin bytes, cmax bytes
+    ("axpby_20000_p3", 20000, 3, 11, 512, 65536),
+    ("axpby_12345_p5", 12345, 5, 29, 64, 16384),
+]
+
+
+def ref_axpby(n, passes, seed, cmin, cmax):
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "y.bin")
+        env = dict(os.environ, DRIVERS="host,2", XKRT_DRIVERS="host,2")
+        r = subprocess.run([os.path.join(REPO, "oracle/_ref/ref_axpby"), str(n), str(passes), str(seed), str(cmin), str(cmax), out],
+                           check=True, capture_output=True, text=True, env=env, cwd=d)
+        import json
+        return np.fromfile(out), json.loads(r.stdout.strip().splitlines()[-1])["tasks"]
+
+
 def main():
+    which = set(sys.argv[1:]) or {"deps", "plan", "axpby"}
+    if "axpby" in which:
+        out = {}
+        for name, n, passes, seed, cmin, cmax in AXPBY_CASES:
+            y, tasks = ref_axpby(n, passes, seed, cmin, cmax)
+            out[name + "__params"] = np.array([n, passes, seed, cmin, cmax], dtype=np.int64)
+            out[name + "__y"] = y
+            out[name + "__tasks"] = np.array([tasks], dtype=np.int64)
+            print(f"{name}: {tasks} tasks")
+        np.savez_compressed(os.path.join(HERE, "axpby_golden.npz"), **out)
+    if "deps" not in which and "plan" not in which:
+        return
     out = {}
     for name, recs in cases():
         e = ref_edges(recs)
         out[name + "__stream"] = recs
         out[name + "__edges"] = e
         print(f"{name}: {len(recs)} accesses, {len(e)} unique edges")
-    np.savez_compressed(os.path.join(HERE, "deps_golden.npz"), **out)
+    if "deps" in which:
+        np.savez_compressed(os.path.join(HERE, "deps_golden.npz"), **out)
+    if "plan" not in which:
+        return
     out = {}
     for name, recs in plan_cases():
         plan, allocs, views = ref_plan(recs)

@@ -79,3 +79,18 @@ def test_reference_runtime_heat_equals_oracle(tmp_path):
                    env=env, check=True, capture_output=True, cwd=str(tmp_path), timeout=120)
     out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
     np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2))
+
+
+AXPBY_GOLDEN = np.load(os.path.join(REPO, "tests", "golden", "axpby_golden.npz"))
+AXPBY_CASES = sorted(k[:-len("__params")] for k in AXPBY_GOLDEN.files if k.endswith("__params"))
+
+
+@pytest.mark.parametrize("case", AXPBY_CASES)
+def test_axpby_chain_oracle_matches_reference_runtime(case):
+    """The oracle's restatement of the seeded axpby task chains (generator + y = a*x + b*y per
+    chunk, in spawn order) equals the final y of the reference's own host runtime bit for bit."""
+    import kernels_oracle as O
+    n, passes, seed, cmin, cmax = (int(v) for v in AXPBY_GOLDEN[case + "__params"])
+    x, y, chunks = O.axpby_chain(n, passes, seed, cmin, cmax)
+    assert len(chunks) == int(AXPBY_GOLDEN[case + "__tasks"][0])
+    np.testing.assert_array_equal(O.axpby_chain_run(x, y, chunks), AXPBY_GOLDEN[case + "__y"])

@@ -91,7 +91,7 @@ def build_examples(verbose=False):
             out.append(exe)
             continue
         cmd = ["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-D_POSIX_C_SOURCE=200809L", "-I" + os.path.join(REPO, "include"),
-               src, "-o", exe, "-L" + PKG, "-lxkb200", "-Wl,-rpath,$ORIGIN/.."]
+               src, "-o", exe, "-L" + PKG, "-lxkb200", "-lm", "-Wl,-rpath,$ORIGIN/.."]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         r = subprocess.run(cmd, capture_output=True, text=True)

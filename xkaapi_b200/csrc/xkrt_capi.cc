@@ -520,6 +520,108 @@ static double ms_since(std::chrono::steady_clock::time_point t0)
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Device array owned by the runtime (freed when replaced or at deinit).
+struct DevArray {
+    void * p = nullptr;
+    size_t bytes = 0;
+    ~DevArray() { if (p) cudaFree(p); }
+    int put(const void * host, size_t n)
+    {
+        if (n > bytes)
+        {
+            if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+            if (cudaMalloc(&p, n) != cudaSuccess) { cudaGetLastError(); return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: device allocation"); }
+            bytes = n;
+        }
+        if (n && cudaMemcpy(p, host, n, cudaMemcpyHostToDevice) != cudaSuccess) return xkb_set_error(XKB_ECUDA, "xkrt_task_wait: copy");
+        return XKB_OK;
+    }
+};
+
+// Moldable execution of long axpby tasks: a built-in axpby task over more than SPLIT elements
+// runs as ceil(len / SPLIT) slice tasks plus a no-op join task. Every predecessor of the task
+// precedes each slice, each slice precedes the join, and the join precedes the task's
+// successors -- the same order constraints, with the element range spread over many teams of
+// the persistent kernel instead of one.
+constexpr int64_t AXPBY_SPLIT = int64_t(1) << 15;
+
+struct SplitGraph {
+    DevArray succ_ptr, succ, npred;
+    std::vector<xkb_task_desc_t> descs;
+    xkb_task_graph_t g{};
+};
+
+// false: nothing to split (descs / g unchanged).
+static int split_moldable(const xkb_task_desc_t * descs, size_t nt, const xkb_task_graph_t & g, SplitGraph & out, bool & split)
+{
+    split = false;
+    std::vector<uint32_t> k(nt);
+    size_t nnew = 0;
+    for (size_t t = 0; t < nt; ++t)
+    {
+        const xkb_task_desc_t & d = descs[t];
+        const int64_t len = d.kind == XKB_TASK_AXPBY ? d.u.axpby.hi - d.u.axpby.lo : 0;
+        k[t] = len > AXPBY_SPLIT ? (uint32_t) ((len + AXPBY_SPLIT - 1) / AXPBY_SPLIT) : 1u;
+        if (k[t] > 1) split = true;
+        nnew += k[t] > 1 ? k[t] + 1 : 1;
+    }
+    if (!split) return XKB_OK;
+    if (nnew >= (size_t(1) << 31)) return xkb_set_error(XKB_ERANGE, "xkrt_task_wait: %zu tasks after splitting", nnew);
+    std::vector<uint32_t> ptr(nt + 1), succ(g.nedges), npred(nt);
+    if (cudaMemcpy(ptr.data(), g.succ_ptr, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        (g.nedges && cudaMemcpy(succ.data(), g.succ, g.nedges * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        cudaMemcpy(npred.data(), g.npred, nt * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return xkb_set_error(XKB_ECUDA, "xkrt_task_wait: graph download");
+    std::vector<uint32_t> first(nt);                         // new id of the task's first node
+    out.descs.resize(nnew);
+    std::vector<uint32_t> np(nnew), nsucc(nnew, 0);
+    uint32_t id = 0;
+    for (size_t t = 0; t < nt; ++t)
+    {
+        first[t] = id;
+        if (k[t] == 1) { out.descs[id] = descs[t]; np[id] = npred[t]; ++id; continue; }
+        const xkb_task_desc_t & d = descs[t];
+        for (uint32_t i = 0; i < k[t]; ++i)
+        {
+            xkb_task_desc_t q = d;
+            q.u.axpby.lo = d.u.axpby.lo + (int64_t) i * AXPBY_SPLIT;
+            q.u.axpby.hi = std::min<int64_t>(q.u.axpby.lo + AXPBY_SPLIT, d.u.axpby.hi);
+            out.descs[id] = q; np[id] = npred[t]; ++id;
+        }
+        xkb_task_desc_t j;
+        memset(&j, 0, sizeof(j));
+        j.kind = XKB_TASK_NOOP;
+        out.descs[id] = j; np[id] = k[t]; ++id;
+    }
+    auto exit_of = [&](size_t t) { return k[t] == 1 ? first[t] : first[t] + k[t]; };
+    // successor counts, then CSR fill in ascending order
+    for (size_t t = 0; t < nt; ++t)
+    {
+        const uint32_t e = exit_of(t);
+        for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i) nsucc[e] += k[succ[i]];
+        if (k[t] > 1) for (uint32_t i = 0; i < k[t]; ++i) nsucc[first[t] + i] = 1;
+    }
+    std::vector<uint32_t> nptr(nnew + 1, 0);
+    for (size_t v = 0; v < nnew; ++v) nptr[v + 1] = nptr[v] + nsucc[v];
+    std::vector<uint32_t> nsc(nptr[nnew]);
+    for (size_t t = 0; t < nt; ++t)
+    {
+        uint32_t at = nptr[exit_of(t)];
+        for (uint32_t i = ptr[t]; i < ptr[t + 1]; ++i)
+            for (uint32_t s2 = 0; s2 < k[succ[i]]; ++s2) nsc[at++] = first[succ[i]] + s2;
+        if (k[t] > 1) for (uint32_t i = 0; i < k[t]; ++i) nsc[nptr[first[t] + i]] = first[t] + k[t];
+    }
+    int rc;
+    if ((rc = out.succ_ptr.put(nptr.data(), nptr.size() * sizeof(uint32_t))) ||
+        (rc = out.succ.put(nsc.data(), std::max<size_t>(nsc.size(), 1) * sizeof(uint32_t))) ||
+        (rc = out.npred.put(np.data(), np.size() * sizeof(uint32_t))))
+        return rc;
+    out.g.ntasks = nnew; out.g.nedges = nsc.size();
+    out.g.succ_ptr = (const uint32_t *) out.succ_ptr.p; out.g.succ = (const uint32_t *) out.succ.p;
+    out.g.npred = (const uint32_t *) out.npred.p;
+    return XKB_OK;
+}
+
 // Records per resolver batch: the resolver's working set grows with the batch, and batches of
 // about a million accesses keep it small while amortising each batch's fixed costs.
 constexpr size_t RESOLVE_CHUNK = size_t(1) << 20;
@@ -640,14 +742,19 @@ static int wait_batch(xkb_runtime * R)
             rc = translate(R, descs[t]);
         }
         const double desc_ms = ms_since(t0) - fetch_ms;
-        if (rc == XKB_OK) rc = xkb_internal_sched_set_tasks_device(R->sched, descs, nt);
+        SplitGraph sg;
+        bool split = false;
+        if (rc == XKB_OK) rc = split_moldable(descs, nt, g, sg, split);
+        const xkb_task_graph_t & run_g = split ? sg.g : g;
+        if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size())
+                                     : xkb_internal_sched_set_tasks_device(R->sched, descs, nt);
         if (getenv("XKB_TRACE_WAIT"))
             fprintf(stderr, "xkrt_task_wait: fetches + copies %.1f ms, descriptors %.1f ms, upload %.1f ms\n", fetch_ms, desc_ms,
                     ms_since(t0) - fetch_ms - desc_ms);
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[1] = ms_since(t0);
         t0 = std::chrono::steady_clock::now();
-        if (rc == XKB_OK) rc = xkb_sched_run(R->sched, &g, XKB_FORM_PERSISTENT);
+        if (rc == XKB_OK) rc = xkb_sched_run(R->sched, &run_g, XKB_FORM_PERSISTENT);
         uint64_t ran = 0;
         if (rc == XKB_OK) rc = xkb_sched_wait(R->sched, &ran);
         R->last_ms[2] = ms_since(t0);
