@@ -133,8 +133,9 @@ XKB_API int xkb_resolver_periodic(xkb_resolver_t * resolver, uint64_t period, xk
 
 /* Counters: tasks added, unique edges, device+host time of the last batch in ms. */
 XKB_API int xkb_resolver_stats(xkb_resolver_t * resolver, uint64_t * ntasks, uint64_t * nedges, double * last_batch_ms);
-/* Where the last batch's time went: building the per-domain op lists on the host, coordinate
- * compression and state refinement on the host, and the whole batch (host and device). */
+/* Where the last batch's time went: building the per-domain op lists (host), coordinate
+ * compression (new boundaries found on the device, merged on the host), state refinement and
+ * mapping of the ops to cells, and the whole batch (host and device). */
 XKB_API int xkb_resolver_timing(xkb_resolver_t * resolver, double * ops_ms, double * compress_ms, double * batch_ms);
 
 /* ---- coherency and transfer planning (1 host + 1 GPU) ------------------------------------ */
