@@ -211,9 +211,12 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
     const bool has_n = lane == 0 && rn >= 0, has_s = lane == 31 && rs < nx;
     const bool lane_rows = (r + VEC > rx0) && (r < rx1);
     const bool full_store = vec_ok && r >= rx0 && r + VEC <= rx1;
-    int64_t pf_rows = nx - rbase; if (pf_rows > 32 * VEC) pf_rows = 32 * VEC;
-    const uint32_t pf_bytes = (uint32_t) ((pf_rows * (int64_t) sizeof(T)) & ~(int64_t) 15);
-    const bool pf_on = pfd > 0 && vec_ok && pf_bytes > 0;
+    // the L2 prefetch of a column covers the strip AND its halo rows (VEC rows on each side keep
+    // the 16-byte alignment), so the lanes' halo loads hit L2 like the strip's own loads
+    const int64_t pf_lo = rbase >= VEC ? rbase - VEC : 0;
+    int64_t pf_hi = rbase + 33 * VEC; if (pf_hi > nx) pf_hi = nx;
+    const uint32_t pf_bytes = (uint32_t) (((pf_hi - pf_lo) * (int64_t) sizeof(T)) & ~(int64_t) 15);
+    const bool pf_on = pfd > 0 && vec_ok && pf_hi > pf_lo && pf_bytes > 0;
     const T * __restrict__ sp = src + r;
     T * __restrict__ dp = dst + r;
     auto load = [&](int64_t j) -> Cells<T, VEC> {
@@ -239,7 +242,7 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
         if (pf_on && lane < PF)
         {
             const int64_t jp = j0 + pfd + lane;
-            if (jp <= cy1) l2_prefetch_bulk(src + jp * ld + rbase, pf_bytes);
+            if (jp <= cy1) l2_prefetch_bulk(src + jp * ld + pf_lo, pf_bytes);
         }
         Cells<T, VEC> nxt[PF];
         T hn[PF], hs[PF];

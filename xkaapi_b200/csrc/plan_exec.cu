@@ -138,8 +138,11 @@ static int issue_host_copies(std::vector<HostCopy> & v, cudaMemcpyKind kind, cud
     coalesce(v);
     for (const HostCopy & c : v)
     {
-        cudaError_t e = cudaMemcpy2DAsync((void *) c.dst, (size_t) c.dp, (const void *) c.src, (size_t) c.sp, (size_t) c.width,
-                                          (size_t) c.rows, kind, st);
+        // a contiguous range (one row, or full-pitch rows) as a plain copy, else pitched
+        const bool flat = c.rows == 1 || (c.width == c.sp && c.width == c.dp);
+        cudaError_t e = flat ? cudaMemcpyAsync((void *) c.dst, (const void *) c.src, (size_t) (c.width * c.rows), kind, st)
+                             : cudaMemcpy2DAsync((void *) c.dst, (size_t) c.dp, (const void *) c.src, (size_t) c.sp,
+                                                 (size_t) c.width, (size_t) c.rows, kind, st);
         if (e != cudaSuccess) return xkb_set_cuda_error(e);
     }
     v.clear();
