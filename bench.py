@@ -124,13 +124,21 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest x over all ranks (every rank calls it in the same order; NCCL reduces a device
+    tensor, gloo a host one)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank, world, seconds_this_rank):
+    """Whole-job throughput of `world` replicas: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / max_over_ranks(seconds_this_rank, world)
 
 
 def cells_all(nx, ny):

@@ -58,6 +58,9 @@ __device__ __forceinline__ void axpby_team(int64_t lo, int64_t hi, double a, con
 constexpr int SCHED_THREADS = 256;
 
 constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (bulk tile body)
+#ifndef XKB_TILE_PF
+#define XKB_TILE_PF 4                    // east columns a tile strip loads ahead into registers
+#endif
 
 // Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
 __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps, int pfd)
@@ -67,14 +70,14 @@ __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int war
         case XKB_TASK_HEAT_F64: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
-            heat_tile_team<double, 2, 4, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
+            heat_tile_team<double, 2, XKB_TILE_PF, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
                                                h.x0, h.x1, h.y0, h.y1, h.c, vok, pfd, warp, nwarps);
             break;
         }
         case XKB_TASK_HEAT_F32: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 4 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
-            heat_tile_team<float, 4, 4, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
+            heat_tile_team<float, 4, XKB_TILE_PF, true>((const float *) h.src, (float *) h.dst, h.ld, h.nx, h.ny,
                                               h.x0, h.x1, h.y0, h.y1, h.c, vok, pfd, warp, nwarps);
             break;
         }
