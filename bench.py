@@ -555,7 +555,7 @@ def main():
         a32 = host.to(device="cuda", dtype=torch.float32); b32 = a32.clone()
         res32, g32, t32 = build_heat_graph(xk, torch, a32, b32, NX, NY, TS, STEPS, stream, esize=4)
         d32 = xk.heat_task_descs((a32.data_ptr(), b32.data_ptr()), NX, NY, NX, TS, TS, STEPS, COEF, f32=True)
-        s32 = xk.Scheduler(stream); s32.set_tasks(d32); del d32
+        s32 = xk.Scheduler(stream); s32.set_team(1); s32.set_tasks(d32); del d32   # one warp per FP32 tile
         with torch.cuda.stream(stream):
             s32.run(g32); s32.wait()
         out32 = (a32 if STEPS % 2 == 0 else b32).double()

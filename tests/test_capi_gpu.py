@@ -30,14 +30,17 @@ def test_ordering_programs(torch_cuda, tmp_path):
     assert out["tasks"] == 6 and out["edges"] >= 4
 
 
-@pytest.mark.parametrize("every", [0, 3])
-def test_heat_example(torch_cuda, tmp_path, every):
+@pytest.mark.parametrize("every,chunk", [(0, None), (3, None), (0, 64), (3, 64)])
+def test_heat_example(torch_cuda, tmp_path, every, chunk):
     nx, ny, ts, steps = 200, 136, 64, 7
     g = O.heat_init(nx, ny, seed=4)
     g.tofile(tmp_path / "init.bin")
     exe = build("heat_capi", tmp_path)
+    env = dict(os.environ)
+    if chunk:
+        env["XKB_RESOLVE_CHUNK"] = str(chunk)         # resolution in the background while spawning
     r = subprocess.run([exe, str(nx), str(ny), str(ts), str(steps), str(every), str(tmp_path / "init.bin"),
-                        str(tmp_path / "out.bin"), str(tmp_path / "sums.txt")], capture_output=True, text=True)
+                        str(tmp_path / "out.bin"), str(tmp_path / "sums.txt")], capture_output=True, text=True, env=env)
     assert r.returncode == 0, r.stderr
     stats = json.loads(r.stdout)
     out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)

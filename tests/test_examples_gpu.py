@@ -89,3 +89,27 @@ def test_axpby_xkrt_long_chunks_split(torch_cuda, tmp_path):
     assert lines[0]["checksum"] == lines[1]["checksum"]
     np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin"), O.axpby_chain_run(x, y, chunks))
     assert lines[0]["h2d_bytes"] >= 2 * 8 * n and lines[0]["d2h_bytes"] >= 8 * n
+
+
+@pytest.mark.parametrize("chunk", [64, 1024])
+def test_background_resolution_small_chunks(torch_cuda, tmp_path, chunk):
+    """With a small resolver batch the runtime's worker thread resolves chunks of spawned tasks
+    while spawning goes on; the heat and axpby results stay the oracle's, bit for bit."""
+    env = dict(os.environ, XKB_RESOLVE_CHUNK=str(chunk))
+    nx, ny, ts, steps = 300, 170, 32, 9
+    g = O.heat_init(nx, ny, seed=17)
+    g.tofile(tmp_path / "init.bin")
+    r = subprocess.run([EXE] + [str(v) for v in (nx, ny, ts, steps, 2, 0, tmp_path / "init.bin", tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(l) for l in r.stdout.strip().splitlines()]
+    assert lines[0]["edges"] == lines[1]["edges"]
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), O.heat_run(g, nx, ny, steps, 0.2))
+    n, passes, seed, cmin, cmax = 200_000, 6, 3, 64, 65536
+    x, y, chunks = O.axpby_chain(n, passes, seed, cmin, cmax)
+    x.tofile(tmp_path / "x.bin"); y.tofile(tmp_path / "y.bin")
+    r = subprocess.run([AXPBY_EXE] + [str(v) for v in (n, passes, seed, 1, cmin, cmax, tmp_path / "x.bin", tmp_path / "y.bin",
+                                                      tmp_path / "out.bin")], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout.strip().splitlines()[-1])["tasks"] == len(chunks)
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin"), O.axpby_chain_run(x, y, chunks))

@@ -2,8 +2,8 @@
 // per-batch pools (spawned tasks, their arguments and accesses, the access records). Growing
 // remaps the pages (mremap) instead of copying them, and the range is marked for transparent
 // huge pages, so filling millions of entries costs one page fault per 2 MB rather than per 4 KB
-// and no copy at all. Element addresses change when the array grows; they are stable while it
-// does not.
+// and no copy at all. Element addresses change when the array grows (stable while it does not),
+// unless the array was given a fixed address-space reservation up front (reserve_fixed).
 #pragma once
 
 #include <sys/mman.h>
@@ -57,12 +57,27 @@ public:
     void release()
     {
         if (p_) munmap(p_, bytes_);
-        p_ = nullptr; n_ = 0; bytes_ = 0;
+        p_ = nullptr; n_ = 0; bytes_ = 0; fixed_ = false;
     }
+    // Reserve `max_elems` elements of address space up front (pages are only backed when first
+    // touched): the array then never moves, so another thread may read elements below a size it
+    // was handed while this one keeps appending. false (array unchanged) if the reservation fails.
+    bool reserve_fixed(size_t max_elems)
+    {
+        if (p_) return false;
+        const size_t nb = max_elems * sizeof(T);
+        void * q = mmap(nullptr, nb, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+        if (q == MAP_FAILED) return false;
+        madvise(q, nb, MADV_HUGEPAGE);
+        p_ = (T *) q; bytes_ = nb; fixed_ = true;
+        return true;
+    }
+    bool fixed() const { return fixed_; }
 
 private:
     bool grow(size_t need)
     {
+        if (fixed_) return false;                 // a fixed reservation never moves
         constexpr size_t HUGE = size_t(2) << 20;
         size_t nb = bytes_ ? 2 * bytes_ : size_t(32) << 20;
         while (nb < need) nb *= 2;
@@ -77,6 +92,7 @@ private:
 
     T * p_ = nullptr;
     size_t n_ = 0, bytes_ = 0;
+    bool fixed_ = false;
 };
 
 } // namespace xkb

@@ -1070,6 +1070,21 @@ extern "C" int xkb_resolver_destroy(xkb_resolver_t * R)
     return XKB_OK;
 }
 
+// Library-internal: forget every task and domain but keep the device work buffers, so the
+// next graph resolves without allocating them again.
+int xkb_internal_resolver_reset(xkb_resolver_t * R)
+{
+    if (!R) return xkb_set_error(XKB_EINVAL, "resolver_reset: null resolver");
+    XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
+    R->interval.xs.clear(); R->interval.ys.clear(); R->interval.ncells = 0; R->interval.ops.clear();
+    R->blas.clear(); R->blas_index.clear(); R->segments.clear();
+    R->ntasks = 0; R->nuniq = 0; R->graph_valid = false;
+    if (R->useg.size() > 1) { R->useg.resize(1); R->useg_n.resize(1); }   // keep the first edge segment
+    for (size_t & n : R->useg_n) n = 0;
+    R->spill_used = 0;
+    return XKB_OK;
+}
+
 extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * recs, size_t n)
 {
     if (!R || (n && !recs)) return xkb_set_error(XKB_EINVAL, "resolver_add: bad arguments");

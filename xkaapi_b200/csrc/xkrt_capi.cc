@@ -18,10 +18,12 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <new>
 #include <thread>
@@ -29,6 +31,10 @@
 #include <vector>
 
 struct xkb_runtime;
+
+// Accesses per resolver batch: the resolver's working set grows with the batch, and batches of
+// about a million accesses keep it small while amortising each batch's fixed costs.
+constexpr size_t RESOLVE_CHUNK = size_t(1) << 20;
 
 namespace {
 
@@ -65,6 +71,21 @@ struct xkb_runtime {
     xkb::PoolArray<void *> replica_pool;              // sized to acc_pool at wait
     xkb::PoolArray<xkb_access_rec_t> recs;            // one record per access, same index (wait)
     bool in_wait = false;
+    // background resolution: with fixed pools, a worker thread resolves chunks of spawned tasks
+    // on the GPU while the program keeps spawning (the reference resolves at spawn time too)
+    bool bg = false;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t handed = 0, handed_acc = 0;                // tasks / accesses handed to the worker
+    size_t claimed = 0, done = 0;                     // tasks the worker took / finished
+    bool stop = false;
+    int bg_rc = XKB_OK;
+    std::string bg_err;                               // the worker's error text
+    int device = 0;
+    size_t chunk = 0;                                 // accesses per resolver batch
+    xkb_resolver_t * res = nullptr;                   // resolver of the batch being spawned
+    bool res_stale = false;                           // res still holds the previous batch
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
     std::map<uint64_t, Region> regions;               // host base -> region
@@ -93,6 +114,18 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     if (!R) return xkb_set_error(XKB_ENOMEM, "xkrt_init: out of host memory");
     int n = 0;
     R->gpu = cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+    if (R->gpu) cudaGetDevice(&R->device);
+    R->chunk = RESOLVE_CHUNK;
+    if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
+        R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
+    // fixed pools (address space only; pages are backed when touched) let a worker thread read
+    // spawned tasks while spawning continues; without them resolution waits for xkrt_task_wait
+    {
+        constexpr size_t MAXT = size_t(1) << 28, MAXA = size_t(1) << 29;
+        R->bg = R->gpu && R->pending.reserve_fixed(MAXT) && R->args_pool.reserve_fixed(MAXT * 64) &&
+                R->acc_pool.reserve_fixed(MAXA) && R->recs.reserve_fixed(MAXA) && R->replica_pool.reserve_fixed(MAXA);
+        if (!R->bg) { R->pending.release(); R->args_pool.release(); R->acc_pool.release(); R->recs.release(); R->replica_pool.release(); }
+    }
     int rc = xkb_planner_create_resident(&R->planner);
     if (rc == XKB_OK && R->gpu)
     {
@@ -109,6 +142,13 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     xkb_runtime * R = RT(runtime);
     if (!R) return xkb_set_error(XKB_EINVAL, "xkrt_deinit: null runtime");
     if (!R->pending.empty()) xkrt_task_wait(runtime);
+    if (R->worker.joinable())
+    {
+        { std::lock_guard<std::mutex> lk(R->mu); R->stop = true; }
+        R->cv.notify_all();
+        R->worker.join();
+    }
+    if (R->res) { xkb_resolver_destroy(R->res); R->res = nullptr; }
     if (R->stream) cudaStreamSynchronize(R->stream);
     for (auto & kv : R->regions)
     {
@@ -123,10 +163,14 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     return st;
 }
 
+static void bg_finish(xkb_runtime * R);
+
 extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
-    if (R) { R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear(); }
+    if (!R) return;
+    bg_finish(R);
+    R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
 }
 
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned)
@@ -245,6 +289,8 @@ extern "C" int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks,
 
 // ---- spawn -----------------------------------------------------------------------------------
 
+static void bg_hand_over(xkb_runtime * R, bool final);
+
 static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
                   const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
 {
@@ -268,6 +314,7 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
         return;
     }
     if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
+    if (R->bg) bg_hand_over(R, false);
 }
 
 extern "C" void xkrt_task_spawn_generic(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
@@ -375,15 +422,26 @@ static bool is_device(const xkb_runtime * R, const Task & t)
     return (t.flags & TASK_FLAG_DEVICE) && t.device != HOST_DEVICE_GLOBAL_ID && (f.builtin >= 0 || f.f[XKRT_TASK_FORMAT_TARGET_CUDA]);
 }
 
-static void * mirror_of(xkb_runtime * R, uint64_t host)
+// Last region a lookup hit (consecutive lookups mostly hit the same one).
+struct RegionHint { uint64_t base = 0, end = 0; uint8_t * mirror = nullptr; };
+
+static void * mirror_lookup(const xkb_runtime * R, uint64_t host, RegionHint & h)
 {
-    if (host >= R->last_base && host < R->last_end) return R->last_mirror + (host - R->last_base);   // same region as last time
+    if (host >= h.base && host < h.end) return h.mirror + (host - h.base);
     auto it = R->regions.upper_bound(host);
     if (it == R->regions.begin()) return nullptr;
     --it;
     if (host >= it->first + it->second.size || !it->second.mirror) return nullptr;
-    R->last_base = it->first; R->last_end = it->first + it->second.size; R->last_mirror = (uint8_t *) it->second.mirror;
+    h.base = it->first; h.end = it->first + it->second.size; h.mirror = (uint8_t *) it->second.mirror;
     return (uint8_t *) it->second.mirror + (host - it->first);
+}
+
+static void * mirror_of(xkb_runtime * R, uint64_t host)
+{
+    RegionHint h{R->last_base, R->last_end, R->last_mirror};
+    void * p = mirror_lookup(R, host, h);
+    R->last_base = h.base; R->last_end = h.end; R->last_mirror = h.mirror;
+    return p;
 }
 
 static int run_copies(xkb_runtime * R)
@@ -404,20 +462,30 @@ static int run_copies(xkb_runtime * R)
 }
 
 // Point a built-in descriptor's host addresses at the device mirrors.
-static int translate(xkb_runtime * R, xkb_task_desc_t & d)
+// false when a pointer lies outside every registered region (no error text: callable from
+// several threads at once)
+static bool translate_hint(const xkb_runtime * R, xkb_task_desc_t & d, RegionHint & h)
 {
     if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
     {
-        void * s = mirror_of(R, d.u.heat.src), * t = mirror_of(R, d.u.heat.dst);
-        if (!s || !t) return xkb_set_error(XKB_EINVAL, "heat task: grid outside every registered region");
+        void * s = mirror_lookup(R, d.u.heat.src, h), * t = mirror_lookup(R, d.u.heat.dst, h);
+        if (!s || !t) return false;
         d.u.heat.src = (uint64_t) s; d.u.heat.dst = (uint64_t) t;
     }
     else if (d.kind == XKB_TASK_AXPBY)
     {
-        void * x = mirror_of(R, d.u.axpby.x), * y = mirror_of(R, d.u.axpby.y);
-        if (!x || !y) return xkb_set_error(XKB_EINVAL, "axpby task: vector outside every registered region");
+        void * x = mirror_lookup(R, d.u.axpby.x, h), * y = mirror_lookup(R, d.u.axpby.y, h);
+        if (!x || !y) return false;
         d.u.axpby.x = (uint64_t) x; d.u.axpby.y = (uint64_t) y;
     }
+    return true;
+}
+
+static int translate(xkb_runtime * R, xkb_task_desc_t & d)
+{
+    RegionHint h{R->last_base, R->last_end, R->last_mirror};
+    if (!translate_hint(R, d, h)) return xkb_set_error(XKB_EINVAL, "task %s outside every registered region",
+                                                       d.kind == XKB_TASK_AXPBY ? "vector" : "grid");
     return XKB_OK;
 }
 
@@ -622,38 +690,27 @@ static int split_moldable(const xkb_task_desc_t * descs, size_t nt, const xkb_ta
     return XKB_OK;
 }
 
-// Records per resolver batch: the resolver's working set grows with the batch, and batches of
-// about a million accesses keep it small while amortising each batch's fixed costs.
-constexpr size_t RESOLVE_CHUNK = size_t(1) << 20;
 
-static int wait_batch(xkb_runtime * R)
+// Records of tasks [t0, t1) (accesses [a0, a1)) into R->recs at their access indices, then into
+// the batch's resolver: directly when every task has a tracked access, else compacted with a
+// one-byte virtual read of the task's own Task object for a task without one (nothing else
+// touches it), so that task numbering stays dense.
+static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1)
 {
-    R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
-    R->last_h2d_bytes = R->last_d2h_bytes = 0;
-    for (double & m : R->last_ms) m = 0;
-    if (R->pending.empty()) return XKB_OK;
-    if (!R->gpu) return xkb_set_error(XKB_ENODEV, "xkrt_task_wait: dependency resolution runs on the GPU and none is visible");
-    auto t0 = std::chrono::steady_clock::now();
-    // (1) dependencies. One record per access, at the access's own index (type REC_NONE when
-    // the access names nothing the runtime tracks). The resolver is fed these records directly
-    // when every task has one; otherwise a compacted copy where a task without any gets a
-    // one-byte virtual read of its own Task object (nothing else touches it), so that the task
-    // numbering stays dense.
-    const size_t nacc = R->acc_pool.size(), ntasks = R->pending.size();
-    if (!R->replica_pool.resize(nacc) || !R->recs.resize(nacc)) return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
-    if (nacc) memset(R->replica_pool.data(), 0, nacc * sizeof(void *));
+    if (t0 >= t1) return XKB_OK;
+    if (!R->recs.resize(a1)) return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
     xkb_access_rec_t * recs = R->recs.data();
     std::atomic<bool> dense(true);
-    parallel_chunks(ntasks, [&](size_t b, size_t e) {
+    parallel_chunks(t1 - t0, [&](size_t b, size_t e) {
         bool d = true;
-        for (size_t t = b; t < e; ++t)
+        for (size_t t = t0 + b; t < t0 + e; ++t)
         {
             const Task & T = R->pending[t];
             bool any = false;
-            for (uint32_t a = 0; a < T.nacc; ++a)
+            for (uint32_t k = 0; k < T.nacc; ++k)
             {
-                xkb_access_rec_t & r = recs[T.acc_off + a];
-                if (to_rec(R->acc_pool[T.acc_off + a], (uint32_t) t, r)) any = true;
+                xkb_access_rec_t & r = recs[T.acc_off + k];
+                if (to_rec(R->acc_pool[T.acc_off + k], (uint32_t) t, r)) any = true;
                 else { r.type = REC_NONE; d = false; }
             }
             d = d && any;
@@ -663,13 +720,13 @@ static int wait_batch(xkb_runtime * R)
     std::vector<xkb_access_rec_t> all;
     if (!dense)
     {
-        all.reserve(nacc + 16);
-        for (size_t t = 0; t < ntasks; ++t)
+        all.reserve(a1 - a0 + 16);
+        for (size_t t = t0; t < t1; ++t)
         {
             const Task & T = R->pending[t];
             bool any = false;
-            for (uint32_t a = 0; a < T.nacc; ++a)
-                if (recs[T.acc_off + a].type != REC_NONE) { all.push_back(recs[T.acc_off + a]); any = true; }
+            for (uint32_t k = 0; k < T.nacc; ++k)
+                if (recs[T.acc_off + k].type != REC_NONE) { all.push_back(recs[T.acc_off + k]); any = true; }
             if (!any)
             {
                 xkb_access_rec_t r;
@@ -680,23 +737,109 @@ static int wait_batch(xkb_runtime * R)
             }
         }
     }
-    const xkb_access_rec_t * feed = dense ? recs : all.data();
-    const size_t nfeed = dense ? nacc : all.size();
-    const double records_ms = ms_since(t0);
-    xkb_resolver_t * res = nullptr;
-    int rc = xkb_resolver_create(&res, R->stream);
-    if (rc) return rc;
+    const xkb_access_rec_t * feed = dense ? recs + a0 : all.data();
+    const size_t nfeed = dense ? a1 - a0 : all.size();
+    int rc = XKB_OK;
+    if (!R->res && (rc = xkb_resolver_create(&R->res, R->stream))) return rc;
+    if (R->res_stale && (rc = xkb_internal_resolver_reset(R->res))) return rc;
+    R->res_stale = false;
     for (size_t b = 0; b < nfeed && rc == XKB_OK;)
     {
-        size_t e = std::min(nfeed, b + RESOLVE_CHUNK);
+        size_t e = std::min(nfeed, b + R->chunk);
         while (e < nfeed && feed[e].task == feed[e - 1].task) ++e;     // whole tasks per batch
-        rc = xkb_resolver_add(res, feed + b, e - b);
+        rc = xkb_resolver_add(R->res, feed + b, e - b);
         b = e;
     }
-    all.clear(); all.shrink_to_fit();
+    return rc;
+}
+
+static void bg_worker(xkb_runtime * R)
+{
+    cudaSetDevice(R->device);
+    for (;;)
+    {
+        size_t t0, t1, a0, a1;
+        bool failed;
+        {
+            std::unique_lock<std::mutex> lk(R->mu);
+            R->cv.wait(lk, [&] { return R->stop || R->handed > R->claimed; });
+            if (R->handed == R->claimed) return;          // stop, nothing pending
+            t0 = R->claimed; t1 = R->handed;
+            a0 = R->pending[t0].acc_off; a1 = R->handed_acc;
+            R->claimed = t1;
+            failed = R->bg_rc != XKB_OK;
+        }
+        const int rc = failed ? XKB_OK : resolve_range(R, t0, t1, a0, a1);
+        {
+            std::lock_guard<std::mutex> lk(R->mu);
+            if (rc && R->bg_rc == XKB_OK) { R->bg_rc = rc; R->bg_err = xkb_last_error(); }
+            R->done = t1;
+        }
+        R->cv.notify_all();
+    }
+}
+
+// Hand the tasks spawned since the last hand-over to the worker: once they hold a batch's worth
+// of accesses, or all of them (final) when the program waits.
+static void bg_hand_over(xkb_runtime * R, bool final)
+{
+    const size_t nacc = R->acc_pool.size(), nt = R->pending.size();
+    if (nt == R->handed || (!final && nacc - R->handed_acc < R->chunk)) return;
+    {
+        std::lock_guard<std::mutex> lk(R->mu);
+        R->handed = nt; R->handed_acc = nacc;
+    }
+    if (!R->worker.joinable()) R->worker = std::thread(bg_worker, R);
+    R->cv.notify_all();
+}
+
+// Wait until the worker has resolved everything handed to it.
+static void bg_wait_done(xkb_runtime * R)
+{
+    std::unique_lock<std::mutex> lk(R->mu);
+    R->cv.wait(lk, [&] { return R->done == R->handed; });
+}
+
+// End of a batch: no work in flight, counters and the batch's resolver reset.
+static void bg_finish(xkb_runtime * R)
+{
+    if (R->worker.joinable()) bg_wait_done(R);
+    R->handed = R->handed_acc = R->claimed = R->done = 0;
+    R->bg_rc = XKB_OK;
+    R->bg_err.clear();
+    R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
+}
+
+static int wait_batch(xkb_runtime * R)
+{
+    R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
+    R->last_h2d_bytes = R->last_d2h_bytes = 0;
+    for (double & m : R->last_ms) m = 0;
+    if (R->pending.empty()) return XKB_OK;
+    if (!R->gpu) return xkb_set_error(XKB_ENODEV, "xkrt_task_wait: dependency resolution runs on the GPU and none is visible");
+    auto t0 = std::chrono::steady_clock::now();
+    // (1) dependencies: everything not yet handed to the background worker is resolved now
+    // (by the worker when it runs, so that chunks stay in spawn order), then the graph is built
+    const size_t nacc = R->acc_pool.size(), ntasks = R->pending.size();
+    int rc = XKB_OK;
+    if (R->worker.joinable())
+    {
+        bg_hand_over(R, true);
+        bg_wait_done(R);
+        if ((rc = R->bg_rc)) xkb_set_error(rc, "%s", R->bg_err.c_str());
+    }
+    else
+        rc = resolve_range(R, 0, ntasks, 0, nacc);
+    if (rc == XKB_OK && (!R->replica_pool.resize(nacc) || !R->recs.resize(nacc)))
+        rc = xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
+    if (rc) return rc;
+    if (nacc) memset(R->replica_pool.data(), 0, nacc * sizeof(void *));
+    xkb_access_rec_t * recs = R->recs.data();
+    const double records_ms = ms_since(t0);
+    xkb_resolver_t * res = R->res;
     xkb_task_graph_t g;
     if (rc == XKB_OK) rc = xkb_resolver_graph(res, &g);
-    if (rc) { xkb_resolver_destroy(res); return rc; }
+    if (rc) return rc;
     R->last_edges = g.nedges;
     R->last_ms[0] = ms_since(t0);
     if (getenv("XKB_TRACE_WAIT"))
@@ -730,17 +873,26 @@ static int wait_batch(xkb_runtime * R)
         std::vector<xkb_task_desc_t> copy;
         xkb_task_desc_t * descs = (xkb_task_desc_t *) R->args_pool.data();
         if (!dense_args) { copy.resize(nt); descs = copy.data(); }
-        for (size_t t = 0; t < nt && rc == XKB_OK; ++t)
-        {
-            const Task & T = R->pending[t];
-            if (!dense_args)
-            {
-                if (T.nargs < sizeof(xkb_task_desc_t)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
-                memcpy(&descs[t], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
-            }
-            descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
-            rc = translate(R, descs[t]);
-        }
+        std::atomic<size_t> bad_args(SIZE_MAX), bad_ptr(SIZE_MAX);     // first failing task, if any
+        if (rc == XKB_OK)
+            parallel_chunks(nt, [&](size_t b, size_t e) {
+                RegionHint h;
+                for (size_t t = b; t < e; ++t)
+                {
+                    const Task & T = R->pending[t];
+                    if (!dense_args)
+                    {
+                        if (T.nargs < sizeof(xkb_task_desc_t)) { size_t x = bad_args; while (t < x && !bad_args.compare_exchange_weak(x, t)) {} continue; }
+                        memcpy(&descs[t], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
+                    }
+                    descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
+                    if (!translate_hint(R, descs[t], h)) { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
+                }
+            });
+        if (rc == XKB_OK && bad_args != SIZE_MAX)
+            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", (size_t) bad_args);
+        else if (rc == XKB_OK && bad_ptr != SIZE_MAX)
+            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region", (size_t) bad_ptr);
         const double desc_ms = ms_since(t0) - fetch_ms;
         SplitGraph sg;
         bool split = false;
@@ -748,6 +900,11 @@ static int wait_batch(xkb_runtime * R)
         const xkb_task_graph_t & run_g = split ? sg.g : g;
         if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size())
                                      : xkb_internal_sched_set_tasks_device(R->sched, descs, nt);
+        // warps per task: FP32-storage tiles (128 rows per strip) run best one warp per task,
+        // everything else two (measured on the 16384^2 graphs)
+        bool all_f32 = true;
+        for (size_t t = 0; t < nt && all_f32; t += 1 + nt / 64) all_f32 = descs[t].kind == XKB_TASK_HEAT_F32;
+        if (rc == XKB_OK) rc = xkb_sched_set_team(R->sched, all_f32 ? 1 : 2);
         if (getenv("XKB_TRACE_WAIT"))
             fprintf(stderr, "xkrt_task_wait: fetches + copies %.1f ms, descriptors %.1f ms, upload %.1f ms\n", fetch_ms, desc_ms,
                     ms_since(t0) - fetch_ms - desc_ms);
@@ -828,7 +985,6 @@ static int wait_batch(xkb_runtime * R)
         if (getenv("XKB_TRACE_WAIT"))
             fprintf(stderr, "xkrt_task_wait: write-back fetches %.1f ms, copies %.1f ms\n", fetch_ms, R->last_ms[3] - fetch_ms);
     }
-    xkb_resolver_destroy(res);
     return rc;
 }
 
@@ -859,6 +1015,7 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     if (!R) return;
     R->in_wait = true;
     fail(R, wait_batch(R));
+    bg_finish(R);
     R->in_wait = false;
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
 }
