@@ -61,6 +61,9 @@ constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (b
 #ifndef XKB_TILE_PF
 #define XKB_TILE_PF 4                    // east columns a tile strip loads ahead into registers
 #endif
+#ifndef XKB_SCHED_MINB
+#define XKB_SCHED_MINB 2                 // persistent CTAs resident per SM (register budget)
+#endif
 
 // Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
 __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps, int pfd)
@@ -155,7 +158,7 @@ __device__ __forceinline__ void team_sync(int id, int nthreads)
 constexpr size_t bulk_smem_bytes(int nbuf) { return (size_t) (SCHED_THREADS / 32) * nbuf * (BULK_SLOT_BYTES + 8); }
 
 template <int TEAM_WARPS, bool BULK = false, int NBUF = SCHED_BULK_NBUF>
-__global__ void __launch_bounds__(SCHED_THREADS, 2) sched_persistent_kernel(SchedArgs a)
+__global__ void __launch_bounds__(SCHED_THREADS, XKB_SCHED_MINB) sched_persistent_kernel(SchedArgs a)
 {
     constexpr int NTEAMS = (SCHED_THREADS / 32) / TEAM_WARPS;
     constexpr int TEAM_THREADS = TEAM_WARPS * 32;
