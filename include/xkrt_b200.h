@@ -50,6 +50,7 @@ XKB_API const char * xkb_version(void);
 #define XKB_ACCESS_MODE_RW  3
 #define XKB_ACCESS_MODE_V   4
 #define XKB_ACCESS_MODE_D   8
+#define XKB_ACCESS_TYPE_HANDLE      0
 #define XKB_ACCESS_TYPE_SEGMENT     1
 #define XKB_ACCESS_TYPE_BLAS_MATRIX 2
 
@@ -58,7 +59,10 @@ XKB_API const char * xkb_version(void);
  * task_dependency_resolve, src/task/task.cc:285-299).
  *  matrix : addr = storage base, ld, offset_m, offset_n, m, n, sizeof_type -- the
  *           arguments of access_t's matrix constructor (include/xkrt/memory/access/access.hpp:539-574)
- *  segment: byte interval [addr, ld)  -- access_t's segment constructor (access.hpp:479-514) */
+ *  segment: byte interval [addr, ld)  -- access_t's segment constructor (access.hpp:479-514)
+ *  handle : addr = the handle (an opaque pointer naming an object, not memory) -- access_t's
+ *           handle constructor; resolved like the reference's DependencyMap
+ *           (include/xkrt/memory/access/handle/dependency-map.hpp), sequential accesses */
 typedef struct xkb_access_rec_t {
     uint32_t task;
     uint8_t  type;

@@ -13,9 +13,10 @@
  * planner: one device mirror per registered host region, H2D/D2H only for blocks the target
  * lacks), runs the tasks -- every task on the device scheduler's persistent kernel when all are
  * built-in device bodies, else one by one in spawn order (host bodies on the calling thread) --
- * and leaves host memory coherent when it returns. Handle accesses and moldable tasks are not
- * supported. Functions that return void in the reference record failures instead; read them
- * with xkb_runtime_status().
+ * and leaves host memory coherent when it returns. Handle accesses order tasks like the
+ * reference's DependencyMap (they carry no data); concurrent-mode accesses and user moldable
+ * tasks are not supported. Functions that return void in the reference record failures
+ * instead; read them with xkb_runtime_status().
  */
 #ifndef XKRT_B200_CAPI_H
 #define XKRT_B200_CAPI_H

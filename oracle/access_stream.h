@@ -12,6 +12,7 @@
  *                  the arguments of access_t's matrix constructor (access.hpp:539-574).
  *   segment access (ACCESS_TYPE_SEGMENT = 1): byte interval [addr, ld) -- the two
  *                  addresses of access_t's segment constructor (access.hpp:479-514).
+ *   handle access  (ACCESS_TYPE_HANDLE = 0): addr = the handle (access_t's handle constructor).
  *   mode: xkrt_access_mode_t bits (R=1, W=2, V=4, D=8; include/xkrt/memory/access/mode.h:54-66).
  */
 #ifndef XK_ORACLE_ACCESS_STREAM_H
@@ -21,6 +22,7 @@
 #include <stdio.h>
 
 #define XK_STREAM_MAGIC   0x314d525453424b58ull   /* "XKBSTRM1" */
+#define XK_STREAM_HANDLE  0
 #define XK_STREAM_SEGMENT 1
 #define XK_STREAM_MATRIX  2
 

@@ -19,6 +19,10 @@
 //               else if writer: edge writer -> A.
 //      PUT(A):  if (A.mode & W): writer = A, readers = {}; else if A.mode == R exactly:
 //               readers += A.
+//  * handles (include/xkrt/memory/access/handle/dependency-map.hpp:157-297): a map from handle
+//    to {last writer, readers}, one point per handle in its own domain, the same LINK, and PUT
+//    recording every mode with the R bit and without the W bit as a reader (sequential and
+//    commutative accesses; the concurrent mode's extra nodes are not restated).
 //  The reference stores the state on tree nodes; its edges are the union of the per-point
 //  edges, so this oracle keeps the state per elementary cell of the domain's coordinate
 //  compression and reports the unique (pred task, succ task) pairs.
@@ -79,6 +83,12 @@ static void add_ops(Domain & d, bool link, const xk_stream_rec_t & r)
 {
     Rect rects[3];
     int n;
+    if (r.type == XK_STREAM_HANDLE)
+    {
+        const uint8_t m = ((r.mode & MODE_R) && !(r.mode & MODE_W)) ? MODE_R : r.mode;
+        d.ops.push_back({link, r.task, m, Rect{r.addr, r.addr + 1, 0, 1}});
+        return;
+    }
     if (d.interval) { rects[0] = {r.addr, r.ld, 0, 1}; n = 1; }
     else if (r.type == XK_STREAM_SEGMENT) n = segment_rects(r.addr, r.ld, d.ld, d.s, rects);
     else n = matrix_rects(r, rects);
@@ -145,6 +155,7 @@ int main(int argc, char ** argv)
 
     // Build every domain's op sequence in the order the reference performs them.
     Domain interval{true, 0, 0, {}};
+    Domain handles{true, 0, 0, {}};
     std::vector<Domain> blas;
     std::map<std::pair<uint64_t, uint64_t>, size_t> blas_index;
     std::vector<size_t> segments_so_far;   // indices into recs, spawn order
@@ -157,7 +168,8 @@ int main(int argc, char ** argv)
         for (size_t a = i; a < j; ++a)   // LINK pass
         {
             const auto & r = recs[a];
-            if (r.type == XK_STREAM_SEGMENT)
+            if (r.type == XK_STREAM_HANDLE) add_ops(handles, true, r);
+            else if (r.type == XK_STREAM_SEGMENT)
             {
                 add_ops(interval, true, r);
                 for (auto & d : blas) add_ops(d, true, r);
@@ -180,7 +192,8 @@ int main(int argc, char ** argv)
         for (size_t a = i; a < j; ++a)   // PUT pass
         {
             const auto & r = recs[a];
-            if (r.type == XK_STREAM_SEGMENT)
+            if (r.type == XK_STREAM_HANDLE) add_ops(handles, false, r);
+            else if (r.type == XK_STREAM_SEGMENT)
             {
                 add_ops(interval, false, r);
                 for (auto & d : blas) add_ops(d, false, r);
@@ -194,6 +207,7 @@ int main(int argc, char ** argv)
 
     std::vector<std::pair<uint32_t, uint32_t>> edges;
     run_domain(interval, edges);
+    run_domain(handles, edges);
     for (auto & d : blas) run_domain(d, edges);
     const size_t cell_edges = edges.size();
     std::sort(edges.begin(), edges.end());

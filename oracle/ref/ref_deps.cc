@@ -64,6 +64,8 @@ int main(int argc, char ** argv)
             if (r.type == XK_STREAM_MATRIX)
                 new (accesses + (a - i)) access_t(task, MATRIX_COLMAJOR, (const void *) r.addr, r.ld,
                                                   r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type, mode);
+            else if (r.type == XK_STREAM_HANDLE)
+                new (accesses + (a - i)) access_t(task, (const void *) r.addr, mode);
             else
                 new (accesses + (a - i)) access_t(task, (uintptr_t) r.addr, (uintptr_t) r.ld, mode);
         }

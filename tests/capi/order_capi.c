@@ -3,6 +3,7 @@
  *   tests/task-dependency-interval-matrix.cc:84-160  interval W [0,100) -> matrix W (3, ld 8, 8x8, s=1)
  *                                                    -> interval W [0,100)
  *   tests/api/c/task-with-access.c:52-90             a team task with a VW segment access
+ *   tests/task-dependency-handle.cc:86-119           W -> R -> RW on one handle
  * Host task bodies check that they run in spawn order (each finds the counter at its own index).
  * Exit status 0 = success. */
 #include <stdio.h>
@@ -67,6 +68,17 @@ int main(void)
     uint64_t tasks = 0, edges = 0;
     xkb_runtime_last_wait(rt, &tasks, &edges, NULL, NULL, NULL);
 
+    /* handle chain: the handle names an object, not memory */
+    for (int t = 6; t < 9; ++t)
+    {
+        xkrt_access_t a = {ACCESS_CONCURRENCY_SEQUENTIAL, modes[t - 6], ACCESS_SCOPE_NONUNIFIED, ACCESS_TYPE_HANDLE, {{0}}};
+        a.region.handle.addr = &counter;
+        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, &t, sizeof(t), &a, 1);
+    }
+    xkrt_task_wait(rt);
+    uint64_t hedges = 0;
+    xkb_runtime_last_wait(rt, NULL, &hedges, NULL, NULL, NULL);
+
     /* team task with a virtual write */
     xkrt_team_t * team = xkrt_team_driver_device_get(rt, XKRT_DRIVER_TYPE_HOST, 0);
     xkrt_access_t vw = segment(ACCESS_MODE_VW, (void *) 0, (void *) 1);
@@ -75,7 +87,8 @@ int main(void)
 
     const int st = xkb_runtime_status(rt);
     if (xkrt_deinit(rt) != 0 || st != 0) { fprintf(stderr, "status %d: %s\n", st, xkb_last_error()); return 1; }
-    if (counter != 6 || errors || !with_access_ran) { fprintf(stderr, "counter %d errors %d\n", counter, errors); return 1; }
-    printf("{\"tasks\": %llu, \"edges\": %llu}\n", (unsigned long long) tasks, (unsigned long long) edges);
+    if (counter != 9 || errors || !with_access_ran) { fprintf(stderr, "counter %d errors %d\n", counter, errors); return 1; }
+    printf("{\"tasks\": %llu, \"edges\": %llu, \"handle_edges\": %llu}\n", (unsigned long long) tasks, (unsigned long long) edges,
+           (unsigned long long) hedges);
     return 0;
 }

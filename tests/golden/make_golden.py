@@ -58,7 +58,33 @@ def mixed(kind, seed, n=60):
     return np.array(rows, dtype=S.REC)
 
 
+def handle_mixed(seed, n=80):
+    """Handle accesses (a few handles, every mode incl. VR/VW/D) mixed with segments and
+    matrices whose addresses reuse the handle values: handles live in their own domain."""
+    rng = np.random.default_rng(seed)
+    modes = [S.R, S.W, S.RW, S.R | S.V, S.W | S.V, S.D, S.R | S.D]
+    handles = [4096, 4100, 0x7000, 12345]
+    rows = []
+    for t in range(n):
+        for _ in range(int(rng.integers(1, 4))):
+            mode = modes[int(rng.integers(0, len(modes)))]
+            k = int(rng.integers(0, 3))
+            if k == 0:
+                rows.append((t, S.HANDLE, mode, 0, handles[int(rng.integers(0, len(handles)))], 0, 0, 0, 0, 0, 0))
+            elif k == 1:
+                a = 4096 + int(rng.integers(0, 64)); rows.append((t, S.SEGMENT, mode, 0, a, a + int(rng.integers(1, 40)), 0, 0, 0, 0, 0))
+            else:
+                m = int(rng.integers(1, 9)); om = int(rng.integers(0, 16 - m + 1))
+                rows.append((t, S.MATRIX, mode, 0, 4096, 16, om, int(rng.integers(0, 4)), m, int(rng.integers(1, 4)), 8))
+    return np.array(rows, dtype=S.REC)
+
+
 def cases():
+    H = 0x5000
+    # restates tests/task-dependency-handle.cc:86-119 (W, R, RW on one handle: T0 -> T1 -> T2)
+    yield "ref_handle_chain", S.from_tuples([[("h", S.W, H)], [("h", S.R, H)], [("h", S.RW, H)]])
+    for seed in range(3):
+        yield f"handle_mixed_{seed}", handle_mixed(seed + 50)
     X = 0x10000
     yield "ref_interval_chain", S.from_tuples([[("s", S.W, X - 64, X + 64)],
                                               [("s", S.R, X, X + 76)],

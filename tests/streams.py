@@ -9,7 +9,7 @@ programs read (oracle/access_stream.h) and the one the C-ABI resolver takes
 import numpy as np
 
 MAGIC = 0x314D525453424B58
-SEGMENT, MATRIX = 1, 2
+HANDLE, SEGMENT, MATRIX = 0, 1, 2
 R, W, RW, V, D = 1, 2, 3, 4, 8
 
 REC = np.dtype([("task", "<u4"), ("type", "u1"), ("mode", "u1"), ("reserved", "<u2"),
@@ -31,13 +31,16 @@ def read_edges(path):
 
 def from_tuples(tasks):
     """tasks: list of lists of access tuples
-    ('m', mode, addr, ld, off_m, off_n, m, n, s) or ('s', mode, a, b)."""
+    ('m', mode, addr, ld, off_m, off_n, m, n, s), ('s', mode, a, b) or ('h', mode, handle)."""
     rows = []
     for t, accs in enumerate(tasks):
         for a in accs:
             if a[0] == "m":
                 _, mode, addr, ld, om, on, m, n, s = a
                 rows.append((t, MATRIX, mode, 0, addr, ld, om, on, m, n, s))
+            elif a[0] == "h":
+                _, mode, h = a
+                rows.append((t, HANDLE, mode, 0, h, 0, 0, 0, 0, 0, 0))
             else:
                 _, mode, lo, hi = a
                 rows.append((t, SEGMENT, mode, 0, lo, hi, 0, 0, 0, 0, 0))

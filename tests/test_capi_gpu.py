@@ -28,6 +28,7 @@ def test_ordering_programs(torch_cuda, tmp_path):
     assert r.returncode == 0, r.stderr
     out = json.loads(r.stdout)
     assert out["tasks"] == 6 and out["edges"] >= 4
+    assert out["handle_edges"] == 2                    # T6 -> T7 -> T8 on the handle
 
 
 @pytest.mark.parametrize("every,chunk", [(0, None), (3, None), (0, 64), (3, 64)])

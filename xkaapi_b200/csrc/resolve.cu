@@ -14,7 +14,10 @@
 //    ld = SIZE_MAX frame (access.hpp:479-514, blas/dependency-tree.hpp:228-256);
 //  * per point: LINK(A): W-mode A with readers -> edges from every reader, else edge from
 //    the writer; PUT(A): W-mode -> writer = A, readers = {}; mode == R exactly -> readers += A
-//    (blas/dependency-tree.hpp:295-355).
+//    (blas/dependency-tree.hpp:295-355);
+//  * handles: one DependencyMap per domain task (src/task/task.cc:226-236), a point per handle
+//    with the same LINK/PUT except that any mode with R and without W is recorded as a reader
+//    (handle/dependency-map.hpp:157-297; sequential and commutative accesses).
 //
 // Method (B200): the host turns the accesses of a batch into each domain's ordered op list
 // and keeps a coordinate compression of the domain (elementary cells between all rect
@@ -495,6 +498,7 @@ using namespace xkb;
 struct xkb_resolver {
     cudaStream_t stream = nullptr;
     Domain interval;
+    Domain handles;                             // handle accesses: one point per handle
     std::vector<std::unique_ptr<Domain>> blas;
     std::map<std::pair<uint64_t, uint64_t>, size_t> blas_index;
     std::vector<xkb_access_rec_t> segments;     // every segment so far, spawn order (replay)
@@ -556,6 +560,14 @@ static void push_ops(Domain & d, bool link, const xkb_access_rec_t & r)
 {
     HRect rects[3];
     int n;
+    if (r.type == XKB_ACCESS_TYPE_HANDLE)
+    {
+        // a handle is one point of its own domain; the handle map records every access with
+        // the R bit and no W bit as a reader (dependency-map.hpp put()), so such modes count as R
+        const uint8_t m = ((r.mode & M_R) && !(r.mode & M_W)) ? M_R : r.mode;
+        d.ops.push_back({r.task, (uint8_t) link, m, HRect{r.addr, r.addr + 1, 0, 1}});
+        return;
+    }
     if (d.interval) { rects[0] = {r.addr, r.ld, 0, 1}; n = 1; }
     else if (r.type == XKB_ACCESS_TYPE_SEGMENT) n = seg_rects_blas(r.addr, r.ld, d.ld, d.s, rects);
     else n = mat_rects(r, rects);
@@ -587,6 +599,8 @@ static int validate(const xkb_access_rec_t * recs, size_t n, uint32_t first_task
         } else if (r.type == XKB_ACCESS_TYPE_BLAS_MATRIX) {
             if (!r.ld || !r.sizeof_type || !r.m || !r.n || r.m > r.ld)
                 return xkb_set_error(XKB_EINVAL, "resolver: access %zu: bad matrix tile", i);
+        } else if (r.type == XKB_ACCESS_TYPE_HANDLE) {
+            if (r.addr == ~0ull) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: handle ~0 is reserved", i);
         } else return xkb_set_error(XKB_EINVAL, "resolver: access %zu: unsupported access type %u", i, r.type);
     }
     return XKB_OK;
@@ -677,7 +691,8 @@ static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
         for (size_t a = i; a < j; ++a)                          // LINK pass
         {
             const xkb_access_rec_t & r = recs[a];
-            if (r.type == XKB_ACCESS_TYPE_SEGMENT)
+            if (r.type == XKB_ACCESS_TYPE_HANDLE) push_ops(R->handles, true, r);
+            else if (r.type == XKB_ACCESS_TYPE_SEGMENT)
             {
                 push_ops(R->interval, true, r);
                 for (auto & d : R->blas) push_ops(*d, true, r);
@@ -700,7 +715,8 @@ static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
         for (size_t a = i; a < j; ++a)                          // PUT pass
         {
             const xkb_access_rec_t & r = recs[a];
-            if (r.type == XKB_ACCESS_TYPE_SEGMENT)
+            if (r.type == XKB_ACCESS_TYPE_HANDLE) push_ops(R->handles, false, r);
+            else if (r.type == XKB_ACCESS_TYPE_SEGMENT)
             {
                 push_ops(R->interval, false, r);
                 for (auto & d : R->blas) push_ops(*d, false, r);
@@ -935,6 +951,7 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
     const auto t1 = clk::now();
     std::vector<Domain *> doms;
     if (!R->interval.ops.empty()) doms.push_back(&R->interval);
+    if (!R->handles.ops.empty()) doms.push_back(&R->handles);
     for (auto & d : R->blas) if (!d->ops.empty()) doms.push_back(d.get());
 
     std::vector<size_t> offs;
@@ -1059,6 +1076,7 @@ extern "C" int xkb_resolver_create(xkb_resolver_t ** out, void * stream)
     xkb_resolver * R = new (std::nothrow) xkb_resolver();
     if (!R) return xkb_set_error(XKB_ENOMEM, "resolver_create: out of host memory");
     R->interval.interval = true;
+    R->handles.interval = true;
     R->stream = (cudaStream_t) stream;
     *out = R;
     return XKB_OK;
@@ -1077,6 +1095,7 @@ int xkb_internal_resolver_reset(xkb_resolver_t * R)
     if (!R) return xkb_set_error(XKB_EINVAL, "resolver_reset: null resolver");
     XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
     R->interval.xs.clear(); R->interval.ys.clear(); R->interval.ncells = 0; R->interval.ops.clear();
+    R->handles.xs.clear(); R->handles.ys.clear(); R->handles.ncells = 0; R->handles.ops.clear();
     R->blas.clear(); R->blas_index.clear(); R->segments.clear();
     R->ntasks = 0; R->nuniq = 0; R->graph_valid = false;
     if (R->useg.size() > 1) { R->useg.resize(1); R->useg_n.resize(1); }   // keep the first edge segment

@@ -297,8 +297,8 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
     if (!R) return;
     if (nacc && !acc) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null accesses")); return; }
     for (size_t i = 0; i < nacc; ++i)
-        if (acc[i].type == ACCESS_TYPE_HANDLE)
-        { fail(R, xkb_set_error(XKB_EINVAL, "spawn: handle accesses are not supported")); return; }
+        if (acc[i].concurrency == ACCESS_CONCURRENCY_CONCURRENT)
+        { fail(R, xkb_set_error(XKB_EINVAL, "spawn: concurrent accesses are not supported")); return; }
     if (args_size && !args) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null arguments")); return; }
     if (R->in_wait) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: spawning from a task body during xkrt_task_wait is not supported")); return; }
     Task t;
@@ -401,6 +401,11 @@ static bool to_rec(const xkrt_access_t & a, uint32_t task, xkb_access_rec_t & r)
     memset(&r, 0, sizeof(r));
     r.task = task;
     r.mode = (uint8_t) a.mode;
+    if (a.type == ACCESS_TYPE_HANDLE)
+    {
+        r.type = XKB_ACCESS_TYPE_HANDLE; r.addr = (uint64_t) a.region.handle.addr;
+        return r.addr != ~0ull;
+    }
     if (a.type == ACCESS_TYPE_SEGMENT)
     {
         r.type = XKB_ACCESS_TYPE_SEGMENT; r.addr = (uint64_t) a.region.segment.a; r.ld = (uint64_t) a.region.segment.b;
@@ -854,7 +859,9 @@ static int wait_batch(xkb_runtime * R)
         // the host data cannot change meanwhile, so the first-touch copies can all go first
         t0 = std::chrono::steady_clock::now();
         {
-            const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) { return recs[k].type != REC_NONE; });
+            const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
+                return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE;      // handles carry no data
+            });
             for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j)
             {
                 const uint32_t k = first[j];
@@ -929,6 +936,7 @@ static int wait_batch(xkb_runtime * R)
             {
                 const xkb_access_rec_t & r = recs[T.acc_off + a];
                 if (r.type == REC_NONE) continue;
+                if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
                 const uint64_t begin = r.type == XKB_ACCESS_TYPE_SEGMENT ? r.addr : r.addr + (r.offset_n * r.ld + r.offset_m) * r.sizeof_type;
                 R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
                 // a host task on memory no region covers: that memory never has a device copy
@@ -973,7 +981,9 @@ static int wait_batch(xkb_runtime * R)
         t0 = std::chrono::steady_clock::now();
         // the blocks device tasks wrote, as reads (records rewritten in place: unused after this)
         const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
-            if (recs[k].type == REC_NONE || !(recs[k].mode & XKB_ACCESS_MODE_W) || !is_device(R, R->pending[recs[k].task])) return false;
+            if (recs[k].type == REC_NONE || recs[k].type == XKB_ACCESS_TYPE_HANDLE || !(recs[k].mode & XKB_ACCESS_MODE_W) ||
+                !is_device(R, R->pending[recs[k].task]))
+                return false;
             recs[k].mode = XKB_ACCESS_MODE_R;
             return true;
         });
