@@ -152,8 +152,40 @@ XKB_API int    xkrt_memory_unregister(xkrt_runtime_t * runtime, void * ptr, size
 XKB_API void * xkrt_memory_host_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size);
 XKB_API void   xkrt_memory_host_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * ptr, size_t size);
 
-/* devices (xkrt.h:134-135): the host is device 0, the GPU device 1 */
+/* memory (xkrt.h:112-125): async registration is synchronous here; unified allocations are
+ * used in place by device tasks (no copies) */
+XKB_API int    xkrt_memory_register_async(xkrt_runtime_t * runtime, void * ptr, size_t size);
+XKB_API int    xkrt_memory_unregister_async(xkrt_runtime_t * runtime, void * ptr, size_t size);
+XKB_API void * xkrt_memory_unified_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size);
+XKB_API void   xkrt_memory_unified_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * ptr, size_t size);
+
+/* drivers and devices (xkrt.h:128-135): the host is device 0, the GPU device 1; bodies receive
+ * these device objects */
+XKB_API xkrt_driver_t * xkrt_driver_get(xkrt_runtime_t * runtime, xkrt_driver_type_t type);
+XKB_API xkrt_device_t * xkrt_device_get(xkrt_runtime_t * runtime, xkrt_device_global_id_t device);
+XKB_API xkrt_driver_t * xkrt_device_driver_get(xkrt_runtime_t * runtime, xkrt_device_t * device);
+XKB_API xkrt_device_driver_id_t xkrt_device_driver_id_get(xkrt_runtime_t * runtime, xkrt_device_t * device);
 XKB_API unsigned int xkrt_get_ndevices(xkrt_runtime_t * runtime);
+XKB_API unsigned int xkrt_get_ndevices_max(xkrt_runtime_t * runtime);
+
+/* task completion (xkrt.h:138-144): a body may detach its task (incr) and complete it later
+ * from any thread (decr back to 0, or complete); successors run after that. Tasks of this API
+ * are committed and scheduled by the spawn calls and xkrt_task_wait: commit and enqueue record
+ * XKB_EINVAL. */
+XKB_API void xkrt_task_detachable_incr(xkrt_runtime_t * runtime, xkrt_task_t * task);
+XKB_API void xkrt_task_detachable_decr(xkrt_runtime_t * runtime, xkrt_task_t * task);
+XKB_API void xkrt_task_complete(xkrt_runtime_t * runtime, xkrt_task_t * task);
+XKB_API void xkrt_task_commit(xkrt_runtime_t * runtime, xkrt_task_t * task);
+XKB_API void xkrt_task_enqueue(xkrt_runtime_t * runtime, xkrt_task_t * task);
+/* the task whose body runs on the calling thread (xkrt.h:156) */
+XKB_API xkrt_task_t * xkrt_task_current(xkrt_runtime_t * runtime);
+
+/* logger (xkrt.h:560-565): messages to stderr; fatal aborts, as in the reference */
+XKB_API void xkrt_logger_info(const char * msg);
+XKB_API void xkrt_logger_debug(const char * msg);
+XKB_API void xkrt_logger_warn(const char * msg);
+XKB_API void xkrt_logger_error(const char * msg);
+XKB_API void xkrt_logger_fatal(const char * msg);
 
 /* tasking (xkrt.h:138-163) */
 XKB_API void xkrt_task_wait(xkrt_runtime_t * runtime);

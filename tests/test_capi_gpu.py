@@ -17,10 +17,18 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def build(name, tmp_path):
     exe = str(tmp_path / name)
     lib = os.path.join(REPO, "xkaapi_b200")
-    subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"),
-                    os.path.join(REPO, "tests", "capi", name + ".c"), "-o", exe, "-L", lib, "-lxkb200",
+    subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-D_POSIX_C_SOURCE=200809L", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "capi", name + ".c"), "-o", exe, "-L", lib, "-lxkb200", "-lpthread",
                     "-Wl,-rpath," + lib], check=True)
     return exe
+
+
+def test_devices_detach_unified_program(torch_cuda, tmp_path):
+    """Device and driver objects, the current task, a task completed from another thread after its
+    body returned (its successor waits), unified memory used in place (no copies), refused calls."""
+    r = subprocess.run([build("api_capi", tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout.strip().splitlines()[-1])["ok"] == 1
 
 
 def test_ordering_programs(torch_cuda, tmp_path):

@@ -56,9 +56,16 @@ struct Task {
     size_t args_off = 0, acc_off = 0;
     xkrt_task_func_t func = nullptr;      // team / plain function spawns
     void * user_data = nullptr;
+    int detach = 0;                       // detachable counter (atomic builtins): completion waits for 0
 };
 
-struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; };
+struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; bool unified; };
+
+// Opaque device and driver objects handed to bodies and returned by the getters.
+struct Device { int global_id; };
+struct Driver { int type; };
+
+thread_local Task * g_current = nullptr;  // task whose body runs on this thread (xkrt_task_current)
 
 } // namespace
 
@@ -98,6 +105,9 @@ struct xkb_runtime {
     int last_fused = 0;
     double last_ms[4] = {0, 0, 0, 0};                 // resolve, coherency + launch prep, run, write-back
     int dummy_team = 0;
+    Device devices[2] = {{0}, {1}};                   // the host, the GPU
+    Driver drivers[2] = {{XKRT_DRIVER_TYPE_HOST}, {XKRT_DRIVER_TYPE_CUDA}};
+    bool any_unified = false;
 };
 
 static xkb_runtime * RT(xkrt_runtime_t * r) { return (xkb_runtime *) r; }
@@ -152,6 +162,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     if (R->stream) cudaStreamSynchronize(R->stream);
     for (auto & kv : R->regions)
     {
+        if (kv.second.unified) { cudaFree(kv.second.mirror); continue; }
         if (kv.second.mirror) cudaFree(kv.second.mirror);
         if (kv.second.pinned_by_us) cudaFreeHost((void *) kv.first);
     }
@@ -173,18 +184,19 @@ extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
 }
 
-static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned)
+static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, bool unified = false)
 {
     int32_t id = -1;
     int rc = xkb_planner_add_region(R->planner, (uint64_t) ptr, size, &id);
     if (rc) return rc;
-    void * mirror = nullptr;
-    if (R->gpu)
+    void * mirror = unified ? ptr : nullptr;          // unified memory: the device uses it in place
+    if (R->gpu && !unified)
     {
         cudaError_t e = cudaMalloc(&mirror, size);
         if (e != cudaSuccess) return xkb_set_cuda_error(e);
     }
-    R->regions[(uint64_t) ptr] = Region{size, mirror, pinned, id};
+    R->regions[(uint64_t) ptr] = Region{size, mirror, pinned, id, unified};
+    R->any_unified = R->any_unified || unified;
     return XKB_OK;
 }
 
@@ -229,6 +241,111 @@ extern "C" unsigned int xkrt_get_ndevices(xkrt_runtime_t * runtime)
     xkb_runtime * R = RT(runtime);
     return R ? (R->gpu ? 2u : 1u) : 0u;
 }
+
+extern "C" unsigned int xkrt_get_ndevices_max(xkrt_runtime_t * runtime)
+{
+    return xkrt_get_ndevices(runtime);           // one host and (at most) one GPU
+}
+
+extern "C" int xkrt_memory_register_async(xkrt_runtime_t * runtime, void * ptr, size_t size)
+{
+    return xkrt_memory_register(runtime, ptr, size);
+}
+
+extern "C" int xkrt_memory_unregister_async(xkrt_runtime_t * runtime, void * ptr, size_t size)
+{
+    return xkrt_memory_unregister(runtime, ptr, size);
+}
+
+extern "C" void * xkrt_memory_unified_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size)
+{
+    xkb_runtime * R = RT(runtime);
+    (void) device;
+    if (!R || !size) return nullptr;
+    if (!R->gpu) { fail(R, xkb_set_error(XKB_ENODEV, "xkrt_memory_unified_allocate: no GPU")); return nullptr; }
+    void * p = nullptr;
+    if (cudaMallocManaged(&p, size) != cudaSuccess) { cudaGetLastError(); fail(R, XKB_ENOMEM); return nullptr; }
+    int rc = add_region(R, p, size, false, true);
+    if (rc) { cudaFree(p); fail(R, rc); return nullptr; }
+    return p;
+}
+
+extern "C" void xkrt_memory_unified_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * ptr, size_t size)
+{
+    (void) runtime; (void) device; (void) ptr; (void) size;   // released by xkrt_deinit
+}
+
+extern "C" xkrt_driver_t * xkrt_driver_get(xkrt_runtime_t * runtime, xkrt_driver_type_t type)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R) return nullptr;
+    if (type == XKRT_DRIVER_TYPE_HOST) return (xkrt_driver_t *) &R->drivers[0];
+    if (type == XKRT_DRIVER_TYPE_CUDA && R->gpu) return (xkrt_driver_t *) &R->drivers[1];
+    return nullptr;
+}
+
+extern "C" xkrt_device_t * xkrt_device_get(xkrt_runtime_t * runtime, xkrt_device_global_id_t device)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || device >= xkrt_get_ndevices(runtime)) return nullptr;
+    return (xkrt_device_t *) &R->devices[device];
+}
+
+extern "C" xkrt_driver_t * xkrt_device_driver_get(xkrt_runtime_t * runtime, xkrt_device_t * device)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || !device) return nullptr;
+    return (xkrt_driver_t *) &R->drivers[((Device *) device)->global_id == 0 ? 0 : 1];
+}
+
+extern "C" xkrt_device_driver_id_t xkrt_device_driver_id_get(xkrt_runtime_t * runtime, xkrt_device_t * device)
+{
+    (void) runtime; (void) device;
+    return 0;                                    // the first (only) device of its driver
+}
+
+extern "C" xkrt_task_t * xkrt_task_current(xkrt_runtime_t * runtime)
+{
+    (void) runtime;
+    return (xkrt_task_t *) g_current;
+}
+
+extern "C" void xkrt_task_detachable_incr(xkrt_runtime_t * runtime, xkrt_task_t * task)
+{
+    (void) runtime;
+    if (task) __atomic_add_fetch(&((Task *) task)->detach, 1, __ATOMIC_ACQ_REL);
+}
+
+extern "C" void xkrt_task_detachable_decr(xkrt_runtime_t * runtime, xkrt_task_t * task)
+{
+    (void) runtime;
+    if (task) __atomic_sub_fetch(&((Task *) task)->detach, 1, __ATOMIC_ACQ_REL);
+}
+
+extern "C" void xkrt_task_complete(xkrt_runtime_t * runtime, xkrt_task_t * task)
+{
+    (void) runtime;
+    if (task) __atomic_store_n(&((Task *) task)->detach, 0, __ATOMIC_RELEASE);
+}
+
+extern "C" void xkrt_task_commit(xkrt_runtime_t * runtime, xkrt_task_t * task)
+{
+    (void) task;       // tasks of this API are committed by the spawn calls
+    fail(RT(runtime), xkb_set_error(XKB_EINVAL, "xkrt_task_commit: tasks are committed when spawned"));
+}
+
+extern "C" void xkrt_task_enqueue(xkrt_runtime_t * runtime, xkrt_task_t * task)
+{
+    (void) task;
+    fail(RT(runtime), xkb_set_error(XKB_EINVAL, "xkrt_task_enqueue: tasks are scheduled by xkrt_task_wait"));
+}
+
+static void logger(const char * level, const char * msg) { fprintf(stderr, "[xkrt] %s: %s\n", level, msg ? msg : ""); }
+extern "C" void xkrt_logger_info (const char * msg) { logger("info", msg); }
+extern "C" void xkrt_logger_debug(const char * msg) { logger("debug", msg); }
+extern "C" void xkrt_logger_warn (const char * msg) { logger("warn", msg); }
+extern "C" void xkrt_logger_error(const char * msg) { logger("error", msg); }
+extern "C" void xkrt_logger_fatal(const char * msg) { logger("fatal", msg); abort(); }   // the reference's contract
 
 extern "C" xkrt_task_format_id_t xkrt_task_format_put(xkrt_runtime_t * runtime, const char * label)
 {
@@ -439,6 +556,23 @@ static void * mirror_lookup(const xkb_runtime * R, uint64_t host, RegionHint & h
     if (host >= it->first + it->second.size || !it->second.mirror) return nullptr;
     h.base = it->first; h.end = it->first + it->second.size; h.mirror = (uint8_t *) it->second.mirror;
     return (uint8_t *) it->second.mirror + (host - it->first);
+}
+
+// First byte an access record touches.
+static uint64_t rec_begin(const xkb_access_rec_t & r)
+{
+    return r.type == XKB_ACCESS_TYPE_SEGMENT ? r.addr : r.addr + (r.offset_n * r.ld + r.offset_m) * r.sizeof_type;
+}
+
+// Is the record's memory unified (used in place by the device, never copied)?
+static bool in_unified(const xkb_runtime * R, const xkb_access_rec_t & r)
+{
+    if (!R->any_unified || r.type == XKB_ACCESS_TYPE_HANDLE) return false;
+    const uint64_t b = rec_begin(r);
+    auto it = R->regions.upper_bound(b);
+    if (it == R->regions.begin()) return false;
+    --it;
+    return it->second.unified && b < it->first + it->second.size;
 }
 
 static void * mirror_of(xkb_runtime * R, uint64_t host)
@@ -860,7 +994,8 @@ static int wait_batch(xkb_runtime * R)
         t0 = std::chrono::steady_clock::now();
         {
             const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
-                return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE;      // handles carry no data
+                // handles carry no data; unified memory is used in place
+                return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE && !in_unified(R, recs[k]);
             });
             for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j)
             {
@@ -937,10 +1072,12 @@ static int wait_batch(xkb_runtime * R)
                 const xkb_access_rec_t & r = recs[T.acc_off + a];
                 if (r.type == REC_NONE) continue;
                 if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
-                const uint64_t begin = r.type == XKB_ACCESS_TYPE_SEGMENT ? r.addr : r.addr + (r.offset_n * r.ld + r.offset_m) * r.sizeof_type;
+                const uint64_t begin = rec_begin(r);
                 R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
-                // a host task on memory no region covers: that memory never has a device copy
+                // a host task on memory no region covers: that memory never has a device copy;
+                // unified memory needs no copy either way
                 if (!dev && !mirror_of(R, begin)) continue;
+                if (in_unified(R, r)) continue;
                 xkb_view_t v;
                 if ((rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v))) break;
             }
@@ -958,17 +1095,35 @@ static int wait_batch(xkb_runtime * R)
                     if ((rc = translate(R, d)) || (rc = xkb_internal_launch_task(&d, R->stream))) break;
                 }
                 else
+                {
+                    g_current = &T;
                     ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_CUDA])(
-                        (xkrt_runtime_t *) R, (xkrt_device_t *) (uintptr_t) 1, (xkrt_task_t *) &T);
+                        (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[1], (xkrt_task_t *) &T);
+                    g_current = nullptr;
+                }
             }
             else
             {
                 if (cudaStreamSynchronize(R->stream) != cudaSuccess) { rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream"); break; }
-                if (T.func) T.func((xkrt_runtime_t *) R, (xkrt_device_t *) nullptr, (xkrt_task_t *) &T, T.user_data);
+                g_current = &T;
+                if (T.func) T.func((xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T, T.user_data);
                 else if (f.f[XKRT_TASK_FORMAT_TARGET_HOST])
                     ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_HOST])(
-                        (xkrt_runtime_t *) R, (xkrt_device_t *) nullptr, (xkrt_task_t *) &T);
-                else if (T.fmtid) { rc = xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t); break; }
+                        (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T);
+                else if (T.fmtid) { g_current = nullptr; rc = xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t); break; }
+                g_current = nullptr;
+            }
+            // a detached task completes when its counter is back to 0 (xkrt_task_detachable_decr
+            // or xkrt_task_complete, from any thread); its successors run after that
+            if (__atomic_load_n(&T.detach, __ATOMIC_ACQUIRE) > 0)
+            {
+                const auto w0 = std::chrono::steady_clock::now();
+                while (__atomic_load_n(&T.detach, __ATOMIC_ACQUIRE) > 0)
+                {
+                    if (ms_since(w0) > 600e3) { rc = xkb_set_error(XKB_ETIMEDOUT, "task %zu: still detached after 600 s", t); break; }
+                    std::this_thread::yield();
+                }
+                if (rc) break;
             }
         }
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
@@ -982,7 +1137,7 @@ static int wait_batch(xkb_runtime * R)
         // the blocks device tasks wrote, as reads (records rewritten in place: unused after this)
         const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
             if (recs[k].type == REC_NONE || recs[k].type == XKB_ACCESS_TYPE_HANDLE || !(recs[k].mode & XKB_ACCESS_MODE_W) ||
-                !is_device(R, R->pending[recs[k].task]))
+                !is_device(R, R->pending[recs[k].task]) || in_unified(R, recs[k]))
                 return false;
             recs[k].mode = XKB_ACCESS_MODE_R;
             return true;
