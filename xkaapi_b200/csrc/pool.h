@@ -73,6 +73,24 @@ public:
         return true;
     }
     bool fixed() const { return fixed_; }
+    // Fault in (writable, contents unchanged) the pages of bytes [from, to) of the reservation
+    // ahead of the writer, so that filling them later costs no page faults on the writer's
+    // thread. Safe while another thread writes the array. Returns the end actually reached.
+    size_t populate(size_t from, size_t to)
+    {
+        if (!fixed_ || from >= bytes_) return from;
+        if (to > bytes_) to = bytes_;
+        const size_t page = 4096;
+        from &= ~(page - 1);
+        to = (to + page - 1) & ~(page - 1);
+        if (to > bytes_) to = bytes_;
+        if (to <= from) return from;
+        unsigned char * b = (unsigned char *) p_;
+        if (madvise(b + from, to - from, 23 /* MADV_POPULATE_WRITE */) != 0)
+            for (size_t o = from; o < to; o += page) __atomic_fetch_add(b + o, (unsigned char) 0, __ATOMIC_RELAXED);
+        return to;
+    }
+    size_t used_bytes() const { return n_ * sizeof(T); }
 
 private:
     bool grow(size_t need)

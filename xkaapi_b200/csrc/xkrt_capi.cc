@@ -93,6 +93,11 @@ struct xkb_runtime {
     size_t chunk = 0;                                 // accesses per resolver batch
     xkb_resolver_t * res = nullptr;                   // resolver of the batch being spawned
     bool res_stale = false;                           // res still holds the previous batch
+    // page prefaulting of the spawn pools: a helper thread keeps the pages the next spawns will
+    // fill backed, so the spawning thread does not take the page faults
+    std::thread prefaulter[3];                        // one per pool: tasks, argument bytes, accesses
+    std::atomic<size_t> pf_want{0};                   // spawned tasks the pools should be ready for
+    std::atomic<bool> pf_stop{false};
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
     std::map<uint64_t, Region> regions;               // host base -> region
@@ -117,6 +122,33 @@ static void fail(xkb_runtime * R, int rc)
     if (R && rc != XKB_OK && R->status == XKB_OK) R->status = rc;
 }
 
+// The prefault helpers (one per spawn pool): while the program spawns, they fault in the pages
+// of the next PREFAULT_AHEAD tasks (argument bytes and two accesses per task assumed; more only
+// means later faults), so that spawning itself takes no page faults. Nothing is populated before
+// the first spawns, and pages stay backed for the next batch.
+constexpr size_t PREFAULT_AHEAD = size_t(1) << 20;
+
+static void prefault_loop(xkb_runtime * R, int pool)
+{
+    const size_t per_task = pool == 0 ? sizeof(Task) : pool == 1 ? 80 : 2 * sizeof(xkrt_access_t);
+    constexpr size_t STEP = size_t(8) << 20;
+    size_t done = 0;
+    while (!R->pf_stop.load(std::memory_order_relaxed))
+    {
+        const size_t want = R->pf_want.load(std::memory_order_relaxed) * per_task;
+        if (want <= done)
+        {
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+            continue;
+        }
+        const size_t to = std::min(want, done + STEP);
+        const size_t got = pool == 0 ? R->pending.populate(done, to) : pool == 1 ? R->args_pool.populate(done, to)
+                                                                          : R->acc_pool.populate(done, to);
+        if (got <= done) { std::this_thread::sleep_for(std::chrono::microseconds(200)); continue; }   // reservation full
+        done = got;
+    }
+}
+
 extern "C" int xkrt_init(xkrt_runtime_t ** out)
 {
     if (!out) return xkb_set_error(XKB_EINVAL, "xkrt_init: null output");
@@ -132,9 +164,15 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     // spawned tasks while spawning continues; without them resolution waits for xkrt_task_wait
     {
         constexpr size_t MAXT = size_t(1) << 28, MAXA = size_t(1) << 29;
-        R->bg = R->gpu && R->pending.reserve_fixed(MAXT) && R->args_pool.reserve_fixed(MAXT * 64) &&
-                R->acc_pool.reserve_fixed(MAXA) && R->recs.reserve_fixed(MAXA) && R->replica_pool.reserve_fixed(MAXA);
-        if (!R->bg) { R->pending.release(); R->args_pool.release(); R->acc_pool.release(); R->recs.release(); R->replica_pool.release(); }
+        const bool fixed = R->pending.reserve_fixed(MAXT) && R->args_pool.reserve_fixed(MAXT * 64) &&
+                           R->acc_pool.reserve_fixed(MAXA) && R->recs.reserve_fixed(MAXA) && R->replica_pool.reserve_fixed(MAXA);
+        if (!fixed) { R->pending.release(); R->args_pool.release(); R->acc_pool.release(); R->recs.release(); R->replica_pool.release(); }
+        R->bg = R->gpu && fixed;
+    }
+    if (R->pending.fixed())
+    {
+        R->pf_want = 0;                            // nothing is populated before the first spawns
+        for (int k = 0; k < 3; ++k) R->prefaulter[k] = std::thread(prefault_loop, R, k);
     }
     int rc = xkb_planner_create_resident(&R->planner);
     if (rc == XKB_OK && R->gpu)
@@ -159,6 +197,8 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
         R->worker.join();
     }
     if (R->res) { xkb_resolver_destroy(R->res); R->res = nullptr; }
+    R->pf_stop = true;
+    for (auto & th : R->prefaulter) if (th.joinable()) th.join();
     if (R->stream) cudaStreamSynchronize(R->stream);
     for (auto & kv : R->regions)
     {
@@ -431,6 +471,8 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
         return;
     }
     if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
+    const size_t nt = R->pending.size();
+    if ((nt & 4095) == 0 && R->prefaulter[0].joinable()) R->pf_want.store(nt + PREFAULT_AHEAD, std::memory_order_relaxed);
     if (R->bg) bg_hand_over(R, false);
 }
 
