@@ -169,7 +169,8 @@ XKB_API unsigned int xkrt_get_ndevices(xkrt_runtime_t * runtime);
 XKB_API unsigned int xkrt_get_ndevices_max(xkrt_runtime_t * runtime);
 
 /* task completion (xkrt.h:138-144): a body may detach its task (incr) and complete it later
- * from any thread (decr back to 0, or complete); successors run after that. Tasks of this API
+ * from any thread (decr back to 0, or complete); successors are released then, and no thread
+ * waits for the detached task meanwhile. Tasks of this API
  * are committed and scheduled by the spawn calls and xkrt_task_wait: commit and enqueue record
  * XKB_EINVAL. */
 XKB_API void xkrt_task_detachable_incr(xkrt_runtime_t * runtime, xkrt_task_t * task);
@@ -229,7 +230,8 @@ XKB_API int xkrt_task_format_set(xkrt_runtime_t * runtime, xkrt_task_format_id_t
 XKB_API xkrt_task_format_id_t xkb_task_format_builtin(xkrt_runtime_t * runtime, int kind);
 /* First failure recorded since the last call (XKB_OK if none); clears it. */
 XKB_API int xkb_runtime_status(xkrt_runtime_t * runtime);
-/* The CUDA stream CUDA-target format bodies launch on (cudaStream_t as void *). */
+/* The CUDA stream CUDA-target format bodies launch on (cudaStream_t as void *): inside a body,
+ * the stream of the host thread running it (each thread of the team has its own). */
 XKB_API void * xkb_runtime_stream(xkrt_runtime_t * runtime);
 /* Counters of the last xkrt_task_wait: tasks run, unique edges, copies H2D / D2H, and whether the
  * persistent scheduler ran the batch (1) or the tasks ran one by one (0). */

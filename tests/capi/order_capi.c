@@ -4,21 +4,22 @@
  *                                                    -> interval W [0,100)
  *   tests/api/c/task-with-access.c:52-90             a team task with a VW segment access
  *   tests/task-dependency-handle.cc:86-119           W -> R -> RW on one handle
- * Host task bodies check that they run in spawn order (each finds the counter at its own index).
- * Exit status 0 = success. */
+ * Each chain's host task bodies check that they run in spawn order (each finds its chain's counter
+ * at its own index); independent chains may run at the same time. Exit status 0 = success. */
 #include <stdio.h>
 #include <stdlib.h>
 
 #include "xkrt_capi.h"
 
-static int counter = 0, errors = 0, with_access_ran = 0;
+static int counter[3] = {0, 0, 0}, errors = 0, with_access_ran = 0;
 
+/* args: {chain, position in the chain}; tasks of one chain never overlap in time */
 static void ordered(xkrt_runtime_t * rt, xkrt_device_t * dev, xkrt_task_t * task)
 {
     (void) rt; (void) dev;
-    const int expected = *(const int *) xkrt_task_args(task);
-    if (expected != counter) { fprintf(stderr, "task %d ran at position %d\n", expected, counter); ++errors; }
-    ++counter;
+    const int * a = (const int *) xkrt_task_args(task);
+    if (a[1] != counter[a[0]]) { fprintf(stderr, "chain %d task %d ran at position %d\n", a[0], a[1], counter[a[0]]); __atomic_add_fetch(&errors, 1, __ATOMIC_RELAXED); }
+    ++counter[a[0]];
 }
 
 static void with_access(xkrt_runtime_t * rt, xkrt_device_t * dev, xkrt_task_t * task, void * ud)
@@ -49,7 +50,8 @@ int main(void)
     for (int t = 0; t < 3; ++t)
     {
         xkrt_access_t a = segment(modes[t], lo[t], hi[t]);
-        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, &t, sizeof(t), &a, 1);
+        const int args[2] = {0, t};
+        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, args, sizeof(args), &a, 1);
     }
     /* interval -> matrix -> interval */
     for (int t = 3; t < 6; ++t)
@@ -62,7 +64,8 @@ int main(void)
             a.region.matrix.m = 8; a.region.matrix.n = 8; a.region.matrix.sizeof_type = 1;
         }
         else a = segment(ACCESS_MODE_W, (void *) 0, (void *) 100);
-        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, &t, sizeof(t), &a, 1);
+        const int args[2] = {1, t - 3};
+        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, args, sizeof(args), &a, 1);
     }
     xkrt_task_wait(rt);
     uint64_t tasks = 0, edges = 0;
@@ -72,8 +75,9 @@ int main(void)
     for (int t = 6; t < 9; ++t)
     {
         xkrt_access_t a = {ACCESS_CONCURRENCY_SEQUENTIAL, modes[t - 6], ACCESS_SCOPE_NONUNIFIED, ACCESS_TYPE_HANDLE, {{0}}};
-        a.region.handle.addr = &counter;
-        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, &t, sizeof(t), &a, 1);
+        a.region.handle.addr = &counter[2];
+        const int args[2] = {2, t - 6};
+        xkrt_task_spawn_with_format_with_accesses(rt, HOST_DEVICE_GLOBAL_ID, fmt, args, sizeof(args), &a, 1);
     }
     xkrt_task_wait(rt);
     uint64_t hedges = 0;
@@ -87,7 +91,8 @@ int main(void)
 
     const int st = xkb_runtime_status(rt);
     if (xkrt_deinit(rt) != 0 || st != 0) { fprintf(stderr, "status %d: %s\n", st, xkb_last_error()); return 1; }
-    if (counter != 9 || errors || !with_access_ran) { fprintf(stderr, "counter %d errors %d\n", counter, errors); return 1; }
+    if (counter[0] != 3 || counter[1] != 3 || counter[2] != 3 || errors || !with_access_ran)
+    { fprintf(stderr, "counters %d %d %d errors %d\n", counter[0], counter[1], counter[2], errors); return 1; }
     printf("{\"tasks\": %llu, \"edges\": %llu, \"handle_edges\": %llu}\n", (unsigned long long) tasks, (unsigned long long) edges,
            (unsigned long long) hedges);
     return 0;

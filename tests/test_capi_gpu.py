@@ -31,6 +31,23 @@ def test_devices_detach_unified_program(torch_cuda, tmp_path):
     assert json.loads(r.stdout.strip().splitlines()[-1])["ok"] == 1
 
 
+@pytest.mark.parametrize("threads", [None, 1])
+def test_dataflow_host_team(torch_cuda, tmp_path, threads):
+    """A non-fused batch runs as a dataflow graph on a team of host threads: independent tasks run
+    at the same time, chains keep their order, a detached task completed by another task's body
+    releases its successor -- also with a single host thread (a detached task holds none)."""
+    env = dict(os.environ)
+    if threads:
+        env["XKB_HOST_THREADS"] = str(threads)
+    r = subprocess.run([build("dataflow_capi", tmp_path)], capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    if threads == 1:
+        assert out["peak"] == 1
+    elif (os.cpu_count() or 1) >= 4:
+        assert out["peak"] >= 4 and out["wide_s"] < 48 * 0.020 / 2
+
+
 def test_ordering_programs(torch_cuda, tmp_path):
     r = subprocess.run([build("order_capi", tmp_path)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <memory>
@@ -56,18 +57,32 @@ struct Task {
     size_t args_off = 0, acc_off = 0;
     xkrt_task_func_t func = nullptr;      // team / plain function spawns
     void * user_data = nullptr;
-    int detach = 0;                       // detachable counter (atomic builtins): completion waits for 0
+    int detach = 0;                       // references (atomic builtins): the running body's, plus each
+                                          // xkrt_task_detachable_incr; the task completes at 0
 };
 
 struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; bool unified; };
+
+// Drop one reference of a task; true when it was the last one (the task completes now).
+// A task already at 0 (completed by xkrt_task_complete) stays there.
+static bool task_unref(Task & T)
+{
+    int v = __atomic_load_n(&T.detach, __ATOMIC_ACQUIRE);
+    while (v > 0)
+        if (__atomic_compare_exchange_n(&T.detach, &v, v - 1, false, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE)) return v == 1;
+    return false;
+}
 
 // Opaque device and driver objects handed to bodies and returned by the getters.
 struct Device { int global_id; };
 struct Driver { int type; };
 
 thread_local Task * g_current = nullptr;  // task whose body runs on this thread (xkrt_task_current)
+thread_local cudaStream_t g_stream = nullptr;   // the stream of the worker running a CUDA body
 
 } // namespace
+
+static void task_completed(::xkb_runtime * R, Task & T);
 
 struct xkb_runtime {
     Format formats[256];
@@ -77,7 +92,7 @@ struct xkb_runtime {
     xkb::PoolArray<xkrt_access_t> acc_pool;
     xkb::PoolArray<void *> replica_pool;              // sized to acc_pool at wait
     xkb::PoolArray<xkb_access_rec_t> recs;            // one record per access, same index (wait)
-    bool in_wait = false;
+    std::atomic<bool> in_wait{false};
     // background resolution: with fixed pools, a worker thread resolves chunks of spawned tasks
     // on the GPU while the program keeps spawning (the reference resolves at spawn time too)
     bool bg = false;
@@ -98,6 +113,11 @@ struct xkb_runtime {
     std::thread prefaulter[3];                        // one per pool: tasks, argument bytes, accesses
     std::atomic<size_t> pf_want{0};                   // spawned tasks the pools should be ready for
     std::atomic<bool> pf_stop{false};
+    // dataflow execution of non-fused batches: a team of host threads, one CUDA stream each;
+    // the planner (coherency decisions and their copies) is used by one task at a time
+    std::vector<cudaStream_t> wstreams;
+    std::mutex plan_mu;
+    std::atomic<struct Dataflow *> df{nullptr};       // the batch being executed (detached completion)
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
     std::map<uint64_t, Region> regions;               // host base -> region
@@ -206,6 +226,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
         if (kv.second.mirror) cudaFree(kv.second.mirror);
         if (kv.second.pinned_by_us) cudaFreeHost((void *) kv.first);
     }
+    for (cudaStream_t w : R->wstreams) cudaStreamDestroy(w);
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
     if (R->stream) cudaStreamDestroy(R->stream);
@@ -356,16 +377,19 @@ extern "C" void xkrt_task_detachable_incr(xkrt_runtime_t * runtime, xkrt_task_t 
     if (task) __atomic_add_fetch(&((Task *) task)->detach, 1, __ATOMIC_ACQ_REL);
 }
 
+// Any thread may drop the reference that completes a task; its successors are released then
+// (src/task.cc:260-270, __task_detachable_decr).
 extern "C" void xkrt_task_detachable_decr(xkrt_runtime_t * runtime, xkrt_task_t * task)
 {
     (void) runtime;
-    if (task) __atomic_sub_fetch(&((Task *) task)->detach, 1, __ATOMIC_ACQ_REL);
+    if (task && task_unref(*(Task *) task)) task_completed(((Task *) task)->rt, *(Task *) task);
 }
 
+// Complete a task now, whatever references it still holds (src/task.cc:405-412).
 extern "C" void xkrt_task_complete(xkrt_runtime_t * runtime, xkrt_task_t * task)
 {
     (void) runtime;
-    if (task) __atomic_store_n(&((Task *) task)->detach, 0, __ATOMIC_RELEASE);
+    if (task && __atomic_exchange_n(&((Task *) task)->detach, 0, __ATOMIC_ACQ_REL) > 0) task_completed(((Task *) task)->rt, *(Task *) task);
 }
 
 extern "C" void xkrt_task_commit(xkrt_runtime_t * runtime, xkrt_task_t * task)
@@ -428,7 +452,8 @@ extern "C" int xkb_runtime_status(xkrt_runtime_t * runtime)
 extern "C" void * xkb_runtime_stream(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
-    return R ? (void *) R->stream : nullptr;
+    if (!R) return nullptr;
+    return (void *) (g_stream ? g_stream : R->stream);      // inside a CUDA body: its worker's stream
 }
 
 extern "C" int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks, uint64_t * edges, uint64_t * h2d,
@@ -625,7 +650,7 @@ static void * mirror_of(xkb_runtime * R, uint64_t host)
     return p;
 }
 
-static int run_copies(xkb_runtime * R)
+static int run_copies(xkb_runtime * R, cudaStream_t stream)
 {
     size_t n = 0;
     int rc = xkb_planner_copies(R->planner, nullptr, 0, &n, 0);
@@ -639,7 +664,7 @@ static int run_copies(xkb_runtime * R)
         (k.kind == XKB_COPY_H2D ? R->last_h2d : R->last_d2h) += 1;
         (k.kind == XKB_COPY_H2D ? R->last_h2d_bytes : R->last_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
     }
-    return xkb_plan_execute(c.data(), n, ptrs.data(), ptrs.size(), R->stream);
+    return xkb_plan_execute(c.data(), n, ptrs.data(), ptrs.size(), stream);
 }
 
 // Point a built-in descriptor's host addresses at the device mirrors.
@@ -991,6 +1016,170 @@ static void bg_finish(xkb_runtime * R)
     R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
 }
 
+// One task of a non-fused batch on the calling worker: its accesses made coherent where it runs
+// (planner fetches and their copies, completed before the planner is released, so the planner's
+// state always describes data that is in place), then its body; a device body runs on the
+// worker's stream and is complete when this returns. The caller then drops the body's reference:
+// a task the body made detachable completes when its last reference goes, on whatever thread.
+static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cudaStream_t stream)
+{
+    Task & T = R->pending[t];
+    const bool dev = is_device(R, T);
+    int rc = XKB_OK;
+    {
+        std::lock_guard<std::mutex> lk(R->plan_mu);
+        for (uint32_t a = 0; a < T.nacc && rc == XKB_OK; ++a)
+        {
+            const xkb_access_rec_t & r = recs[T.acc_off + a];
+            if (r.type == REC_NONE) continue;
+            if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
+            const uint64_t begin = rec_begin(r);
+            R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
+            // a host task on memory no region covers: that memory never has a device copy;
+            // unified memory needs no copy either way
+            if (!dev && !mirror_of(R, begin)) continue;
+            if (in_unified(R, r)) continue;
+            xkb_view_t v;
+            rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v);
+        }
+        if (rc == XKB_OK) rc = run_copies(R, stream);
+        if (rc == XKB_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: copies");
+    }
+    if (rc) return rc;
+    const Format & f = R->formats[T.fmtid];
+    __atomic_add_fetch(&T.detach, 1, __ATOMIC_ACQ_REL);        // the body's own reference
+    g_current = &T;
+    if (dev)
+    {
+        if (f.builtin >= 0)
+        {
+            xkb_task_desc_t d;
+            if (T.nargs < sizeof(d)) rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t);
+            else
+            {
+                memcpy(&d, R->args_pool.data() + T.args_off, sizeof(d));
+                d.kind = (uint32_t) f.builtin;
+                RegionHint h;
+                if (!translate_hint(R, d, h)) rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region", t);
+                else rc = xkb_internal_launch_task(&d, stream);
+            }
+        }
+        else
+        {
+            g_stream = stream;
+            ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_CUDA])(
+                (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[1], (xkrt_task_t *) &T);
+            g_stream = nullptr;
+        }
+        if (rc == XKB_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "task %zu: device body", t);
+    }
+    else if (T.func) T.func((xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T, T.user_data);
+    else if (f.f[XKRT_TASK_FORMAT_TARGET_HOST])
+        ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_HOST])(
+            (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T);
+    else if (T.fmtid) rc = xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t);
+    g_current = nullptr;
+    return rc;
+}
+
+// The successor graph of a non-fused batch being executed: wait counters, the ready queue, and
+// the number of completed tasks.
+struct Dataflow {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<uint32_t> ready;
+    std::vector<uint32_t> ptr, succ, wc;
+    size_t nt = 0, done = 0;
+    int err = XKB_OK;
+    std::string err_text;
+};
+
+// A task of the running batch completed: its successors' wait counters drop, the ready ones are
+// queued (src/task.cc:160-245, __task_complete).
+static void task_completed(::xkb_runtime * R, Task & T)
+{
+    Dataflow * D = R ? R->df.load(std::memory_order_acquire) : nullptr;
+    if (!D) return;
+    const size_t t = (size_t) (&T - R->pending.data());
+    if (t >= D->nt) return;
+    std::lock_guard<std::mutex> lk(D->mu);
+    for (uint32_t i = D->ptr[t]; i < D->ptr[t + 1]; ++i)
+        if (--D->wc[D->succ[i]] == 0) D->ready.push_back(D->succ[i]);
+    ++D->done;
+    D->cv.notify_all();
+}
+
+// A non-fused batch: ready tasks (all predecessors completed) run on a team of host threads,
+// XKB_HOST_THREADS or one per hardware thread (at most 64) -- the reference's host team and
+// device threads executing ready tasks as their predecessors complete. A detached task holds no
+// thread; the batch ends when every task completed (600 s without progress is an error).
+static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_access_rec_t * recs)
+{
+    const size_t nt = R->pending.size();
+    Dataflow D;
+    D.nt = nt;
+    D.ptr.resize(nt + 1); D.succ.resize(g.nedges ? g.nedges : 1); D.wc.resize(nt);
+    if (cudaMemcpyAsync(D.ptr.data(), g.succ_ptr, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, R->stream) != cudaSuccess ||
+        (g.nedges && cudaMemcpyAsync(D.succ.data(), g.succ, g.nedges * sizeof(uint32_t), cudaMemcpyDeviceToHost, R->stream) != cudaSuccess) ||
+        cudaMemcpyAsync(D.wc.data(), g.npred, nt * sizeof(uint32_t), cudaMemcpyDeviceToHost, R->stream) != cudaSuccess ||
+        cudaStreamSynchronize(R->stream) != cudaSuccess)
+        return xkb_set_error(XKB_ECUDA, "xkrt_task_wait: graph download");
+    size_t nw = std::thread::hardware_concurrency();
+    if (const char * e = getenv("XKB_HOST_THREADS")) nw = strtoul(e, nullptr, 10);
+    nw = std::max<size_t>(1, std::min<size_t>({nw ? nw : 1, 64, nt}));
+    while (R->wstreams.size() < nw)
+    {
+        cudaStream_t st;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
+        R->wstreams.push_back(st);
+    }
+    for (size_t t = 0; t < nt; ++t) if (D.wc[t] == 0) D.ready.push_back((uint32_t) t);
+    R->df.store(&D, std::memory_order_release);
+    auto worker = [&](size_t k) {
+        cudaSetDevice(R->device);
+        auto progress = std::chrono::steady_clock::now();
+        size_t seen = 0;
+        for (;;)
+        {
+            uint32_t t;
+            {
+                std::unique_lock<std::mutex> lk(D.mu);
+                D.cv.wait_for(lk, std::chrono::milliseconds(100), [&] { return D.err != XKB_OK || D.done == nt || !D.ready.empty(); });
+                if (D.err != XKB_OK || D.done == nt) return;
+                if (D.ready.empty())
+                {
+                    if (D.done != seen) { seen = D.done; progress = std::chrono::steady_clock::now(); }
+                    else if (ms_since(progress) > 600e3)
+                    {
+                        D.err = xkb_set_error(XKB_ETIMEDOUT, "xkrt_task_wait: %zu of %zu tasks completed, none for 600 s (a detached task never completed?)", D.done, nt);
+                        D.err_text = xkb_last_error();
+                        D.cv.notify_all();
+                        return;
+                    }
+                    continue;
+                }
+                t = D.ready.front(); D.ready.pop_front();
+            }
+            const int rc = run_one(R, t, recs, R->wstreams[k]);
+            if (rc)
+            {
+                std::lock_guard<std::mutex> lk(D.mu);
+                if (D.err == XKB_OK) { D.err = rc; D.err_text = xkb_last_error(); }
+                D.cv.notify_all();
+                return;
+            }
+            if (task_unref(R->pending[t])) task_completed(R, R->pending[t]);
+        }
+    };
+    std::vector<std::thread> team;
+    for (size_t k = 1; k < nw; ++k) team.emplace_back(worker, k);
+    worker(0);
+    for (auto & th : team) th.join();
+    R->df.store(nullptr, std::memory_order_release);
+    if (D.err != XKB_OK) return xkb_set_error(D.err, "%s", D.err_text.c_str());
+    return XKB_OK;
+}
+
 static int wait_batch(xkb_runtime * R)
 {
     R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
@@ -1045,7 +1234,7 @@ static int wait_batch(xkb_runtime * R)
                 rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
             }
         }
-        if (rc == XKB_OK) rc = run_copies(R);
+        if (rc == XKB_OK) rc = run_copies(R, R->stream);
         const double fetch_ms = ms_since(t0);
         // the descriptors: when every task's args are exactly one descriptor, the args pool is
         // already the descriptor array (16-byte aligned 64-byte entries back to back) and is
@@ -1103,71 +1292,9 @@ static int wait_batch(xkb_runtime * R)
     }
     else
     {
-        // (3) task by task in spawn order
+        // (3) the batch as a dataflow graph on a team of host threads
         t0 = std::chrono::steady_clock::now();
-        for (size_t t = 0; t < R->pending.size() && rc == XKB_OK; ++t)
-        {
-            Task & T = R->pending[t];
-            const bool dev = is_device(R, T);
-            for (uint32_t a = 0; a < T.nacc; ++a)
-            {
-                const xkb_access_rec_t & r = recs[T.acc_off + a];
-                if (r.type == REC_NONE) continue;
-                if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
-                const uint64_t begin = rec_begin(r);
-                R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
-                // a host task on memory no region covers: that memory never has a device copy;
-                // unified memory needs no copy either way
-                if (!dev && !mirror_of(R, begin)) continue;
-                if (in_unified(R, r)) continue;
-                xkb_view_t v;
-                if ((rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v))) break;
-            }
-            if (rc) break;
-            if ((rc = run_copies(R))) break;
-            const Format & f = R->formats[T.fmtid];
-            if (dev)
-            {
-                if (f.builtin >= 0)
-                {
-                    xkb_task_desc_t d;
-                    if (T.nargs < sizeof(d)) { rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t); break; }
-                    memcpy(&d, R->args_pool.data() + T.args_off, sizeof(d));
-                    d.kind = (uint32_t) f.builtin;
-                    if ((rc = translate(R, d)) || (rc = xkb_internal_launch_task(&d, R->stream))) break;
-                }
-                else
-                {
-                    g_current = &T;
-                    ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_CUDA])(
-                        (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[1], (xkrt_task_t *) &T);
-                    g_current = nullptr;
-                }
-            }
-            else
-            {
-                if (cudaStreamSynchronize(R->stream) != cudaSuccess) { rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream"); break; }
-                g_current = &T;
-                if (T.func) T.func((xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T, T.user_data);
-                else if (f.f[XKRT_TASK_FORMAT_TARGET_HOST])
-                    ((void (*)(xkrt_runtime_t *, xkrt_device_t *, xkrt_task_t *)) f.f[XKRT_TASK_FORMAT_TARGET_HOST])(
-                        (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T);
-                else if (T.fmtid) { g_current = nullptr; rc = xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t); break; }
-                g_current = nullptr;
-            }
-            // a detached task completes when its counter is back to 0 (xkrt_task_detachable_decr
-            // or xkrt_task_complete, from any thread); its successors run after that
-            if (__atomic_load_n(&T.detach, __ATOMIC_ACQUIRE) > 0)
-            {
-                const auto w0 = std::chrono::steady_clock::now();
-                while (__atomic_load_n(&T.detach, __ATOMIC_ACQUIRE) > 0)
-                {
-                    if (ms_since(w0) > 600e3) { rc = xkb_set_error(XKB_ETIMEDOUT, "task %zu: still detached after 600 s", t); break; }
-                    std::this_thread::yield();
-                }
-                if (rc) break;
-            }
-        }
+        rc = run_dataflow(R, g, recs);
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[2] = ms_since(t0);
     }
@@ -1186,7 +1313,7 @@ static int wait_batch(xkb_runtime * R)
         });
         for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j) rc = xkb_planner_fetch(R->planner, &recs[first[j]], 0, 0, nullptr);
         const double fetch_ms = ms_since(t0);
-        if (rc == XKB_OK) rc = run_copies(R);
+        if (rc == XKB_OK) rc = run_copies(R, R->stream);
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[3] = ms_since(t0);
         if (getenv("XKB_TRACE_WAIT"))
