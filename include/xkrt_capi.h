@@ -4,16 +4,17 @@
  * API (api/c/include/xkrt/xkrt.h:61-566 and the headers it includes: memory/access/mode.h,
  * concurrency.h, scope.h, type.h, blas/matrix-storage.h, task/flag.h, task/format.h,
  * driver/driver-type.h, consts.h), so a C program written against that API compiles against
- * this header and links against libxkb200.so. Only the part of the API on the dataflow path is
- * provided: runtime init/deinit, task formats, task spawn with segment and matrix accesses,
- * task wait, task argument/access accessors, host memory allocation and registration.
+ * this header and links against libxkb200.so: runtime init/deinit, task formats, task spawn with
+ * segment, matrix and handle accesses, task wait and completion, task argument/access accessors,
+ * host / device / unified memory, asynchronous file I/O tasks, and the driver interface (queues,
+ * transfers, modules, kernel launches) of the host and the GPU.
  *
  * Execution model: spawned tasks are buffered; xkrt_task_wait resolves their dependencies on the
  * GPU (xkb_resolver), makes the data each task touches coherent where it runs (resident
  * planner: one device mirror per registered host region, H2D/D2H only for blocks the target
  * lacks), runs the tasks -- every task on the device scheduler's persistent kernel when all are
- * built-in device bodies, else one by one in spawn order (host bodies on the calling thread) --
- * and leaves host memory coherent when it returns. Handle accesses order tasks like the
+ * built-in device bodies, else as a dataflow graph on a team of host threads, each with its own
+ * CUDA stream -- and leaves host memory coherent when it returns. Handle accesses order tasks like the
  * reference's DependencyMap (they carry no data); concurrent-mode accesses and user moldable
  * tasks are not supported. Functions that return void in the reference record failures
  * instead; read them with xkb_runtime_status().
@@ -35,6 +36,8 @@ typedef void * xkrt_task_t;
 typedef void * xkrt_team_t;
 typedef void * xkrt_driver_t;
 typedef void * xkrt_device_t;
+typedef void * xkrt_queue_t;
+typedef void * xkrt_command_t;
 
 typedef uint8_t  xkrt_device_global_id_t;
 typedef uint8_t  xkrt_device_driver_id_t;
@@ -42,6 +45,9 @@ typedef uint16_t xkrt_task_wait_counter_type_t;
 typedef uint16_t xkrt_task_access_counter_type_t;
 typedef uint8_t  xkrt_task_flag_bitfield_t;
 typedef uint8_t  xkrt_task_format_id_t;
+typedef uint16_t xkrt_device_global_id_bitfield_t;
+typedef uint8_t  xkrt_driver_type_bitfield_t;
+typedef unsigned int xkrt_queue_command_list_counter_t;
 
 #define HOST_DEVICE_GLOBAL_ID        ((xkrt_device_global_id_t) 0)
 #define XKRT_DEVICES_MAX             (16)
@@ -222,6 +228,142 @@ XKB_API xkrt_task_format_id_t xkrt_task_format_put(xkrt_runtime_t * runtime, con
 XKB_API int xkrt_task_format_set(xkrt_runtime_t * runtime, xkrt_task_format_id_t fmtid, xkrt_task_format_target_t target,
                                  xkrt_task_format_func_t func);
 
+/* device memory (xkrt.h:116-117): a plain device pointer (cudaMalloc) for the GPU, host memory
+ * for device 0 -- the reference returns its allocator's chunk object instead */
+XKB_API void * xkrt_memory_device_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size);
+XKB_API void   xkrt_memory_device_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * chunk);
+
+/* asynchronous file I/O (xkrt.h:114-115; src/file/readwrite.cc:104-170): spawns nchunks host
+ * tasks, each with a virtual write (VW) segment access on its slice of the buffer, that read
+ * (pread) or write (pwrite) that slice at the same offset of the file; they run at the next
+ * xkrt_task_wait, and tasks that access the buffer after them wait for them. 0 or XKB_EINVAL. */
+XKB_API int xkrt_file_read_async(xkrt_runtime_t * runtime, int fd, void * buffer, size_t n, unsigned int nchunks);
+XKB_API int xkrt_file_write_async(xkrt_runtime_t * runtime, int fd, void * buffer, size_t n, unsigned int nchunks);
+
+/* teams (xkrt.h:207-208) */
+XKB_API xkrt_team_t * xkrt_team_driver_get(xkrt_runtime_t * runtime, xkrt_driver_type_t type);
+XKB_API xkrt_team_t * xkrt_team_driver_get_any(xkrt_runtime_t * runtime, xkrt_driver_type_bitfield_t types);
+
+/* ---- driver interface (xkrt.h:231-558; include/xkrt/driver/driver.h:62-232) ---------------- */
+typedef enum xkrt_queue_type_t {
+    XKRT_QUEUE_TYPE_H2D      = 0,
+    XKRT_QUEUE_TYPE_D2H      = 1,
+    XKRT_QUEUE_TYPE_D2D      = 2,
+    XKRT_QUEUE_TYPE_KERN     = 3,
+    XKRT_QUEUE_TYPE_FD_READ  = 4,
+    XKRT_QUEUE_TYPE_FD_WRITE = 5,
+    XKRT_QUEUE_TYPE_ALL
+} xkrt_queue_type_t;
+
+typedef enum xkrt_driver_module_format_t {
+    XKRT_DRIVER_MODULE_FORMAT_SPIRV,
+    XKRT_DRIVER_MODULE_FORMAT_NATIVE,
+    XKRT_DRIVER_MODULE_FORMAT_UNKWN
+} xkrt_driver_module_format_t;
+
+typedef void * xkrt_driver_module_t;
+typedef void * xkrt_driver_module_fn_t;
+
+typedef struct xkrt_power_counter_t { uint64_t b1, b2, b3, b4; } xkrt_power_counter_t;
+typedef struct xkrt_power_t {
+    struct priv_t { uint64_t t1, t2; xkrt_power_counter_t c1, c2; } priv;
+    double dt;   /* seconds between start and stop */
+    double P;    /* mean power in W over that time (0 when the energy counter is unavailable) */
+} xkrt_power_t;
+
+/* A kernel launcher (include/xkrt/driver/kernel-launcher.h:44-51): called by
+ * xkrt_task_kernel_launch with the queue the task's kernels go to and the command index to pass
+ * on to xkrt_device_kernel_launch. */
+typedef void (*xkrt_kernel_launcher_t)(void * runtime, void * device, void * task, void * queue, void * cmd,
+                                       xkrt_queue_command_list_counter_t idx);
+
+/* Inside a CUDA-target body: call launcher(runtime, device, task, queue, NULL, 0) with the queue of
+ * the host thread running the body; the task completes once its kernels did (synchronous or
+ * not). Outside a body: XKB_EINVAL (recorded). */
+XKB_API void xkrt_task_kernel_launch(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_task_t * task, int synchronous,
+                                     xkrt_kernel_launcher_t launcher);
+/* Launch fn (from xkrt_driver_module_get_fn) on the queue: args is the packed parameter buffer
+ * of args_size bytes (the kernel's parameters at their natural alignment), as the reference's
+ * CUDA driver passes it (src/driver/driver_cu.cc:1085-1131); records the queue's event idx when
+ * the queue has one. 0 or an XKB_E* code. */
+XKB_API int xkrt_device_kernel_launch(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_queue_t * queue,
+                                      xkrt_queue_command_list_counter_t idx, const xkrt_driver_module_fn_t * fn,
+                                      const unsigned int gx, const unsigned int gy, const unsigned int gz,
+                                      const unsigned int bx, const unsigned int by, const unsigned int bz,
+                                      const unsigned int shared_memory_bytes, void * args, const size_t args_size);
+XKB_API int xkrt_driver_kernel_launch(xkrt_driver_t * driver, xkrt_queue_t * queue, xkrt_queue_command_list_counter_t idx,
+                                      const xkrt_driver_module_fn_t * fn, const unsigned int gx, const unsigned int gy,
+                                      const unsigned int gz, const unsigned int bx, const unsigned int by,
+                                      const unsigned int bz, const unsigned int shared_memory_bytes, void * args,
+                                      const size_t args_size);
+
+/* driver meta data and lifecycle: the runtime brings its drivers up in xkrt_init, so init returns
+ * 0 and finalize does nothing */
+XKB_API const char * xkrt_driver_get_name(xkrt_driver_t * driver);
+XKB_API unsigned int xkrt_driver_get_ndevices_max(xkrt_driver_t * driver);
+XKB_API int  xkrt_driver_init(xkrt_driver_t * driver, unsigned int ndevices, int use_p2p);
+XKB_API void xkrt_driver_finalize(xkrt_driver_t * driver);
+
+/* devices of a driver: the host driver has device 0, the CUDA driver the runtime's GPU as its
+ * device 0; commit sets the device's own bit (global id) in affinity[0] */
+XKB_API xkrt_device_t * xkrt_driver_device_create(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id);
+XKB_API void xkrt_driver_device_init(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id);
+XKB_API int  xkrt_driver_device_commit(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                       xkrt_device_global_id_bitfield_t * affinity);
+XKB_API int  xkrt_driver_device_destroy(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id);
+XKB_API void xkrt_driver_device_info(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id, char * buffer,
+                                     size_t size);
+
+/* memory of a driver (area_idx is ignored: one area per device) */
+XKB_API void * xkrt_driver_memory_device_allocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                  const size_t size, int area_idx);
+XKB_API void   xkrt_driver_memory_device_deallocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                    void * ptr, const size_t size, int area_idx);
+XKB_API void * xkrt_driver_memory_host_allocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                const size_t size);
+XKB_API void   xkrt_driver_memory_host_deallocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                  void * mem, const size_t size);
+XKB_API void * xkrt_driver_memory_unified_allocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                   const size_t size);
+XKB_API void   xkrt_driver_memory_unified_deallocate(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                     void * mem, const size_t size);
+XKB_API int xkrt_driver_memory_host_register(xkrt_driver_t * driver, void * mem, uint64_t size);
+XKB_API int xkrt_driver_memory_host_unregister(xkrt_driver_t * driver, void * mem, uint64_t size);
+XKB_API int xkrt_driver_memory_unified_advise_device(xkrt_driver_t * driver, const xkrt_device_driver_id_t device_global_id,
+                                                     const void * addr, const size_t size);
+XKB_API int xkrt_driver_memory_unified_advise_host(xkrt_driver_t * driver, const void * addr, const size_t size);
+XKB_API int xkrt_driver_memory_unified_prefetch_device(xkrt_driver_t * driver, const xkrt_device_driver_id_t device_global_id,
+                                                       const void * addr, const size_t size);
+XKB_API int xkrt_driver_memory_unified_prefetch_host(xkrt_driver_t * driver, const void * addr, const size_t size);
+
+/* transfers: synchronous ones complete before returning; asynchronous ones are ordered on the
+ * queue (a host-driver queue copies synchronously) */
+XKB_API int xkrt_driver_transfer_h2d(xkrt_driver_t * driver, void * dst, void * src, const size_t size);
+XKB_API int xkrt_driver_transfer_d2h(xkrt_driver_t * driver, void * dst, void * src, const size_t size);
+XKB_API int xkrt_driver_transfer_d2d(xkrt_driver_t * driver, void * dst, void * src, const size_t size);
+XKB_API int xkrt_driver_transfer_h2d_async(xkrt_driver_t * driver, void * dst, void * src, const size_t size, xkrt_queue_t * queue);
+XKB_API int xkrt_driver_transfer_d2h_async(xkrt_driver_t * driver, void * dst, void * src, const size_t size, xkrt_queue_t * queue);
+XKB_API int xkrt_driver_transfer_d2d_async(xkrt_driver_t * driver, void * dst, void * src, const size_t size, xkrt_queue_t * queue);
+
+/* queues: a CUDA queue is a non-blocking stream with `capacity` events, one per command index;
+ * delete waits for the queue's work first */
+XKB_API int xkrt_driver_queue_suggest(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id, xkrt_queue_type_t qtype);
+XKB_API xkrt_queue_t * xkrt_driver_queue_create(xkrt_driver_t * driver, xkrt_device_t * device, xkrt_queue_type_t qtype,
+                                                xkrt_queue_command_list_counter_t capacity);
+XKB_API void xkrt_driver_queue_delete(xkrt_driver_t * driver, xkrt_queue_t * queue);
+
+/* modules: NATIVE images (cubin, fatbin or PTX for this GPU) loaded with the driver's module
+ * loader; SPIR-V is refused (NULL) */
+XKB_API xkrt_driver_module_t xkrt_driver_module_load(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id,
+                                                     uint8_t * bin, size_t binsize, xkrt_driver_module_format_t format);
+XKB_API void xkrt_driver_module_unload(xkrt_driver_t * driver, xkrt_driver_module_t module);
+XKB_API xkrt_driver_module_fn_t xkrt_driver_module_get_fn(xkrt_driver_t * driver, xkrt_driver_module_t module, const char * name);
+
+/* energy (driver.h power_start/stop): wall time between the two calls, and the GPU's mean power
+ * from its energy counter (read through NVML when the library is present) */
+XKB_API void xkrt_driver_power_start(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id, xkrt_power_t * pwr);
+XKB_API void xkrt_driver_power_stop(xkrt_driver_t * driver, xkrt_device_driver_id_t device_driver_id, xkrt_power_t * pwr);
+
 /* ---- additions of this library (no counterpart in the reference API) --------------------- */
 /* A format whose device body is one of the library's built-in tile bodies (XKB_TASK_HEAT_F64,
  * XKB_TASK_HEAT_F32, XKB_TASK_AXPBY): the task's args are an xkb_task_desc_t whose grid / vector
@@ -234,7 +376,7 @@ XKB_API int xkb_runtime_status(xkrt_runtime_t * runtime);
  * the stream of the host thread running it (each thread of the team has its own). */
 XKB_API void * xkb_runtime_stream(xkrt_runtime_t * runtime);
 /* Counters of the last xkrt_task_wait: tasks run, unique edges, copies H2D / D2H, and whether the
- * persistent scheduler ran the batch (1) or the tasks ran one by one (0). */
+ * persistent scheduler ran the batch (1) or the host team ran it as a dataflow graph (0). */
 XKB_API int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks, uint64_t * edges, uint64_t * h2d,
                                   uint64_t * d2h, int * fused);
 /* Bytes the last xkrt_task_wait copied host -> device and device -> host. */

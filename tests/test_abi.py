@@ -41,6 +41,41 @@ def test_c_api_symbols_exported():
     assert all(hasattr(L, n) for n in names)
 
 
+# Every function of the reference's C API (api/c/include/xkrt/xkrt.h:104-566), except the two it
+# compiles out (#if 0: xkrt_driver_memory_device_info, xkrt_driver_device_cpuset).
+REFERENCE_C_API = """
+xkrt_init xkrt_deinit xkrt_reset xkrt_memory_register xkrt_memory_unregister xkrt_memory_register_async
+xkrt_memory_unregister_async xkrt_file_read_async xkrt_file_write_async xkrt_memory_device_allocate
+xkrt_memory_device_deallocate xkrt_memory_host_allocate xkrt_memory_host_deallocate xkrt_memory_unified_allocate
+xkrt_memory_unified_deallocate xkrt_driver_get xkrt_device_get xkrt_device_driver_get xkrt_device_driver_id_get
+xkrt_get_ndevices xkrt_get_ndevices_max xkrt_task_detachable_incr xkrt_task_detachable_decr xkrt_task_complete
+xkrt_task_commit xkrt_task_enqueue xkrt_task_wait xkrt_task_args xkrt_task_accesses xkrt_task_access
+xkrt_task_access_replica xkrt_task_current xkrt_task_spawn_generic xkrt_task_spawn_with_format
+xkrt_task_spawn_with_format_with_accesses xkrt_task_spawn xkrt_task_kernel_launch xkrt_team_driver_device_get
+xkrt_team_driver_get xkrt_team_driver_get_any xkrt_team_task_spawn xkrt_team_task_spawn_with_accesses
+xkrt_task_format_put xkrt_task_format_set xkrt_driver_get_name xkrt_driver_get_ndevices_max xkrt_driver_init
+xkrt_driver_finalize xkrt_driver_device_create xkrt_driver_device_init xkrt_driver_device_commit
+xkrt_driver_device_destroy xkrt_driver_device_info xkrt_driver_memory_device_allocate
+xkrt_driver_memory_device_deallocate xkrt_driver_memory_host_allocate xkrt_driver_memory_host_deallocate
+xkrt_driver_memory_unified_allocate xkrt_driver_memory_unified_deallocate xkrt_driver_memory_host_register
+xkrt_driver_memory_host_unregister xkrt_driver_memory_unified_advise_device xkrt_driver_memory_unified_advise_host
+xkrt_driver_memory_unified_prefetch_device xkrt_driver_memory_unified_prefetch_host xkrt_driver_transfer_h2d
+xkrt_driver_transfer_d2h xkrt_driver_transfer_d2d xkrt_driver_transfer_h2d_async xkrt_driver_transfer_d2h_async
+xkrt_driver_transfer_d2d_async xkrt_device_kernel_launch xkrt_driver_kernel_launch xkrt_driver_queue_suggest
+xkrt_driver_queue_create xkrt_driver_queue_delete xkrt_driver_module_load xkrt_driver_module_unload
+xkrt_driver_module_get_fn xkrt_driver_power_start xkrt_driver_power_stop xkrt_logger_info xkrt_logger_debug
+xkrt_logger_warn xkrt_logger_error xkrt_logger_fatal
+""".split()
+
+
+def test_reference_c_api_complete():
+    """A program using any function of the reference's C API finds it declared and exported."""
+    names = declared_symbols()
+    assert set(REFERENCE_C_API) <= names, sorted(set(REFERENCE_C_API) - names)
+    L = xk.lib()
+    assert all(hasattr(L, n) for n in REFERENCE_C_API)
+
+
 def test_version_reports_sm100a():
     assert b"sm_100a" in xk.lib().xkb_version()
 

@@ -31,6 +31,20 @@ def test_devices_detach_unified_program(torch_cuda, tmp_path):
     assert json.loads(r.stdout.strip().splitlines()[-1])["ok"] == 1
 
 
+def test_driver_interface_program(torch_cuda, tmp_path):
+    """Drivers, devices, driver memory and queued transfers, a module image (cubin built here)
+    whose kernel runs from a queue and from a CUDA task body (xkrt_task_kernel_launch), device
+    memory, file I/O tasks ordered before a reader task, teams, the energy counter."""
+    cubin = str(tmp_path / "scale.cubin")
+    subprocess.run(["nvcc", "-cubin", "-gencode", "arch=compute_100a,code=sm_100a", "-o", cubin,
+                    os.path.join(REPO, "tests", "capi", "scale_kernel.cu")], check=True)
+    r = subprocess.run([build("driver_capi", tmp_path), cubin, str(tmp_path / "scratch.bin")], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["ok"] == 1 and "B200" in out["info"]
+
+
 @pytest.mark.parametrize("threads", [None, 1])
 def test_dataflow_host_team(torch_cuda, tmp_path, threads):
     """A non-fused batch runs as a dataflow graph on a team of host threads: independent tasks run

@@ -8,15 +8,19 @@
 // B200 design: spawns are buffered until xkrt_task_wait; the batch's dependencies are resolved
 // on the GPU; data coherency uses the resident planner (one device mirror per registered host
 // region, copies only for blocks the executing side lacks); a batch of built-in device bodies
-// runs as one persistent-scheduler launch, any other batch runs task by task in spawn order
-// (a topological order). Host memory is coherent again when xkrt_task_wait returns.
+// runs as one persistent-scheduler launch, any other batch as a dataflow graph on a team of host
+// threads. Host memory is coherent again when xkrt_task_wait returns.
+#include "capi_objects.h"
 #include "common.cuh"
 #include "internal.h"
 #include "pool.h"
 #include "../../include/xkrt_capi.h"
 
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -73,9 +77,9 @@ static bool task_unref(Task & T)
     return false;
 }
 
-// Opaque device and driver objects handed to bodies and returned by the getters.
-struct Device { int global_id; };
-struct Driver { int type; };
+using xkb_capi::Device;
+using xkb_capi::Driver;
+using xkb_capi::Queue;
 
 thread_local Task * g_current = nullptr;  // task whose body runs on this thread (xkrt_task_current)
 thread_local cudaStream_t g_stream = nullptr;   // the stream of the worker running a CUDA body
@@ -125,13 +129,14 @@ struct xkb_runtime {
     xkb_sched_t * sched = nullptr;
     cudaStream_t stream = nullptr;
     bool gpu = false;
-    int status = XKB_OK;
+    std::atomic<int> status{XKB_OK};                 // first failure recorded (any thread)
     uint64_t last_tasks = 0, last_edges = 0, last_h2d = 0, last_d2h = 0, last_h2d_bytes = 0, last_d2h_bytes = 0;
     int last_fused = 0;
     double last_ms[4] = {0, 0, 0, 0};                 // resolve, coherency + launch prep, run, write-back
     int dummy_team = 0;
     Device devices[2] = {{0}, {1}};                   // the host, the GPU
-    Driver drivers[2] = {{XKRT_DRIVER_TYPE_HOST}, {XKRT_DRIVER_TYPE_CUDA}};
+    Driver drivers[2] = {{XKRT_DRIVER_TYPE_HOST, -1, &devices[0]}, {XKRT_DRIVER_TYPE_CUDA, 0, &devices[1]}};
+    xkrt_task_format_id_t fmt_file[2] = {0, 0};       // file read / write tasks
     bool any_unified = false;
 };
 
@@ -139,7 +144,8 @@ static xkb_runtime * RT(xkrt_runtime_t * r) { return (xkb_runtime *) r; }
 
 static void fail(xkb_runtime * R, int rc)
 {
-    if (R && rc != XKB_OK && R->status == XKB_OK) R->status = rc;
+    int ok = XKB_OK;
+    if (R && rc != XKB_OK) R->status.compare_exchange_strong(ok, rc);
 }
 
 // The prefault helpers (one per spawn pool): while the program spawns, they fault in the pages
@@ -169,6 +175,44 @@ static void prefault_loop(xkb_runtime * R, int pool)
     }
 }
 
+// File I/O task body (src/file/readwrite.cc:60-90 submits the same read or write as an io_uring
+// command): pread / pwrite of the task's slice of the buffer at the same offset of the file.
+struct FileArgs { int fd; int write; size_t offset; void * buffer; size_t size; };
+
+static void file_body(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_task_t * task)
+{
+    (void) device;
+    FileArgs a;
+    memcpy(&a, xkrt_task_args(task), sizeof(a));
+    size_t done = 0;
+    while (done < a.size)
+    {
+        char * p = (char *) a.buffer + done;
+        const ssize_t k = a.write ? pwrite(a.fd, p, a.size - done, (off_t) (a.offset + done))
+                                  : pread(a.fd, p, a.size - done, (off_t) (a.offset + done));
+        if (k < 0 && errno == EINTR) continue;
+        if (k <= 0)
+        {
+            fail(RT(runtime), xkb_set_error(XKB_EINVAL, "file %s: %zu of %zu bytes at offset %zu (%s)", a.write ? "write" : "read", done,
+                                             a.size, a.offset, k < 0 ? strerror(errno) : "end of file"));
+            return;
+        }
+        done += (size_t) k;
+    }
+}
+
+static void register_file_formats(xkb_runtime * R)
+{
+    for (int w = 0; w < 2; ++w)
+    {
+        const int id = R->next_fmtid++;
+        R->formats[id].used = true;
+        R->formats[id].label = w ? "file_write_async" : "file_read_async";
+        R->formats[id].f[XKRT_TASK_FORMAT_TARGET_HOST] = (xkrt_task_format_func_t) file_body;
+        R->fmt_file[w] = (xkrt_task_format_id_t) id;
+    }
+}
+
 extern "C" int xkrt_init(xkrt_runtime_t ** out)
 {
     if (!out) return xkb_set_error(XKB_EINVAL, "xkrt_init: null output");
@@ -177,6 +221,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     int n = 0;
     R->gpu = cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
     if (R->gpu) cudaGetDevice(&R->device);
+    R->drivers[1].ordinal = R->device;
     R->chunk = RESOLVE_CHUNK;
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
@@ -194,6 +239,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
         R->pf_want = 0;                            // nothing is populated before the first spawns
         for (int k = 0; k < 3; ++k) R->prefaulter[k] = std::thread(prefault_loop, R, k);
     }
+    register_file_formats(R);
     int rc = xkb_planner_create_resident(&R->planner);
     if (rc == XKB_OK && R->gpu)
     {
@@ -444,9 +490,7 @@ extern "C" int xkb_runtime_status(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
     if (!R) return XKB_EINVAL;
-    const int s = R->status;
-    R->status = XKB_OK;
-    return s;
+    return R->status.exchange(XKB_OK);
 }
 
 extern "C" void * xkb_runtime_stream(xkrt_runtime_t * runtime)
@@ -553,6 +597,97 @@ extern "C" void xkrt_team_task_spawn_with_accesses(xkrt_runtime_t * runtime, xkr
     (void) team;
     spawn(RT(runtime), HOST_DEVICE_GLOBAL_ID, TASK_FLAG_DEPENDENT, 0, nullptr, 0, accesses, naccesses > 0 ? (size_t) naccesses : 0,
           func, user_data);
+}
+
+extern "C" xkrt_team_t * xkrt_team_driver_get(xkrt_runtime_t * runtime, xkrt_driver_type_t type)
+{
+    return xkrt_team_driver_device_get(runtime, type, 0);
+}
+
+extern "C" xkrt_team_t * xkrt_team_driver_get_any(xkrt_runtime_t * runtime, xkrt_driver_type_bitfield_t types)
+{
+    return (types & (1u << XKRT_DRIVER_TYPE_HOST)) ? xkrt_team_driver_device_get(runtime, XKRT_DRIVER_TYPE_HOST, 0) : nullptr;
+}
+
+// Spawn n tasks over [buffer, buffer + size), split as the reference's runtime_t::foreach does
+// (include/xkrt/runtime.h:333-352: n = min(n, size) chunks of size / n bytes, the last one takes
+// the rest), each reading or writing its slice of the file (src/file/readwrite.cc:104-170). The
+// reference declares a virtual write (VW) on the slice, which orders the tasks but moves no data;
+// here a read declares W and a write RW: the same dependencies (W and RW order exactly like VW),
+// and the buffer is also coherent on the host when the body runs and owned by it after a read.
+static int file_async(xkrt_runtime_t * runtime, int fd, void * buffer, size_t size, unsigned int n, int write)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || !buffer || fd < 0 || n == 0) return xkb_set_error(XKB_EINVAL, "xkrt_file_%s_async: bad arguments", write ? "write" : "read");
+    if (size == 0) return XKB_OK;
+    if (size < n) n = (unsigned) size;
+    const size_t chunk = size / n;
+    const uintptr_t p = (uintptr_t) buffer;
+    for (unsigned i = 0; i < n; ++i)
+    {
+        const uintptr_t a = p + i * chunk, b = i == n - 1 ? p + size : p + (i + 1) * chunk;
+        FileArgs f{fd, write, (size_t) (a - p), (void *) a, (size_t) (b - a)};
+        xkrt_access_t acc;
+        memset(&acc, 0, sizeof(acc));
+        acc.concurrency = ACCESS_CONCURRENCY_SEQUENTIAL; acc.mode = write ? ACCESS_MODE_RW : ACCESS_MODE_W;
+        acc.scope = ACCESS_SCOPE_NONUNIFIED; acc.type = ACCESS_TYPE_SEGMENT;
+        acc.region.segment.a = (void *) a; acc.region.segment.b = (void *) b;
+        xkrt_task_spawn_with_format_with_accesses(runtime, HOST_DEVICE_GLOBAL_ID, R->fmt_file[write], &f, sizeof(f), &acc, 1);
+    }
+    return XKB_OK;
+}
+
+extern "C" int xkrt_file_read_async(xkrt_runtime_t * runtime, int fd, void * buffer, size_t n, unsigned int nchunks)
+{
+    return file_async(runtime, fd, buffer, n, nchunks, 0);
+}
+
+extern "C" int xkrt_file_write_async(xkrt_runtime_t * runtime, int fd, void * buffer, size_t n, unsigned int nchunks)
+{
+    return file_async(runtime, fd, buffer, n, nchunks, 1);
+}
+
+extern "C" void * xkrt_memory_device_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || device > 1 || (device == 1 && !R->gpu)) { fail(R, xkb_set_error(XKB_EINVAL, "xkrt_memory_device_allocate: no device %d", (int) device)); return nullptr; }
+    void * p = xkrt_driver_memory_device_allocate((xkrt_driver_t *) &R->drivers[device], 0, size, 0);
+    if (!p) fail(R, XKB_ENOMEM);
+    return p;
+}
+
+extern "C" void xkrt_memory_device_deallocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, void * chunk)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || device > 1) { fail(R, XKB_EINVAL); return; }
+    xkrt_driver_memory_device_deallocate((xkrt_driver_t *) &R->drivers[device], 0, chunk, 0, 0);
+}
+
+// The launcher gets the queue of the host thread running the CUDA body (its stream); the task's
+// kernels are complete when the body's task completes (src/sched.cc:469-505 records an event on
+// the kernel queue and completes the task from its callback).
+extern "C" void xkrt_task_kernel_launch(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_task_t * task, int synchronous,
+                                        xkrt_kernel_launcher_t launcher)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || !launcher) { fail(R, xkb_set_error(XKB_EINVAL, "xkrt_task_kernel_launch: no runtime or launcher")); return; }
+    if (!g_stream) { fail(R, xkb_set_error(XKB_EINVAL, "xkrt_task_kernel_launch: called outside a CUDA task body")); return; }
+    Queue q{XKRT_DRIVER_TYPE_CUDA, XKRT_QUEUE_TYPE_KERN, R->device, g_stream, false, 0, nullptr};
+    launcher(runtime, device, task, &q, nullptr, 0);
+    if (synchronous && cudaStreamSynchronize(g_stream) != cudaSuccess) fail(R, xkb_set_cuda_error(cudaGetLastError()));
+}
+
+extern "C" int xkrt_device_kernel_launch(xkrt_runtime_t * runtime, xkrt_device_t * device, xkrt_queue_t * queue,
+                                         xkrt_queue_command_list_counter_t idx, const xkrt_driver_module_fn_t * fn,
+                                         const unsigned int gx, const unsigned int gy, const unsigned int gz, const unsigned int bx,
+                                         const unsigned int by, const unsigned int bz, const unsigned int shared_memory_bytes,
+                                         void * args, const size_t args_size)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || !device || ((Device *) device)->global_id != 1 || !R->gpu)
+        return xkb_set_error(XKB_EINVAL, "xkrt_device_kernel_launch: kernels run on the GPU device");
+    return xkrt_driver_kernel_launch((xkrt_driver_t *) &R->drivers[1], queue, idx, fn, gx, gy, gz, bx, by, bz, shared_memory_bytes,
+                                     args, args_size);
 }
 
 // ---- task accessors --------------------------------------------------------------------------
