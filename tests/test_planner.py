@@ -99,3 +99,40 @@ def test_resident_mode_moves_each_byte_once():
     assert int((c[:, 11] * c[:, 12]).sum()) == (nx - 2) ** 2       # the interior the tasks wrote
     with pytest.raises(xk.XkbError):                                # outside every region
         P.fetch(S.from_tuples([[("m", S.R, 1 << 20, nx, 0, 0, 8, 8, 8)]])[0], 0, 1)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_resident_mode_matches_model(seed):
+    """Random accesses -- tiles of two matrices with different (ld, sizeof), tiles that wrap the
+    leading dimension, segments, every mode incl. virtual ones, fetches to the GPU and to the
+    host -- give the copies and views of the Python model of the resident planner, in order."""
+    import numpy as np
+    import streams as S
+    from resident_model import ResidentModel
+    rng = np.random.default_rng(seed)
+    P, M = xk.Planner(resident=True), ResidentModel()
+    # (base, ld, sizeof, columns); the first base is not a multiple of ld*sizeof, so tiles wrap
+    mats = [((1 << 20) + 24, 64, 8, 40), ((1 << 21), 50, 4, 30)]
+    seg_base, seg_len = 1 << 22, 5000
+    for base, ld, s, cols in mats:
+        assert P.add_region(base, ld * cols * s + 64) == M.add_region(base, ld * cols * s + 64)
+    assert P.add_region(seg_base, seg_len) == M.add_region(seg_base, seg_len)
+    modes = [S.R, S.W, S.RW, S.R | S.V, S.W | S.V]
+    for t in range(300):
+        mode = int(rng.choice(modes, p=[0.35, 0.2, 0.25, 0.1, 0.1]))
+        kind = rng.integers(0, 3)
+        if kind < 2:
+            base, ld, s, cols = mats[kind]
+            m, n = int(rng.integers(1, ld + 1)), int(rng.integers(1, 8))
+            om, on = int(rng.integers(0, ld - m + 1)), int(rng.integers(0, cols - n))
+            rec = S.from_tuples([[("m", mode, base, ld, om, on, m, n, s)]])[0]
+        else:
+            lo = int(rng.integers(0, seg_len - 1))
+            hi = int(rng.integers(lo + 1, min(seg_len, lo + 700) + 1))
+            rec = S.from_tuples([[("s", mode, seg_base + lo, seg_base + hi)]])[0]
+        rec["task"] = t
+        dev = int(rng.random() < 0.7)
+        v = P.fetch(rec, t % 3, dev)
+        assert tuple(v) == M.fetch(rec, t % 3, dev), t
+        got = [tuple(int(x) for x in row) for row in P.copies(take=True)]
+        assert got == M.take(), t
