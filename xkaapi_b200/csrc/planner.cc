@@ -32,6 +32,7 @@
 //    coherent or not -- as the reference selects it, :1110-1160); completion sets the host bit.
 #include "common.cuh"
 
+#include <algorithm>
 #include <cstring>
 #include <iterator>
 #include <map>
@@ -135,6 +136,95 @@ inline int64_t view_off(const View & v, uint64_t x, uint64_t y, uint64_t s)
     return ((int64_t) x - v.ox) + ((int64_t) y - v.oy) * (int64_t) v.ld * (int64_t) s;
 }
 
+// The same canonical partition for the resident mode, whose blocks carry only the device bits:
+// sorted arrays instead of trees (a fetch is a few binary searches over cache-resident arrays;
+// the partition only grows while the first accesses of each shape arrive).
+struct RSlab {
+    uint64_t x1;
+    std::vector<uint64_t> ys, ends;     // block starts (ascending) and ends
+    std::vector<uint8_t> st;            // DEV_HOST | DEV_GPU per block
+};
+struct RFrame {
+    std::vector<uint64_t> xs;           // slab starts, ascending
+    std::vector<RSlab> slabs;
+};
+struct RPartite { uint64_t x0, x1, y0, y1; uint8_t * st; };
+
+void rsplit_y(RSlab & sl, uint64_t y)
+{
+    size_t i = (size_t) (std::upper_bound(sl.ys.begin(), sl.ys.end(), y) - sl.ys.begin());
+    if (i == 0) return;
+    --i;
+    if (sl.ys[i] < y && y < sl.ends[i])
+    {
+        sl.ys.insert(sl.ys.begin() + i + 1, y);
+        sl.ends.insert(sl.ends.begin() + i + 1, sl.ends[i]);
+        sl.st.insert(sl.st.begin() + i + 1, sl.st[i]);
+        sl.ends[i] = y;
+    }
+}
+
+void rsplit_x(RFrame & f, uint64_t x)
+{
+    size_t i = (size_t) (std::upper_bound(f.xs.begin(), f.xs.end(), x) - f.xs.begin());
+    if (i == 0) return;
+    --i;
+    if (f.xs[i] < x && x < f.slabs[i].x1)
+    {
+        RSlab right = f.slabs[i];
+        f.slabs[i].x1 = x;
+        f.xs.insert(f.xs.begin() + i + 1, x);
+        f.slabs.insert(f.slabs.begin() + i + 1, std::move(right));
+    }
+}
+
+void rinsert(RFrame & f, const Rect & r)
+{
+    rsplit_x(f, r.x0);
+    rsplit_x(f, r.x1);
+    uint64_t x = r.x0;
+    size_t i = (size_t) (std::lower_bound(f.xs.begin(), f.xs.end(), r.x0) - f.xs.begin());
+    const size_t first = i;
+    while (x < r.x1)                                   // slabs over the x-gaps of [x0, x1)
+    {
+        if (i < f.xs.size() && f.xs[i] == x) { x = f.slabs[i].x1; ++i; continue; }
+        const uint64_t end = (i < f.xs.size() && f.xs[i] < r.x1) ? f.xs[i] : r.x1;
+        f.xs.insert(f.xs.begin() + i, x);
+        RSlab sl; sl.x1 = end;
+        f.slabs.insert(f.slabs.begin() + i, std::move(sl));
+        ++i;
+        x = end;
+    }
+    for (i = first; i < f.xs.size() && f.xs[i] < r.x1; ++i)
+    {
+        RSlab & sl = f.slabs[i];
+        rsplit_y(sl, r.y0);
+        rsplit_y(sl, r.y1);
+        uint64_t y = r.y0;
+        size_t j = (size_t) (std::lower_bound(sl.ys.begin(), sl.ys.end(), r.y0) - sl.ys.begin());
+        while (y < r.y1)                               // blocks over the y-gaps of [y0, y1)
+        {
+            if (j < sl.ys.size() && sl.ys[j] == y) { y = sl.ends[j]; ++j; continue; }
+            const uint64_t end = (j < sl.ys.size() && sl.ys[j] < r.y1) ? sl.ys[j] : r.y1;
+            sl.ys.insert(sl.ys.begin() + j, y);
+            sl.ends.insert(sl.ends.begin() + j, end);
+            sl.st.insert(sl.st.begin() + j, (uint8_t) 0);
+            ++j;
+            y = end;
+        }
+    }
+}
+
+void rpartites(RFrame & f, const Rect & r, std::vector<RPartite> & out)
+{
+    for (size_t i = (size_t) (std::lower_bound(f.xs.begin(), f.xs.end(), r.x0) - f.xs.begin()); i < f.xs.size() && f.xs[i] < r.x1; ++i)
+    {
+        RSlab & sl = f.slabs[i];
+        for (size_t j = (size_t) (std::lower_bound(sl.ys.begin(), sl.ys.end(), r.y0) - sl.ys.begin()); j < sl.ys.size() && sl.ys[j] < r.y1; ++j)
+            out.push_back({f.xs[i], sl.x1, sl.ys[j], sl.ends[j], &sl.st[j]});
+    }
+}
+
 } // namespace
 
 struct xkb_planner {
@@ -145,6 +235,8 @@ struct xkb_planner {
     // resident mode: one device mirror per registered host region (base -> (size, index))
     bool resident = false;
     std::map<uint64_t, std::pair<uint64_t, int32_t>> regions;
+    std::map<std::pair<uint64_t, uint64_t>, std::unique_ptr<RFrame>> rframes;
+    std::vector<RPartite> rscratch;
 };
 
 // The access's rects in its (ld, sizeof) frame (access.hpp:204-287): one rect, or two when the
@@ -211,16 +303,16 @@ static int resident_fetch(xkb_planner * P, const xkb_access_rec_t & a, int64_t a
     const uint64_t end = seg ? a.ld : begin + ((a.n - 1) * a.ld + a.m) * a.sizeof_type;
     if (begin < rbase || end > rbase + rsize) return xkb_set_error(XKB_EINVAL, "planner: access crosses the end of its region");
     if (view) { view->alloc = region; view->off = (int64_t) (begin - rbase); view->ld = seg ? (int64_t) (a.ld - a.addr) : (int64_t) a.ld; }
-    std::unique_ptr<Frame> & fp = P->frames[{ld, s}];
-    if (!fp) { fp.reset(new (std::nothrow) Frame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); fp->ld = ld; fp->s = s; }
-    for (int k = 0; k < nr; ++k) insert(*fp, rr[k]);
-    P->scratch.clear();
-    for (int k = 0; k < nr; ++k) partites(*fp, rr[k], P->scratch);
+    std::unique_ptr<RFrame> & fp = P->rframes[{ld, s}];
+    if (!fp) { fp.reset(new (std::nothrow) RFrame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); }
+    for (int k = 0; k < nr; ++k) rinsert(*fp, rr[k]);
+    P->rscratch.clear();
+    for (int k = 0; k < nr; ++k) rpartites(*fp, rr[k], P->rscratch);
     const uint8_t me = device == 0 ? DEV_HOST : DEV_GPU;
-    for (const Partite & p : P->scratch)
+    for (const RPartite & p : P->rscratch)
     {
-        State & st = *p.st;
-        const bool host_ok = st.dev == 0 || (st.dev & DEV_HOST), gpu_ok = st.dev & DEV_GPU;
+        uint8_t & dev = *p.st;
+        const bool host_ok = dev == 0 || (dev & DEV_HOST), gpu_ok = dev & DEV_GPU;
         if (a.mode & XKB_ACCESS_MODE_R && !(a.mode & XKB_ACCESS_MODE_V) && !(me == DEV_HOST ? host_ok : gpu_ok))
         {
             const uint64_t h = p.x0 + p.y0 * stride;
@@ -234,9 +326,9 @@ static int resident_fetch(xkb_planner * P, const xkb_access_rec_t & a, int64_t a
             if (seg) { c.m = (int64_t) (p.x1 - p.x0); c.n = 1; c.sizeof_type = 1; }
             else { c.m = (int64_t) ((p.x1 - p.x0) / s); c.n = (int64_t) (p.y1 - p.y0); c.sizeof_type = (int64_t) s; }
             P->copies.push_back(c);
-            st.dev |= (st.dev == 0 ? DEV_HOST : 0) | me;
+            dev |= (dev == 0 ? DEV_HOST : 0) | me;
         }
-        if (a.mode & XKB_ACCESS_MODE_W && !(a.mode & XKB_ACCESS_MODE_V)) st.dev = me;
+        if (a.mode & XKB_ACCESS_MODE_W && !(a.mode & XKB_ACCESS_MODE_V)) dev = me;
     }
     return XKB_OK;
 }
