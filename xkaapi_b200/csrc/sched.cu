@@ -357,23 +357,13 @@ struct xkb_sched {
 static int check_tasks(const xkb_task_desc_t * t, size_t n)
 {
     for (size_t i = 0; i < n; ++i)
-    {
-        const xkb_task_desc_t & d = t[i];
-        if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
+        if (!xkb_internal_task_valid(t[i]))
         {
-            const auto & h = d.u.heat;
-            if (!h.src || !h.dst || h.src == h.dst || h.ld < h.nx || h.nx < 0 || h.ny < 0 || h.x0 > h.x1 || h.y0 > h.y1)
-                return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad heat tile", i);
+            const uint32_t k = t[i].kind;
+            if (k == XKB_TASK_HEAT_F64 || k == XKB_TASK_HEAT_F32) return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad heat tile", i);
+            if (k == XKB_TASK_AXPBY) return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad axpby range", i);
+            return xkb_set_error(XKB_EINVAL, "sched: task %zu: unknown kind %u", i, k);
         }
-        else if (d.kind == XKB_TASK_AXPBY)
-        {
-            const auto & a = d.u.axpby;
-            if (a.lo < 0 || a.lo > a.hi || (a.hi > a.lo && (!a.x || !a.y)))
-                return xkb_set_error(XKB_EINVAL, "sched: task %zu: bad axpby range", i);
-        }
-        else if (d.kind != XKB_TASK_NOOP)
-            return xkb_set_error(XKB_EINVAL, "sched: task %zu: unknown kind %u", i, d.kind);
-    }
     return XKB_OK;
 }
 
@@ -419,10 +409,10 @@ extern "C" int xkb_sched_set_tasks(xkb_sched_t * S, const xkb_task_desc_t * task
 
 // Library-internal: the descriptors go to the device only (no host copy, so only the persistent
 // forms can run them); for callers that hand over millions of descriptors for one run.
-int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks)
+int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks, bool checked)
 {
     if (!S || (ntasks && !tasks)) return xkb_set_error(XKB_EINVAL, "sched_set_tasks: bad arguments");
-    int rc = check_tasks(tasks, ntasks);
+    int rc = checked ? XKB_OK : check_tasks(tasks, ntasks);
     if (rc) return rc;
     S->host_tasks.clear(); S->host_tasks.shrink_to_fit();
     S->ntasks = ntasks;

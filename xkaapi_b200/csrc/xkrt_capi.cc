@@ -121,6 +121,9 @@ struct xkb_runtime {
     // the planner (coherency decisions and their copies) is used by one task at a time
     std::vector<cudaStream_t> wstreams;
     std::mutex plan_mu;
+    // page-locked prefix of the args pool (the descriptor upload of fused batches reads it)
+    size_t args_pinned = 0;
+    std::vector<std::pair<void *, size_t>> pinned_ranges;
     std::atomic<struct Dataflow *> df{nullptr};       // the batch being executed (detached completion)
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
@@ -273,6 +276,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
         if (kv.second.pinned_by_us) cudaFreeHost((void *) kv.first);
     }
     for (cudaStream_t w : R->wstreams) cudaStreamDestroy(w);
+    for (auto & r : R->pinned_ranges) cudaHostUnregister(r.first);
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
     if (R->stream) cudaStreamDestroy(R->stream);
@@ -1315,6 +1319,22 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
     return XKB_OK;
 }
 
+// Page-lock the args pool up to `bytes` (rounded up to 2 MB, within the reservation) so that the
+// descriptor upload of a fused batch runs at DMA speed instead of through the driver's pageable
+// staging; the locked prefix only grows and is released with the runtime. If locking fails the
+// pool stays pageable and the upload is just slower.
+static void pin_args(xkb_runtime * R, size_t bytes)
+{
+    constexpr size_t STEP = size_t(2) << 20;
+    if (!R->args_pool.fixed()) return;
+    const size_t want = std::min((bytes + STEP - 1) & ~(STEP - 1), R->args_pool.capacity_bytes());
+    if (want <= R->args_pinned) return;
+    uint8_t * p = R->args_pool.data() + R->args_pinned;
+    if (cudaHostRegister(p, want - R->args_pinned, cudaHostRegisterDefault) != cudaSuccess) { cudaGetLastError(); return; }
+    R->pinned_ranges.push_back({p, want - R->args_pinned});
+    R->args_pinned = want;
+}
+
 static int wait_batch(xkb_runtime * R)
 {
     R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
@@ -1352,22 +1372,21 @@ static int wait_batch(xkb_runtime * R)
 
     bool fused = true;
     for (size_t t = 0; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
+    std::vector<uint32_t> fused_first;      // fused batches: first occurrence of every distinct record
 
     if (fused)
     {
         // (2) every access made coherent on the device up front: with no host task in the batch
         // the host data cannot change meanwhile, so the first-touch copies can all go first
         t0 = std::chrono::steady_clock::now();
+        fused_first = distinct_records(recs, nacc, [&](size_t k) {
+            // handles carry no data; unified memory is used in place
+            return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE && !in_unified(R, recs[k]);
+        });
+        for (size_t j = 0; j < fused_first.size() && rc == XKB_OK; ++j)
         {
-            const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
-                // handles carry no data; unified memory is used in place
-                return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE && !in_unified(R, recs[k]);
-            });
-            for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j)
-            {
-                const uint32_t k = first[j];
-                rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
-            }
+            const uint32_t k = fused_first[j];
+            rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
         }
         if (rc == XKB_OK) rc = run_copies(R, R->stream);
         const double fetch_ms = ms_since(t0);
@@ -1394,20 +1413,23 @@ static int wait_batch(xkb_runtime * R)
                         memcpy(&descs[t], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
                     }
                     descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
-                    if (!translate_hint(R, descs[t], h)) { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
+                    if (!translate_hint(R, descs[t], h) || !xkb_internal_task_valid(descs[t]))
+                    { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
                 }
             });
         if (rc == XKB_OK && bad_args != SIZE_MAX)
             rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", (size_t) bad_args);
         else if (rc == XKB_OK && bad_ptr != SIZE_MAX)
-            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region", (size_t) bad_ptr);
+            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region, or the "
+                                           "tile or range is malformed", (size_t) bad_ptr);
+        if (rc == XKB_OK && dense_args) pin_args(R, nt * sizeof(xkb_task_desc_t));
         const double desc_ms = ms_since(t0) - fetch_ms;
         SplitGraph sg;
         bool split = false;
         if (rc == XKB_OK) rc = split_moldable(descs, nt, g, sg, split);
         const xkb_task_graph_t & run_g = split ? sg.g : g;
-        if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size())
-                                     : xkb_internal_sched_set_tasks_device(R->sched, descs, nt);
+        if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size(), true)
+                                     : xkb_internal_sched_set_tasks_device(R->sched, descs, nt, true);
         // warps per task: FP32-storage tiles (128 rows per strip) run best one warp per task,
         // everything else two (measured on the 16384^2 graphs)
         bool all_f32 = true;
@@ -1438,14 +1460,24 @@ static int wait_batch(xkb_runtime * R)
     if (rc == XKB_OK)
     {
         t0 = std::chrono::steady_clock::now();
-        // the blocks device tasks wrote, as reads (records rewritten in place: unused after this)
-        const std::vector<uint32_t> first = distinct_records(recs, nacc, [&](size_t k) {
-            if (recs[k].type == REC_NONE || recs[k].type == XKB_ACCESS_TYPE_HANDLE || !(recs[k].mode & XKB_ACCESS_MODE_W) ||
-                !is_device(R, R->pending[recs[k].task]) || in_unified(R, recs[k]))
-                return false;
-            recs[k].mode = XKB_ACCESS_MODE_R;
-            return true;
-        });
+        // the blocks device tasks wrote, as reads (records rewritten in place: unused after this).
+        // A fused batch already has the first occurrence of every distinct record, all of device
+        // tasks: its writing ones are the blocks to read back (a W and an RW record on the same
+        // bytes both come back as R; the second fetch finds the host coherent and copies nothing).
+        std::vector<uint32_t> first;
+        if (fused)
+        {
+            for (uint32_t k : fused_first)
+                if (recs[k].mode & XKB_ACCESS_MODE_W) { recs[k].mode = XKB_ACCESS_MODE_R; first.push_back(k); }
+        }
+        else
+            first = distinct_records(recs, nacc, [&](size_t k) {
+                if (recs[k].type == REC_NONE || recs[k].type == XKB_ACCESS_TYPE_HANDLE || !(recs[k].mode & XKB_ACCESS_MODE_W) ||
+                    !is_device(R, R->pending[recs[k].task]) || in_unified(R, recs[k]))
+                    return false;
+                recs[k].mode = XKB_ACCESS_MODE_R;
+                return true;
+            });
         for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j) rc = xkb_planner_fetch(R->planner, &recs[first[j]], 0, 0, nullptr);
         const double fetch_ms = ms_since(t0);
         if (rc == XKB_OK) rc = run_copies(R, R->stream);
