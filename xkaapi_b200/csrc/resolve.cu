@@ -29,6 +29,7 @@
 // scans and scatters the pairs into a successor CSR. Cell state stays in HBM between batches.
 #include "common.cuh"
 #include "scan.cuh"
+#include "workpool.h"
 
 #include <algorithm>
 #include <chrono>
@@ -488,7 +489,32 @@ struct Domain {
     DevBuf<int> state[2];
     int cur = 0;
     size_t ncells = 0;
-    std::vector<HOp> ops;               // ops of the batch being resolved
+    std::vector<HOp> ops;               // ops of the batch being resolved (sequential build)
+    size_t nops = 0;                    // ops of the batch (in `ops`, or in the staging buffer)
+    size_t stage_off = 0;               // where they start in the staging buffer
+};
+
+// Page-locked host memory the parallel build writes the batch's ops into, reused batch after
+// batch, so their upload runs at DMA speed.
+struct HostStage {
+    HOp * p = nullptr;
+    size_t cap = 0;
+    HostStage() = default;
+    HostStage(const HostStage &) = delete;
+    HostStage & operator=(const HostStage &) = delete;
+    ~HostStage() { if (p) cudaFreeHost(p); }
+    int reserve(size_t n)
+    {
+        if (n <= cap) return XKB_OK;
+        size_t c = cap ? cap : size_t(1) << 20;
+        while (c < n) c *= 2;
+        HOp * q = nullptr;
+        cudaError_t e = cudaHostAlloc((void **) &q, c * sizeof(HOp), cudaHostAllocDefault);
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        if (p) cudaFreeHost(p);
+        p = q; cap = c;
+        return XKB_OK;
+    }
 };
 
 } // namespace xkb
@@ -528,6 +554,10 @@ struct xkb_resolver {
     bool graph_valid = false;
     double last_device_ms = 0;
     double last_ops_ms = 0, last_compress_ms = 0;   // host phases of the last batch
+    // parallel host passes (validation, op build): the host team and the page-locked staging buffer
+    std::unique_ptr<WorkPool> pool;
+    HostStage stage;
+    bool staged = false;                        // this batch's ops are in `stage`
 };
 
 namespace xkb {
@@ -584,106 +614,137 @@ static void push_ops(Domain & d, bool link, const xkb_access_rec_t & r)
     }
 }
 
-static int validate(const xkb_access_rec_t * recs, size_t n, uint32_t first_task)
+// First record of [b, e) that is malformed or breaks the dense task numbering (its task must be
+// the previous record's or the next one, starting at first_task), with the reason; e if none.
+static size_t first_invalid(const xkb_access_rec_t * recs, size_t b, size_t e, uint32_t first_task, const char ** why)
 {
-    uint32_t prev = first_task;
-    for (size_t i = 0; i < n; ++i)
+    for (size_t i = b; i < e; ++i)
     {
         const xkb_access_rec_t & r = recs[i];
-        if (r.task < prev || r.task > prev + 1 || (i == 0 && r.task != first_task))
-            return xkb_set_error(XKB_EINVAL, "resolver: access %zu: task ids must be dense, in spawn order, continuing at %u", i, first_task);
-        prev = r.task;
-        if (r.mode == 0 || (r.mode & ~15u)) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: bad mode %u", i, r.mode);
+        const uint32_t prev = i == 0 ? first_task : recs[i - 1].task;
+        if (r.task < prev || r.task > prev + 1 || (i == 0 && r.task != first_task)) { *why = "task ids must be dense, in spawn order"; return i; }
+        if (r.mode == 0 || (r.mode & ~15u)) { *why = "bad mode"; return i; }
         if (r.type == XKB_ACCESS_TYPE_SEGMENT) {
-            if (r.ld <= r.addr) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: empty segment", i);
+            if (r.ld <= r.addr) { *why = "empty segment"; return i; }
         } else if (r.type == XKB_ACCESS_TYPE_BLAS_MATRIX) {
-            if (!r.ld || !r.sizeof_type || !r.m || !r.n || r.m > r.ld)
-                return xkb_set_error(XKB_EINVAL, "resolver: access %zu: bad matrix tile", i);
+            if (!r.ld || !r.sizeof_type || !r.m || !r.n || r.m > r.ld) { *why = "bad matrix tile"; return i; }
         } else if (r.type == XKB_ACCESS_TYPE_HANDLE) {
-            if (r.addr == ~0ull) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: handle ~0 is reserved", i);
-        } else return xkb_set_error(XKB_EINVAL, "resolver: access %zu: unsupported access type %u", i, r.type);
+            if (r.addr == ~0ull) { *why = "handle ~0 is reserved"; return i; }
+        } else { *why = "unsupported access type"; return i; }
     }
+    return e;
+}
+
+// Validate a batch (on the host team when it is large).
+static int validate(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n, uint32_t first_task)
+{
+    const char * why = "";
+    size_t bad = n;
+    if (n >= 65536 && R->pool && R->pool->size() > 1)
+    {
+        const unsigned nc = R->pool->size();
+        std::vector<size_t> at(nc, n);
+        std::vector<const char *> w(nc, "");
+        R->pool->run([&](unsigned c) {
+            const size_t e = n * (c + 1) / nc;
+            const size_t x = first_invalid(recs, n * c / nc, e, first_task, &w[c]);
+            at[c] = x == e ? n : x;
+        });
+        for (unsigned c = 0; c < nc; ++c) if (at[c] < bad) { bad = at[c]; why = w[c]; }
+    }
+    else bad = first_invalid(recs, 0, n, first_task, &why);
+    if (bad < n) return xkb_set_error(XKB_EINVAL, "resolver: access %zu: %s (tasks continue at %u)", bad, why, first_task);
     return XKB_OK;
+}
+
+// Rects of a matrix record in its frame (mat_rects' count only).
+static inline int mat_nrects(const xkb_access_rec_t & r)
+{
+    const uint64_t LDs = r.ld * r.sizeof_type, A = r.addr + (r.offset_n * r.ld + r.offset_m) * r.sizeof_type;
+    return (A % LDs) + r.m * r.sizeof_type <= LDs ? 1 : 2;
 }
 
 // Matrix-only batches whose every (ld, sizeof) already has a domain: each record's ops go to its
 // own domain only (LINK ops of a task's records, then their PUT ops), so chunks of whole tasks
-// can be built on several host threads and appended in chunk order. Returns false (nothing
-// built) when the batch needs the sequential path: a segment, or a matrix key seen for the first
-// time (a new domain replays earlier segments at that point of the stream).
-static bool build_ops_parallel(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
+// are built by the host team: a counting pass, then every chunk writes its ops straight into the
+// page-locked staging buffer, domain after domain and chunks in order within a domain -- the
+// order of the sequential build. Counters and cursors live on each member's own stack while it
+// runs (members sharing cache lines would serialise on them). Returns 1 (built), 0 (the batch
+// needs the sequential path: a segment or handle, a matrix key seen for the first time -- a new
+// domain replays earlier segments at that point of the stream -- or a small batch), or an error.
+static int build_ops_staged(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nthreads = std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 32768));
-    if (nthreads < 2) return false;
-    std::vector<uint32_t> dom(n);
-    {
-        uint64_t lk = ~0ull, ls = ~0ull;
-        uint32_t li = 0;
-        for (size_t i = 0; i < n; ++i)
-        {
-            const xkb_access_rec_t & r = recs[i];
-            if (r.type != XKB_ACCESS_TYPE_BLAS_MATRIX) return false;
-            if (r.ld != lk || r.sizeof_type != ls)
-            {
-                auto it = R->blas_index.find(std::make_pair(r.ld, r.sizeof_type));
-                if (it == R->blas_index.end()) return false;
-                lk = r.ld; ls = r.sizeof_type; li = (uint32_t) it->second;
-            }
-            dom[i] = li;
-        }
-    }
+    if (n < 65536 || R->blas.empty() || !R->pool) return 0;
+    const unsigned nc = R->pool->size();
+    if (nc < 2) return 0;
     const size_t nd = R->blas.size();
-    std::vector<size_t> cut(nthreads + 1, n);
+    std::vector<uint64_t> keys(2 * nd);
+    for (size_t k = 0; k < nd; ++k) { keys[2 * k] = R->blas[k]->ld; keys[2 * k + 1] = R->blas[k]->s; }
+    auto dom_of = [&](const xkb_access_rec_t & r, uint64_t & lk, uint64_t & ls, size_t & li) {
+        if (r.ld == lk && r.sizeof_type == ls) return true;
+        for (size_t k = 0; k < nd; ++k)
+            if (keys[2 * k] == r.ld && keys[2 * k + 1] == r.sizeof_type) { lk = r.ld; ls = r.sizeof_type; li = k; return true; }
+        return false;
+    };
+    std::vector<size_t> cut(nc + 1, n);
     cut[0] = 0;
-    for (size_t t = 1; t < nthreads; ++t)
+    for (unsigned t = 1; t < nc; ++t)
     {
-        size_t c = std::max(cut[t - 1], n * t / nthreads);
+        size_t c = std::max(cut[t - 1], n * t / nc);
         while (c > cut[t - 1] && c < n && recs[c].task == recs[c - 1].task) ++c;     // whole tasks per chunk
         cut[t] = c;
     }
-    std::vector<std::vector<Domain>> local(nthreads);
-    auto work = [&](size_t t) {
-        std::vector<Domain> & L = local[t];
-        L.resize(nd);
-        for (size_t k = 0; k < nd; ++k) { L[k].ld = R->blas[k]->ld; L[k].s = R->blas[k]->s; }
-        for (size_t i = cut[t]; i < cut[t + 1];)
+    std::vector<size_t> cnt(nc * nd, 0);
+    std::vector<char> ok(nc, 1);
+    R->pool->run([&](unsigned c) {
+        uint64_t lk = ~0ull, ls = ~0ull;
+        size_t li = 0;
+        std::vector<size_t> my(nd, 0);
+        for (size_t i = cut[c]; i < cut[c + 1]; ++i)
         {
-            size_t j = i;
-            while (j < cut[t + 1] && recs[j].task == recs[i].task) ++j;
-            for (size_t a = i; a < j; ++a) push_ops(L[dom[a]], true, recs[a]);
-            for (size_t a = i; a < j; ++a) push_ops(L[dom[a]], false, recs[a]);
-            i = j;
+            const xkb_access_rec_t & r = recs[i];
+            if (r.type != XKB_ACCESS_TYPE_BLAS_MATRIX || !dom_of(r, lk, ls, li)) { ok[c] = 0; return; }
+            my[li] += 2 * (size_t) mat_nrects(r);
         }
-    };
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto & th : pool) th.join();
-    pool.clear();
-    // append in chunk order: offsets per (domain, chunk), then parallel copies
-    std::vector<size_t> off(nd * nthreads);
+        std::copy(my.begin(), my.end(), cnt.begin() + c * nd);
+    });
+    for (char o : ok) if (!o) return 0;
+    std::vector<size_t> pos(nc * nd);
+    size_t total = 0;
     for (size_t k = 0; k < nd; ++k)
     {
-        size_t o = R->blas[k]->ops.size();
-        for (size_t t = 0; t < nthreads; ++t) { off[k * nthreads + t] = o; o += local[t][k].ops.size(); }
-        R->blas[k]->ops.resize(o);
+        R->blas[k]->stage_off = total;
+        for (unsigned c = 0; c < nc; ++c) { pos[c * nd + k] = total; total += cnt[c * nd + k]; }
+        R->blas[k]->nops = total - R->blas[k]->stage_off;
     }
-    auto copy = [&](size_t t) {
-        for (size_t k = 0; k < nd; ++k)
-            if (!local[t][k].ops.empty())
-                memcpy(R->blas[k]->ops.data() + off[k * nthreads + t], local[t][k].ops.data(), local[t][k].ops.size() * sizeof(HOp));
-    };
-    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(copy, t);
-    copy(0);
-    for (auto & th : pool) th.join();
-    return true;
+    if (int rc = R->stage.reserve(total ? total : 1)) return rc;
+    HOp * out = R->stage.p;
+    R->pool->run([&](unsigned c) {
+        uint64_t lk = ~0ull, ls = ~0ull;
+        size_t li = 0;
+        std::vector<size_t> p(pos.begin() + c * nd, pos.begin() + (c + 1) * nd);
+        for (size_t i = cut[c]; i < cut[c + 1];)
+        {
+            size_t j = i;
+            while (j < cut[c + 1] && recs[j].task == recs[i].task) ++j;
+            for (int pass = 0; pass < 2; ++pass)                 // LINK ops, then PUT ops
+                for (size_t a = i; a < j; ++a)
+                {
+                    dom_of(recs[a], lk, ls, li);
+                    HRect rr[2];
+                    const int nr = mat_rects(recs[a], rr);
+                    for (int q = 0; q < nr; ++q) out[p[li]++] = HOp{recs[a].task, (uint8_t) (pass == 0), recs[a].mode, rr[q]};
+                }
+            i = j;
+        }
+    });
+    R->staged = true;
+    return 1;
 }
 
 // Build every domain's op list for the batch, in the order the reference performs them.
 static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 {
-    if (build_ops_parallel(R, recs, n)) return;
     for (size_t i = 0; i < n;)
     {
         size_t j = i;
@@ -947,22 +1008,35 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
     int rc;
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
-    build_ops(R, recs, n);
+    R->staged = false;
+    rc = build_ops_staged(R, recs, n);
+    if (rc < 0) return rc;
+    if (!R->staged)
+    {
+        build_ops(R, recs, n);
+        R->interval.nops = R->interval.ops.size(); R->handles.nops = R->handles.ops.size();
+        for (auto & d : R->blas) d->nops = d->ops.size();
+    }
     const auto t1 = clk::now();
     std::vector<Domain *> doms;
-    if (!R->interval.ops.empty()) doms.push_back(&R->interval);
-    if (!R->handles.ops.empty()) doms.push_back(&R->handles);
-    for (auto & d : R->blas) if (!d->ops.empty()) doms.push_back(d.get());
+    if (R->interval.nops) doms.push_back(&R->interval);
+    if (R->handles.nops) doms.push_back(&R->handles);
+    for (auto & d : R->blas) if (d->nops) doms.push_back(d.get());
 
     std::vector<size_t> offs;
     size_t total = 0;
-    for (Domain * d : doms) { offs.push_back(total); total += d->ops.size(); }
+    for (Domain * d : doms) { offs.push_back(total); total += d->nops; }
     if ((rc = R->hops.reserve(total ? total : 1)) || (rc = R->dops.reserve(total ? total : 1))) return rc;
+    if (R->staged)          // domain-major in the staging buffer, in the order of `doms`
+    {
+        if (total) XKB_CUDA_TRY(cudaMemcpyAsync(R->hops.p, R->stage.p, total * sizeof(HOp), cudaMemcpyHostToDevice, R->stream));
+    }
+    else
+        for (size_t k = 0; k < doms.size(); ++k)
+            XKB_CUDA_TRY(cudaMemcpyAsync(R->hops.p + offs[k], doms[k]->ops.data(), doms[k]->nops * sizeof(HOp),
+                                         cudaMemcpyHostToDevice, R->stream));
     for (size_t k = 0; k < doms.size(); ++k)
-        XKB_CUDA_TRY(cudaMemcpyAsync(R->hops.p + offs[k], doms[k]->ops.data(), doms[k]->ops.size() * sizeof(HOp),
-                                     cudaMemcpyHostToDevice, R->stream));
-    for (size_t k = 0; k < doms.size(); ++k)
-        if ((rc = compress_domain(R, *doms[k], R->hops.p + offs[k], R->dops.p + offs[k], doms[k]->ops.size()))) return rc;
+        if ((rc = compress_domain(R, *doms[k], R->hops.p + offs[k], R->dops.p + offs[k], doms[k]->nops))) return rc;
     R->last_ops_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     R->last_compress_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
 
@@ -978,7 +1052,7 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
         XKB_CUDA_TRY(cudaMemsetAsync(R->counters.p, 0, 2 * sizeof(unsigned long long), R->stream));
         for (size_t k = 0; k < doms.size(); ++k)
         {
-            const size_t nops = doms[k]->ops.size();
+            const size_t nops = doms[k]->nops;
             // states must exist for every cell (ncells > 0 when the domain has >= 1 op)
             if ((rc = R->emit.reserve(emit_guess))) return rc;
             if (doms[k]->ncells == 0) continue;
@@ -1010,7 +1084,9 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
             {
                 std::unique_ptr<DevBuf<unsigned long long>> seg(new (std::nothrow) DevBuf<unsigned long long>());
                 if (!seg) return xkb_set_error(XKB_ENOMEM, "resolver: out of host memory");
-                if ((rc = seg->reserve(std::max<size_t>((size_t) nemit, size_t(1) << 24)))) return rc;
+                // segments double in size, so a long stream allocates a few of them, not one per batch
+                const size_t last = R->useg.empty() ? 0 : R->useg.back()->cap;
+                if ((rc = seg->reserve(std::max<size_t>({(size_t) nemit, size_t(1) << 24, 2 * last})))) return rc;
                 R->useg.push_back(std::move(seg));
                 R->useg_n.push_back(0);
             }
@@ -1027,10 +1103,11 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
             R->nuniq += nu - nu0;
             R->useg_n.back() = nu;
         }
-        for (Domain * d : doms) { d->cur ^= 1; d->ops.clear(); }
+        for (Domain * d : doms) { d->cur ^= 1; d->ops.clear(); d->nops = 0; }
         if (trace)
-            fprintf(stderr, "resolver batch: %zu ops, attempt %d, regions %.1f ms, dedupe %.1f ms, %llu emitted, %.1f MB allocated\n",
-                    total, attempt, std::chrono::duration<double, std::milli>(tb - ta).count(),
+            fprintf(stderr, "resolver batch: %zu ops (built in %.1f ms, compressed in %.1f ms), attempt %d, regions %.1f ms, dedupe %.1f ms, "
+                    "%llu emitted, %.1f MB allocated\n",
+                    total, R->last_ops_ms, R->last_compress_ms, attempt, std::chrono::duration<double, std::milli>(tb - ta).count(),
                     std::chrono::duration<double, std::milli>(clk::now() - tb).count(), nemit, (g_realloc_bytes - realloc0) / 1e6);
         return XKB_OK;
     }
@@ -1094,8 +1171,8 @@ int xkb_internal_resolver_reset(xkb_resolver_t * R)
 {
     if (!R) return xkb_set_error(XKB_EINVAL, "resolver_reset: null resolver");
     XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
-    R->interval.xs.clear(); R->interval.ys.clear(); R->interval.ncells = 0; R->interval.ops.clear();
-    R->handles.xs.clear(); R->handles.ys.clear(); R->handles.ncells = 0; R->handles.ops.clear();
+    R->interval.xs.clear(); R->interval.ys.clear(); R->interval.ncells = 0; R->interval.ops.clear(); R->interval.nops = 0;
+    R->handles.xs.clear(); R->handles.ys.clear(); R->handles.ncells = 0; R->handles.ops.clear(); R->handles.nops = 0;
     R->blas.clear(); R->blas_index.clear(); R->segments.clear();
     R->ntasks = 0; R->nuniq = 0; R->graph_valid = false;
     if (R->useg.size() > 1) { R->useg.resize(1); R->useg_n.resize(1); }   // keep the first edge segment
@@ -1108,7 +1185,12 @@ extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * rec
 {
     if (!R || (n && !recs)) return xkb_set_error(XKB_EINVAL, "resolver_add: bad arguments");
     if (n == 0) return XKB_OK;
-    int rc = validate(recs, n, R->ntasks);
+    if (!R->pool)
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        R->pool.reset(new (std::nothrow) WorkPool(std::min(16u, std::max(1u, hw))));
+    }
+    int rc = validate(R, recs, n, R->ntasks);
     if (rc) return rc;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
