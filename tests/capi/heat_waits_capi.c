@@ -1,7 +1,8 @@
 /* The heat example through the XKRT C API with an xkrt_task_wait every WAIT_EVERY steps in the
  * same runtime: each batch depends on the previous one only through the grids (resolved anew,
  * the runtime's resolver reused, host memory coherent between batches), and the program
- * re-initialises no data between waits.
+ * re-initialises no data between waits. WAIT_EVERY < 0: a wait after steps 1, 2, 4, 8, ... (and
+ * the last), so every batch is larger than the one before.
  * usage: heat_waits_capi NX NY TS STEPS WAIT_EVERY init.bin out.bin */
 #include <stdio.h>
 #include <stdlib.h>
@@ -59,7 +60,8 @@ int main(int argc, char ** argv)
                 xkrt_task_spawn_with_format_with_accesses(rt, 1, heat, &d, sizeof(d), acc, 2);
             }
         double * t = src; src = dst; dst = t;
-        if ((s + 1) % every == 0 || s + 1 == steps) { xkrt_task_wait(rt); ++waits; }
+        const int at = every > 0 ? (s + 1) % every == 0 : ((s + 1) & s) == 0;
+        if (at || s + 1 == steps) { xkrt_task_wait(rt); ++waits; }
     }
     f = fopen(argv[7], "wb");
     fwrite(src, sizeof(double), NX * NY, f);

@@ -121,9 +121,11 @@ struct xkb_runtime {
     // the planner (coherency decisions and their copies) is used by one task at a time
     std::vector<cudaStream_t> wstreams;
     std::mutex plan_mu;
-    // page-locked prefix of the args pool (the descriptor upload of fused batches reads it)
+    // page-locked prefix of the args pool (the descriptor upload of fused batches reads it; one
+    // registration per growth, and an upload never spans two of them)
     size_t args_pinned = 0;
     std::vector<std::pair<void *, size_t>> pinned_ranges;
+    bool args_dense = true;                           // every task's args: one descriptor, back to back
     std::atomic<struct Dataflow *> df{nullptr};       // the batch being executed (detached completion)
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
@@ -293,6 +295,7 @@ extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
     if (!R) return;
     bg_finish(R);
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
+    R->args_dense = true;
 }
 
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, bool unified = false)
@@ -545,6 +548,7 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
     }
     if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
     const size_t nt = R->pending.size();
+    if (args_size != sizeof(xkb_task_desc_t) || t.args_off != (nt - 1) * sizeof(xkb_task_desc_t)) R->args_dense = false;
     if ((nt & 4095) == 0 && R->prefaulter[0].joinable()) R->pf_want.store(nt + PREFAULT_AHEAD, std::memory_order_relaxed);
     if (R->bg) bg_hand_over(R, false);
 }
@@ -1321,17 +1325,24 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
 
 // Page-lock the args pool up to `bytes` (rounded up to 2 MB, within the reservation) so that the
 // descriptor upload of a fused batch runs at DMA speed instead of through the driver's pageable
-// staging; the locked prefix only grows and is released with the runtime. If locking fails the
-// pool stays pageable and the upload is just slower.
+// staging. The locked prefix is ONE registration (a copy must not span two), replaced when a
+// larger batch needs more, and released with the runtime. If locking fails the pool stays
+// pageable and the upload is just slower. Runs on its own thread while the wait plans coherency.
 static void pin_args(xkb_runtime * R, size_t bytes)
 {
     constexpr size_t STEP = size_t(2) << 20;
-    if (!R->args_pool.fixed()) return;
+    if (!R->args_pool.fixed() || !R->gpu) return;
     const size_t want = std::min((bytes + STEP - 1) & ~(STEP - 1), R->args_pool.capacity_bytes());
     if (want <= R->args_pinned) return;
-    uint8_t * p = R->args_pool.data() + R->args_pinned;
-    if (cudaHostRegister(p, want - R->args_pinned, cudaHostRegisterDefault) != cudaSuccess) { cudaGetLastError(); return; }
-    R->pinned_ranges.push_back({p, want - R->args_pinned});
+    cudaSetDevice(R->device);
+    if (R->args_pinned) { cudaHostUnregister(R->args_pool.data()); R->pinned_ranges.clear(); R->args_pinned = 0; }
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = cudaHostRegister(R->args_pool.data(), want, cudaHostRegisterDefault);
+    if (getenv("XKB_TRACE_WAIT"))
+        fprintf(stderr, "xkrt_task_wait: page-locking %zu MB of descriptors: %s, %.1f ms\n", want >> 20, cudaGetErrorString(e),
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    if (e != cudaSuccess) { cudaGetLastError(); return; }
+    R->pinned_ranges.push_back({R->args_pool.data(), want});
     R->args_pinned = want;
 }
 
@@ -1377,8 +1388,11 @@ static int wait_batch(xkb_runtime * R)
     if (fused)
     {
         // (2) every access made coherent on the device up front: with no host task in the batch
-        // the host data cannot change meanwhile, so the first-touch copies can all go first
+        // the host data cannot change meanwhile, so the first-touch copies can all go first.
+        // Meanwhile another thread page-locks the descriptors for their upload.
         t0 = std::chrono::steady_clock::now();
+        std::thread pinner;
+        if (R->args_dense) pinner = std::thread(pin_args, R, ntasks * sizeof(xkb_task_desc_t));
         fused_first = distinct_records(recs, nacc, [&](size_t k) {
             // handles carry no data; unified memory is used in place
             return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE && !in_unified(R, recs[k]);
@@ -1394,13 +1408,12 @@ static int wait_batch(xkb_runtime * R)
         // already the descriptor array (16-byte aligned 64-byte entries back to back) and is
         // rewritten in place (nothing reads these args after a fused batch)
         const size_t nt = R->pending.size();
-        bool dense_args = true;
-        for (size_t t = 0; t < nt && dense_args; ++t)
-            dense_args = R->pending[t].nargs == sizeof(xkb_task_desc_t) && R->pending[t].args_off == t * sizeof(xkb_task_desc_t);
+        const bool dense_args = R->args_dense;
         std::vector<xkb_task_desc_t> copy;
         xkb_task_desc_t * descs = (xkb_task_desc_t *) R->args_pool.data();
         if (!dense_args) { copy.resize(nt); descs = copy.data(); }
         std::atomic<size_t> bad_args(SIZE_MAX), bad_ptr(SIZE_MAX);     // first failing task, if any
+        std::atomic<bool> long_axpby(false);                           // some task splits (moldable)
         if (rc == XKB_OK)
             parallel_chunks(nt, [&](size_t b, size_t e) {
                 RegionHint h;
@@ -1415,6 +1428,8 @@ static int wait_batch(xkb_runtime * R)
                     descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
                     if (!translate_hint(R, descs[t], h) || !xkb_internal_task_valid(descs[t]))
                     { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
+                    if (descs[t].kind == XKB_TASK_AXPBY && descs[t].u.axpby.hi - descs[t].u.axpby.lo > AXPBY_SPLIT && !long_axpby)
+                        long_axpby.store(true, std::memory_order_relaxed);
                 }
             });
         if (rc == XKB_OK && bad_args != SIZE_MAX)
@@ -1422,11 +1437,11 @@ static int wait_batch(xkb_runtime * R)
         else if (rc == XKB_OK && bad_ptr != SIZE_MAX)
             rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region, or the "
                                            "tile or range is malformed", (size_t) bad_ptr);
-        if (rc == XKB_OK && dense_args) pin_args(R, nt * sizeof(xkb_task_desc_t));
+        if (pinner.joinable()) pinner.join();
         const double desc_ms = ms_since(t0) - fetch_ms;
         SplitGraph sg;
         bool split = false;
-        if (rc == XKB_OK) rc = split_moldable(descs, nt, g, sg, split);
+        if (rc == XKB_OK && long_axpby) rc = split_moldable(descs, nt, g, sg, split);
         const xkb_task_graph_t & run_g = split ? sg.g : g;
         if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size(), true)
                                      : xkb_internal_sched_set_tasks_device(R->sched, descs, nt, true);
@@ -1519,4 +1534,5 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     bg_finish(R);
     R->in_wait = false;
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
+    R->args_dense = true;
 }
