@@ -137,91 +137,90 @@ inline int64_t view_off(const View & v, uint64_t x, uint64_t y, uint64_t s)
 }
 
 // The same canonical partition for the resident mode, whose blocks carry only the device bits:
-// sorted arrays instead of trees (a fetch is a few binary searches over cache-resident arrays;
-// the partition only grows while the first accesses of each shape arrive).
-struct RSlab {
-    uint64_t x1;
-    std::vector<uint64_t> ys, ends;     // block starts (ascending) and ends
-    std::vector<uint8_t> st;            // DEV_HOST | DEV_GPU per block
-};
-struct RFrame {
-    std::vector<uint64_t> xs;           // slab starts, ascending
-    std::vector<RSlab> slabs;
-};
+// an ordered map of slabs (a stream of segments can cut thousands of them), each slab's blocks
+// in one sorted array (a fetch is a few binary searches over cache-resident arrays; a slab's cuts
+// only grow while the first accesses of each shape arrive).
+struct RBlock { uint64_t y0, y1; uint8_t st; };     // st: DEV_HOST | DEV_GPU
+struct RSlab { uint64_t x1; std::vector<RBlock> b; };
+struct RFrame { std::map<uint64_t, RSlab> slabs; };
 struct RPartite { uint64_t x0, x1, y0, y1; uint8_t * st; };
+
+inline size_t first_at_or_after(const std::vector<RBlock> & b, uint64_t y)
+{
+    return (size_t) (std::lower_bound(b.begin(), b.end(), y, [](const RBlock & q, uint64_t v) { return q.y0 < v; }) - b.begin());
+}
 
 void rsplit_y(RSlab & sl, uint64_t y)
 {
-    size_t i = (size_t) (std::upper_bound(sl.ys.begin(), sl.ys.end(), y) - sl.ys.begin());
+    size_t i = (size_t) (std::upper_bound(sl.b.begin(), sl.b.end(), y, [](uint64_t v, const RBlock & q) { return v < q.y0; }) - sl.b.begin());
     if (i == 0) return;
     --i;
-    if (sl.ys[i] < y && y < sl.ends[i])
+    if (sl.b[i].y0 < y && y < sl.b[i].y1)
     {
-        sl.ys.insert(sl.ys.begin() + i + 1, y);
-        sl.ends.insert(sl.ends.begin() + i + 1, sl.ends[i]);
-        sl.st.insert(sl.st.begin() + i + 1, sl.st[i]);
-        sl.ends[i] = y;
+        RBlock right = sl.b[i];
+        right.y0 = y;
+        sl.b[i].y1 = y;
+        sl.b.insert(sl.b.begin() + i + 1, right);
     }
 }
 
-void rsplit_x(RFrame & f, uint64_t x)
+// Cut the slab at `it` (which starts before x and ends after it) at x; returns the right part.
+std::map<uint64_t, RSlab>::iterator rcut_x(RFrame & f, std::map<uint64_t, RSlab>::iterator it, uint64_t x)
 {
-    size_t i = (size_t) (std::upper_bound(f.xs.begin(), f.xs.end(), x) - f.xs.begin());
-    if (i == 0) return;
-    --i;
-    if (f.xs[i] < x && x < f.slabs[i].x1)
-    {
-        RSlab right = f.slabs[i];
-        f.slabs[i].x1 = x;
-        f.xs.insert(f.xs.begin() + i + 1, x);
-        f.slabs.insert(f.slabs.begin() + i + 1, std::move(right));
-    }
+    RSlab right = it->second;
+    it->second.x1 = x;
+    return f.slabs.emplace_hint(std::next(it), x, std::move(right));
 }
 
-void rinsert(RFrame & f, const Rect & r)
+// Cut the slab's blocks at y0 and y1, fill its y-gaps in [y0, y1), append its blocks there.
+void rslab_fill(uint64_t x0, RSlab & sl, const Rect & r, std::vector<RPartite> & out)
 {
-    rsplit_x(f, r.x0);
-    rsplit_x(f, r.x1);
+    rsplit_y(sl, r.y0);
+    rsplit_y(sl, r.y1);
+    uint64_t y = r.y0;
+    const size_t j0 = first_at_or_after(sl.b, r.y0);
+    size_t j = j0;
+    while (y < r.y1)                                   // blocks over the y-gaps of [y0, y1)
+    {
+        if (j < sl.b.size() && sl.b[j].y0 == y) { y = sl.b[j].y1; ++j; continue; }
+        const uint64_t end = (j < sl.b.size() && sl.b[j].y0 < r.y1) ? sl.b[j].y0 : r.y1;
+        sl.b.insert(sl.b.begin() + j, RBlock{y, end, 0});
+        ++j;
+        y = end;
+    }
+    for (size_t k = j0; k < j; ++k) out.push_back({x0, sl.x1, sl.b[k].y0, sl.b[k].y1, &sl.b[k].st});
+}
+
+// Insert the rect and append its blocks (x-slab by x-slab, blocks by y) to out, in one walk over
+// the slabs from x0: cut the slab straddling x0, then per step either a slab starting where the
+// walk is (cut at x1 if it reaches past it) or a new slab over the gap up to the next one. The
+// blocks of an earlier rect of the same access stay valid: a wrapped tile's second rect ends
+// left of where its first one starts, so it only cuts slabs the first one does not cover.
+void rinsert(RFrame & f, const Rect & r, std::vector<RPartite> & out)
+{
+    auto it = f.slabs.upper_bound(r.x0);
+    if (it != f.slabs.begin())
+    {
+        auto prev = std::prev(it);
+        if (prev->first == r.x0) it = prev;
+        else if (r.x0 < prev->second.x1) it = rcut_x(f, prev, r.x0);
+    }
     uint64_t x = r.x0;
-    size_t i = (size_t) (std::lower_bound(f.xs.begin(), f.xs.end(), r.x0) - f.xs.begin());
-    const size_t first = i;
-    while (x < r.x1)                                   // slabs over the x-gaps of [x0, x1)
+    while (x < r.x1)
     {
-        if (i < f.xs.size() && f.xs[i] == x) { x = f.slabs[i].x1; ++i; continue; }
-        const uint64_t end = (i < f.xs.size() && f.xs[i] < r.x1) ? f.xs[i] : r.x1;
-        f.xs.insert(f.xs.begin() + i, x);
-        RSlab sl; sl.x1 = end;
-        f.slabs.insert(f.slabs.begin() + i, std::move(sl));
-        ++i;
-        x = end;
-    }
-    for (i = first; i < f.xs.size() && f.xs[i] < r.x1; ++i)
-    {
-        RSlab & sl = f.slabs[i];
-        rsplit_y(sl, r.y0);
-        rsplit_y(sl, r.y1);
-        uint64_t y = r.y0;
-        size_t j = (size_t) (std::lower_bound(sl.ys.begin(), sl.ys.end(), r.y0) - sl.ys.begin());
-        while (y < r.y1)                               // blocks over the y-gaps of [y0, y1)
+        if (it != f.slabs.end() && it->first == x)
         {
-            if (j < sl.ys.size() && sl.ys[j] == y) { y = sl.ends[j]; ++j; continue; }
-            const uint64_t end = (j < sl.ys.size() && sl.ys[j] < r.y1) ? sl.ys[j] : r.y1;
-            sl.ys.insert(sl.ys.begin() + j, y);
-            sl.ends.insert(sl.ends.begin() + j, end);
-            sl.st.insert(sl.st.begin() + j, (uint8_t) 0);
-            ++j;
-            y = end;
+            if (it->second.x1 > r.x1) rcut_x(f, it, r.x1);
         }
-    }
-}
-
-void rpartites(RFrame & f, const Rect & r, std::vector<RPartite> & out)
-{
-    for (size_t i = (size_t) (std::lower_bound(f.xs.begin(), f.xs.end(), r.x0) - f.xs.begin()); i < f.xs.size() && f.xs[i] < r.x1; ++i)
-    {
-        RSlab & sl = f.slabs[i];
-        for (size_t j = (size_t) (std::lower_bound(sl.ys.begin(), sl.ys.end(), r.y0) - sl.ys.begin()); j < sl.ys.size() && sl.ys[j] < r.y1; ++j)
-            out.push_back({f.xs[i], sl.x1, sl.ys[j], sl.ends[j], &sl.st[j]});
+        else
+        {
+            const uint64_t end = (it != f.slabs.end() && it->first < r.x1) ? it->first : r.x1;
+            RSlab sl; sl.x1 = end;
+            it = f.slabs.emplace_hint(it, x, std::move(sl));
+        }
+        rslab_fill(it->first, it->second, r, out);
+        x = it->second.x1;
+        ++it;
     }
 }
 
@@ -305,9 +304,8 @@ static int resident_fetch(xkb_planner * P, const xkb_access_rec_t & a, int64_t a
     if (view) { view->alloc = region; view->off = (int64_t) (begin - rbase); view->ld = seg ? (int64_t) (a.ld - a.addr) : (int64_t) a.ld; }
     std::unique_ptr<RFrame> & fp = P->rframes[{ld, s}];
     if (!fp) { fp.reset(new (std::nothrow) RFrame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); }
-    for (int k = 0; k < nr; ++k) rinsert(*fp, rr[k]);
     P->rscratch.clear();
-    for (int k = 0; k < nr; ++k) rpartites(*fp, rr[k], P->rscratch);
+    for (int k = 0; k < nr; ++k) rinsert(*fp, rr[k], P->rscratch);
     const uint8_t me = device == 0 ? DEV_HOST : DEV_GPU;
     for (const RPartite & p : P->rscratch)
     {
