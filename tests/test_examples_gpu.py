@@ -91,11 +91,12 @@ def test_axpby_xkrt_long_chunks_split(torch_cuda, tmp_path):
     assert lines[0]["h2d_bytes"] >= 2 * 8 * n and lines[0]["d2h_bytes"] >= 8 * n
 
 
-@pytest.mark.parametrize("chunk", [64, 1024])
-def test_background_resolution_small_chunks(torch_cuda, tmp_path, chunk):
+@pytest.mark.parametrize("chunk,stream", [(64, 1), (1024, 1), (1024, 0)])
+def test_background_resolution_small_chunks(torch_cuda, tmp_path, chunk, stream):
     """With a small resolver batch the runtime's worker thread resolves chunks of spawned tasks
-    while spawning goes on; the heat and axpby results stay the oracle's, bit for bit."""
-    env = dict(os.environ, XKB_RESOLVE_CHUNK=str(chunk))
+    while spawning goes on, and (stream=1) runs each resolved window on the GPU before the wait;
+    the heat and axpby results stay the oracle's, bit for bit."""
+    env = dict(os.environ, XKB_RESOLVE_CHUNK=str(chunk), XKB_STREAM=str(stream))
     nx, ny, ts, steps = 300, 170, 32, 9
     g = O.heat_init(nx, ny, seed=17)
     g.tofile(tmp_path / "init.bin")

@@ -29,3 +29,30 @@ static inline bool xkb_internal_task_valid(const xkb_task_desc_t & d)
 
 // Reset a resolver to no tasks, keeping its device buffers for the next graph.
 int xkb_internal_resolver_reset(xkb_resolver_t * R);
+
+// A point of a resolver's edge store: the tasks added so far and where the next unique edge goes.
+typedef struct xkb_edge_mark_t { size_t seg, off; uint32_t ntasks; } xkb_edge_mark_t;
+int xkb_internal_resolver_edge_mark(xkb_resolver_t * R, xkb_edge_mark_t * m);
+// Reserve the working memory of a batch of about nops ops up front.
+int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops);
+// Reserve the device buffers of runs of up to ntasks tasks up front.
+int xkb_internal_sched_reserve(xkb_sched_t * S, size_t ntasks);
+// Unique edges stored so far (no graph build).
+size_t xkb_internal_resolver_nedges(const xkb_resolver_t * R);
+// The window of the graph from the mark's first task to the last task added: successor CSR of
+// tasks [m->ntasks, ntasks) renumbered from 0, with the edges stored since the mark whose both
+// ends lie in the window (every edge into a task is stored by the batch that added the task, so
+// the window keeps all edges among its tasks and drops those from earlier tasks). Device buffers
+// owned by the resolver, valid until the next window (in stream order) or reset.
+int xkb_internal_resolver_window_graph(xkb_resolver_t * R, const xkb_edge_mark_t * m, xkb_task_graph_t * g);
+
+// Run tasks as one persistent launch on the scheduler's stream without waiting for it: the
+// descriptors are copied in stream order (host memory may be pageable), the launch's status and
+// executed count are added to the scheduler's running totals, read and cleared by
+// xkb_internal_sched_windows_wait.
+int xkb_internal_sched_run_window(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks, const xkb_task_graph_t * g);
+// The two halves of a window run: the descriptors' copy (queued now, so that it can go ahead of
+// the window's graph), then the launch on the graph of the same ntasks tasks.
+int xkb_internal_sched_upload_window(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks);
+int xkb_internal_sched_launch_window(xkb_sched_t * S, const xkb_task_graph_t * g);
+int xkb_internal_sched_windows_wait(xkb_sched_t * S, uint64_t * executed);

@@ -28,6 +28,7 @@
 // __match_any_sync. A GPU hash set keeps the unique pairs; finalising counts predecessors,
 // scans and scatters the pairs into a successor CSR. Cell state stays in HBM between batches.
 #include "common.cuh"
+#include "internal.h"
 #include "scan.cuh"
 #include "workpool.h"
 
@@ -377,6 +378,30 @@ __global__ void scatter_edges_kernel(const unsigned long long * __restrict__ e, 
     succ[pos] = (uint32_t) k;
 }
 
+// A window of the graph: edges whose ends are both >= first, renumbered from first.
+__global__ void count_window_edges_kernel(const unsigned long long * __restrict__ e, size_t n, uint32_t first, uint32_t * nsucc,
+                                          uint32_t * npred)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = e[i];
+    const uint32_t p = (uint32_t) (k >> 32), q = (uint32_t) k;
+    if (p < first || q < first) return;
+    atomicAdd(nsucc + (p - first), 1u);
+    atomicAdd(npred + (q - first), 1u);
+}
+
+__global__ void scatter_window_edges_kernel(const unsigned long long * __restrict__ e, size_t n, uint32_t first, uint32_t * cursor,
+                                            uint32_t * succ)
+{
+    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = e[i];
+    const uint32_t p = (uint32_t) (k >> 32), q = (uint32_t) k;
+    if (p < first || q < first) return;
+    succ[atomicAdd(cursor + (p - first), 1u)] = q - first;
+}
+
 // Sort each successor list ascending (deterministic CSR). Short lists: one thread, insertion sort.
 __global__ void sort_segments_kernel(const uint32_t * __restrict__ ptr, uint32_t * succ, uint32_t ntasks)
 {
@@ -548,6 +573,7 @@ struct xkb_resolver {
     size_t nuniq = 0;
     // graph
     DevBuf<uint32_t> succ_ptr, succ, npred, tmp;
+    DevBuf<uint32_t> win_ptr, win_succ, win_npred, win_tmp;   // window graphs (a runtime running the graph in pieces)
     DevBuf<uint32_t> periodic;                  // packed arrays of the periodic form
     DevBuf<unsigned> bin_off, bin_cur;          // ops binned to regions: offsets, fill cursors
     DevBuf<int> bin_list, bin_flag;             // op indices per region; region-too-long flag
@@ -1167,6 +1193,40 @@ extern "C" int xkb_resolver_destroy(xkb_resolver_t * R)
 
 // Library-internal: forget every task and domain but keep the device work buffers, so the
 // next graph resolves without allocating them again.
+// Reserve, up front, the working memory one batch of about `nops` ops uses (the buffers grow on
+// demand otherwise): op lists, compression hash sets, emitted and unique edges, staging, the host
+// team. The cell states of each domain depend on its boundaries and still grow on demand.
+int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops)
+{
+    if (!R) return xkb_set_error(XKB_EINVAL, "resolver_prepare: null resolver");
+    if (nops == 0) return XKB_OK;
+    if (!R->pool)
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        R->pool.reset(new (std::nothrow) WorkPool(std::min(16u, std::max(1u, hw))));
+    }
+    size_t cap = 1024;
+    while (cap < 4 * nops) cap *= 2;
+    const size_t emit = std::max<size_t>(1 << 16, nops * 8);
+    size_t tcap = 1024;
+    while (tcap < 2 * emit) tcap *= 2;
+    int rc;
+    if ((rc = R->hops.reserve(nops)) || (rc = R->dops.reserve(nops)) || (rc = R->hset.reserve(2 * cap)) ||
+        (rc = R->ukeys.reserve(4 * nops)) || (rc = R->ucount.reserve(3)) || (rc = R->emit.reserve(emit)) ||
+        (rc = R->counters.reserve(2)) || (rc = R->table.reserve(tcap)) || (rc = R->stage.reserve(nops)) || (rc = spill_reserve(R, 1)))
+        return rc;
+    if (R->useg.empty())
+    {
+        std::unique_ptr<DevBuf<unsigned long long>> seg(new (std::nothrow) DevBuf<unsigned long long>());
+        if (!seg) return xkb_set_error(XKB_ENOMEM, "resolver: out of host memory");
+        if ((rc = seg->reserve(std::max<size_t>(emit, size_t(1) << 24)))) return rc;
+        R->useg.push_back(std::move(seg));
+        R->useg_n.push_back(0);
+    }
+    XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
+    return XKB_OK;
+}
+
 int xkb_internal_resolver_reset(xkb_resolver_t * R)
 {
     if (!R) return xkb_set_error(XKB_EINVAL, "resolver_reset: null resolver");
@@ -1203,6 +1263,59 @@ extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * rec
     R->last_device_ms = ms;
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     return rc;
+}
+
+size_t xkb_internal_resolver_nedges(const xkb_resolver_t * R) { return R ? R->nuniq : 0; }
+
+int xkb_internal_resolver_edge_mark(xkb_resolver_t * R, xkb_edge_mark_t * m)
+{
+    if (!R || !m) return xkb_set_error(XKB_EINVAL, "resolver_edge_mark: bad arguments");
+    m->seg = R->useg.empty() ? 0 : R->useg.size() - 1;
+    m->off = R->useg.empty() ? 0 : R->useg_n.back();
+    m->ntasks = R->ntasks;
+    return XKB_OK;
+}
+
+int xkb_internal_resolver_window_graph(xkb_resolver_t * R, const xkb_edge_mark_t * m, xkb_task_graph_t * g)
+{
+    if (!R || !m || !g || m->ntasks > R->ntasks) return xkb_set_error(XKB_EINVAL, "resolver_window_graph: bad arguments");
+    const uint32_t first = m->ntasks;
+    const size_t nt = R->ntasks - first;
+    int rc;
+    if ((rc = R->win_ptr.reserve(nt + 1)) || (rc = R->win_npred.reserve(nt + 1)) ||
+        (rc = R->win_tmp.reserve(nt + 1 + (nt + 1) / SCAN_TILE + 2)))
+        return rc;
+    cudaStream_t st = R->stream;
+    XKB_CUDA_TRY(cudaMemsetAsync(R->win_ptr.p, 0, (nt + 1) * sizeof(uint32_t), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(R->win_npred.p, 0, (nt + 1) * sizeof(uint32_t), st));
+    // the edges stored since the mark: the rest of its segment, then every later segment
+    auto each_range = [&](auto && fn) {
+        for (size_t k = m->seg; k < R->useg.size(); ++k)
+        {
+            const size_t b = k == m->seg ? m->off : 0;
+            if (R->useg_n[k] > b) fn(R->useg[k]->p + b, R->useg_n[k] - b);
+        }
+    };
+    each_range([&](const unsigned long long * e, size_t n) {
+        count_window_edges_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(e, n, first, R->win_ptr.p, R->win_npred.p);
+    });
+    if ((rc = device_exclusive_scan(R->win_ptr.p, R->win_ptr.p, nt + 1, R->win_tmp.p + nt + 1, nullptr, st))) return rc;
+    uint32_t ne = 0;
+    XKB_CUDA_TRY(cudaMemcpyAsync(&ne, R->win_ptr.p + nt, sizeof(ne), cudaMemcpyDeviceToHost, st));
+    XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = R->win_succ.reserve(ne ? ne : 1))) return rc;
+    XKB_CUDA_TRY(cudaMemcpyAsync(R->win_tmp.p, R->win_ptr.p, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    each_range([&](const unsigned long long * e, size_t n) {
+        scatter_window_edges_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(e, n, first, R->win_tmp.p, R->win_succ.p);
+    });
+    if (nt) sort_segments_kernel<<<(unsigned) ((nt + 255) / 256), 256, 0, st>>>(R->win_ptr.p, R->win_succ.p, (uint32_t) nt);
+    XKB_CUDA_TRY(cudaGetLastError());
+    g->ntasks = nt;
+    g->nedges = ne;
+    g->succ_ptr = R->win_ptr.p;
+    g->succ = R->win_succ.p;
+    g->npred = R->win_npred.p;
+    return XKB_OK;
 }
 
 extern "C" int xkb_resolver_graph(xkb_resolver_t * R, xkb_task_graph_t * g)

@@ -335,6 +335,7 @@ struct xkb_sched {
     Dev<xkb_task_desc_t> tasks;
     Dev<int> wc, queue;
     Dev<unsigned> ctr;
+    Dev<unsigned long long> wsum;             // windows run without waiting: [0] first status, [1] executed
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     const void * graph_key = nullptr;
@@ -616,6 +617,93 @@ extern "C" int xkb_sched_run_periodic(xkb_sched_t * S, const xkb_periodic_graph_
     S->last_form = XKB_FORM_PERSISTENT;
     S->last_total = total;
     return launch_persistent(S, a);
+}
+
+// Fold one launch's status and executed count into the windows' running totals.
+__global__ void window_status_kernel(const unsigned * __restrict__ ctr, unsigned long long * sum)
+{
+    if (threadIdx.x != 0) return;
+    if (sum[0] == 0 && ctr[2] != 0) sum[0] = ctr[2];
+    sum[1] += ctr[3];
+}
+
+int xkb_internal_sched_reserve(xkb_sched_t * S, size_t ntasks)
+{
+    if (!S) return xkb_set_error(XKB_EINVAL, "sched_reserve: null scheduler");
+    int rc;
+    if ((rc = S->tasks.reserve(ntasks)) || (rc = S->wc.reserve(ntasks)) || (rc = S->queue.reserve(ntasks)) || (rc = S->ctr.reserve(4)))
+        return rc;
+    if (!S->wsum.p)
+    {
+        if ((rc = S->wsum.reserve(2))) return rc;
+        XKB_CUDA_TRY(cudaMemsetAsync(S->wsum.p, 0, 2 * sizeof(unsigned long long), S->stream));
+    }
+    return XKB_OK;
+}
+
+int xkb_internal_sched_upload_window(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks)
+{
+    if (!S || (ntasks && !tasks) || ntasks >= (size_t(1) << 31)) return xkb_set_error(XKB_EINVAL, "sched_upload_window: bad arguments");
+    int rc;
+    if (ntasks > S->tasks.cap || ntasks > S->wc.cap || ntasks > S->queue.cap)
+    {
+        // earlier windows may still be reading these buffers
+        XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+        const size_t c = ntasks + ntasks / 2;
+        if ((rc = S->tasks.reserve(c)) || (rc = S->wc.reserve(c)) || (rc = S->queue.reserve(c))) return rc;
+    }
+    if (ntasks) XKB_CUDA_TRY(cudaMemcpyAsync(S->tasks.p, tasks, ntasks * sizeof(xkb_task_desc_t), cudaMemcpyHostToDevice, S->stream));
+    S->host_tasks.clear();
+    S->ntasks = ntasks;
+    S->graph_key = nullptr;
+    return XKB_OK;
+}
+
+int xkb_internal_sched_launch_window(xkb_sched_t * S, const xkb_task_graph_t * g)
+{
+    if (!S || !g || g->ntasks != S->ntasks) return xkb_set_error(XKB_EINVAL, "sched_launch_window: the graph and the uploaded window differ");
+    int rc;
+    if (!S->wsum.p)
+    {
+        if ((rc = S->wsum.reserve(2))) return rc;
+        XKB_CUDA_TRY(cudaMemsetAsync(S->wsum.p, 0, 2 * sizeof(unsigned long long), S->stream));
+    }
+    const size_t ntasks = S->ntasks;
+    if (ntasks == 0) return XKB_OK;
+    if ((rc = S->ctr.reserve(4))) return rc;
+    SchedArgs a;
+    a.tasks = S->tasks.p; a.ntasks = (uint32_t) ntasks; a.period = (uint32_t) ntasks; a.succ_ptr = g->succ_ptr; a.succ = g->succ;
+    a.xsucc_ptr = nullptr; a.xsucc = nullptr; a.npred_first = g->npred; a.npred_next = g->npred;
+    a.wc = S->wc.p; a.queue = S->queue.p; a.ctr = S->ctr.p; a.timeout_ns = S->timeout_ns; a.pfd = S->pfd;
+    if ((rc = launch_persistent(S, a))) return rc;
+    window_status_kernel<<<1, 32, 0, S->stream>>>(S->ctr.p, S->wsum.p);
+    XKB_CUDA_TRY(cudaGetLastError());
+    S->last_form = XKB_FORM_PERSISTENT;
+    S->last_total = ntasks;
+    return XKB_OK;
+}
+
+int xkb_internal_sched_run_window(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks, const xkb_task_graph_t * g)
+{
+    if (!S || (ntasks && !tasks) || !g || g->ntasks != ntasks || ntasks >= (size_t(1) << 31))
+        return xkb_set_error(XKB_EINVAL, "sched_run_window: bad arguments");
+    int rc = xkb_internal_sched_upload_window(S, tasks, ntasks);
+    return rc ? rc : xkb_internal_sched_launch_window(S, g);
+}
+
+int xkb_internal_sched_windows_wait(xkb_sched_t * S, uint64_t * executed)
+{
+    if (!S) return xkb_set_error(XKB_EINVAL, "sched_windows_wait: null scheduler");
+    XKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    unsigned long long sum[2] = {0, 0};
+    if (S->wsum.p)
+    {
+        XKB_CUDA_TRY(cudaMemcpy(sum, S->wsum.p, sizeof(sum), cudaMemcpyDeviceToHost));
+        XKB_CUDA_TRY(cudaMemset(S->wsum.p, 0, sizeof(sum)));
+    }
+    if (executed) *executed = sum[1];
+    if (sum[0] != 0) return xkb_set_error(-(int) sum[0], "sched: a device wait ran out of time in a window run");
+    return XKB_OK;
 }
 
 extern "C" int xkb_sched_wait(xkb_sched_t * S, uint64_t * executed)

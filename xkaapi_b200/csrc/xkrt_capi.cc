@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <memory>
@@ -84,6 +85,71 @@ using xkb_capi::Queue;
 thread_local Task * g_current = nullptr;  // task whose body runs on this thread (xkrt_task_current)
 thread_local cudaStream_t g_stream = nullptr;   // the stream of the worker running a CUDA body
 
+// Records that name the same bytes in the same mode: fetching them again to the same device is a
+// no-op (a device fetch never invalidates the device's copy of other data), so batches whose
+// fetches all go one way fetch each distinct record once. The set grows with the number of
+// DISTINCT records (a few per tile for a stencil), so it stays in cache however long the batch.
+class RecordSet {
+public:
+    RecordSet() : slot_(1024, UINT32_MAX) {}
+    // true if r (task id ignored) was not in the set; it is now
+    bool insert(const xkb_access_rec_t * recs, uint32_t i)
+    {
+        if (2 * (used_ + 1) > slot_.size()) rehash(recs);
+        const size_t mask = slot_.size() - 1;
+        size_t h = key_hash(recs[i]) & mask;
+        while (slot_[h] != UINT32_MAX)
+        {
+            if (same(recs[slot_[h]], recs[i])) return false;
+            h = (h + 1) & mask;
+        }
+        slot_[h] = i;
+        ++used_;
+        return true;
+    }
+    // whether a record equal to recs[i] is in the set (read only: callable from several threads)
+    bool contains(const xkb_access_rec_t * recs, uint32_t i) const
+    {
+        const size_t mask = slot_.size() - 1;
+        size_t h = key_hash(recs[i]) & mask;
+        while (slot_[h] != UINT32_MAX)
+        {
+            if (same(recs[slot_[h]], recs[i])) return true;
+            h = (h + 1) & mask;
+        }
+        return false;
+    }
+    void reset() { slot_.assign(1024, UINT32_MAX); used_ = 0; }
+private:
+    void rehash(const xkb_access_rec_t * recs)
+    {
+        std::vector<uint32_t> old(2 * slot_.size(), UINT32_MAX);
+        old.swap(slot_);
+        const size_t mask = slot_.size() - 1;
+        for (uint32_t i : old)
+            if (i != UINT32_MAX)
+            {
+                size_t h = key_hash(recs[i]) & mask;
+                while (slot_[h] != UINT32_MAX) h = (h + 1) & mask;
+                slot_[h] = i;
+            }
+    }
+    static uint64_t mix(uint64_t h, uint64_t v) { h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2); return h; }
+    static uint64_t key_hash(const xkb_access_rec_t & r)
+    {
+        uint64_t h = ((uint64_t) r.type << 8) | r.mode;
+        for (uint64_t v : {r.addr, r.ld, r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type}) h = mix(h, v);
+        return h * 0xff51afd7ed558ccdull;
+    }
+    static bool same(const xkb_access_rec_t & a, const xkb_access_rec_t & b)
+    {
+        return a.type == b.type && a.mode == b.mode && a.addr == b.addr && a.ld == b.ld && a.offset_m == b.offset_m &&
+               a.offset_n == b.offset_n && a.m == b.m && a.n == b.n && a.sizeof_type == b.sizeof_type;
+    }
+    std::vector<uint32_t> slot_;
+    size_t used_ = 0;
+};
+
 } // namespace
 
 static void task_completed(::xkb_runtime * R, Task & T);
@@ -104,6 +170,7 @@ struct xkb_runtime {
     std::mutex mu;
     std::condition_variable cv;
     size_t handed = 0, handed_acc = 0;                // tasks / accesses handed to the worker
+    std::deque<std::pair<size_t, size_t>> hand_q;     // ends (tasks, accesses) of the hand-overs not yet claimed
     size_t claimed = 0, done = 0;                     // tasks the worker took / finished
     bool stop = false;
     int bg_rc = XKB_OK;
@@ -125,7 +192,19 @@ struct xkb_runtime {
     // registration per growth, and an upload never spans two of them)
     size_t args_pinned = 0;
     std::vector<std::pair<void *, size_t>> pinned_ranges;
-    bool args_dense = true;                           // every task's args: one descriptor, back to back
+    std::atomic<bool> args_dense{true};               // every task's args: one descriptor, back to back
+    // streaming: while the program spawns, the worker hands each resolved window of a batch made
+    // only of built-in device tasks to the GPU (coherency, descriptors, one persistent launch)
+    size_t streamed = 0;                              // tasks [0, streamed) are on the GPU
+    bool stream_ok = true;                            // the batch can still be streamed
+    bool stream_on = true;                            // XKB_STREAM=0 turns streaming off
+    xkb_edge_mark_t rest_mark{};                      // edge mark at task `streamed` once streaming stopped
+    RecordSet dset;                                   // distinct records of the batch made coherent so far
+    std::vector<uint32_t> dfirst;                     //   their first occurrences, in record order
+    uint64_t cur_h2d = 0, cur_d2h = 0, cur_h2d_bytes = 0, cur_d2h_bytes = 0;   // copies of the batch in progress
+    // page-locked descriptor slots of streamed windows (a slot is reused once its copy is done)
+    struct DescSlot { xkb_task_desc_t * p = nullptr; size_t cap = 0; cudaEvent_t ev = nullptr; } dslot[2];
+    int dslot_next = 0;
     std::atomic<struct Dataflow *> df{nullptr};       // the batch being executed (detached completion)
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
@@ -228,6 +307,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     if (R->gpu) cudaGetDevice(&R->device);
     R->drivers[1].ordinal = R->device;
     R->chunk = RESOLVE_CHUNK;
+    if (const char * e = getenv("XKB_STREAM")) R->stream_on = atoi(e) != 0;
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
     // fixed pools (address space only; pages are backed when touched) let a worker thread read
@@ -251,7 +331,33 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
         if (cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_init: stream");
         else rc = xkb_sched_create(&R->sched, R->stream);
     }
-    if (rc) { delete R; return rc; }
+    if (rc == XKB_OK && R->bg)
+    {
+        // the working memory of one background batch (about R->chunk accesses: twice as many
+        // resolver ops, up to half as many tasks), reserved here rather than while the program spawns
+        if ((rc = xkb_resolver_create(&R->res, R->stream)) == XKB_OK) rc = xkb_internal_resolver_prepare(R->res, 2 * R->chunk);
+        if (rc == XKB_OK) rc = xkb_internal_sched_reserve(R->sched, R->chunk / 2 + R->chunk / 8 + 64);
+        for (auto & d : R->dslot)
+        {
+            if (rc != XKB_OK) break;
+            const size_t c = R->chunk / 2 + R->chunk / 8 + 64;
+            if (cudaHostAlloc((void **) &d.p, c * sizeof(xkb_task_desc_t), cudaHostAllocDefault) != cudaSuccess)
+                rc = xkb_set_error(XKB_ENOMEM, "xkrt_init: page-locked descriptor slots");
+            else d.cap = c;
+        }
+    }
+    if (rc)
+    {
+        R->pf_stop = true;
+        for (auto & th : R->prefaulter) if (th.joinable()) th.join();
+        if (R->res) xkb_resolver_destroy(R->res);
+        if (R->sched) xkb_sched_destroy(R->sched);
+        for (auto & d : R->dslot) if (d.p) cudaFreeHost(d.p);
+        if (R->stream) cudaStreamDestroy(R->stream);
+        if (R->planner) xkb_planner_destroy(R->planner);
+        delete R;
+        return rc;
+    }
     *out = (xkrt_runtime_t *) R;
     return XKB_OK;
 }
@@ -279,6 +385,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     }
     for (cudaStream_t w : R->wstreams) cudaStreamDestroy(w);
     for (auto & r : R->pinned_ranges) cudaHostUnregister(r.first);
+    for (auto & d : R->dslot) { if (d.ev) cudaEventDestroy(d.ev); if (d.p) cudaFreeHost(d.p); }
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
     if (R->stream) cudaStreamDestroy(R->stream);
@@ -288,18 +395,23 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
 }
 
 static void bg_finish(xkb_runtime * R);
+static void bg_wait_done(xkb_runtime * R);
 
 extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
 {
     xkb_runtime * R = RT(runtime);
     if (!R) return;
+    if (R->worker.joinable()) bg_wait_done(R);
+    if (R->streamed && R->sched) xkb_internal_sched_windows_wait(R->sched, nullptr);   // windows already on the GPU finish
     bg_finish(R);
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
     R->args_dense = true;
+    R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = 0;
 }
 
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, bool unified = false)
 {
+    std::lock_guard<std::mutex> lk(R->plan_mu);       // the worker may be streaming a window
     int32_t id = -1;
     int rc = xkb_planner_add_region(R->planner, (uint64_t) ptr, size, &id);
     if (rc) return rc;
@@ -804,8 +916,8 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
     for (auto & kv : R->regions) ptrs[kv.second.id] = kv.second.mirror;
     for (const xkb_copy_t & k : c)
     {
-        (k.kind == XKB_COPY_H2D ? R->last_h2d : R->last_d2h) += 1;
-        (k.kind == XKB_COPY_H2D ? R->last_h2d_bytes : R->last_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
+        (k.kind == XKB_COPY_H2D ? R->cur_h2d : R->cur_d2h) += 1;
+        (k.kind == XKB_COPY_H2D ? R->cur_h2d_bytes : R->cur_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
     }
     return xkb_plan_execute(c.data(), n, ptrs.data(), ptrs.size(), stream);
 }
@@ -853,58 +965,6 @@ static void parallel_chunks(size_t n, F fn)
     for (auto & th : pool) th.join();
 }
 
-// Records that name the same bytes in the same mode: fetching them again to the same device is a
-// no-op (a device fetch never invalidates the device's copy of other data), so batches whose
-// fetches all go one way fetch each distinct record once. The set grows with the number of
-// DISTINCT records (a few per tile for a stencil), so it stays in cache however long the batch.
-class RecordSet {
-public:
-    RecordSet() : slot_(1024, UINT32_MAX) {}
-    // true if r (task id ignored) was not in the set; it is now
-    bool insert(const xkb_access_rec_t * recs, uint32_t i)
-    {
-        if (2 * (used_ + 1) > slot_.size()) rehash(recs);
-        const size_t mask = slot_.size() - 1;
-        size_t h = key_hash(recs[i]) & mask;
-        while (slot_[h] != UINT32_MAX)
-        {
-            if (same(recs[slot_[h]], recs[i])) return false;
-            h = (h + 1) & mask;
-        }
-        slot_[h] = i;
-        ++used_;
-        return true;
-    }
-private:
-    void rehash(const xkb_access_rec_t * recs)
-    {
-        std::vector<uint32_t> old(2 * slot_.size(), UINT32_MAX);
-        old.swap(slot_);
-        const size_t mask = slot_.size() - 1;
-        for (uint32_t i : old)
-            if (i != UINT32_MAX)
-            {
-                size_t h = key_hash(recs[i]) & mask;
-                while (slot_[h] != UINT32_MAX) h = (h + 1) & mask;
-                slot_[h] = i;
-            }
-    }
-    static uint64_t mix(uint64_t h, uint64_t v) { h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2); return h; }
-    static uint64_t key_hash(const xkb_access_rec_t & r)
-    {
-        uint64_t h = ((uint64_t) r.type << 8) | r.mode;
-        for (uint64_t v : {r.addr, r.ld, r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type}) h = mix(h, v);
-        return h * 0xff51afd7ed558ccdull;
-    }
-    static bool same(const xkb_access_rec_t & a, const xkb_access_rec_t & b)
-    {
-        return a.type == b.type && a.mode == b.mode && a.addr == b.addr && a.ld == b.ld && a.offset_m == b.offset_m &&
-               a.offset_n == b.offset_n && a.m == b.m && a.n == b.n && a.sizeof_type == b.sizeof_type;
-    }
-    std::vector<uint32_t> slot_;
-    size_t used_ = 0;
-};
-
 // Indices of the first occurrence of every distinct record among those `keep` accepts, in
 // record order. Chunks of records are scanned on host threads, each keeping its own first
 // occurrences; merging the chunks' lists in chunk order keeps the global first occurrences.
@@ -930,6 +990,36 @@ static std::vector<uint32_t> distinct_records(const xkb_access_rec_t * recs, siz
         for (uint32_t i : f)
             if (seen.insert(recs, i)) out.push_back(i);
     return out;
+}
+
+// The records of accesses [a0, a1) that carry data to make coherent on the device (not handles,
+// not unified memory) and were not seen before in this batch: their first occurrences are added
+// to R->dfirst in record order; returns where they start there. Host threads scan chunks of the
+// range, each skipping what the batch's set already holds and keeping its own first occurrences;
+// adding the chunks' lists in chunk order keeps the first occurrences.
+static size_t add_distinct(xkb_runtime * R, size_t a0, size_t a1)
+{
+    const xkb_access_rec_t * recs = R->recs.data();
+    const size_t start = R->dfirst.size(), n = a1 - a0;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nth = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536)));
+    std::vector<std::vector<uint32_t>> firsts(nth);
+    const RecordSet & known = R->dset;
+    auto scan = [&](size_t k) {
+        RecordSet seen;
+        for (size_t i = a0 + n * k / nth; i < a0 + n * (k + 1) / nth; ++i)
+            if (recs[i].type != REC_NONE && recs[i].type != XKB_ACCESS_TYPE_HANDLE && !known.contains(recs, (uint32_t) i) &&
+                !in_unified(R, recs[i]) && seen.insert(recs, (uint32_t) i))
+                firsts[k].push_back((uint32_t) i);
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < nth; ++k) pool.emplace_back(scan, k);
+    scan(0);
+    for (auto & th : pool) th.join();
+    for (auto & f : firsts)
+        for (uint32_t i : f)
+            if (R->dset.insert(recs, i)) R->dfirst.push_back(i);
+    return start;
 }
 
 static double ms_since(std::chrono::steady_clock::time_point t0)
@@ -1044,7 +1134,11 @@ static int split_moldable(const xkb_task_desc_t * descs, size_t nt, const xkb_ta
 // the batch's resolver: directly when every task has a tracked access, else compacted with a
 // one-byte virtual read of the task's own Task object for a task without one (nothing else
 // touches it), so that task numbering stays dense.
-static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1)
+// Resolve tasks [t0, t1) (accesses [a0, a1)); *mark (optional) receives the resolver's edge mark
+// before them.
+// before_add (optional) runs once the records are converted, before the resolver works on them.
+static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1, xkb_edge_mark_t * mark = nullptr,
+                         const std::function<int()> * before_add = nullptr)
 {
     if (t0 >= t1) return XKB_OK;
     if (!R->recs.resize(a1)) return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
@@ -1092,6 +1186,8 @@ static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_
     if (!R->res && (rc = xkb_resolver_create(&R->res, R->stream))) return rc;
     if (R->res_stale && (rc = xkb_internal_resolver_reset(R->res))) return rc;
     R->res_stale = false;
+    if (mark && (rc = xkb_internal_resolver_edge_mark(R->res, mark))) return rc;
+    if (before_add && (rc = (*before_add)())) return rc;
     for (size_t b = 0; b < nfeed && rc == XKB_OK;)
     {
         size_t e = std::min(nfeed, b + R->chunk);
@@ -1102,9 +1198,13 @@ static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_
     return rc;
 }
 
+static int stream_prepare(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1, bool * ok);
+static int stream_launch(xkb_runtime * R, const xkb_edge_mark_t & mark);
+
 static void bg_worker(xkb_runtime * R)
 {
     cudaSetDevice(R->device);
+    static const bool trace = getenv("XKB_TRACE_WAIT") != nullptr;
     for (;;)
     {
         size_t t0, t1, a0, a1;
@@ -1113,15 +1213,30 @@ static void bg_worker(xkb_runtime * R)
             std::unique_lock<std::mutex> lk(R->mu);
             R->cv.wait(lk, [&] { return R->stop || R->handed > R->claimed; });
             if (R->handed == R->claimed) return;          // stop, nothing pending
-            t0 = R->claimed; t1 = R->handed;
-            a0 = R->pending[t0].acc_off; a1 = R->handed_acc;
+            // one hand-over at a time: windows of about a resolver batch, so the GPU starts on
+            // the first ones while later ones are resolved
+            t0 = R->claimed; t1 = R->hand_q.front().first;
+            a0 = R->pending[t0].acc_off; a1 = R->hand_q.front().second;
+            R->hand_q.pop_front();
             R->claimed = t1;
             failed = R->bg_rc != XKB_OK;
         }
-        const int rc = failed ? XKB_OK : resolve_range(R, t0, t1, a0, a1);
+        xkb_edge_mark_t mark{};
+        const auto w0 = std::chrono::steady_clock::now();
+        bool streamed = false;
+        const std::function<int()> prep = [&] { return stream_prepare(R, t0, t1, a0, a1, &streamed); };
+        int rc = failed ? XKB_OK : resolve_range(R, t0, t1, a0, a1, &mark, &prep);
+        const double res_ms = ms_since(w0);
+        if (!failed && rc == XKB_OK && streamed) rc = stream_launch(R, mark);
+        if (rc) streamed = false;
+        if (trace)
+            fprintf(stderr, "worker: tasks [%zu, %zu) prepared and resolved in %.1f ms, %s in %.1f ms\n", t0, t1, res_ms,
+                    streamed ? "launched" : "kept", ms_since(w0) - res_ms);
         {
             std::lock_guard<std::mutex> lk(R->mu);
             if (rc && R->bg_rc == XKB_OK) { R->bg_rc = rc; R->bg_err = xkb_last_error(); }
+            if (streamed) R->streamed = t1;
+            else if (R->stream_ok) { R->stream_ok = false; R->rest_mark = mark; }
             R->done = t1;
         }
         R->cv.notify_all();
@@ -1137,6 +1252,7 @@ static void bg_hand_over(xkb_runtime * R, bool final)
     {
         std::lock_guard<std::mutex> lk(R->mu);
         R->handed = nt; R->handed_acc = nacc;
+        R->hand_q.emplace_back(nt, nacc);
     }
     if (!R->worker.joinable()) R->worker = std::thread(bg_worker, R);
     R->cv.notify_all();
@@ -1154,8 +1270,13 @@ static void bg_finish(xkb_runtime * R)
 {
     if (R->worker.joinable()) bg_wait_done(R);
     R->handed = R->handed_acc = R->claimed = R->done = 0;
+    R->hand_q.clear();
     R->bg_rc = XKB_OK;
     R->bg_err.clear();
+    R->streamed = 0;
+    R->stream_ok = true;
+    R->dset.reset();
+    R->dfirst.clear();
     R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
 }
 
@@ -1232,6 +1353,7 @@ struct Dataflow {
     std::condition_variable cv;
     std::deque<uint32_t> ready;
     std::vector<uint32_t> ptr, succ, wc;
+    size_t base = 0;                    // graph task k is the batch's task base + k
     size_t nt = 0, done = 0;
     int err = XKB_OK;
     std::string err_text;
@@ -1243,8 +1365,9 @@ static void task_completed(::xkb_runtime * R, Task & T)
 {
     Dataflow * D = R ? R->df.load(std::memory_order_acquire) : nullptr;
     if (!D) return;
-    const size_t t = (size_t) (&T - R->pending.data());
-    if (t >= D->nt) return;
+    const size_t g = (size_t) (&T - R->pending.data());
+    if (g < D->base || g - D->base >= D->nt) return;
+    const size_t t = g - D->base;
     std::lock_guard<std::mutex> lk(D->mu);
     for (uint32_t i = D->ptr[t]; i < D->ptr[t + 1]; ++i)
         if (--D->wc[D->succ[i]] == 0) D->ready.push_back(D->succ[i]);
@@ -1252,14 +1375,16 @@ static void task_completed(::xkb_runtime * R, Task & T)
     D->cv.notify_all();
 }
 
-// A non-fused batch: ready tasks (all predecessors completed) run on a team of host threads,
+// A non-fused batch (its tasks from `base` on; the earlier ones completed): ready tasks (all
+// predecessors completed) run on a team of host threads,
 // XKB_HOST_THREADS or one per hardware thread (at most 64) -- the reference's host team and
 // device threads executing ready tasks as their predecessors complete. A detached task holds no
 // thread; the batch ends when every task completed (600 s without progress is an error).
-static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_access_rec_t * recs)
+static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_access_rec_t * recs, size_t base)
 {
-    const size_t nt = R->pending.size();
+    const size_t nt = R->pending.size() - base;
     Dataflow D;
+    D.base = base;
     D.nt = nt;
     D.ptr.resize(nt + 1); D.succ.resize(g.nedges ? g.nedges : 1); D.wc.resize(nt);
     if (cudaMemcpyAsync(D.ptr.data(), g.succ_ptr, (nt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, R->stream) != cudaSuccess ||
@@ -1303,7 +1428,7 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
                 }
                 t = D.ready.front(); D.ready.pop_front();
             }
-            const int rc = run_one(R, t, recs, R->wstreams[k]);
+            const int rc = run_one(R, base + t, recs, R->wstreams[k]);
             if (rc)
             {
                 std::lock_guard<std::mutex> lk(D.mu);
@@ -1311,7 +1436,7 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
                 D.cv.notify_all();
                 return;
             }
-            if (task_unref(R->pending[t])) task_completed(R, R->pending[t]);
+            if (task_unref(R->pending[base + t])) task_completed(R, R->pending[base + t]);
         }
     };
     std::vector<std::thread> team;
@@ -1335,7 +1460,13 @@ static void pin_args(xkb_runtime * R, size_t bytes)
     const size_t want = std::min((bytes + STEP - 1) & ~(STEP - 1), R->args_pool.capacity_bytes());
     if (want <= R->args_pinned) return;
     cudaSetDevice(R->device);
-    if (R->args_pinned) { cudaHostUnregister(R->args_pool.data()); R->pinned_ranges.clear(); R->args_pinned = 0; }
+    if (R->args_pinned)
+    {
+        cudaStreamSynchronize(R->stream);          // streamed windows may still copy descriptors from it
+        cudaHostUnregister(R->args_pool.data());
+        R->pinned_ranges.clear();
+        R->args_pinned = 0;
+    }
     const auto t0 = std::chrono::steady_clock::now();
     const cudaError_t e = cudaHostRegister(R->args_pool.data(), want, cudaHostRegisterDefault);
     if (getenv("XKB_TRACE_WAIT"))
@@ -1346,16 +1477,150 @@ static void pin_args(xkb_runtime * R, size_t bytes)
     R->args_pinned = want;
 }
 
+// Translate and check the built-in descriptors of tasks [t0, t1) for the device (host grid and
+// vector pointers to the mirrors), into `out` when given. Otherwise dense args (one descriptor
+// per task, back to back) are rewritten in place (nothing reads them as args after that), or
+// `copy` receives them.
+// *descs points at the result; *long_axpby tells whether some axpby task must be split.
+static int translate_descs(xkb_runtime * R, size_t t0, size_t t1, std::vector<xkb_task_desc_t> & copy, xkb_task_desc_t ** descs,
+                           bool * long_axpby, xkb_task_desc_t * out = nullptr)
+{
+    const size_t nt = t1 - t0;
+    const bool dense_args = R->args_dense && !out;
+    xkb_task_desc_t * d = (xkb_task_desc_t *) R->args_pool.data() + t0;
+    if (out) d = out;
+    else if (!dense_args) { copy.resize(nt); d = copy.data(); }
+    std::atomic<size_t> bad_args(SIZE_MAX), bad_ptr(SIZE_MAX);     // first failing task, if any
+    std::atomic<bool> longa(false);
+    parallel_chunks(nt, [&](size_t b, size_t e) {
+        RegionHint h;
+        for (size_t k = b; k < e; ++k)
+        {
+            const size_t t = t0 + k;
+            const Task & T = R->pending[t];
+            if (!dense_args)
+            {
+                if (T.nargs < sizeof(xkb_task_desc_t)) { size_t x = bad_args; while (t < x && !bad_args.compare_exchange_weak(x, t)) {} continue; }
+                memcpy(&d[k], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
+            }
+            d[k].kind = (uint32_t) R->formats[T.fmtid].builtin;
+            if (!translate_hint(R, d[k], h) || !xkb_internal_task_valid(d[k]))
+            { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
+            if (d[k].kind == XKB_TASK_AXPBY && d[k].u.axpby.hi - d[k].u.axpby.lo > AXPBY_SPLIT && !longa)
+                longa.store(true, std::memory_order_relaxed);
+        }
+    });
+    *descs = d;
+    *long_axpby = longa;
+    if (bad_args != SIZE_MAX) return xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", (size_t) bad_args);
+    if (bad_ptr != SIZE_MAX)
+        return xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region, or the "
+                                         "tile or range is malformed", (size_t) bad_ptr);
+    return XKB_OK;
+}
+
+// Warps per task: FP32-storage tiles (128 rows per strip) run best one warp per task, everything
+// else two (measured on the 16384^2 graphs).
+static int team_for(xkb_runtime * R, const xkb_task_desc_t * d, size_t n)
+{
+    bool all_f32 = true;
+    for (size_t t = 0; t < n && all_f32; t += 1 + n / 64) all_f32 = d[t].kind == XKB_TASK_HEAT_F32;
+    return xkb_sched_set_team(R->sched, all_f32 ? 1 : 2);
+}
+
+// Make the new distinct records of accesses [a0, a1) coherent on the device (copies issued on the
+// runtime's stream, in order).
+static int fetch_new_to_device(xkb_runtime * R, size_t a0, size_t a1)
+{
+    const size_t first = add_distinct(R, a0, a1);
+    const xkb_access_rec_t * recs = R->recs.data();
+    int rc = XKB_OK;
+    for (size_t j = first; j < R->dfirst.size() && rc == XKB_OK; ++j)
+    {
+        const uint32_t k = R->dfirst[j];
+        rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
+    }
+    if (rc == XKB_OK) rc = run_copies(R, R->stream);
+    return rc;
+}
+
+// Streaming a window of tasks [t0, t1) (accesses [a0, a1)) to the GPU while the program keeps
+// spawning, when the batch is still streamable: every task so far a built-in device body with
+// one descriptor as args, no axpby long enough to be split. In two halves around the window's
+// dependency resolution, so that the host work of the first half overlaps the GPU's run of the
+// previous window:
+//  * prepare (records converted, not yet resolved; under the planner lock, as the program may
+//    register memory meanwhile): the window's new distinct records made coherent on the device
+//    (copies in stream order), its descriptors translated into a page-locked slot and their copy
+//    queued; *ok = false when the window cannot go (nothing done; streaming stops for the batch);
+//  * launch (resolved): the window's graph (the edges among its tasks; those from earlier tasks
+//    are satisfied, as the earlier windows run before it on the same stream) and one persistent
+//    launch, not waited for.
+static int stream_prepare(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1, bool * ok)
+{
+    *ok = false;
+    if (!R->stream_ok || !R->stream_on || !R->args_dense || !R->sched || t0 != R->streamed || t0 >= t1) return XKB_OK;
+    const xkb_task_desc_t * raw = (const xkb_task_desc_t *) R->args_pool.data();
+    for (size_t t = t0; t < t1; ++t)
+    {
+        const Task & T = R->pending[t];
+        const int b = R->formats[T.fmtid].builtin;
+        if (b < 0 || !is_device(R, T)) return XKB_OK;
+        if (b == XKB_TASK_AXPBY && raw[t].u.axpby.hi - raw[t].u.axpby.lo > AXPBY_SPLIT) return XKB_OK;
+    }
+    std::lock_guard<std::mutex> lk(R->plan_mu);
+    static const bool trace = getenv("XKB_TRACE_WAIT") != nullptr;
+    const auto w0 = std::chrono::steady_clock::now();
+    int rc = fetch_new_to_device(R, a0, a1);
+    const double f_ms = ms_since(w0);
+    // a slot whose previous copy is done
+    xkb_runtime::DescSlot & sl = R->dslot[R->dslot_next];
+    R->dslot_next ^= 1;
+    const size_t n = t1 - t0;
+    if (rc == XKB_OK && sl.ev && cudaEventSynchronize(sl.ev) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt: descriptor slot");
+    if (rc == XKB_OK && n > sl.cap)
+    {
+        if (sl.p) cudaFreeHost(sl.p);
+        sl.p = nullptr; sl.cap = 0;
+        const size_t c = n + n / 4;
+        if (cudaHostAlloc((void **) &sl.p, c * sizeof(xkb_task_desc_t), cudaHostAllocDefault) != cudaSuccess)
+            rc = xkb_set_error(XKB_ENOMEM, "xkrt: %zu page-locked descriptors", c);
+        else sl.cap = c;
+    }
+    if (rc == XKB_OK && !sl.ev && cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess)
+        rc = xkb_set_error(XKB_ECUDA, "xkrt: event");
+    std::vector<xkb_task_desc_t> copy;
+    xkb_task_desc_t * descs = nullptr;
+    bool longa = false;
+    if (rc == XKB_OK) rc = translate_descs(R, t0, t1, copy, &descs, &longa, sl.p);
+    const double d_ms = ms_since(w0) - f_ms;
+    if (rc == XKB_OK) rc = team_for(R, descs, n);
+    if (rc == XKB_OK) rc = xkb_internal_sched_upload_window(R->sched, descs, n);
+    if (rc == XKB_OK && cudaEventRecord(sl.ev, R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt: event");
+    if (trace)
+        fprintf(stderr, "  window: coherency %.1f ms, descriptors %.1f ms, upload %.1f ms\n", f_ms, d_ms, ms_since(w0) - f_ms - d_ms);
+    if (rc == XKB_OK) *ok = true;
+    return rc;
+}
+
+static int stream_launch(xkb_runtime * R, const xkb_edge_mark_t & mark)
+{
+    xkb_task_graph_t g;
+    int rc = xkb_internal_resolver_window_graph(R->res, &mark, &g);
+    if (rc == XKB_OK) rc = xkb_internal_sched_launch_window(R->sched, &g);
+    return rc;
+}
+
 static int wait_batch(xkb_runtime * R)
 {
-    R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_h2d = R->last_d2h = 0; R->last_fused = 0;
-    R->last_h2d_bytes = R->last_d2h_bytes = 0;
+    R->last_tasks = R->pending.size(); R->last_edges = 0; R->last_fused = 0;
     for (double & m : R->last_ms) m = 0;
     if (R->pending.empty()) return XKB_OK;
     if (!R->gpu) return xkb_set_error(XKB_ENODEV, "xkrt_task_wait: dependency resolution runs on the GPU and none is visible");
     auto t0 = std::chrono::steady_clock::now();
     // (1) dependencies: everything not yet handed to the background worker is resolved now
-    // (by the worker when it runs, so that chunks stay in spawn order), then the graph is built
+    // (by the worker when it runs, so that chunks stay in spawn order; it also streams the last
+    // window when it can), then the graph of the tasks not yet on the GPU is built
     const size_t nacc = R->acc_pool.size(), ntasks = R->pending.size();
     int rc = XKB_OK;
     if (R->worker.joinable())
@@ -1368,24 +1633,41 @@ static int wait_batch(xkb_runtime * R)
         rc = resolve_range(R, 0, ntasks, 0, nacc);
     if (rc == XKB_OK && (!R->replica_pool.resize(nacc) || !R->recs.resize(nacc)))
         rc = xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
-    if (rc) return rc;
+    if (rc)
+    {
+        if (R->streamed) xkb_internal_sched_windows_wait(R->sched, nullptr);      // nothing left running
+        return rc;
+    }
     if (nacc) memset(R->replica_pool.data(), 0, nacc * sizeof(void *));
     xkb_access_rec_t * recs = R->recs.data();
     const double records_ms = ms_since(t0);
+    // tasks [P, ntasks) still to run; [0, P) were streamed to the GPU during the spawns
+    const size_t P = R->streamed;
+    const size_t a_P = P < ntasks ? R->pending[P].acc_off : nacc;
     xkb_resolver_t * res = R->res;
-    xkb_task_graph_t g;
-    if (rc == XKB_OK) rc = xkb_resolver_graph(res, &g);
-    if (rc) return rc;
-    R->last_edges = g.nedges;
+    xkb_task_graph_t g{};
+    if (P == 0) rc = xkb_resolver_graph(res, &g);
+    else if (P < ntasks) rc = xkb_internal_resolver_window_graph(res, &R->rest_mark, &g);
+    if (rc) { if (P) xkb_internal_sched_windows_wait(R->sched, nullptr); return rc; }
+    R->last_edges = P == 0 ? g.nedges : xkb_internal_resolver_nedges(res);
     R->last_ms[0] = ms_since(t0);
     if (getenv("XKB_TRACE_WAIT"))
-        fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms\n", nacc, records_ms, R->last_ms[0] - records_ms);
+        fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms, %zu of %zu tasks streamed\n", nacc, records_ms,
+                R->last_ms[0] - records_ms, P, ntasks);
 
     bool fused = true;
-    for (size_t t = 0; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
-    std::vector<uint32_t> fused_first;      // fused batches: first occurrence of every distinct record
+    for (size_t t = P; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
 
-    if (fused)
+    if (fused && P == ntasks)
+    {
+        // every window already on the GPU
+        t0 = std::chrono::steady_clock::now();
+        uint64_t ran = 0;
+        rc = xkb_internal_sched_windows_wait(R->sched, &ran);
+        R->last_ms[2] = ms_since(t0);
+        R->last_fused = 1;
+    }
+    else if (fused)
     {
         // (2) every access made coherent on the device up front: with no host task in the batch
         // the host data cannot change meanwhile, so the first-touch copies can all go first.
@@ -1393,80 +1675,55 @@ static int wait_batch(xkb_runtime * R)
         t0 = std::chrono::steady_clock::now();
         std::thread pinner;
         if (R->args_dense) pinner = std::thread(pin_args, R, ntasks * sizeof(xkb_task_desc_t));
-        fused_first = distinct_records(recs, nacc, [&](size_t k) {
-            // handles carry no data; unified memory is used in place
-            return recs[k].type != REC_NONE && recs[k].type != XKB_ACCESS_TYPE_HANDLE && !in_unified(R, recs[k]);
-        });
-        for (size_t j = 0; j < fused_first.size() && rc == XKB_OK; ++j)
-        {
-            const uint32_t k = fused_first[j];
-            rc = xkb_planner_fetch(R->planner, &recs[k], (uint32_t) (k - R->pending[recs[k].task].acc_off), 1, nullptr);
-        }
-        if (rc == XKB_OK) rc = run_copies(R, R->stream);
+        rc = fetch_new_to_device(R, a_P, nacc);
         const double fetch_ms = ms_since(t0);
-        // the descriptors: when every task's args are exactly one descriptor, the args pool is
-        // already the descriptor array (16-byte aligned 64-byte entries back to back) and is
-        // rewritten in place (nothing reads these args after a fused batch)
-        const size_t nt = R->pending.size();
-        const bool dense_args = R->args_dense;
         std::vector<xkb_task_desc_t> copy;
-        xkb_task_desc_t * descs = (xkb_task_desc_t *) R->args_pool.data();
-        if (!dense_args) { copy.resize(nt); descs = copy.data(); }
-        std::atomic<size_t> bad_args(SIZE_MAX), bad_ptr(SIZE_MAX);     // first failing task, if any
-        std::atomic<bool> long_axpby(false);                           // some task splits (moldable)
-        if (rc == XKB_OK)
-            parallel_chunks(nt, [&](size_t b, size_t e) {
-                RegionHint h;
-                for (size_t t = b; t < e; ++t)
-                {
-                    const Task & T = R->pending[t];
-                    if (!dense_args)
-                    {
-                        if (T.nargs < sizeof(xkb_task_desc_t)) { size_t x = bad_args; while (t < x && !bad_args.compare_exchange_weak(x, t)) {} continue; }
-                        memcpy(&descs[t], R->args_pool.data() + T.args_off, sizeof(xkb_task_desc_t));
-                    }
-                    descs[t].kind = (uint32_t) R->formats[T.fmtid].builtin;
-                    if (!translate_hint(R, descs[t], h) || !xkb_internal_task_valid(descs[t]))
-                    { size_t x = bad_ptr; while (t < x && !bad_ptr.compare_exchange_weak(x, t)) {} }
-                    if (descs[t].kind == XKB_TASK_AXPBY && descs[t].u.axpby.hi - descs[t].u.axpby.lo > AXPBY_SPLIT && !long_axpby)
-                        long_axpby.store(true, std::memory_order_relaxed);
-                }
-            });
-        if (rc == XKB_OK && bad_args != SIZE_MAX)
-            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", (size_t) bad_args);
-        else if (rc == XKB_OK && bad_ptr != SIZE_MAX)
-            rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: a grid or vector lies outside every registered region, or the "
-                                           "tile or range is malformed", (size_t) bad_ptr);
+        xkb_task_desc_t * descs = nullptr;
+        bool long_axpby = false;
+        const size_t nt = ntasks - P;
+        if (rc == XKB_OK) rc = translate_descs(R, P, ntasks, copy, &descs, &long_axpby);
         if (pinner.joinable()) pinner.join();
         const double desc_ms = ms_since(t0) - fetch_ms;
         SplitGraph sg;
         bool split = false;
         if (rc == XKB_OK && long_axpby) rc = split_moldable(descs, nt, g, sg, split);
         const xkb_task_graph_t & run_g = split ? sg.g : g;
-        if (rc == XKB_OK) rc = split ? xkb_internal_sched_set_tasks_device(R->sched, sg.descs.data(), sg.descs.size(), true)
-                                     : xkb_internal_sched_set_tasks_device(R->sched, descs, nt, true);
-        // warps per task: FP32-storage tiles (128 rows per strip) run best one warp per task,
-        // everything else two (measured on the 16384^2 graphs)
-        bool all_f32 = true;
-        for (size_t t = 0; t < nt && all_f32; t += 1 + nt / 64) all_f32 = descs[t].kind == XKB_TASK_HEAT_F32;
-        if (rc == XKB_OK) rc = xkb_sched_set_team(R->sched, all_f32 ? 1 : 2);
-        if (getenv("XKB_TRACE_WAIT"))
-            fprintf(stderr, "xkrt_task_wait: fetches + copies %.1f ms, descriptors %.1f ms, upload %.1f ms\n", fetch_ms, desc_ms,
-                    ms_since(t0) - fetch_ms - desc_ms);
-        if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
-        R->last_ms[1] = ms_since(t0);
-        t0 = std::chrono::steady_clock::now();
-        if (rc == XKB_OK) rc = xkb_sched_run(R->sched, &run_g, XKB_FORM_PERSISTENT);
-        uint64_t ran = 0;
-        if (rc == XKB_OK) rc = xkb_sched_wait(R->sched, &ran);
+        const xkb_task_desc_t * run_d = split ? sg.descs.data() : descs;
+        const size_t run_n = split ? sg.descs.size() : nt;
+        if (rc == XKB_OK) rc = team_for(R, run_d, run_n);
+        if (P == 0)
+        {
+            if (rc == XKB_OK) rc = xkb_internal_sched_set_tasks_device(R->sched, run_d, run_n, true);
+            if (getenv("XKB_TRACE_WAIT"))
+                fprintf(stderr, "xkrt_task_wait: fetches + copies %.1f ms, descriptors %.1f ms, upload %.1f ms\n", fetch_ms, desc_ms,
+                        ms_since(t0) - fetch_ms - desc_ms);
+            if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
+            R->last_ms[1] = ms_since(t0);
+            t0 = std::chrono::steady_clock::now();
+            if (rc == XKB_OK) rc = xkb_sched_run(R->sched, &run_g, XKB_FORM_PERSISTENT);
+            uint64_t ran = 0;
+            if (rc == XKB_OK) rc = xkb_sched_wait(R->sched, &ran);
+        }
+        else
+        {
+            // the rest of a streamed batch: one more window behind the streamed ones
+            if (rc == XKB_OK) rc = xkb_internal_sched_run_window(R->sched, run_d, run_n, &run_g);
+            R->last_ms[1] = ms_since(t0);
+            t0 = std::chrono::steady_clock::now();
+            uint64_t ran = 0;
+            const int wrc = xkb_internal_sched_windows_wait(R->sched, &ran);
+            if (rc == XKB_OK) rc = wrc;
+        }
         R->last_ms[2] = ms_since(t0);
         R->last_fused = 1;
     }
     else
     {
-        // (3) the batch as a dataflow graph on a team of host threads
+        // (3) the rest of the batch as a dataflow graph on a team of host threads, once the
+        // streamed windows (its completed predecessors) are done
         t0 = std::chrono::steady_clock::now();
-        rc = run_dataflow(R, g, recs);
+        if (P) rc = xkb_internal_sched_windows_wait(R->sched, nullptr);
+        if (rc == XKB_OK) rc = run_dataflow(R, g, recs, P);
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[2] = ms_since(t0);
     }
@@ -1482,7 +1739,7 @@ static int wait_batch(xkb_runtime * R)
         std::vector<uint32_t> first;
         if (fused)
         {
-            for (uint32_t k : fused_first)
+            for (uint32_t k : R->dfirst)
                 if (recs[k].mode & XKB_ACCESS_MODE_W) { recs[k].mode = XKB_ACCESS_MODE_R; first.push_back(k); }
         }
         else
@@ -1532,6 +1789,8 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     R->in_wait = true;
     fail(R, wait_batch(R));
     bg_finish(R);
+    R->last_h2d = R->cur_h2d; R->last_d2h = R->cur_d2h; R->last_h2d_bytes = R->cur_h2d_bytes; R->last_d2h_bytes = R->cur_d2h_bytes;
+    R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = 0;
     R->in_wait = false;
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
     R->args_dense = true;
