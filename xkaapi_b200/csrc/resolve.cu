@@ -700,9 +700,43 @@ static inline int mat_nrects(const xkb_access_rec_t & r)
 // domain replays earlier segments at that point of the stream -- or a small batch), or an error.
 static int build_ops_staged(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
 {
-    if (n < 65536 || R->blas.empty() || !R->pool) return 0;
+    if (n < 65536 || !R->pool) return 0;
     const unsigned nc = R->pool->size();
     if (nc < 2) return 0;
+    if (R->segments.empty())
+    {
+        // no segment seen yet, so a new matrix domain replays nothing: create the batch's new
+        // ones up front, in the order the sequential build would meet them
+        std::vector<char> other(nc, 0), fresh(nc, 0);
+        R->pool->run([&](unsigned c) {
+            uint64_t lk = ~0ull, ls = ~0ull;
+            for (size_t i = n * c / nc; i < n * (c + 1) / nc; ++i)
+            {
+                const xkb_access_rec_t & r = recs[i];
+                if (r.type != XKB_ACCESS_TYPE_BLAS_MATRIX) { other[c] = 1; return; }
+                if (r.ld == lk && r.sizeof_type == ls) continue;
+                lk = r.ld; ls = r.sizeof_type;
+                if (!R->blas_index.count(std::make_pair(r.ld, r.sizeof_type))) fresh[c] = 1;
+            }
+        });
+        for (char o : other) if (o) return 0;
+        bool any = false;
+        for (char f : fresh) any = any || f;
+        uint64_t lk = ~0ull, ls = ~0ull;
+        if (any)
+            for (size_t i = 0; i < n; ++i)
+            {
+                if (recs[i].ld == lk && recs[i].sizeof_type == ls) continue;
+                lk = recs[i].ld; ls = recs[i].sizeof_type;
+                const auto key = std::make_pair(lk, ls);
+                if (R->blas_index.count(key)) continue;
+                std::unique_ptr<Domain> d(new Domain());
+                d->ld = key.first; d->s = key.second;
+                R->blas.push_back(std::move(d));
+                R->blas_index.emplace(key, R->blas.size() - 1);
+            }
+    }
+    if (R->blas.empty()) return 0;
     const size_t nd = R->blas.size();
     std::vector<uint64_t> keys(2 * nd);
     for (size_t k = 0; k < nd; ++k) { keys[2 * k] = R->blas[k]->ld; keys[2 * k + 1] = R->blas[k]->s; }

@@ -120,6 +120,12 @@ public:
         return false;
     }
     void reset() { slot_.assign(1024, UINT32_MAX); used_ = 0; }
+    static uint64_t key_hash(const xkb_access_rec_t & r)
+    {
+        uint64_t h = ((uint64_t) r.type << 8) | r.mode;
+        for (uint64_t v : {r.addr, r.ld, r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type}) h = mix(h, v);
+        return h * 0xff51afd7ed558ccdull;
+    }
 private:
     void rehash(const xkb_access_rec_t * recs)
     {
@@ -135,12 +141,6 @@ private:
             }
     }
     static uint64_t mix(uint64_t h, uint64_t v) { h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2); return h; }
-    static uint64_t key_hash(const xkb_access_rec_t & r)
-    {
-        uint64_t h = ((uint64_t) r.type << 8) | r.mode;
-        for (uint64_t v : {r.addr, r.ld, r.offset_m, r.offset_n, r.m, r.n, r.sizeof_type}) h = mix(h, v);
-        return h * 0xff51afd7ed558ccdull;
-    }
     static bool same(const xkb_access_rec_t & a, const xkb_access_rec_t & b)
     {
         return a.type == b.type && a.mode == b.mode && a.addr == b.addr && a.ld == b.ld && a.offset_m == b.offset_m &&
@@ -1016,9 +1016,33 @@ static size_t add_distinct(xkb_runtime * R, size_t a0, size_t a1)
     for (size_t k = 1; k < nth; ++k) pool.emplace_back(scan, k);
     scan(0);
     for (auto & th : pool) th.join();
-    for (auto & f : firsts)
-        for (uint32_t i : f)
-            if (R->dset.insert(recs, i)) R->dfirst.push_back(i);
+    pool.clear();
+    size_t total = 0;
+    for (auto & f : firsts) total += f.size();
+    if (nth == 1 || total < 65536)
+    {
+        for (auto & f : firsts)
+            for (uint32_t i : f)
+                if (R->dset.insert(recs, i)) R->dfirst.push_back(i);
+        return start;
+    }
+    // many candidates (a first window): the threads split the keys by hash, each keeping the
+    // first occurrence of its keys (lists in chunk order); sorted by index, the winners are the
+    // first occurrences in record order
+    std::vector<std::vector<uint32_t>> part(nth);
+    auto merge = [&](size_t j) {
+        RecordSet mine;
+        for (auto & f : firsts)
+            for (uint32_t i : f)
+                if ((RecordSet::key_hash(recs[i]) >> 40) % nth == j && mine.insert(recs, i)) part[j].push_back(i);
+    };
+    for (size_t k = 1; k < nth; ++k) pool.emplace_back(merge, k);
+    merge(0);
+    for (auto & th : pool) th.join();
+    std::vector<uint32_t> win;
+    for (auto & q : part) win.insert(win.end(), q.begin(), q.end());
+    std::sort(win.begin(), win.end());
+    for (uint32_t i : win) { R->dset.insert(recs, i); R->dfirst.push_back(i); }
     return start;
 }
 
@@ -1248,7 +1272,10 @@ static void bg_worker(xkb_runtime * R)
 static void bg_hand_over(xkb_runtime * R, bool final)
 {
     const size_t nacc = R->acc_pool.size(), nt = R->pending.size();
-    if (nt == R->handed || (!final && nacc - R->handed_acc < R->chunk)) return;
+    // the first hand-over of a batch comes early (an eighth of a batch), so that the GPU starts
+    // on the first window while the rest is spawned
+    const size_t want = R->handed ? R->chunk : std::max<size_t>(16, R->chunk / 8);
+    if (nt == R->handed || (!final && nacc - R->handed_acc < want)) return;
     {
         std::lock_guard<std::mutex> lk(R->mu);
         R->handed = nt; R->handed_acc = nacc;
