@@ -9,12 +9,13 @@
  * host / device / unified memory, asynchronous file I/O tasks, and the driver interface (queues,
  * transfers, modules, kernel launches) of the host and the GPU.
  *
- * Execution model: spawned tasks are buffered; xkrt_task_wait resolves their dependencies on the
- * GPU (xkb_resolver), makes the data each task touches coherent where it runs (resident
- * planner: one device mirror per registered host region, H2D/D2H only for blocks the target
- * lacks), runs the tasks -- every task on the device scheduler's persistent kernel when all are
- * built-in device bodies, else as a dataflow graph on a team of host threads, each with its own
- * CUDA stream -- and leaves host memory coherent when it returns. Handle accesses order tasks like the
+ * Execution model: spawned tasks are resolved on the GPU (xkb_resolver) by a background worker
+ * while the program keeps spawning, their data made coherent where they run (resident planner:
+ * one device mirror per registered host region, H2D/D2H only for blocks the target lacks), and
+ * run -- built-in device bodies on the device scheduler's persistent kernel, window by window
+ * as soon as they are resolved while every task so far is one; otherwise, at xkrt_task_wait, as
+ * a dataflow graph on a team of host threads, each with its own CUDA stream. xkrt_task_wait
+ * returns when every task completed and host memory is coherent again. Handle accesses order tasks like the
  * reference's DependencyMap (they carry no data); concurrent-mode accesses and user moldable
  * tasks are not supported. Functions that return void in the reference record failures
  * instead; read them with xkb_runtime_status().
