@@ -187,6 +187,13 @@ XKB_API int xkb_planner_allocations(xkb_planner_t * planner, uint64_t * sizes, s
  * the writer's copy the only coherent one. Blocks are the same canonical partition as above. */
 XKB_API int xkb_planner_create_resident(xkb_planner_t ** planner);
 XKB_API int xkb_planner_add_region(xkb_planner_t * planner, uint64_t host_base, uint64_t size, int32_t * region);
+/* Resident mode: make the host coherent again for every block whose only coherent copy is on
+ * the GPU -- what fetching every record device tasks wrote back to the host does, without the
+ * records (one walk over the partition). Blocks that follow one another in a slab and in the
+ * same region are copied together (one D2H record per run, task and access -1); the blocks
+ * become coherent on both sides. Replaces the write-back fetches of memory_coherent_async
+ * (src/memory/coherent.cc:137-231) over the whole registered memory. */
+XKB_API int xkb_planner_flush_to_host(xkb_planner_t * planner);
 
 /* Run planned copies in order on `stream`: H2D and D2H with cudaMemcpy2DAsync, the D2D copies
  * of each access as one gather kernel (one CTA per copy). alloc_ptrs[k] is the device

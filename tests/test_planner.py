@@ -136,3 +136,71 @@ def test_resident_mode_matches_model(seed):
         assert tuple(v) == M.fetch(rec, t % 3, dev), t
         got = [tuple(int(x) for x in row) for row in P.copies(take=True)]
         assert got == M.take(), t
+
+
+def _copied_bytes(copies):
+    """Host byte intervals a list of D2H copies writes (merged)."""
+    iv = []
+    for c in copies:
+        dst, ld, m, n, s = int(c[9]), int(c[10]), int(c[11]), int(c[12]), int(c[13])
+        w = m * s
+        for r in range(n):
+            iv.append((dst + r * ld * s, dst + r * ld * s + w))
+    iv.sort()
+    out = []
+    for a, b in iv:
+        if out and a <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], b))
+        else:
+            out.append((a, b))
+    return out
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_flush_to_host_matches_write_back_fetches(seed):
+    """After random device work, flushing the resident planner copies back exactly the bytes
+    that fetching every device-written record to the host copies, and leaves the host coherent
+    (a second flush copies nothing)."""
+    import numpy as np
+    import streams as S
+    rng = np.random.default_rng(100 + seed)
+    mats = [((1 << 20) + 24, 64, 8, 40), ((1 << 21), 50, 4, 30)]
+    seg_base, seg_len = 1 << 22, 5000
+    stream = []
+    for t in range(250):
+        mode = int(rng.choice([S.R, S.W, S.RW]))
+        kind = rng.integers(0, 3)
+        if kind < 2:
+            base, ld, s, cols = mats[kind]
+            m, n = int(rng.integers(1, ld + 1)), int(rng.integers(1, 8))
+            om, on = int(rng.integers(0, ld - m + 1)), int(rng.integers(0, cols - n))
+            rec = S.from_tuples([[("m", mode, base, ld, om, on, m, n, s)]])[0]
+        else:
+            lo = int(rng.integers(0, seg_len - 1))
+            hi = int(rng.integers(lo + 1, min(seg_len, lo + 700) + 1))
+            rec = S.from_tuples([[("s", mode, seg_base + lo, seg_base + hi)]])[0]
+        rec["task"] = t
+        stream.append((rec, int(rng.random() < 0.8)))
+
+    def replay():
+        P = xk.Planner(resident=True)
+        for base, ld, s, cols in mats:
+            P.add_region(base, ld * cols * s + 64)
+        P.add_region(seg_base, seg_len)
+        for rec, dev in stream:
+            P.fetch(rec, 0, dev)
+        P.copies(take=True)
+        return P
+
+    P1, P2 = replay(), replay()
+    for rec, dev in stream:
+        if dev and rec["mode"] & S.W:
+            r = rec.copy()
+            r["mode"] = S.R
+            P1.fetch(r, 0, 0)
+    P2.flush_to_host()
+    a, b = P1.copies(take=True), P2.copies(take=True)
+    assert len(b) and set(b[:, 2]) == {xk.COPY_D2H}
+    assert _copied_bytes(a) == _copied_bytes(b)
+    P2.flush_to_host()
+    assert len(P2.copies(take=True)) == 0

@@ -512,6 +512,55 @@ extern "C" int xkb_planner_create_resident(xkb_planner_t ** out)
     return rc;
 }
 
+extern "C" int xkb_planner_flush_to_host(xkb_planner_t * P)
+{
+    if (!P || !P->resident) return xkb_set_error(XKB_EINVAL, "planner_flush_to_host: needs a resident planner");
+    for (auto & kv : P->rframes)
+    {
+        const uint64_t ld = kv.first.first, s = kv.first.second;
+        const bool seg = ld == ~0ull;
+        const uint64_t stride = seg ? 0 : ld * s;
+        for (auto & sk : kv.second->slabs)
+        {
+            const uint64_t x0 = sk.first, x1 = sk.second.x1;
+            std::vector<RBlock> & b = sk.second.b;
+            size_t k = 0;
+            while (k < b.size())
+            {
+                if (!(b[k].st != 0 && !(b[k].st & DEV_HOST))) { ++k; continue; }
+                // the region of the run's first block
+                const uint64_t h0 = x0 + b[k].y0 * stride;
+                auto rit = P->regions.upper_bound(h0);
+                if (rit == P->regions.begin()) return xkb_set_error(XKB_EINVAL, "planner_flush_to_host: a block in no region");
+                --rit;
+                const uint64_t rbase = rit->first, rend = rit->first + rit->second.first;
+                size_t e = k;
+                uint64_t y1 = b[k].y1;
+                b[k].st |= DEV_HOST;
+                // the next blocks of the run: contiguous rows, device-only, same region
+                while (e + 1 < b.size() && b[e + 1].y0 == y1 && b[e + 1].st != 0 && !(b[e + 1].st & DEV_HOST) &&
+                       x0 + b[e + 1].y0 * stride >= rbase && x0 + b[e + 1].y0 * stride < rend)
+                {
+                    ++e;
+                    y1 = b[e].y1;
+                    b[e].st |= DEV_HOST;
+                }
+                xkb_copy_t c;
+                c.task = -1; c.access = -1; c.kind = XKB_COPY_D2H;
+                c.src_dev = 1; c.dst_dev = 0;
+                c.src_alloc = rit->second.second; c.dst_alloc = -1;
+                c.src_off = (int64_t) (h0 - rbase); c.dst_off = (int64_t) h0;
+                c.src_ld = c.dst_ld = seg ? 0 : (int64_t) ld;
+                if (seg) { c.m = (int64_t) (x1 - x0); c.n = 1; c.sizeof_type = 1; }
+                else { c.m = (int64_t) ((x1 - x0) / s); c.n = (int64_t) (y1 - b[k].y0); c.sizeof_type = (int64_t) s; }
+                P->copies.push_back(c);
+                k = e + 1;
+            }
+        }
+    }
+    return XKB_OK;
+}
+
 extern "C" int xkb_planner_add_region(xkb_planner_t * P, uint64_t host_base, uint64_t size, int32_t * region)
 {
     if (!P || !P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_add_region: needs a resident planner and a size");

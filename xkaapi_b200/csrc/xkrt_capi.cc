@@ -1685,13 +1685,11 @@ static int wait_batch(xkb_runtime * R)
     bool fused = true;
     for (size_t t = P; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
 
-    if (fused && P == ntasks)
+    const bool all_streamed = fused && P == ntasks;
+    if (all_streamed)
     {
-        // every window already on the GPU
-        t0 = std::chrono::steady_clock::now();
-        uint64_t ran = 0;
-        rc = xkb_internal_sched_windows_wait(R->sched, &ran);
-        R->last_ms[2] = ms_since(t0);
+        // every window already on the GPU: the write-back below is planned and its copies queued
+        // behind the last windows while they run; the wait for them comes after it
         R->last_fused = 1;
     }
     else if (fused)
@@ -1754,34 +1752,26 @@ static int wait_batch(xkb_runtime * R)
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[2] = ms_since(t0);
     }
-    // (4) host memory coherent again: read back every block a device task wrote (every fetch
-    // here goes to the host, so each distinct record is fetched once)
+    // (4) host memory coherent again: read back every block a device task wrote
     if (rc == XKB_OK)
     {
         t0 = std::chrono::steady_clock::now();
-        // the blocks device tasks wrote, as reads (records rewritten in place: unused after this).
-        // A fused batch already has the first occurrence of every distinct record, all of device
-        // tasks: its writing ones are the blocks to read back (a W and an RW record on the same
-        // bytes both come back as R; the second fetch finds the host coherent and copies nothing).
-        std::vector<uint32_t> first;
-        if (fused)
-        {
-            for (uint32_t k : R->dfirst)
-                if (recs[k].mode & XKB_ACCESS_MODE_W) { recs[k].mode = XKB_ACCESS_MODE_R; first.push_back(k); }
-        }
-        else
-            first = distinct_records(recs, nacc, [&](size_t k) {
-                if (recs[k].type == REC_NONE || recs[k].type == XKB_ACCESS_TYPE_HANDLE || !(recs[k].mode & XKB_ACCESS_MODE_W) ||
-                    !is_device(R, R->pending[recs[k].task]) || in_unified(R, recs[k]))
-                    return false;
-                recs[k].mode = XKB_ACCESS_MODE_R;
-                return true;
-            });
-        for (size_t j = 0; j < first.size() && rc == XKB_OK; ++j) rc = xkb_planner_fetch(R->planner, &recs[first[j]], 0, 0, nullptr);
+        // every block whose only coherent copy is on the GPU (exactly the blocks device tasks
+        // wrote: each wait leaves the host coherent), one walk over the planner's partition
+        rc = xkb_planner_flush_to_host(R->planner);
         const double fetch_ms = ms_since(t0);
         if (rc == XKB_OK) rc = run_copies(R, R->stream);
+        if (all_streamed)
+        {
+            // the windows (and the copies queued behind them) end here
+            const auto tw = std::chrono::steady_clock::now();
+            uint64_t ran = 0;
+            const int wrc = xkb_internal_sched_windows_wait(R->sched, &ran);
+            if (rc == XKB_OK) rc = wrc;
+            R->last_ms[2] = ms_since(tw);
+        }
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
-        R->last_ms[3] = ms_since(t0);
+        R->last_ms[3] = ms_since(t0) - (all_streamed ? R->last_ms[2] : 0.0);
         if (getenv("XKB_TRACE_WAIT"))
             fprintf(stderr, "xkrt_task_wait: write-back fetches %.1f ms, copies %.1f ms\n", fetch_ms, R->last_ms[3] - fetch_ms);
     }
