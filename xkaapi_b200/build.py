@@ -19,6 +19,8 @@ LIB = os.path.join(PKG, "libxkb200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include")]
+# XKB_NVCC_DEFINES: extra compile-time settings for tuning sweeps, e.g. "-DXKB_TILE_PF=3"
+NVCC_FLAGS += os.environ.get("XKB_NVCC_DEFINES", "").split()
 LINK_FLAGS = ["-shared", "-lcudart", "-lpthread"]
 
 

@@ -41,6 +41,10 @@ __device__ __forceinline__ Cells<T, VEC> ld_cells(const T * __restrict__ g, int6
         } else if constexpr (VEC == 4 && sizeof(T) == 4) {
             float4 v = CG ? __ldcg((const float4 *) p) : __ldg((const float4 *) p);
             c.v[0] = v.x; c.v[1] = v.y; c.v[2] = v.z; c.v[3] = v.w;
+        } else if constexpr (VEC == 4 && sizeof(T) == 8) {
+            double2 a = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
+            double2 b = CG ? __ldcg((const double2 *) p + 1) : __ldg((const double2 *) p + 1);
+            c.v[0] = a.x; c.v[1] = a.y; c.v[2] = b.x; c.v[3] = b.y;
         } else {
 #pragma unroll
             for (int e = 0; e < VEC; ++e) c.v[e] = ld_scalar<CG>(p + e);
@@ -107,6 +111,10 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
             if constexpr (VEC == 2 && sizeof(T) == 8) {
                 double2 v = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
                 q.v[0] = v.x; q.v[1] = v.y;
+            } else if constexpr (VEC == 4 && sizeof(T) == 8) {
+                double2 a = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
+                double2 b = CG ? __ldcg((const double2 *) p + 1) : __ldg((const double2 *) p + 1);
+                q.v[0] = a.x; q.v[1] = a.y; q.v[2] = b.x; q.v[3] = b.y;
             } else {
                 float4 v = CG ? __ldcg((const float4 *) p) : __ldg((const float4 *) p);
                 q.v[0] = v.x; q.v[1] = v.y; q.v[2] = v.z; q.v[3] = v.w;
@@ -151,6 +159,11 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
             if (full_store)
             {
                 if constexpr (VEC == 2 && sizeof(T) == 8) *(double2 *) q = make_double2(out.v[0], out.v[1]);
+                else if constexpr (VEC == 4 && sizeof(T) == 8)
+                {
+                    ((double2 *) q)[0] = make_double2(out.v[0], out.v[1]);
+                    ((double2 *) q)[1] = make_double2(out.v[2], out.v[3]);
+                }
                 else *(float4 *) q = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
             }
             else
@@ -226,6 +239,10 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
             if constexpr (VEC == 2 && sizeof(T) == 8) {
                 double2 v = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
                 q.v[0] = v.x; q.v[1] = v.y;
+            } else if constexpr (VEC == 4 && sizeof(T) == 8) {
+                double2 a = CG ? __ldcg((const double2 *) p) : __ldg((const double2 *) p);
+                double2 b = CG ? __ldcg((const double2 *) p + 1) : __ldg((const double2 *) p + 1);
+                q.v[0] = a.x; q.v[1] = a.y; q.v[2] = b.x; q.v[3] = b.y;
             } else {
                 float4 v = CG ? __ldcg((const float4 *) p) : __ldg((const float4 *) p);
                 q.v[0] = v.x; q.v[1] = v.y; q.v[2] = v.z; q.v[3] = v.w;
@@ -278,6 +295,11 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
                 if (full_store)
                 {
                     if constexpr (VEC == 2 && sizeof(T) == 8) *(double2 *) q = make_double2(out.v[0], out.v[1]);
+                    else if constexpr (VEC == 4 && sizeof(T) == 8)
+                    {
+                        ((double2 *) q)[0] = make_double2(out.v[0], out.v[1]);
+                        ((double2 *) q)[1] = make_double2(out.v[2], out.v[3]);
+                    }
                     else *(float4 *) q = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
                 }
                 else

@@ -59,7 +59,13 @@ constexpr int SCHED_THREADS = 256;
 
 constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (bulk tile body)
 #ifndef XKB_TILE_PF
-#define XKB_TILE_PF 4                    // east columns a tile strip loads ahead into registers
+#define XKB_TILE_PF 4                    // east columns an FP32 tile strip loads ahead into registers
+#endif
+#ifndef XKB_F64_VEC
+#define XKB_F64_VEC 4                    // rows per lane of the FP64 tile body: one warp covers 128 rows
+#endif
+#ifndef XKB_F64_PF
+#define XKB_F64_PF 2                     // east columns the FP64 tile strip loads ahead (32 B per lane each)
 #endif
 #ifndef XKB_SCHED_MINB
 #define XKB_SCHED_MINB 2                 // persistent CTAs resident per SM (register budget)
@@ -73,7 +79,7 @@ __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int war
         case XKB_TASK_HEAT_F64: {
             const auto & h = d.u.heat;
             const bool vok = (h.ld % 2 == 0) && (h.src % 16 == 0) && (h.dst % 16 == 0);
-            heat_tile_team<double, 2, XKB_TILE_PF, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
+            heat_tile_team<double, XKB_F64_VEC, XKB_F64_PF, true>((const double *) h.src, (double *) h.dst, h.ld, h.nx, h.ny,
                                                h.x0, h.x1, h.y0, h.y1, h.c, vok, pfd, warp, nwarps);
             break;
         }
@@ -341,9 +347,9 @@ struct xkb_sched {
     const void * graph_key = nullptr;
     int last_form = -1;
     int grid = 0;
-    int team_warps = 2;
+    int team_warps = 1;                       // one warp per 128-row tile (FP64 and FP32 bodies)
     int bulk = 0;                             // 1: bulk-staged heat tile body (measured slower; opt-in)
-    int pfd = 8;
+    int pfd = 4;                              // L2 prefetch distance in columns (3-5 measured best)
     uint64_t last_total = 0;                  // tasks of the last run
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;

@@ -217,6 +217,9 @@ extern "C" int xkb_server_create(xkb_server_t ** out, const xkb_server_cfg_t * c
         XKB_CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
         int rc;
         if ((rc = xkb_sched_create(&sl.sch, sl.stream))) return rc;
+        // two warps per tile and an 8-column L2 prefetch: with many graphs side by side and a
+        // CTA budget per graph from its width, this sharing of the SMs measured best
+        if ((rc = xkb_sched_set_team(sl.sch, 2)) || (rc = xkb_sched_set_prefetch(sl.sch, 8))) return rc;
     }
     int sms = 148, per = 2;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->dev);

@@ -1546,13 +1546,13 @@ static int translate_descs(xkb_runtime * R, size_t t0, size_t t1, std::vector<xk
     return XKB_OK;
 }
 
-// Warps per task: FP32-storage tiles (128 rows per strip) run best one warp per task, everything
-// else two (measured on the 16384^2 graphs).
+// Warps per task: heat tiles (one warp strip covers 128 rows in FP64 and FP32) run best one warp
+// per task, axpby slices two (measured on the 16384^2 graphs and the axpby chains).
 static int team_for(xkb_runtime * R, const xkb_task_desc_t * d, size_t n)
 {
-    bool all_f32 = true;
-    for (size_t t = 0; t < n && all_f32; t += 1 + n / 64) all_f32 = d[t].kind == XKB_TASK_HEAT_F32;
-    return xkb_sched_set_team(R->sched, all_f32 ? 1 : 2);
+    bool heat = true;
+    for (size_t t = 0; t < n && heat; t += 1 + n / 64) heat = d[t].kind == XKB_TASK_HEAT_F32 || d[t].kind == XKB_TASK_HEAT_F64;
+    return xkb_sched_set_team(R->sched, heat ? 1 : 2);
 }
 
 // Make the new distinct records of accesses [a0, a1) coherent on the device (copies issued on the
