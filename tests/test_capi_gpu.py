@@ -17,7 +17,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def build(name, tmp_path):
     exe = str(tmp_path / name)
     lib = os.path.join(REPO, "xkaapi_b200")
-    subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-D_POSIX_C_SOURCE=200809L", "-I", os.path.join(REPO, "include"),
+    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-Wall", "-Werror", "-D_POSIX_C_SOURCE=200809L", "-I", os.path.join(REPO, "include"),
                     os.path.join(REPO, "tests", "capi", name + ".c"), "-o", exe, "-L", lib, "-lxkb200", "-lpthread",
                     "-Wl,-rpath," + lib], check=True)
     return exe
@@ -60,6 +60,20 @@ def test_dataflow_host_team(torch_cuda, tmp_path, threads):
         assert out["peak"] == 1
     elif (os.cpu_count() or 1) >= 4:
         assert out["peak"] >= 4 and out["wide_s"] < 48 * 0.020 / 2
+
+
+def test_streaming_stops_midway(torch_cuda, tmp_path):
+    """Short axpby chunks stream window by window; a pass of chunks that must be split stops the
+    streaming; the rest runs at the wait behind the streamed windows (with the split) -- y is the
+    host's result bit for bit."""
+    import re
+    env = dict(os.environ, XKB_RESOLVE_CHUNK="16", XKB_TRACE_WAIT="1")
+    r = subprocess.run([build("stream_rest_capi", tmp_path)], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["mismatches"] == 0 and out["fused"] == 1
+    m = re.search(r"(\d+) of (\d+) tasks streamed", r.stderr)
+    assert m and 0 < int(m.group(1)) < int(m.group(2)) == out["tasks"]
 
 
 def test_ordering_programs(torch_cuda, tmp_path):
