@@ -1272,9 +1272,10 @@ static void bg_worker(xkb_runtime * R)
 static void bg_hand_over(xkb_runtime * R, bool final)
 {
     const size_t nacc = R->acc_pool.size(), nt = R->pending.size();
-    // the first hand-over of a batch comes early (an eighth of a batch), so that the GPU starts
-    // on the first window while the rest is spawned
-    const size_t want = R->handed ? R->chunk : std::max<size_t>(16, R->chunk / 8);
+    // the first hand-over of a batch comes early (a 32nd of a batch), so that the GPU starts on
+    // the first window while the rest is spawned: a small first window also makes only part of
+    // the data coherent, the rest coming with the next windows while the GPU runs
+    const size_t want = R->handed ? R->chunk : std::max<size_t>(16, R->chunk / 32);
     if (nt == R->handed || (!final && nacc - R->handed_acc < want)) return;
     {
         std::lock_guard<std::mutex> lk(R->mu);
