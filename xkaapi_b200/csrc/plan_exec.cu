@@ -85,13 +85,15 @@ __global__ void __launch_bounds__(256) diffusion_views_kernel(const T * __restri
 
 using namespace xkb;
 
-// One host copy: rows x width bytes from src (pitch sp) to dst (pitch dp).
+// One host copy: rows x width bytes from src (pitch sp) to dst (pitch dp). A byte range of a
+// segment has no pitch (sp = dp = 0): such ranges merge whenever they continue each other.
 struct HostCopy { uintptr_t src, dst; int64_t sp, dp, width, rows; };
 
 static size_t coalesce(std::vector<HostCopy> & v)
 {
     if (v.size() < 2) return v.size();
-    // side by side: same rows and pitches, each continuing the previous one in both spaces
+    // side by side: same rows and pitches, each continuing the previous one in both spaces (byte
+    // ranges: any widths)
     std::sort(v.begin(), v.end(), [](const HostCopy & a, const HostCopy & b) {
         if (a.sp != b.sp) return a.sp < b.sp;
         if (a.dp != b.dp) return a.dp < b.dp;
@@ -103,11 +105,12 @@ static size_t coalesce(std::vector<HostCopy> & v)
     {
         HostCopy & a = v[k];
         const HostCopy & b = v[i];
+        const bool range = a.sp == 0 && a.dp == 0;
         if (a.sp == b.sp && a.dp == b.dp && a.rows == b.rows && b.src == a.src + (uintptr_t) a.width &&
-            b.dst == a.dst + (uintptr_t) a.width && (a.rows == 1 || a.width + b.width <= std::min(a.sp, a.dp)))
+            b.dst == a.dst + (uintptr_t) a.width && (range || a.rows == 1 || a.width + b.width <= std::min(a.sp, a.dp)))
         {
             a.width += b.width;
-            if (a.rows == 1) { a.sp = std::max(a.sp, a.width); a.dp = std::max(a.dp, a.width); }
+            if (a.rows == 1 && !range) { a.sp = std::max(a.sp, a.width); a.dp = std::max(a.dp, a.width); }
         }
         else v[++k] = b;
     }
@@ -204,13 +207,15 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
         {
             uint8_t * d = dev_ptr(c.dst_alloc, c.dst_off);
             if (!d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
-            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, sp, dp, row_bytes, c.n});
+            const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
+            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n});
         }
         else if (c.kind == XKB_COPY_D2H)
         {
             const uint8_t * s = dev_ptr(c.src_alloc, c.src_off);
             if (!s) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
-            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, sp, dp, row_bytes, c.n});
+            const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
+            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n});
         }
         else { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu has an unknown kind", i); break; }
         hkind = c.kind;

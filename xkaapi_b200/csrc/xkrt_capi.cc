@@ -1805,8 +1805,11 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     xkb_runtime * R = RT(runtime);
     if (!R) return;
     R->in_wait = true;
+    const auto w0 = std::chrono::steady_clock::now();
     fail(R, wait_batch(R));
+    const double wb_ms = ms_since(w0);
     bg_finish(R);
+    if (getenv("XKB_TRACE_WAIT")) fprintf(stderr, "xkrt_task_wait: %.1f ms in all, %.1f ms to finish\n", wb_ms, ms_since(w0) - wb_ms);
     R->last_h2d = R->cur_h2d; R->last_d2h = R->cur_d2h; R->last_h2d_bytes = R->cur_h2d_bytes; R->last_d2h_bytes = R->cur_d2h_bytes;
     R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = 0;
     R->in_wait = false;
