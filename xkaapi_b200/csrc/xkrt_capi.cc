@@ -636,6 +636,12 @@ extern "C" int xkb_runtime_last_wait(xkrt_runtime_t * runtime, uint64_t * tasks,
 
 static void bg_hand_over(xkb_runtime * R, bool final);
 
+static inline void copy64(void * dst, const void * src)
+{
+    struct B64 { unsigned char b[64]; };
+    *(B64 *) dst = *(const B64 *) src;
+}
+
 static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
                   const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
 {
@@ -653,16 +659,21 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
     t.acc_off = R->acc_pool.size();
     t.func = func; t.user_data = ud;
     const size_t args_end = args_size ? t.args_off + args_size : R->args_pool.size();
-    if (!R->args_pool.resize(args_end) || !R->acc_pool.append(acc, nacc) || !R->pending.push_back(t))
+    if (!R->args_pool.resize(args_end) || !R->acc_pool.resize(t.acc_off + nacc) || !R->pending.push_back(t))
     {
         fail(R, xkb_set_error(XKB_ENOMEM, "spawn: out of host memory"));
         return;
     }
-    if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
+    for (size_t k = 0; k < nacc; ++k) R->acc_pool[t.acc_off + k] = acc[k];
+    if (args_size == sizeof(xkb_task_desc_t)) copy64(R->args_pool.data() + t.args_off, args);   // a descriptor: fixed-size copy
+    else if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
     const size_t nt = R->pending.size();
     if (args_size != sizeof(xkb_task_desc_t) || t.args_off != (nt - 1) * sizeof(xkb_task_desc_t)) R->args_dense = false;
     if ((nt & 4095) == 0 && R->prefaulter[0].joinable()) R->pf_want.store(nt + PREFAULT_AHEAD, std::memory_order_relaxed);
-    if (R->bg) bg_hand_over(R, false);
+    // hand over once a batch's worth of accesses is spawned (the same test as bg_hand_over's,
+    // inlined: the spawn loop runs it every time)
+    if (R->bg && R->acc_pool.size() - R->handed_acc >= (R->handed ? R->chunk : std::max<size_t>(16, R->chunk / 32)))
+        bg_hand_over(R, false);
 }
 
 extern "C" void xkrt_task_spawn_generic(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
