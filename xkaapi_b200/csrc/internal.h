@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <thread>
+
 #include "../../include/xkrt_b200.h"
 
 // Launch one task descriptor as its own kernel (the plain per-task form) on `stream`.
@@ -25,6 +28,16 @@ static inline bool xkb_internal_task_valid(const xkb_task_desc_t & d)
         return a.lo >= 0 && a.lo <= a.hi && (a.hi == a.lo || (a.x && a.y));
     }
     return d.kind == XKB_TASK_NOOP;
+}
+
+// Host threads for the parallel passes of background work (resolution, coherency, descriptor
+// translation): XKB_HELPERS, else the hardware threads minus four (the spawning thread, the
+// worker and the page-fault helpers keep theirs), between 1 and 16.
+static inline unsigned xkb_internal_helpers()
+{
+    if (const char * e = getenv("XKB_HELPERS")) { const int v = atoi(e); if (v > 0) return v < 64 ? (unsigned) v : 64u; }
+    const unsigned hw = std::thread::hardware_concurrency();
+    return hw > 5 ? (hw - 4 < 16 ? hw - 4 : 16) : 1;
 }
 
 // Reset a resolver to no tasks, keeping its device buffers for the next graph.

@@ -1236,8 +1236,7 @@ int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops)
     if (nops == 0) return XKB_OK;
     if (!R->pool)
     {
-        const unsigned hw = std::thread::hardware_concurrency();
-        R->pool.reset(new (std::nothrow) WorkPool(std::min(16u, std::max(1u, hw))));
+        R->pool.reset(new (std::nothrow) WorkPool(xkb_internal_helpers()));
     }
     size_t cap = 1024;
     while (cap < 4 * nops) cap *= 2;
@@ -1281,8 +1280,7 @@ extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * rec
     if (n == 0) return XKB_OK;
     if (!R->pool)
     {
-        const unsigned hw = std::thread::hardware_concurrency();
-        R->pool.reset(new (std::nothrow) WorkPool(std::min(16u, std::max(1u, hw))));
+        R->pool.reset(new (std::nothrow) WorkPool(xkb_internal_helpers()));
     }
     int rc = validate(R, recs, n, R->ntasks);
     if (rc) return rc;

@@ -967,8 +967,7 @@ constexpr uint8_t REC_NONE = 0xff;                     // record type of an untr
 template <typename F>
 static void parallel_chunks(size_t n, F fn)
 {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nth = std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536));
+    const size_t nth = std::min<size_t>(xkb_internal_helpers(), n / 65536);
     if (nth < 2) { fn(0, n); return; }
     std::vector<std::thread> pool;
     for (size_t k = 1; k < nth; ++k) pool.emplace_back(fn, n * k / nth, n * (k + 1) / nth);
@@ -982,8 +981,7 @@ static void parallel_chunks(size_t n, F fn)
 template <typename Keep>
 static std::vector<uint32_t> distinct_records(const xkb_access_rec_t * recs, size_t n, Keep keep)
 {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nth = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536)));
+    const size_t nth = std::max<size_t>(1, std::min<size_t>(xkb_internal_helpers(), n / 65536));
     std::vector<std::vector<uint32_t>> firsts(nth);
     auto scan = [&](size_t k) {
         RecordSet seen;
@@ -1012,8 +1010,7 @@ static size_t add_distinct(xkb_runtime * R, size_t a0, size_t a1)
 {
     const xkb_access_rec_t * recs = R->recs.data();
     const size_t start = R->dfirst.size(), n = a1 - a0;
-    const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nth = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, std::min<size_t>(16, n / 65536)));
+    const size_t nth = std::max<size_t>(1, std::min<size_t>(xkb_internal_helpers(), n / 65536));
     std::vector<std::vector<uint32_t>> firsts(nth);
     const RecordSet & known = R->dset;
     auto scan = [&](size_t k) {
