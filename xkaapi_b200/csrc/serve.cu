@@ -28,6 +28,16 @@
 #include <tuple>
 #include <vector>
 
+
+#ifndef XKB_SERVE_TEAM
+#define XKB_SERVE_TEAM 1                 // warps per tile task of a served graph
+#endif
+#ifndef XKB_SERVE_PFD
+#define XKB_SERVE_PFD 4                  // L2 prefetch distance (columns) of a served graph
+#endif
+#ifndef XKB_SERVE_TASKS_PER_CTA
+#define XKB_SERVE_TASKS_PER_CTA 2        // a graph gets one CTA per this many tasks of a step
+#endif
 namespace {
 
 // ---- best-fit arena -------------------------------------------------------------------------
@@ -217,9 +227,12 @@ extern "C" int xkb_server_create(xkb_server_t ** out, const xkb_server_cfg_t * c
         XKB_CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
         int rc;
         if ((rc = xkb_sched_create(&sl.sch, sl.stream))) return rc;
-        // two warps per tile and an 8-column L2 prefetch: with many graphs side by side and a
-        // CTA budget per graph from its width, this sharing of the SMs measured best
-        if ((rc = xkb_sched_set_team(sl.sch, 2)) || (rc = xkb_sched_set_prefetch(sl.sch, 8))) return rc;
+        // warps per tile and L2 prefetch distance for many graphs side by side, each with a CTA
+        // budget from its width (one warp per tile, 4 columns ahead, a CTA per two tasks of a
+        // step: 3.1 TB/s capacity and p99 155 ms at 80 % load on 1000 graphs; two warps per tile
+        // and 8 columns ahead: 1.9 TB/s; a CTA per four or eight tasks: higher closed-loop
+        // capacity that the open-loop trace then overloads)
+        if ((rc = xkb_sched_set_team(sl.sch, XKB_SERVE_TEAM)) || (rc = xkb_sched_set_prefetch(sl.sch, XKB_SERVE_PFD))) return rc;
     }
     int sms = 148, per = 2;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->dev);
@@ -262,7 +275,7 @@ static int launch_request(xkb_server * S, Slot & sl, xkb_request_t & q, uint8_t 
         heat_descs(s, 2, (uint64_t) a, (uint64_t) b, q.c, d);
         if ((rc = xkb_sched_set_tasks(sl.sch, d.data(), d.size()))) return rc;
         // a small graph cannot use many CTAs; leave the SMs to the requests beside it
-        int ctas = (int) std::min<uint64_t>((uint64_t) S->max_ctas, std::max<uint64_t>(4, w->per_step / 2));
+        int ctas = (int) std::min<uint64_t>((uint64_t) S->max_ctas, std::max<uint64_t>(4, w->per_step / XKB_SERVE_TASKS_PER_CTA));
         if ((rc = xkb_sched_set_grid(sl.sch, ctas))) return rc;
     }
     if (q.f32) init_grid_kernel<float><<<1184, 256, 0, sl.stream>>>((float *) a, (float *) b, q.nx, q.ny, q.seed);
