@@ -62,7 +62,11 @@ XKB_API const char * xkb_version(void);
  *  segment: byte interval [addr, ld)  -- access_t's segment constructor (access.hpp:479-514)
  *  handle : addr = the handle (an opaque pointer naming an object, not memory) -- access_t's
  *           handle constructor; resolved like the reference's DependencyMap
- *           (include/xkrt/memory/access/handle/dependency-map.hpp), sequential accesses */
+ *           (include/xkrt/memory/access/handle/dependency-map.hpp)
+ *  reserved: bits 8-15 = the access's concurrency (xkrt_access_concurrency_t: 0 or 1 sequential,
+ *           2 commutative, 4 concurrent); bits 0-7 are ignored by the resolver. The resolver
+ *           takes sequential and commutative accesses (ordered alike, as in the reference); a
+ *           stream with concurrent handle accesses goes through xkb_handle_map_expand first. */
 typedef struct xkb_access_rec_t {
     uint32_t task;
     uint8_t  type;
@@ -108,6 +112,28 @@ XKB_API int xkb_resolver_destroy(xkb_resolver_t * resolver);
  * thread_t::resolve (include/xkrt/thread/thread.h:264-271) -> task_dependency_resolve
  * (src/task/task.cc:285-299). */
 XKB_API int xkb_resolver_add(xkb_resolver_t * resolver, const xkb_access_rec_t * accesses, size_t naccesses);
+
+/* Concurrent-mode handle accesses (ACCESS_CONCURRENCY_CONCURRENT), ordered as the reference's
+ * DependencyMap orders them (include/xkrt/memory/access/handle/dependency-map.hpp:157-297): a
+ * concurrent write depends on the last sequential write only, the next sequential access waits
+ * for all the concurrent writes, and where the reference inserts an extra empty writer task
+ * (insert_empty_write, :93-137) the expanded stream has one. xkb_handle_map_expand rewrites
+ * records (tasks dense, in spawn order, continuing across calls like xkb_resolver_add) into a
+ * stream the resolver takes: each extra task is a task of its own, numbered just before the task
+ * whose access needed it (one handle access, mode VW), later tasks renumbered after it (task id
+ * + extra tasks so far), and each concurrent write of a handle becomes a read of it. `out` needs
+ * naccesses + (handle accesses) records at most (XKB_ERANGE if `cap` is smaller); *nout
+ * receives the count. XKB_EINVAL for a concurrent access to a segment or matrix (the reference
+ * asserts these sequential or commutative, access.hpp:500-502), and for the two forms whose
+ * reference order no point-wise state expresses: a task listing a handle again after an access
+ * that needs an extra writer, and a concurrent read-only access while concurrent writes of
+ * earlier tasks are pending. After an error the map holds the state of the tasks before the
+ * failing one. */
+typedef struct xkb_handle_map xkb_handle_map_t;
+XKB_API int xkb_handle_map_create(xkb_handle_map_t ** map);
+XKB_API int xkb_handle_map_destroy(xkb_handle_map_t * map);
+XKB_API int xkb_handle_map_expand(xkb_handle_map_t * map, const xkb_access_rec_t * in, size_t naccesses,
+                                  xkb_access_rec_t * out, size_t cap, size_t * nout);
 
 /* Build (if needed) and return the successor CSR of every task added so far. */
 XKB_API int xkb_resolver_graph(xkb_resolver_t * resolver, xkb_task_graph_t * graph);

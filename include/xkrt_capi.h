@@ -16,9 +16,14 @@
  * as soon as they are resolved while every task so far is one; otherwise, at xkrt_task_wait, as
  * a dataflow graph on a team of host threads, each with its own CUDA stream. xkrt_task_wait
  * returns when every task completed and host memory is coherent again. Handle accesses order tasks like the
- * reference's DependencyMap (they carry no data); concurrent-mode accesses and user moldable
- * tasks are not supported. Functions that return void in the reference record failures
- * instead; read them with xkb_runtime_status().
+ * reference's DependencyMap (they carry no data), concurrent-mode ones included: where the
+ * reference's map inserts an extra empty writer task (dependency-map.hpp:93-137) the batch gets
+ * one, a host task with no body spawned just before the task that needed it (it counts among
+ * the batch's tasks). Two rare forms are ordered at least as strictly as the reference, not edge
+ * for edge (xkb_handle_map_expand in xkrt_b200.h names them). Concurrent mode on a segment or
+ * matrix access is rejected (XKB_EINVAL; the reference asserts it away) and user moldable tasks
+ * are not supported. Functions that return void in the reference record failures instead; read
+ * them with xkb_runtime_status().
  */
 #ifndef XKRT_B200_CAPI_H
 #define XKRT_B200_CAPI_H

@@ -19,11 +19,15 @@
 //               else if writer: edge writer -> A.
 //      PUT(A):  if (A.mode & W): writer = A, readers = {}; else if A.mode == R exactly:
 //               readers += A.
-//  * handles (include/xkrt/memory/access/handle/dependency-map.hpp:157-297): a map from handle
-//    to {last writer, readers}, one point per handle in its own domain, the same LINK, and PUT
-//    recording every mode with the R bit and without the W bit as a reader (sequential and
-//    commutative accesses; the concurrent mode's extra nodes are not restated).
-//  The reference stores the state on tree nodes; its edges are the union of the per-point
+//  * handles (include/xkrt/memory/access/handle/dependency-map.hpp:57-335): the map itself,
+//    handle -> {sequential reads, concurrent writes, last sequential write}, with its LINK
+//    (:186-297) and PUT (:300-332) for every concurrency (record field `reserved` >> 8:
+//    0/1 sequential, 2 commutative, 4 concurrent), including the extra empty writer task that
+//    LINK inserts before a concurrent write after sequential reads, or before a read after
+//    concurrent writes (insert_empty_write, :93-137). An extra task is numbered in creation
+//    order: just before the task whose LINK pass created it, every later task renumbered after
+//    it. No task completes, so no list entry is ever popped and every extra task is kept.
+//  The reference stores the tree state on nodes; its edges are the union of the per-point
 //  edges, so this oracle keeps the state per elementary cell of the domain's coordinate
 //  compression and reports the unique (pred task, succ task) pairs.
 //
@@ -34,6 +38,7 @@
 #include <cstdio>
 #include <map>
 #include <string>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -83,12 +88,6 @@ static void add_ops(Domain & d, bool link, const xk_stream_rec_t & r)
 {
     Rect rects[3];
     int n;
-    if (r.type == XK_STREAM_HANDLE)
-    {
-        const uint8_t m = ((r.mode & MODE_R) && !(r.mode & MODE_W)) ? MODE_R : r.mode;
-        d.ops.push_back({link, r.task, m, Rect{r.addr, r.addr + 1, 0, 1}});
-        return;
-    }
     if (d.interval) { rects[0] = {r.addr, r.ld, 0, 1}; n = 1; }
     else if (r.type == XK_STREAM_SEGMENT) n = segment_rects(r.addr, r.ld, d.ld, d.s, rects);
     else n = matrix_rects(r, rects);
@@ -144,6 +143,58 @@ static void run_domain(const Domain & d, std::vector<std::pair<uint32_t, uint32_
     }
 }
 
+// The handle map, restated with its lists (dependency-map.hpp:57-335). Task ids here are virtual:
+// a stream task keeps its id, extra task k is EXTRA + k; main() renumbers at the end.
+constexpr uint32_t EXTRA = 0x80000000u;
+constexpr int CONCURRENT = 4;
+
+struct HandleMap {
+    struct Node { std::vector<uint32_t> seq_reads, conc_writes; int64_t last_seq_write = -1; };
+    std::unordered_map<uint64_t, Node> map;
+    std::vector<uint32_t> extra_owner;          // per extra task: the stream task whose LINK created it
+    std::vector<std::pair<uint32_t, uint32_t>> edges;
+
+    void link(uint64_t h, uint8_t mode, int conc, uint32_t task, uint32_t owner)
+    {
+        auto it = map.find(h);
+        if (it == map.end()) return;
+        Node & node = it->second;               // stays valid: unordered_map never moves its nodes
+        bool transitive = false;
+        if (!node.seq_reads.empty() && (mode & MODE_W))
+        {
+            if (conc == CONCURRENT) insert_empty_write(h, owner);
+            else { for (uint32_t p : node.seq_reads) edges.emplace_back(p, task); transitive = true; }
+        }
+        if (!node.conc_writes.empty() && conc != CONCURRENT)
+        {
+            if (mode & MODE_W) { for (uint32_t p : node.conc_writes) edges.emplace_back(p, task); transitive = true; }
+            else insert_empty_write(h, owner);
+        }
+        if (node.last_seq_write >= 0 && !transitive) edges.emplace_back((uint32_t) node.last_seq_write, task);
+    }
+
+    void put(uint64_t h, uint8_t mode, int conc, uint32_t task)
+    {
+        Node & node = map[h];
+        if (mode & MODE_W)
+        {
+            if (conc == CONCURRENT) node.conc_writes.push_back(task);
+            else { node.seq_reads.clear(); node.conc_writes.clear(); node.last_seq_write = task; }
+        }
+        else if (mode & MODE_R) { node.conc_writes.clear(); node.seq_reads.push_back(task); }
+    }
+
+    // An empty task with one sequential VW access of h, linked and put at once; it always has a
+    // predecessor here (the non-empty list that called for it), so it is always put.
+    void insert_empty_write(uint64_t h, uint32_t owner)
+    {
+        const uint32_t e = EXTRA + (uint32_t) extra_owner.size();
+        extra_owner.push_back(owner);
+        link(h, MODE_W | 4, 1, e, owner);
+        put(h, MODE_W | 4, 1, e);
+    }
+};
+
 } // namespace
 
 int main(int argc, char ** argv)
@@ -155,7 +206,7 @@ int main(int argc, char ** argv)
 
     // Build every domain's op sequence in the order the reference performs them.
     Domain interval{true, 0, 0, {}};
-    Domain handles{true, 0, 0, {}};
+    HandleMap handles;
     std::vector<Domain> blas;
     std::map<std::pair<uint64_t, uint64_t>, size_t> blas_index;
     std::vector<size_t> segments_so_far;   // indices into recs, spawn order
@@ -168,7 +219,7 @@ int main(int argc, char ** argv)
         for (size_t a = i; a < j; ++a)   // LINK pass
         {
             const auto & r = recs[a];
-            if (r.type == XK_STREAM_HANDLE) add_ops(handles, true, r);
+            if (r.type == XK_STREAM_HANDLE) handles.link(r.addr, r.mode, r.reserved >> 8, r.task, r.task);
             else if (r.type == XK_STREAM_SEGMENT)
             {
                 add_ops(interval, true, r);
@@ -192,7 +243,7 @@ int main(int argc, char ** argv)
         for (size_t a = i; a < j; ++a)   // PUT pass
         {
             const auto & r = recs[a];
-            if (r.type == XK_STREAM_HANDLE) add_ops(handles, false, r);
+            if (r.type == XK_STREAM_HANDLE) handles.put(r.addr, r.mode, r.reserved >> 8, r.task);
             else if (r.type == XK_STREAM_SEGMENT)
             {
                 add_ops(interval, false, r);
@@ -207,8 +258,22 @@ int main(int argc, char ** argv)
 
     std::vector<std::pair<uint32_t, uint32_t>> edges;
     run_domain(interval, edges);
-    run_domain(handles, edges);
     for (auto & d : blas) run_domain(d, edges);
+    edges.insert(edges.end(), handles.edges.begin(), handles.edges.end());
+    // final ids: stream task t -> t + (extra tasks created up to its own LINK pass);
+    // extra task k, created in task o's LINK pass -> o + k
+    const size_t nextra = handles.extra_owner.size();
+    if (nextra)
+    {
+        std::vector<uint32_t> shift(ntasks, 0);
+        for (uint32_t o : handles.extra_owner) ++shift[o];
+        for (size_t t = 1; t < ntasks; ++t) shift[t] += shift[t - 1];
+        auto final_id = [&](uint32_t v) {
+            return v >= EXTRA ? handles.extra_owner[v - EXTRA] + (v - EXTRA) : v + shift[v];
+        };
+        for (auto & e : edges) e = {final_id(e.first), final_id(e.second)};
+        ntasks += nextra;
+    }
     const size_t cell_edges = edges.size();
     std::sort(edges.begin(), edges.end());
     edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
@@ -223,9 +288,9 @@ int main(int argc, char ** argv)
     FILE * f = fopen((pfx + ".edges").c_str(), "wb");
     for (auto & e : edges) { uint32_t v[2] = {e.first, e.second}; fwrite(v, 4, 2, f); }
     fclose(f);
-    printf("{\"ntasks\": %zu, \"naccesses\": %zu, \"cell_edges\": %zu, \"unique_edges\": %zu, "
+    printf("{\"ntasks\": %zu, \"extra_tasks\": %zu, \"naccesses\": %zu, \"cell_edges\": %zu, \"unique_edges\": %zu, "
            "\"max_preds\": %u, \"domains\": %zu, \"resolve_s\": %.6f}\n",
-           ntasks, recs.size(), cell_edges, edges.size(), maxp, blas.size() + (interval.ops.empty() ? 0 : 1),
+           ntasks, nextra, recs.size(), cell_edges, edges.size(), maxp, blas.size() + (interval.ops.empty() ? 0 : 1),
            std::chrono::duration<double>(t1 - t0).count());
     return 0;
 }

@@ -139,11 +139,6 @@ H
 CXX="${XK_ORACLE_CXX:-g++}"   # the g++ on PATH (g++ 13.3); a CXX from the environment may lack C++23 <stdatomic.h>
 CXXFLAGS="-std=c++20 -O2 -DNDEBUG -D_Static_assert=static_assert -include list -w -I$OUT/include -I$OUT/shim -I$REF/api/c/include"
 
-# ---- dependency oracle: reference trees driven by src/task/task.cc --------------------------
-"$CXX" $CXXFLAGS -o "$OUT/ref_deps" \
-    "$HERE/ref_deps.cc" "$HERE/seams.cc" "$REF/src/task/task.cc" "$REF/src/logger/logger.cc" -lpthread
-echo "built $OUT/ref_deps"
-
 # ---- transfer-plan oracle: reference memory tree under the canonical schedule ----------------
 "$CXX" $CXXFLAGS -include array -o "$OUT/ref_plan" \
     "$HERE/ref_plan.cc" "$HERE/seams.cc" "$REF/src/task/task.cc" "$REF/src/logger/logger.cc" -lpthread
@@ -164,6 +159,10 @@ for s in $RT_SRCS; do
     OBJS="$OBJS $o"
 done
 wait
+# ---- dependency oracle: reference trees driven by src/task/task.cc; the runtime's thread
+# sources give the handle map's extra tasks their task stack (thread_t::get_tls)
+"$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_deps" "$HERE/ref_deps.cc" $OBJS -lpthread -ldl
+echo "built $OUT/ref_deps"
 "$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_heat" "$HERE/ref_heat.cc" $OBJS -lpthread -ldl
 echo "built $OUT/ref_heat"
 "$CXX" ${CXXFLAGS/-std=c++20/-std=c++23} -o "$OUT/ref_axpby" "$HERE/ref_axpby.cc" $OBJS -lpthread -ldl

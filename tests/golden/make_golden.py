@@ -79,12 +79,25 @@ def handle_mixed(seed, n=80):
     return np.array(rows, dtype=S.REC)
 
 
+def handle_diagrams():
+    """The handle map's two diagrams on one handle (dependency-map.hpp:200-223, :247-262):
+    W; 4 concurrent W; 3 R (an extra writer before the first); 2 concurrent W (an extra writer
+    before the first); W."""
+    ops = [S.W, "c", "c", "c", "c", S.R, S.R, S.R, "c", "c", S.W]
+    rows = [(t, S.HANDLE, S.W if o == "c" else o, (4 if o == "c" else 1) << 8, 0x5000, 0, 0, 0, 0, 0, 0)
+            for t, o in enumerate(ops)]
+    return np.array(rows, dtype=S.REC)
+
+
 def cases():
     H = 0x5000
     # restates tests/task-dependency-handle.cc:86-119 (W, R, RW on one handle: T0 -> T1 -> T2)
     yield "ref_handle_chain", S.from_tuples([[("h", S.W, H)], [("h", S.R, H)], [("h", S.RW, H)]])
     for seed in range(3):
         yield f"handle_mixed_{seed}", handle_mixed(seed + 50)
+    yield "handle_concurrent_diagrams", handle_diagrams()
+    for seed in range(4):
+        yield f"handle_concurrent_{seed}", S.handle_concurrent_stream(seed + 70)
     X = 0x10000
     yield "ref_interval_chain", S.from_tuples([[("s", S.W, X - 64, X + 64)],
                                               [("s", S.R, X, X + 76)],

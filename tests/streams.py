@@ -112,3 +112,25 @@ def mixed_stream(ntasks, seed, base=1 << 20, span=1 << 14):
                 om = int(rng.integers(0, ld)); on = int(rng.integers(0, 24))
                 rows.append((t, MATRIX, mode, 0, base, ld, om, on, m, n, s))
     return np.array(rows, dtype=REC)
+
+
+def handle_concurrent_stream(seed, n=80):
+    """Handle accesses of every concurrency -- sequential, commutative, concurrent writes (record
+    field `reserved` >> 8 = 1, 2, 4) -- over three handles, one access per handle in a task,
+    mixed with segment accesses; the reference's handle map inserts its extra writer tasks
+    (include/xkrt/memory/access/handle/dependency-map.hpp:93-137), numbered in creation order just
+    before the task that needed them."""
+    rng = np.random.default_rng(seed)
+    modes = [R, W, RW, R | V, W | V]
+    handles = [0x1000, 0x1008, 0x2000]
+    rows = []
+    for t in range(n):
+        order = rng.permutation(len(handles))[: int(rng.integers(1, 3))]
+        for h in order:
+            mode = modes[int(rng.integers(0, len(modes)))]
+            conc = [1, 2, 4, 4][int(rng.integers(0, 4))] if mode & W else [1, 2][int(rng.integers(0, 2))]
+            rows.append((t, HANDLE, mode, conc << 8, handles[h], 0, 0, 0, 0, 0, 0))
+        if rng.random() < 0.3:
+            a = 0x1000 + int(rng.integers(0, 64))
+            rows.append((t, SEGMENT, modes[int(rng.integers(0, 3))], 0, a, a + int(rng.integers(1, 64)), 0, 0, 0, 0, 0))
+    return np.array(rows, dtype=REC)

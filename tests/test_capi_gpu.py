@@ -84,6 +84,16 @@ def test_ordering_programs(torch_cuda, tmp_path):
     assert out["handle_edges"] == 2                    # T6 -> T7 -> T8 on the handle
 
 
+def test_concurrent_handle_program(torch_cuda, tmp_path):
+    """Concurrent writes of a handle: they run after the last sequential write and before the
+    next reads, the handle map's two extra writer tasks run (13 tasks), the 18 edges are the
+    reference's (two diagrams of dependency-map.hpp), and a concurrent segment access is refused."""
+    r = subprocess.run([build("concurrent_capi", tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr + r.stdout
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out == {"x": 482, "ran": 13, "edges": 18, "order": 1, "refused": 1}
+
+
 @pytest.mark.parametrize("every,chunk", [(0, None), (3, None), (0, 64), (3, 64)])
 def test_heat_example(torch_cuda, tmp_path, every, chunk):
     nx, ny, ts, steps = 200, 136, 64, 7

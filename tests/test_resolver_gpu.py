@@ -22,9 +22,28 @@ def gpu_edges(recs, batches=1, seed=0):
     return e
 
 
+def expanded(recs):
+    """Concurrent-mode handle accesses go through the handle map's expansion first."""
+    if not ((recs["reserved"] >> 8) == 4).any():
+        return recs
+    m = xk.HandleMap()
+    out = m.expand(recs)
+    m.close()
+    return out
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_golden_reference_edges(torch_cuda, case):
-    np.testing.assert_array_equal(gpu_edges(GOLDEN[case + "__stream"]), GOLDEN[case + "__edges"])
+    np.testing.assert_array_equal(gpu_edges(expanded(GOLDEN[case + "__stream"])), GOLDEN[case + "__edges"])
+
+
+@pytest.mark.parametrize("seed", range(3))
+@pytest.mark.parametrize("batches", [1, 5])
+def test_concurrent_handle_streams_vs_oracle(torch_cuda, seed, batches):
+    """Longer concurrent-mode handle streams: the GPU resolver on the expanded stream (in batches)
+    against the oracle's restatement of the handle map on the stream as spawned."""
+    recs = S.handle_concurrent_stream(seed + 300, n=3000)
+    np.testing.assert_array_equal(gpu_edges(expanded(recs), batches, seed=seed), U.oracle_edges(recs))
 
 
 @pytest.mark.parametrize("case", ["heat_1024_t128_s3", "microbench_1024_2000", "mixed_segmat_0", "mixed_mat_1"])
@@ -141,6 +160,11 @@ def test_rejects_bad_streams(torch_cuda):
     bad2 = S.from_tuples([[("m", 0, 4096, 64, 0, 0, 8, 8, 8)]])    # mode 0
     with pytest.raises(xk.XkbError):
         r.add(bad2)
+    bad3 = S.from_tuples([[("h", S.W, 4096)]])
+    bad3["reserved"] = 4 << 8                # a concurrent access that was not expanded
+    with pytest.raises(xk.XkbError) as ei:
+        r.add(bad3)
+    assert "xkb_handle_map_expand" in str(ei.value)
     ok = S.from_tuples([[("m", S.W, 4096, 64, 0, 0, 8, 8, 8)], [("m", S.R, 4096, 64, 0, 0, 8, 8, 8)]])
     r.add(ok)
     np.testing.assert_array_equal(r.edges(), [[0, 1]])

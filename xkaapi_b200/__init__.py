@@ -104,6 +104,9 @@ SIGNATURES = {
     "xkb_resolver_periodic": (_int, [_vp, ctypes.c_uint64, ctypes.POINTER(PeriodicGraph)]),
     "xkb_sched_run_periodic": (_int, [_vp, ctypes.POINTER(PeriodicGraph), ctypes.c_uint32, ctypes.c_uint32]),
     "xkb_resolver_destroy": (_int, [_vp]),
+    "xkb_handle_map_create": (_int, [ctypes.POINTER(_vp)]),
+    "xkb_handle_map_destroy": (_int, [_vp]),
+    "xkb_handle_map_expand": (_int, [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
     "xkb_resolver_graph": (_int, [_vp, ctypes.POINTER(TaskGraph)]),
     "xkb_resolver_edges": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
@@ -357,6 +360,36 @@ class Planner:
     def close(self):
         if self._h:
             lib().xkb_planner_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HandleMap:
+    """xkb_handle_map_t (host code: no GPU needed): expands access records holding
+    concurrent-mode handle accesses (record field `reserved` >> 8 == 4) into a stream the
+    resolver takes -- the reference handle map's extra writer tasks inserted, later tasks
+    renumbered, concurrent writes resolved as reads. Keeps its state across calls."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        check(lib().xkb_handle_map_create(ctypes.byref(self._h)))
+
+    def expand(self, recs):
+        import numpy as np
+        recs = np.ascontiguousarray(recs)
+        out = np.zeros(2 * len(recs), dtype=recs.dtype)
+        n = ctypes.c_size_t()
+        check(lib().xkb_handle_map_expand(self._h, recs.ctypes.data, len(recs), out.ctypes.data, len(out), ctypes.byref(n)))
+        return out[:n.value]
+
+    def close(self):
+        if self._h:
+            lib().xkb_handle_map_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -650,6 +650,9 @@ static size_t first_invalid(const xkb_access_rec_t * recs, size_t b, size_t e, u
         const uint32_t prev = i == 0 ? first_task : recs[i - 1].task;
         if (r.task < prev || r.task > prev + 1 || (i == 0 && r.task != first_task)) { *why = "task ids must be dense, in spawn order"; return i; }
         if (r.mode == 0 || (r.mode & ~15u)) { *why = "bad mode"; return i; }
+        const unsigned conc = r.reserved >> 8;      // sequential (0, 1) or commutative (2)
+        if (conc == 4) { *why = "a concurrent access: expand the stream with xkb_handle_map_expand first"; return i; }
+        if (conc > 2) { *why = "bad concurrency"; return i; }
         if (r.type == XKB_ACCESS_TYPE_SEGMENT) {
             if (r.ld <= r.addr) { *why = "empty segment"; return i; }
         } else if (r.type == XKB_ACCESS_TYPE_BLAS_MATRIX) {

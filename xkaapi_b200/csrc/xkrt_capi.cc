@@ -12,6 +12,7 @@
 // threads. Host memory is coherent again when xkrt_task_wait returns.
 #include "capi_objects.h"
 #include "common.cuh"
+#include "handles.h"
 #include "internal.h"
 #include "pool.h"
 #include "../../include/xkrt_capi.h"
@@ -200,6 +201,9 @@ struct xkb_runtime {
     bool stream_on = true;                            // XKB_STREAM=0 turns streaming off
     xkb_edge_mark_t rest_mark{};                      // edge mark at task `streamed` once streaming stopped
     RecordSet dset;                                   // distinct records of the batch made coherent so far
+    xkb_handles::Map hmap;                            // handle states of the batch (concurrent-mode accesses)
+    std::vector<xkb_handles::Access> hacc;            //   a spawn's handle accesses
+    std::vector<uint64_t> hextra;                     //   handles that get an extra writer task before it
     std::vector<uint32_t> dfirst;                     //   their first occurrences, in record order
     uint64_t cur_h2d = 0, cur_d2h = 0, cur_h2d_bytes = 0, cur_d2h_bytes = 0;   // copies of the batch in progress
     // page-locked descriptor slots of streamed windows (a slot is reused once its copy is done)
@@ -642,16 +646,50 @@ static inline void copy64(void * dst, const void * src)
     *(B64 *) dst = *(const B64 *) src;
 }
 
+static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
+                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud);
+
 static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
                   const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
 {
     if (!R) return;
     if (nacc && !acc) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null accesses")); return; }
+    bool handles = false;
     for (size_t i = 0; i < nacc; ++i)
-        if (acc[i].concurrency == ACCESS_CONCURRENCY_CONCURRENT)
-        { fail(R, xkb_set_error(XKB_EINVAL, "spawn: concurrent accesses are not supported")); return; }
+    {
+        if (acc[i].type == ACCESS_TYPE_HANDLE) handles = true;
+        else if (acc[i].concurrency == ACCESS_CONCURRENCY_CONCURRENT)    // asserted away in access.hpp:500-502
+        { fail(R, xkb_set_error(XKB_EINVAL, "spawn: concurrent mode applies to handle accesses only")); return; }
+    }
     if (args_size && !args) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null arguments")); return; }
     if (R->in_wait) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: spawning from a task body during xkrt_task_wait is not supported")); return; }
+    if (handles)
+    {
+        // the handle map's extra empty writer tasks go first, each with one sequential VW access
+        // of its handle (dependency-map.hpp:93-137)
+        R->hacc.clear(); R->hextra.clear();
+        for (size_t i = 0; i < nacc; ++i)
+            if (acc[i].type == ACCESS_TYPE_HANDLE)
+                R->hacc.push_back({(uint64_t) (uintptr_t) acc[i].region.handle.addr, (uint8_t) acc[i].mode, (int) acc[i].concurrency});
+        const char * why = "";
+        if (R->hmap.task(R->hacc.data(), R->hacc.size(), false, R->hextra, &why))
+        { fail(R, xkb_set_error(XKB_EINVAL, "spawn: %s", why)); return; }
+        for (uint64_t h : R->hextra)
+        {
+            xkrt_access_t e;
+            memset(&e, 0, sizeof(e));
+            e.concurrency = ACCESS_CONCURRENCY_SEQUENTIAL; e.mode = ACCESS_MODE_VW; e.scope = ACCESS_SCOPE_NONUNIFIED;
+            e.type = ACCESS_TYPE_HANDLE; e.region.handle.addr = (void *) (uintptr_t) h;
+            spawn_task(R, HOST_DEVICE_GLOBAL_ID, 0, XKRT_TASK_FORMAT_NULL, nullptr, 0, &e, 1, nullptr, nullptr);
+        }
+    }
+    spawn_task(R, device, flags, fmtid, args, args_size, acc, nacc, func, ud);
+}
+
+// Append one task to the batch (arguments already checked).
+static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
+                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
+{
     Task t;
     t.rt = R; t.fmtid = fmtid; t.flags = flags; t.device = device;
     t.nargs = (uint32_t) args_size; t.nacc = (uint32_t) nacc;
@@ -853,6 +891,8 @@ static bool to_rec(const xkrt_access_t & a, uint32_t task, xkb_access_rec_t & r)
     r.mode = (uint8_t) a.mode;
     if (a.type == ACCESS_TYPE_HANDLE)
     {
+        // a concurrent write of a handle is resolved as a read of it (handles.h)
+        r.mode = xkb_handles::resolve_mode(r.mode, (int) a.concurrency);
         r.type = XKB_ACCESS_TYPE_HANDLE; r.addr = (uint64_t) a.region.handle.addr;
         return r.addr != ~0ull;
     }
@@ -1313,6 +1353,7 @@ static void bg_finish(xkb_runtime * R)
     R->stream_ok = true;
     R->dset.reset();
     R->dfirst.clear();
+    R->hmap.clear();                      // every task of the batch completed: no handle orders anything
     R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
 }
 
