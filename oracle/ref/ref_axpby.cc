@@ -108,6 +108,9 @@ int main(int argc, char ** argv)
     printf("{\"tasks\": %zu, \"seconds\": %.6f, \"tasks_per_s\": %.1f, \"checksum\": %.17g}\n", plan.size(), secs,
            plan.size() / secs, checksum);
     fflush(stdout);
-    runtime.deinit();
-    return 0;
+    // The result is out; the process ends here instead of in runtime.deinit(): the reference's
+    // thread_t destructor frees memory_stack_ptr, not memory_stack_bottom
+    // (include/xkrt/thread/thread.h:211-214), a pointer into the middle of its task stack once a
+    // task was allocated, and glibc then aborts or crashes depending on the bytes before it.
+    std::_Exit(0);
 }
