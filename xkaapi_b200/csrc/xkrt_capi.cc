@@ -1460,6 +1460,13 @@ static void task_completed(::xkb_runtime * R, Task & T)
 static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_access_rec_t * recs, size_t base)
 {
     const size_t nt = R->pending.size() - base;
+    // the replicas the bodies read (xkrt_task_access_replica): set as each task's accesses are
+    // made coherent, null until then; only tasks run here have bodies that read them
+    if (nt)
+    {
+        const size_t a0 = R->pending[base].acc_off;
+        memset(R->replica_pool.data() + a0, 0, (R->acc_pool.size() - a0) * sizeof(void *));
+    }
     Dataflow D;
     D.base = base;
     D.nt = nt;
@@ -1715,7 +1722,6 @@ static int wait_batch(xkb_runtime * R)
         if (R->streamed) xkb_internal_sched_windows_wait(R->sched, nullptr);      // nothing left running
         return rc;
     }
-    if (nacc) memset(R->replica_pool.data(), 0, nacc * sizeof(void *));
     xkb_access_rec_t * recs = R->recs.data();
     const double records_ms = ms_since(t0);
     // tasks [P, ntasks) still to run; [0, P) were streamed to the GPU during the spawns
