@@ -17,7 +17,8 @@
 //    (blas/dependency-tree.hpp:295-355);
 //  * handles: one DependencyMap per domain task (src/task/task.cc:226-236), a point per handle
 //    with the same LINK/PUT except that any mode with R and without W is recorded as a reader
-//    (handle/dependency-map.hpp:157-297; sequential and commutative accesses).
+//    (handle/dependency-map.hpp:157-297; sequential and commutative accesses -- a stream with
+//    concurrent ones is expanded first by xkb_handle_map_expand, handles.h).
 //
 // Method (B200): the host turns the accesses of a batch into each domain's ordered op list
 // and keeps a coordinate compression of the domain (elementary cells between all rect
