@@ -272,7 +272,7 @@ XKB_API int xkb_sched_destroy(xkb_sched_t * sched);
 /* Host array of task descriptors, in spawn order (task i of the graph = tasks[i]); copied. */
 XKB_API int xkb_sched_set_tasks(xkb_sched_t * sched, const xkb_task_desc_t * tasks, size_t ntasks);
 /* Longest time a persistent CTA waits for its next queue slot before it gives up and reports
- * XKB_ETIMEDOUT (default 10 s). */
+ * XKB_ETIMEDOUT (default 10 s; finite, above 0 and at most 3600 s, else XKB_EINVAL). */
 XKB_API int xkb_sched_set_timeout(xkb_sched_t * sched, double seconds);
 /* CTAs of the persistent kernel (default: SMs x resident CTAs per SM). */
 XKB_API int xkb_sched_set_grid(xkb_sched_t * sched, int ctas);
@@ -287,7 +287,7 @@ XKB_API int xkb_sched_set_staging(xkb_sched_t * sched, int bulk);
  * of 8 warps runs 8 / warps_per_task tasks at a time, each team taking and releasing tasks on
  * its own. */
 XKB_API int xkb_sched_set_team(xkb_sched_t * sched, int warps_per_task);
-/* Distance, in columns, of the L2 bulk prefetch ahead of a heat tile's sweep (0 = off; default 8). */
+/* Distance, in columns, of the L2 bulk prefetch ahead of a heat tile's sweep (0 = off; default 4). */
 XKB_API int xkb_sched_set_prefetch(xkb_sched_t * sched, int columns);
 /* Enqueue one execution of the whole graph on the scheduler's stream (asynchronous). */
 XKB_API int xkb_sched_run(xkb_sched_t * sched, const xkb_task_graph_t * graph, int form);
@@ -314,10 +314,22 @@ XKB_API int xkb_sched_run_periodic(xkb_sched_t * sched, const xkb_periodic_graph
  * loads it, held until the process exits), so a graph may have at most XKB_NOALLOC_MAX_TASKS
  * tasks; larger graphs get XKB_ERANGE. `tasks` is a DEVICE array of descriptors, `graph` the
  * resolver's device CSR. The call waits for the run to finish and returns XKB_ETIMEDOUT if a
- * device wait gave up after timeout_s seconds; *executed (optional) = tasks run. The first call
- * on each device looks up the array's device address (do it before any stream capture). Every
- * call shares the array: calls whose runs overlap on the GPU (other streams, other host
- * threads) race and must be serialised by the caller. */
+ * device wait gave up after timeout_s seconds (finite, above 0, at most 3600 s); *executed
+ * (optional) = tasks run.
+ *
+ * Set-up: the array and the kernels are device memory that the CUDA driver creates when the
+ * library's module is first used on a device (modules load lazily), and the first call in each
+ * CUDA context looks up the array's device address. Make one call with an empty graph
+ * (ntasks = 0, tasks may be null) on each device before reserving device memory for other uses
+ * and before any stream capture: it loads the module, the array and the kernels, so later
+ * calls need no device memory at all.
+ *
+ * Descriptors are checked on the device before anything runs (the checks of
+ * xkb_sched_set_tasks): a bad one returns XKB_EINVAL and no task runs. The successor CSR is
+ * trusted: successor ids at or beyond ntasks are skipped, but wrong wait counts make the run
+ * wait until timeout_s and return XKB_ETIMEDOUT. Every call shares the array: calls whose runs
+ * overlap on the GPU (other streams, other host threads) race and must be serialised by the
+ * caller. */
 #define XKB_NOALLOC_MAX_TASKS (1u << 20)
 XKB_API int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_task_graph_t * graph, int warps_per_task,
                                   double timeout_s, void * stream, uint64_t * executed);

@@ -14,8 +14,16 @@ int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream);
 // checked: the caller validated every descriptor with xkb_internal_task_valid.
 int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks, bool checked);
 
+#ifdef __CUDACC__
+#define XKB_HD __host__ __device__
+#else
+#define XKB_HD
+#endif
+
 // The descriptor checks of xkb_sched_set_tasks: a known kind with a well-formed tile or range.
-static inline bool xkb_internal_task_valid(const xkb_task_desc_t & d)
+// (Heat tile bodies clip their tile to the grid's interior, so a tile beyond nx/ny is harmless
+// once ld >= nx.) Also evaluated on the device by xkb_sched_run_noalloc.
+static inline XKB_HD bool xkb_internal_task_valid(const xkb_task_desc_t & d)
 {
     if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
     {

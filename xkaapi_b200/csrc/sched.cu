@@ -22,6 +22,10 @@
 #include "heat_bulk.cuh"
 #include "internal.h"
 
+#include <cuda.h>
+
+#include <cmath>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -70,6 +74,11 @@ constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (b
 #ifndef XKB_SCHED_MINB
 #define XKB_SCHED_MINB 2                 // persistent CTAs resident per SM (register budget)
 #endif
+constexpr int SCHED_PFD_DEFAULT = 4;     // L2 prefetch distance of heat tiles in columns (3-5 measured best)
+constexpr double SCHED_TIMEOUT_MAX_S = 3600.0;   // longest device wait a caller may ask for
+
+// A device wait limit in seconds is usable when finite, positive and at most an hour.
+static inline bool timeout_ok(double s) { return std::isfinite(s) && s > 0 && s <= SCHED_TIMEOUT_MAX_S; }
 
 // Run one task with a team of `nwarps` warps; `warp` is the warp's index in the team.
 __device__ __forceinline__ void run_task_team(const xkb_task_desc_t & d, int warp, int nwarps, int pfd)
@@ -140,6 +149,7 @@ __global__ void sched_seed_kernel(SchedArgs a)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.ntasks) return;
+    if (*(volatile unsigned *) (a.ctr + 2) != 0) return;   // a check before the run failed: nothing becomes ready
     const uint32_t w = t / a.period, l = t - w * a.period;
     if ((w == 0 ? a.npred_first[l] : a.npred_next[l]) != 0) return;
     const unsigned pos = atomicAdd(a.ctr + 1, 1u);
@@ -349,7 +359,7 @@ struct xkb_sched {
     int grid = 0;
     int team_warps = 1;                       // one warp per 128-row tile (FP64 and FP32 bodies)
     int bulk = 0;                             // 1: bulk-staged heat tile body (measured slower; opt-in)
-    int pfd = 4;                              // L2 prefetch distance in columns (3-5 measured best)
+    int pfd = SCHED_PFD_DEFAULT;              // L2 prefetch distance in columns
     uint64_t last_total = 0;                  // tasks of the last run
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the persistent kernel of the last run
     uint64_t timeout_ns = 10ull * 1000 * 1000 * 1000;
@@ -434,7 +444,7 @@ int xkb_internal_sched_set_tasks_device(xkb_sched_t * S, const xkb_task_desc_t *
 
 extern "C" int xkb_sched_set_timeout(xkb_sched_t * S, double seconds)
 {
-    if (!S || !(seconds > 0)) return xkb_set_error(XKB_EINVAL, "sched_set_timeout: bad arguments");
+    if (!S || !timeout_ok(seconds)) return xkb_set_error(XKB_EINVAL, "sched_set_timeout: the limit must be finite, above 0 and at most 3600 s");
     S->timeout_ns = (uint64_t) (seconds * 1e9);
     return XKB_OK;
 }
@@ -747,34 +757,85 @@ extern "C" int xkb_sched_kernel_ms(xkb_sched_t * S, double * ms)
 // scheduler's working set -- wait counters, queue slots and four counters -- in the file-scope
 // array below instead, sized for at most XKB_NOALLOC_MAX_TASKS tasks (8 MiB + 256 B held by
 // every GPU that loads the library, until the process exits).
-static __device__ __align__(256) int g_sched_noalloc_scratch[2 * XKB_NOALLOC_MAX_TASKS + 64];
+static __device__ __align__(256) int g_sched_noalloc_scratch[2 * XKB_NOALLOC_MAX_TASKS + 64];   // + counters
 
-// Device address of the scratch array for the current device. In host code the array's name
-// only stands for it; its device address is looked up once per device, with that device
-// current, on the first call made on that device.
+// Counters of a no-allocation run, after the wait counters and queue: [0] head, [1] tail,
+// [2] status, [3] executed, [4] the lowest task index whose descriptor failed the check.
+constexpr int NOALLOC_CTRS = 8;
+
+// Every descriptor of a no-allocation run is checked on the device with the host checks of
+// xkb_sched_set_tasks before anything runs: a bad one sets the status to XKB_EINVAL, records
+// the lowest such index, and the seed kernel then makes no task ready, so no tile is touched.
+__global__ void noalloc_check_kernel(const xkb_task_desc_t * __restrict__ tasks, uint32_t n, unsigned * ctr)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    if (!xkb_internal_task_valid(tasks[t]))
+    {
+        atomicCAS(ctr + 2, 0u, (unsigned) -XKB_EINVAL);
+        atomicMin(ctr + 4, t);
+    }
+}
+
+// Device address of the scratch array in the current context. In host code the array's name
+// only stands for it; its device address is looked up with the device current, on the first
+// call made in each CUDA context (a context destroyed by cudaDeviceReset and made again gets a
+// fresh lookup). The same set-up loads the kernels the run launches, so that with lazy module
+// loading a later call needs no module memory either.
+struct NoallocSlot { CUcontext ctx = nullptr; int * ptr = nullptr; };
+
 static int noalloc_scratch(int ** out)
 {
-    static int * cache[256] = {};
+    static std::mutex mu;
+    static NoallocSlot slots[256];
+    static CUresult (*ctx_current)(CUcontext *) = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void * f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            ctx_current = (CUresult (*)(CUcontext *)) f;
+        else
+            cudaGetLastError();
+    });
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return xkb_set_cuda_error(e);
     if (dev < 0 || dev >= 256) return xkb_set_error(XKB_ENODEV, "sched_run_noalloc: device %d out of range", dev);
-    if (!cache[dev])
+    e = cudaSetDevice(dev);                     // makes the device's primary context current (CUDA 12)
+    if (e != cudaSuccess) return xkb_set_cuda_error(e);
+    CUcontext ctx = nullptr;
+    if (!ctx_current || ctx_current(&ctx) != CUDA_SUCCESS || !ctx)
+        return xkb_set_error(XKB_ENODEV, "sched_run_noalloc: no current CUDA context on device %d", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    NoallocSlot & sl = slots[dev];
+    if (sl.ctx != ctx || !sl.ptr)
     {
         void * p = nullptr;
         e = cudaGetSymbolAddress(&p, g_sched_noalloc_scratch);
         if (e != cudaSuccess) return xkb_set_cuda_error(e);
-        cache[dev] = (int *) p;
+        cudaFuncAttributes fa;
+        const void * kernels[] = {(const void *) noalloc_check_kernel, (const void *) sched_init_kernel,
+                                  (const void *) sched_seed_kernel, (const void *) sched_persistent_kernel<1>,
+                                  (const void *) sched_persistent_kernel<2>, (const void *) sched_persistent_kernel<4>,
+                                  (const void *) sched_persistent_kernel<8>};
+        for (const void * k : kernels)
+            if ((e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess) return xkb_set_cuda_error(e);
+        sl.ctx = ctx;
+        sl.ptr = (int *) p;
     }
-    *out = cache[dev];
+    *out = sl.ptr;
     return XKB_OK;
 }
 
 extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_task_graph_t * graph, int warps_per_task,
                                      double timeout_s, void * stream, uint64_t * executed)
 {
-    if (!graph || (graph->ntasks && (!tasks || !graph->succ_ptr || !graph->npred)) || !(timeout_s > 0))
+    if (!graph || (graph->ntasks && (!tasks || !graph->succ_ptr || !graph->npred)))
         return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: bad arguments");
+    if (!timeout_ok(timeout_s))
+        return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: the time limit must be finite, above 0 and at most 3600 s");
     if (warps_per_task != 1 && warps_per_task != 2 && warps_per_task != 4 && warps_per_task != 8)
         return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: warps per task must be 1, 2, 4 or 8");
     if (graph->ntasks > XKB_NOALLOC_MAX_TASKS)
@@ -791,10 +852,11 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
     a.wc = scratch; a.queue = scratch + XKB_NOALLOC_MAX_TASKS;
     a.ctr = (unsigned *) (scratch + 2 * XKB_NOALLOC_MAX_TASKS);
     a.timeout_ns = (uint64_t) (timeout_s * 1e9);
-    a.pfd = 8;
-    // the array keeps the previous call's contents: the counters are zeroed here, and the init
-    // kernel rewrites every wait counter and queue slot this run uses
+    a.pfd = SCHED_PFD_DEFAULT;
+    // the array keeps the previous call's contents: the counters are cleared here (the lowest bad
+    // index to all ones), and the init kernel rewrites every wait counter and queue slot this run uses
     XKB_CUDA_TRY(cudaMemsetAsync(a.ctr, 0, 4 * sizeof(unsigned), st));
+    XKB_CUDA_TRY(cudaMemsetAsync(a.ctr + 4, 0xff, (NOALLOC_CTRS - 4) * sizeof(unsigned), st));
     if (n)
     {
         int dev = 0, sms = 148, per = 2;
@@ -802,6 +864,7 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
         XKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         XKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sched_persistent_kernel<2>, SCHED_THREADS, 0));
         const unsigned grid = (unsigned) (sms * (per > 0 ? per : 1));
+        noalloc_check_kernel<<<(n + 255) / 256, 256, 0, st>>>(tasks, n, a.ctr);
         sched_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
         sched_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(a);
         switch (warps_per_task)
@@ -813,10 +876,12 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
         }
         XKB_CUDA_TRY(cudaGetLastError());
     }
-    unsigned ctr[4] = {0, 0, 0, 0};
+    unsigned ctr[NOALLOC_CTRS] = {};
     XKB_CUDA_TRY(cudaMemcpyAsync(ctr, a.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
     XKB_CUDA_TRY(cudaStreamSynchronize(st));
     if (executed) *executed = ctr[3];
+    if (ctr[2] == (unsigned) -XKB_EINVAL)
+        return xkb_set_error(XKB_EINVAL, "sched_run_noalloc: task %u: bad descriptor (unknown kind, bad heat tile or axpby range); nothing ran", ctr[4]);
     if (ctr[2] != 0)
         return xkb_set_error(-(int) ctr[2], "sched_run_noalloc: a device wait ran out of time (%u of %u tasks were made ready)", ctr[1], n);
     return XKB_OK;
