@@ -16,12 +16,16 @@
 #          -D_Static_assert=static_assert -include list -DNDEBUG
 #   generated: support.h (CMake defaults, every vendor driver off), version.h, an hwloc shim.
 #
-# Usage: oracle/ref/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
+# Usage: oracle/ref/build_ref.sh REFERENCE_ROOT   (or XK_REFERENCE_ROOT in the environment)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/../.." && pwd)"
-REF="${1:-${XK_REFERENCE_ROOT:-/root/reference}}"
+REF="${1:-${XK_REFERENCE_ROOT:-}}"
 OUT="$REPO/oracle/_ref"
+if [ -z "$REF" ]; then
+    echo "usage: $0 REFERENCE_ROOT (or set XK_REFERENCE_ROOT)" >&2
+    exit 2
+fi
 
 if [ ! -d "$REF/include/xkrt" ]; then
     echo "build_ref.sh: reference tree not found at $REF; skipping (prebuilt binaries, if any, are kept)" >&2

@@ -16,7 +16,10 @@
 #include "internal.h"
 #include "pool.h"
 #include "../../include/xkrt_capi.h"
+#include "../../include/xkrt/b200/api.hpp"
+#include "../../include/xkrt/driver/driver-cu.h"
 
+#include <sys/mman.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -65,6 +68,7 @@ struct Task {
     void * user_data = nullptr;
     int detach = 0;                       // references (atomic builtins): the running body's, plus each
                                           // xkrt_task_detachable_incr; the task completes at 0
+    void * cxx = nullptr;                 // the task_t of a task built with the C++ source API
 };
 
 struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; bool unified; };
@@ -226,6 +230,8 @@ struct xkb_runtime {
     Driver drivers[2] = {{XKRT_DRIVER_TYPE_HOST, -1, &devices[0]}, {XKRT_DRIVER_TYPE_CUDA, 0, &devices[1]}};
     xkrt_task_format_id_t fmt_file[2] = {0, 0};       // file read / write tasks
     bool any_unified = false;
+    void * cxx_rt = nullptr;                          // the C++ runtime_t bodies of C++ tasks receive
+    bool cxx_task_first = false;                      // XKB_CXX_HOST_BODY=task: host bodies of C++ tasks get the task first
 };
 
 static xkb_runtime * RT(xkrt_runtime_t * r) { return (xkb_runtime *) r; }
@@ -312,6 +318,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     R->drivers[1].ordinal = R->device;
     R->chunk = RESOLVE_CHUNK;
     if (const char * e = getenv("XKB_STREAM")) R->stream_on = atoi(e) != 0;
+    if (const char * e = getenv("XKB_CXX_HOST_BODY")) R->cxx_task_first = strcmp(e, "task") == 0;
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
     // fixed pools (address space only; pages are backed when touched) let a worker thread read
@@ -561,15 +568,20 @@ extern "C" void xkrt_task_complete(xkrt_runtime_t * runtime, xkrt_task_t * task)
     if (task && __atomic_exchange_n(&((Task *) task)->detach, 0, __ATOMIC_ACQ_REL) > 0) task_completed(((Task *) task)->rt, *(Task *) task);
 }
 
+// Tasks of the spawn calls are committed when spawned; a task built by hand with the C++ source
+// API (include/xkrt/task/task.hpp) is committed here (api/c/src/xkrt.cc:278-285). Anything else
+// records XKB_EINVAL.
 extern "C" void xkrt_task_commit(xkrt_runtime_t * runtime, xkrt_task_t * task)
 {
-    (void) task;       // tasks of this API are committed by the spawn calls
-    fail(RT(runtime), xkb_set_error(XKB_EINVAL, "xkrt_task_commit: tasks are committed when spawned"));
+    if (task && ((const xkrt::task_t *) task)->magic == xkrt::TASK_MAGIC) { xkb_cxx_commit(runtime, task); return; }
+    fail(RT(runtime), xkb_set_error(XKB_EINVAL, "xkrt_task_commit: not a task built with the C++ source API (spawned tasks are committed when spawned)"));
 }
 
+// The reference pushes an already ready task to a queue; here a hand-built task is committed (its
+// accesses still order it after earlier tasks, which a ready task has no pending ones of).
 extern "C" void xkrt_task_enqueue(xkrt_runtime_t * runtime, xkrt_task_t * task)
 {
-    (void) task;
+    if (task && ((const xkrt::task_t *) task)->magic == xkrt::TASK_MAGIC) { xkb_cxx_commit(runtime, task); return; }
     fail(RT(runtime), xkb_set_error(XKB_EINVAL, "xkrt_task_enqueue: tasks are scheduled by xkrt_task_wait"));
 }
 
@@ -647,10 +659,14 @@ static inline void copy64(void * dst, const void * src)
 }
 
 static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
-                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud);
+                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud,
+                       void * cxx = nullptr, int detach0 = 0);
 
+// cxx: the task_t of a C++ task (its body receives it); detach0: the detachable counter's
+// initial value (the task completes once its body returned and the counter is back to 0)
 static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
-                  const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
+                  const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud,
+                  void * cxx = nullptr, int detach0 = 0)
 {
     if (!R) return;
     if (nacc && !acc) { fail(R, xkb_set_error(XKB_EINVAL, "spawn: null accesses")); return; }
@@ -683,15 +699,17 @@ static void spawn(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_fla
             spawn_task(R, HOST_DEVICE_GLOBAL_ID, 0, XKRT_TASK_FORMAT_NULL, nullptr, 0, &e, 1, nullptr, nullptr);
         }
     }
-    spawn_task(R, device, flags, fmtid, args, args_size, acc, nacc, func, ud);
+    spawn_task(R, device, flags, fmtid, args, args_size, acc, nacc, func, ud, cxx, detach0);
 }
 
 // Append one task to the batch (arguments already checked).
 static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_task_flag_bitfield_t flags, xkrt_task_format_id_t fmtid,
-                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud)
+                       const void * args, size_t args_size, const xkrt_access_t * acc, size_t nacc, xkrt_task_func_t func, void * ud,
+                       void * cxx, int detach0)
 {
     Task t;
     t.rt = R; t.fmtid = fmtid; t.flags = flags; t.device = device;
+    t.cxx = cxx; t.detach = detach0;
     t.nargs = (uint32_t) args_size; t.nacc = (uint32_t) nacc;
     t.args_off = (R->args_pool.size() + 15) & ~(size_t) 15;
     t.acc_off = R->acc_pool.size();
@@ -703,6 +721,11 @@ static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_tas
         return;
     }
     for (size_t k = 0; k < nacc; ++k) R->acc_pool[t.acc_off + k] = acc[k];
+    if (cxx)
+    {
+        ((xkrt::task_t *) cxx)->impl = R->pending.size() - 1;
+        ((xkrt::task_t *) cxx)->state.value = xkrt::TASK_STATE_READY;
+    }
     if (args_size == sizeof(xkb_task_desc_t)) copy64(R->args_pool.data() + t.args_off, args);   // a descriptor: fixed-size copy
     else if (args_size) memcpy(R->args_pool.data() + t.args_off, args, args_size);
     const size_t nt = R->pending.size();
@@ -721,8 +744,10 @@ extern "C" void xkrt_task_spawn_generic(xkrt_runtime_t * runtime, const xkrt_dev
                                         const xkrt_task_access_counter_type_t ocr_access,
                                         const xkrt_task_wait_counter_type_t detachable_counter_initial)
 {
-    (void) ocr_access; (void) detachable_counter_initial;
-    spawn(RT(runtime), device_global_id, flags, fmtid, args, args_size, accesses, naccesses, nullptr, nullptr);
+    // one GPU: every owner of the ocr access is that GPU, so the placement hint changes nothing
+    (void) ocr_access;
+    spawn(RT(runtime), device_global_id, flags, fmtid, args, args_size, accesses, naccesses, nullptr, nullptr, nullptr,
+          (flags & TASK_FLAG_DETACHABLE) ? (int) detachable_counter_initial : 0);
 }
 
 extern "C" void xkrt_task_spawn_with_format(xkrt_runtime_t * runtime, const xkrt_device_global_id_t device_global_id,
@@ -914,7 +939,9 @@ static bool to_rec(const xkrt_access_t & a, uint32_t task, xkb_access_rec_t & r)
 static bool is_device(const xkb_runtime * R, const Task & t)
 {
     const Format & f = R->formats[t.fmtid];
-    return (t.flags & TASK_FLAG_DEVICE) && t.device != HOST_DEVICE_GLOBAL_ID && (f.builtin >= 0 || f.f[XKRT_TASK_FORMAT_TARGET_CUDA]);
+    // a device task with no format (XKRT_TASK_FORMAT_NULL) places its data on the device and runs nothing
+    return (t.flags & TASK_FLAG_DEVICE) && t.device != HOST_DEVICE_GLOBAL_ID &&
+           (f.builtin >= 0 || f.f[XKRT_TASK_FORMAT_TARGET_CUDA] || t.fmtid == XKRT_TASK_FORMAT_NULL);
 }
 
 // Last region a lookup hit (consecutive lookups mostly hit the same one).
@@ -1357,6 +1384,42 @@ static void bg_finish(xkb_runtime * R)
     R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
 }
 
+// The body of a task built with the C++ source API: each access's device_view points at the
+// access's first element where the body runs (its leading dimension in elements), then the
+// format's function is called as f(runtime, device, task) with the program's runtime_t and
+// task_t (a CUDA-target body on the worker's stream; a device task without format runs nothing).
+static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStream_t stream)
+{
+    xkrt::task_t * task = (xkrt::task_t *) T.cxx;
+    xkrt::access_t * acc = (task->flags & TASK_FLAG_DEPENDENT) ? xkrt::TASK_ACCESSES(task) : nullptr;
+    for (uint32_t a = 0; a < T.nacc && acc; ++a)
+    {
+        const uintptr_t addr = (uintptr_t) R->replica_pool[T.acc_off + a];
+        const xkrt::memory_view_t & h = acc[a].host_view;
+        acc[a].device_view = xkrt::memory_replica_view_t(addr, acc[a].type == ACCESS_TYPE_BLAS_MATRIX ? h.ld : h.m);
+        acc[a].state = xkrt::ACCESS_STATE_FETCHED;
+    }
+    task->state.value = xkrt::TASK_STATE_EXECUTING;
+    const Format & f = R->formats[T.fmtid];
+    typedef void (*body3_t)(void *, void *, void *);
+    if (dev)
+    {
+        if (!f.f[XKRT_TASK_FORMAT_TARGET_CUDA]) return XKB_OK;
+        g_stream = stream;
+        ((body3_t) f.f[XKRT_TASK_FORMAT_TARGET_CUDA])(R->cxx_rt, &R->devices[1], task);
+        g_stream = nullptr;
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return xkb_set_error(XKB_ECUDA, "task %zu: device body", t);
+        return XKB_OK;
+    }
+    if (f.f[XKRT_TASK_FORMAT_TARGET_HOST])
+    {
+        if (R->cxx_task_first) ((body3_t) f.f[XKRT_TASK_FORMAT_TARGET_HOST])(task, &R->devices[0], task);
+        else ((body3_t) f.f[XKRT_TASK_FORMAT_TARGET_HOST])(R->cxx_rt, &R->devices[0], task);
+        return XKB_OK;
+    }
+    return T.fmtid ? xkb_set_error(XKB_EINVAL, "task %zu: its format has no host body", t) : XKB_OK;
+}
+
 // One task of a non-fused batch on the calling worker: its accesses made coherent where it runs
 // (planner fetches and their copies, completed before the planner is released, so the planner's
 // state always describes data that is in place), then its body; a device body runs on the
@@ -1390,7 +1453,9 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     const Format & f = R->formats[T.fmtid];
     __atomic_add_fetch(&T.detach, 1, __ATOMIC_ACQ_REL);        // the body's own reference
     g_current = &T;
-    if (dev)
+    if (T.cxx) rc = run_cxx_body(R, T, t, dev, stream);
+    else if (dev && T.fmtid == XKRT_TASK_FORMAT_NULL) {}         // placement only
+    else if (dev)
     {
         if (f.builtin >= 0)
         {
@@ -1440,6 +1505,7 @@ struct Dataflow {
 // queued (src/task.cc:160-245, __task_complete).
 static void task_completed(::xkb_runtime * R, Task & T)
 {
+    if (T.cxx) ((xkrt::task_t *) T.cxx)->state.value = xkrt::TASK_STATE_COMPLETED;
     Dataflow * D = R ? R->df.load(std::memory_order_acquire) : nullptr;
     if (!D) return;
     const size_t g = (size_t) (&T - R->pending.data());
@@ -1871,3 +1937,127 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
     R->args_dense = true;
 }
+
+// ---- C++ source API bridge (include/xkrt/b200/api.hpp) ----------------------------------------
+
+extern "C" void xkb_cxx_bind(xkrt_runtime_t * runtime, void * cxx_runtime)
+{
+    if (xkb_runtime * R = RT(runtime)) R->cxx_rt = cxx_runtime;
+}
+
+// A hand-built task joins the batch like a spawned one: its accesses (the first dep_info->ac of
+// them when it is DEPENDENT) become the C API's access records, its target the device the
+// runtime runs it on (TASK_FLAG_DEVICE: the targeted device, or the GPU when unspecified), its
+// detachable counter's initial value is kept (src/task.cc:249-288), and its body gets the task.
+extern "C" void xkb_cxx_commit(xkrt_runtime_t * runtime, void * task)
+{
+    xkb_runtime * R = RT(runtime);
+    xkrt::task_t * t = (xkrt::task_t *) task;
+    if (!R || !t || t->magic != xkrt::TASK_MAGIC)
+    {
+        fail(R, xkb_set_error(XKB_EINVAL, "task_commit: not a task built with the C++ source API"));
+        return;
+    }
+    const uint8_t flags = t->flags & ~TASK_FLAG_REQUEUE;
+    const size_t n = (flags & TASK_FLAG_DEPENDENT) ? xkrt::TASK_DEP_INFO(t)->ac : 0;
+    static thread_local std::vector<xkrt_access_t> acc;
+    acc.resize(n);
+    const xkrt::access_t * a = n ? xkrt::TASK_ACCESSES(t) : nullptr;
+    for (size_t i = 0; i < n; ++i)
+    {
+        xkrt_access_t & c = acc[i];
+        memset(&c, 0, sizeof(c));
+        c.concurrency = a[i].concurrency; c.mode = a[i].mode; c.scope = a[i].scope; c.type = a[i].type;
+        const xkrt::memory_view_t & h = a[i].host_view;
+        if (c.type == ACCESS_TYPE_HANDLE) c.region.handle.addr = (void *) h.addr;
+        else if (c.type == ACCESS_TYPE_SEGMENT) { c.region.segment.a = (void *) h.addr; c.region.segment.b = (void *) (h.addr + h.m); }
+        else if (c.type == ACCESS_TYPE_BLAS_MATRIX)
+            c.region.matrix = {h.storage, (void *) h.addr, h.ld, h.offset_m, h.offset_n, h.m, h.n, h.sizeof_type};
+    }
+    xkrt_device_global_id_t device = HOST_DEVICE_GLOBAL_ID;
+    if (flags & TASK_FLAG_DEVICE)
+    {
+        device = xkrt::TASK_DEV_INFO(t)->targeted_device_id;
+        if (device == UNSPECIFIED_DEVICE_GLOBAL_ID || device > 1) device = R->gpu ? 1 : HOST_DEVICE_GLOBAL_ID;
+        xkrt::TASK_DEV_INFO(t)->elected_device_id = device;
+    }
+    const int detach0 = (flags & TASK_FLAG_DETACHABLE) ? (int) xkrt::TASK_DET_INFO(t)->wc.load() : 0;
+    if (flags & TASK_FLAG_DEPENDENT) xkrt::TASK_DEP_INFO(t)->wc.store(0);
+    spawn(R, device, flags, t->fmtid, nullptr, 0, acc.data(), n, nullptr, nullptr, t, detach0);
+}
+
+// +1: detachable_incr, -1: detachable_decr, 0: complete -- on the batch task a commit made.
+extern "C" void xkb_cxx_detachable(xkrt_runtime_t * runtime, void * task, int delta)
+{
+    xkb_runtime * R = RT(runtime);
+    xkrt::task_t * t = (xkrt::task_t *) task;
+    if (!R || !t || t->magic != xkrt::TASK_MAGIC || t->impl >= R->pending.size() || R->pending[t->impl].cxx != task)
+    {
+        fail(R, xkb_set_error(XKB_EINVAL, "task_detachable: not a committed task of this runtime"));
+        return;
+    }
+    xkrt_task_t * T = (xkrt_task_t *) &R->pending[t->impl];
+    if (delta > 0) xkrt_task_detachable_incr(runtime, T);
+    else if (delta < 0) xkrt_task_detachable_decr(runtime, T);
+    else xkrt_task_complete(runtime, T);
+}
+
+// The launcher gets the C++ runtime, the device, the task and a queue_cu_t whose stream is the one
+// of the thread running the CUDA body and whose event 0 the launcher may record (the reference's
+// launcher records it to signal completion, src/sched.cc:469-505); the task completes when the
+// stream's work did.
+extern "C" void xkb_cxx_kernel_launch(xkrt_runtime_t * runtime, void * device, void * task, int synchronous,
+                                      xkrt_kernel_launcher_t launcher)
+{
+    xkb_runtime * R = RT(runtime);
+    if (!R || !launcher) { fail(R, xkb_set_error(XKB_EINVAL, "task_kernel_launch: no runtime or launcher")); return; }
+    if (!g_stream) { fail(R, xkb_set_error(XKB_EINVAL, "task_kernel_launch: called outside a CUDA task body")); return; }
+    static thread_local cudaEvent_t ev = nullptr;
+    if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+    {
+        fail(R, xkb_set_cuda_error(cudaGetLastError()));
+        return;
+    }
+    xkrt::queue_cu_t q;
+    q.driver_type = XKRT_DRIVER_TYPE_CUDA; q.qtype = XKRT_QUEUE_TYPE_KERN;
+    q.cu.handle.high = q.cu.handle.low = g_stream;
+    q.cu.events.buffer = &ev; q.cu.events.capacity = 1;
+    launcher(R->cxx_rt, device, task, &q, nullptr, 0);
+    if (synchronous && cudaStreamSynchronize(g_stream) != cudaSuccess) fail(R, xkb_set_cuda_error(cudaGetLastError()));
+}
+
+// Task memory of a thread: 64-byte aligned pieces of 64 MiB chunks (pages backed on first touch),
+// never freed one by one -- the reference's per-thread task stack (src/thread/thread.cc:105-124).
+namespace {
+struct TaskArena {
+    std::vector<std::pair<void *, size_t>> chunks;
+    uint8_t * cur = nullptr;
+    size_t left = 0;
+    void release()
+    {
+        for (auto & c : chunks) munmap(c.first, c.second);
+        chunks.clear(); cur = nullptr; left = 0;
+    }
+    ~TaskArena() { release(); }
+};
+thread_local TaskArena g_task_arena;
+} // namespace
+
+extern "C" void * xkb_cxx_allocate_task(size_t size)
+{
+    TaskArena & A = g_task_arena;
+    size = (size + 63) & ~(size_t) 63;
+    if (size > A.left)
+    {
+        const size_t chunk = std::max<size_t>(size_t(64) << 20, (size + 4095) & ~(size_t) 4095);
+        void * p = mmap(nullptr, chunk, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+        if (p == MAP_FAILED) return nullptr;
+        A.chunks.emplace_back(p, chunk);
+        A.cur = (uint8_t *) p; A.left = chunk;
+    }
+    void * r = A.cur;
+    A.cur += size; A.left -= size;
+    return r;
+}
+
+extern "C" void xkb_cxx_release_tasks(void) { g_task_arena.release(); }
