@@ -14,8 +14,9 @@ the written blocks back -- timed spawn -> wait, as the reference's runtime is ti
 Beside it: the same graph's first two steps in the plain one-launch-per-task form and as a CUDA
 graph (the fused/plain ratio), the whole-step stencil kernel's HBM GB/s (FP64 and FP32
 storage), the resolver on the dependency microbench (65,536 tasks, 1-4 accesses on an 8192^2
-FP64 matrix), and the CPU baseline (the C restatement of the same tile bodies on the host's
-cores, a bounded sample).
+FP64 matrix), and the CPU baseline: a bounded sample of the same heat graph on the reference's
+own host-only runtime built from its sources (oracle/_ref/ref_heat) with all host threads, or the
+C restatement of the tile body on the host's cores where that binary is absent.
 
 --impl reference times the reference's own CPU implementation of the path -- its host-only
 runtime built from its sources (oracle/_ref/ref_heat) running the same heat graph on all host
@@ -196,18 +197,32 @@ def host_threads():
 REF_HEAT = os.path.join(HERE, "oracle", "_ref", "ref_heat")
 
 
-def ref_heat_sample(nthreads, steps, n=NX):
+REF_FAILURES = []          # runs of the reference binaries that ended abnormally (kept for the line)
+
+
+def _ref_run(cmd, env, timeout=600, tries=3):
+    """Run a reference harness; an abnormal end (the reference's host runtime now and then dies
+    of a signal in the middle of a run, before its result line) is recorded and the run is made
+    again, up to `tries` times. A result line printed before a crash is kept."""
+    for _ in range(tries):
+        with tempfile.TemporaryDirectory() as d:
+            r = subprocess.run(cmd, env=env, cwd=d, capture_output=True, text=True, timeout=timeout)
+        lines = [l for l in r.stdout.strip().splitlines() if l.startswith("{")]
+        if r.returncode != 0:
+            tail = [l for l in r.stderr.splitlines() if "[LOGGER]" not in l][-3:]
+            REF_FAILURES.append({"cmd": os.path.basename(cmd[0]) + " " + " ".join(cmd[1:]), "rc": r.returncode,
+                                 "result_kept": bool(lines), "stderr": " | ".join(tail)[-200:]})
+        if lines:
+            return json.loads(lines[-1])
+    raise RuntimeError(f"reference run {os.path.basename(cmd[0])} failed {tries} times: {REF_FAILURES[-1]}")
+
+
+def ref_heat_sample(nthreads, steps, n=NX, ts=TS):
     """The reference's own host-only runtime (built from its sources by oracle/ref/build_ref.sh)
-    running `steps` Jacobi steps of the n x n heat graph with 128^2 tile tasks on `nthreads`
+    running `steps` Jacobi steps of the n x n heat graph with ts^2 tile tasks on `nthreads`
     host threads; returns (tasks/s, seconds, tasks) as the harness times spawn -> task_wait."""
     env = dict(os.environ, DRIVERS=f"host,{nthreads}", XKRT_DRIVERS=f"host,{nthreads}")
-    with tempfile.TemporaryDirectory() as d:
-        r = subprocess.run([REF_HEAT, str(n), str(n), str(TS), str(steps)], env=env, cwd=d, capture_output=True,
-                           text=True, timeout=600)
-    if r.returncode != 0:
-        tail = [l for l in r.stderr.splitlines() if "[LOGGER]" not in l][-5:]
-        raise RuntimeError(f"reference heat run exited {r.returncode}: {' | '.join(tail)}")
-    out = json.loads(r.stdout.strip().splitlines()[-1])
+    out = _ref_run([REF_HEAT, str(n), str(n), str(ts), str(steps)], env)
     return out["tasks_per_s"], out["seconds"], out["tasks"]
 
 
@@ -227,6 +242,8 @@ def cpu_baseline_sample(target_s=10.0):
                      "C restatement of the tile body on POSIX threads"}
     if why:
         out["reference_failed"] = why
+    if REF_FAILURES:
+        out["reference_abnormal_ends"] = REF_FAILURES
     return out
 
 
@@ -234,9 +251,12 @@ def _ref_baseline(cores, target_s):
     v, secs, tasks = ref_heat_sample(cores, 1)
     steps = max(1, min(200, int(target_s / max(secs, 1e-3))))
     v, secs, tasks = ref_heat_sample(cores, steps)
-    return {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "reference",
-            "sample": f"{steps} Jacobi steps of the {NX}^2 FP64 heat graph ({tasks} tile tasks of {TS}^2, {secs:.1f} s): "
-                      f"the reference's own host-only runtime (DRIVERS=host,{cores}) with a host-format tile body"}
+    out = {"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": "reference",
+           "sample": f"{steps} Jacobi steps of the {NX}^2 FP64 heat graph ({tasks} tile tasks of {TS}^2, {secs:.1f} s): "
+                     f"the reference's own host-only runtime (DRIVERS=host,{cores}) with a host-format tile body"}
+    if REF_FAILURES:
+        out["reference_abnormal_ends"] = REF_FAILURES
+    return out
 
 
 def run_reference(args):
@@ -259,7 +279,11 @@ def run_reference(args):
     tasks, secs = 0, 0.0
     for _ in range(args.steps):
         if use_ref:
-            _, s, n = ref_heat_sample(cores, sample_steps)
+            try:
+                _, s, n = ref_heat_sample(cores, sample_steps)
+            except Exception as ex:          # three abnormal ends in a row: the port times the rest
+                use_ref, why = False, str(ex)[:300]
+                _, s, n = cpu_heat_sample(cores, steps=None, target_s=5.0)
         else:
             _, s, n = cpu_heat_sample(cores, steps=None, target_s=5.0)
         tasks += n; secs += s
@@ -275,7 +299,8 @@ def run_reference(args):
         "config": {"workload": f"batched heat-diffusion-2d: {NX}x{NY} FP64 grid, {TS}x{TS} tile tasks; each bench step "
                                "times a bounded sample of Jacobi steps on the host", "parallelism": f"{cores} host threads"},
         "cpu_baseline": dict({"value": round(v, 1), "unit": "tasks/s", "cores": cores, "kind": kind, "sample": sample},
-                             **({"reference_failed": why} if why else {})),
+                             **({"reference_failed": why} if why else {}),
+                             **({"reference_abnormal_ends": REF_FAILURES} if REF_FAILURES else {})),
         "e2e": {"value": round(v, 1), "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -311,6 +336,64 @@ def capi_e2e(reps, world, local, warm=1):
             "checksum": lines[-1]["checksum"]}
 
 
+HEAT_CXX = os.path.join(HERE, "xkaapi_b200", "examples", "heat_cxx")
+
+
+def _example_lines(exe, argv, local, timeout=900):
+    env = dict(os.environ)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = vis.split(",")[local] if vis else str(local)
+    r = subprocess.run([exe] + [str(a) for a in argv], env=env, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} failed: {r.stderr[-400:]}")
+    return [json.loads(l) for l in r.stdout.strip().splitlines()]
+
+
+def config_h_study(local, n=1024, ts=128, steps=100):
+    """The plain heat configuration (1024^2 FP64, 128^2 tiles, 100 steps: 6,400 tile tasks), spawn
+    -> wait, three ways: the C API with the library's tile body (heat_xkrt), the C++ source API
+    with the program's own CUDA kernel launched from its task body (heat_cxx), and the reference's
+    host-only runtime on all host threads (oracle/_ref/ref_heat); median of the repetitions after
+    a warm-up one."""
+    out = {"workload": f"heat {n}^2 FP64, {ts}^2 tiles, {steps} steps ({(n // ts) ** 2 * steps} tasks), spawn -> wait, fresh runtime"}
+    try:
+        ln = _example_lines(HEAT_XKRT, [n, n, ts, steps, 6], local)[1:]
+        out["capi_builtin_body"] = {"tasks_per_s": round(statistics.median(l["tasks_per_s"] for l in ln), 1),
+                                    "fused": ln[-1]["fused"], "reps": len(ln)}
+    except Exception as ex:
+        out["capi_builtin_body"] = {"failed": str(ex)[:300]}
+    try:
+        ln = _example_lines(HEAT_CXX, [n, n, ts, steps, 4], local)[1:]
+        out["cxx_user_body"] = {"tasks_per_s": round(statistics.median(l["tasks_per_s"] for l in ln), 1), "reps": len(ln),
+                                "same_result_as_capi": ln[-1]["checksum"] == _example_lines(HEAT_XKRT, [n, n, ts, steps, 1], local)[0]["checksum"]}
+    except Exception as ex:
+        out["cxx_user_body"] = {"failed": str(ex)[:300]}
+    if os.path.exists(REF_HEAT):
+        cores = host_threads()
+        try:
+            vals = [ref_heat_sample(cores, steps, n=n, ts=ts)[0] for _ in range(4)][1:]
+            out["reference_cpu"] = {"tasks_per_s": round(statistics.median(vals), 1), "cores": cores,
+                                    "what": "the reference's host-only runtime (oracle/_ref/ref_heat), same graph, spawn -> task_wait"}
+        except Exception as ex:
+            out["reference_cpu"] = {"failed": str(ex)[:300]}
+    return out
+
+
+def user_body_study(local, n=NX, ts=TS, steps=10):
+    """The drop-in path of a program that brings its own CUDA tile kernel (examples/heat_cxx: tasks
+    built by hand with the C++ source API, kernel launched through task_detachable_kernel_launch,
+    run by the host dataflow team) on the headline grid for a few steps; spawn -> wait."""
+    try:
+        ln = _example_lines(HEAT_CXX, [n, n, ts, steps, 2], local)[1:]
+    except Exception as ex:
+        return {"failed": str(ex)[:300]}
+    return {"tasks": ln[-1]["tasks"], "tasks_per_s": round(ln[-1]["tasks_per_s"], 1), "seconds": round(ln[-1]["seconds"], 3),
+            "spawn_s": round(ln[-1]["spawn_s"], 3),
+            "workload": f"heat {n}^2 FP64, {ts}^2 tiles, {steps} steps, C++ source API, user CUDA kernel per task; the grids "
+                        "placed on the GPU by distribute_async before the timed part, the written blocks copied back to the "
+                        "host inside it (at the wait)"}
+
+
 AXPBY_XKRT = os.path.join(HERE, "xkaapi_b200", "examples", "axpby_xkrt")
 REF_AXPBY = os.path.join(HERE, "oracle", "_ref", "ref_axpby")
 AXPBY_N, AXPBY_PASSES, AXPBY_SEED, AXPBY_CMIN, AXPBY_CMAX = 1 << 28, 10, 2026, 65536, 16 << 20
@@ -342,11 +425,11 @@ def axpby_study(local):
     if os.path.exists(REF_AXPBY):
         cores = host_threads()
         renv = dict(os.environ, DRIVERS=f"host,{cores}", XKRT_DRIVERS=f"host,{cores}")
-        with tempfile.TemporaryDirectory() as d:
-            rr = subprocess.run([REF_AXPBY] + args + [str(AXPBY_CMIN), str(AXPBY_CMAX)], env=renv, cwd=d,
-                                capture_output=True, text=True, timeout=900)
-        if rr.returncode == 0:
-            rl = json.loads(rr.stdout.strip().splitlines()[-1])
+        try:
+            rl = _ref_run([REF_AXPBY] + args + [str(AXPBY_CMIN), str(AXPBY_CMAX)], renv, timeout=900)
+        except Exception as ex:
+            rl, out["reference_cpu"] = None, {"failed": str(ex)[:300]}
+        if rl:
             out["reference_cpu"] = {"tasks_per_s": rl["tasks_per_s"], "seconds": rl["seconds"], "cores": cores,
                                     "same_result": rl["checksum"] == ln["checksum"],
                                     "what": "the reference's host-only runtime (oracle/_ref/ref_axpby), same graph, spawn -> task_wait"}
@@ -535,6 +618,10 @@ def main():
     # possible at this size; the parity suite covers correctness. Keep a checksum instead.
     res_grid = a if STEPS % 2 == 0 else b
     checksum = float(res_grid.sum().item())
+    # FP64 checks of the last step: the other grid holds the state one step earlier
+    extra["checks_fp64"] = {"f64": xk.heat_norms(b if STEPS % 2 == 0 else a, res_grid, NX, NY, NX, COEF, stream=stream),
+                            "what": "xkb_heat_norms on the last Jacobi step of the graph: boundary max |g| (Dirichlet 0), "
+                                    "interior L2 norm, residual max |dst - update(src)| with the update in FP64"}
 
     # ---------------- e2e replay: the resolved graph re-run with host grids copied in and out --
     torch.cuda.synchronize()
@@ -566,6 +653,8 @@ def main():
         s32 = xk.Scheduler(stream); s32.set_team(1); s32.set_tasks(d32); del d32   # one warp per FP32 tile
         with torch.cuda.stream(stream):
             s32.run(g32); s32.wait()
+        extra["checks_fp64"]["f32"] = xk.heat_norms(b32 if STEPS % 2 == 0 else a32, a32 if STEPS % 2 == 0 else b32,
+                                                    NX, NY, NX, COEF, stream=stream)
         out32 = (a32 if STEPS % 2 == 0 else b32).double()
         err32 = float((out32 - res_grid).abs().max().item()) / float(res_grid.abs().max().item())
         del out32
@@ -654,8 +743,15 @@ def main():
         r3 = xk.Resolver(stream)
         t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+        visits = int(((recs["m"] // 64) * (recs["n"] // 64)).sum())          # 64 x 64-element cells per access
+        mb_bytes = 32.0 * len(recs) + 8.0 * int(g3.nedges) + 16.0 * visits
         extra["resolver_microbench"] = {"tasks": mb_tasks, "accesses": int(len(recs)), "unique_edges": int(g3.nedges),
-                                        "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt)}
+                                        "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt),
+                                        "roofline": {"bound": "hbm", "achieved": round(mb_bytes / dt / 1e9, 2), "peak": hbm_peak,
+                                                     "unit": "GB/s", "frac": round(mb_bytes / dt / 1e9 / hbm_peak, 5),
+                                                     "algorithmic_bytes": mb_bytes, "cell_visits": visits,
+                                                     "what": "32 B per access + 8 B per unique edge + 16 B per visit of a "
+                                                             "64 x 64-element cell, over the wall time of add + graph"}}
         r3.close()
         ref = ref_deps_time(recs)
         if ref:
@@ -670,6 +766,8 @@ def main():
     # ---------------- e2e: the drop-in C API, spawn -> wait, resolution included ------------
     e2e = capi_e2e(max(2, min(args.steps, 3)), world, local)
     if rank == 0 and not args.no_side:
+        extra["config_h"] = config_h_study(local)
+        extra["e2e_user_body"] = user_body_study(local)
         extra["axpby_chains"] = axpby_study(local)
     if rank == 0 and not args.no_side:
         extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000)

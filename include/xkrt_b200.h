@@ -410,6 +410,17 @@ typedef struct xkb_heat_cfg_t {
 XKB_API int xkb_heat_step_cfg(int dtype, const void * src, void * dst, int64_t ld, int64_t nx, int64_t ny,
                               double c, const xkb_heat_cfg_t * cfg, void * stream);
 
+/* FP64 checks of one Jacobi step's result, whatever the storage type (a precision mode keeps its
+ * checks in FP64): into the DEVICE array out[4] -- out[0] the largest |dst| on the grid boundary
+ * (0 for the Dirichlet-0 condition, which no task writes), out[1] the sum of dst^2 over the
+ * interior (its square root is the grid's L2 norm), out[2] the residual of the step: the largest
+ * |dst - (src + c*lap(src))| over the interior with src promoted to double and the update in the
+ * reference's order (0 for FP64 grids; the storage rounding for FP32 ones), out[3] the largest
+ * interior |dst|. No counterpart in the reference, whose example checks its grid by exporting it
+ * (examples/heat-diffusion-2d/src/main.cc:115-163). Asynchronous on `stream`. */
+XKB_API int xkb_heat_norms(int dtype, const void * src, const void * dst, int64_t ld, int64_t nx, int64_t ny, double c,
+                           double * out, void * stream);
+
 /* ---- axpby tile body -------------------------------------------------------------------- */
 /* y[i] = a*x[i] + b*y[i] for i in [0, n), FP64, computed as (a*x) + (b*y) with no fused
  * multiply-add. No reference kernel exists; nearest reference task body is the byte-wise

@@ -7,6 +7,7 @@
 // example program (xkaapi_b200/examples/axpby_xkrt.c), so both run the same graph.
 //
 // usage: ref_axpby N PASSES SEED CMIN CMAX [out.bin]  -> JSON line {tasks, seconds, tasks_per_s, checksum}
+#include <xkrt/internals.h>
 #include <xkrt/runtime.h>
 #include <xkrt/thread/thread.h>
 
@@ -72,6 +73,13 @@ int main(int argc, char ** argv)
     axpby_fmt = runtime.task_format_create(&format);
 
     std::vector<double> x(n), y(n);
+    // the segment coherency controller, created here on the spawning thread instead of lazily by
+    // the first concurrent fetches (an unlocked check-then-create, src/task/task.cc:69-95)
+    {
+        thread_t * thread = thread_t::get_tls();
+        access_t proto(thread->current_task, (uintptr_t) x.data(), (uintptr_t) (x.data() + 1), ACCESS_MODE_R);
+        task_get_memory_controller(&runtime, thread->current_task, &proto);
+    }
     uint64_t s = seed;
     for (int64_t i = 0; i < n; ++i) x[i] = 2.0 * unit(&s) - 1.0;
     for (int64_t i = 0; i < n; ++i) y[i] = 2.0 * unit(&s) - 1.0;

@@ -8,6 +8,7 @@
 // "host,N").
 //
 // usage: ref_heat NX NY TS STEPS [init.bin out.bin]   -> JSON line {tasks, seconds, tasks_per_s}
+#include <xkrt/internals.h>
 #include <xkrt/runtime.h>
 #include <xkrt/thread/thread.h>
 
@@ -96,6 +97,17 @@ int main(int argc, char ** argv)
                 a[j * NX + i] = (i == 0 || j == 0 || i == NX - 1 || j == NY - 1) ? 0.0 : u(rng);
     }
     memcpy(b, a, NX * NY * sizeof(double));
+    // The reference creates a domain's coherency controller lazily, from the first fetch of an
+    // access of that (ld, sizeof), without a lock (src/task/task.cc:50-150 called from
+    // src/sched.cc:232): device threads fetching their first tasks at the same time push onto the
+    // same std::vector and one of them can read a freed buffer (SIGSEGV in
+    // task_get_memory_controller). Creating it here, on the spawning thread, before any task
+    // exists, is what that first fetch does in a run without the race.
+    {
+        thread_t * thread = thread_t::get_tls();
+        access_t proto(thread->current_task, MATRIX_COLMAJOR, a, NX, 0, 0, 1, 1, sizeof(double), ACCESS_MODE_R);
+        task_get_memory_controller(&runtime, thread->current_task, &proto);
+    }
     const long ntx = (NX + TS - 1) / TS, nty = (NY + TS - 1) / TS;
     auto t0 = std::chrono::steady_clock::now();
     double * src = a, * dst = b;

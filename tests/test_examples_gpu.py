@@ -114,3 +114,24 @@ def test_background_resolution_small_chunks(torch_cuda, tmp_path, chunk, stream)
     assert r.returncode == 0, r.stderr
     assert json.loads(r.stdout.strip().splitlines()[-1])["tasks"] == len(chunks)
     np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin"), O.axpby_chain_run(x, y, chunks))
+
+
+CXX_EXE = os.path.join(REPO, "xkaapi_b200", "examples", "heat_cxx")
+
+
+@pytest.mark.parametrize("nx,ny,ts,steps", [(256, 256, 64, 6), (300, 170, 64, 5), (129, 65, 32, 4)])
+def test_heat_cxx_user_body(torch_cuda, tmp_path, nx, ny, ts, steps):
+    """examples/heat_cxx: tasks built by hand through the C++ source API, as the reference's heat
+    example builds them, with the program's own CUDA tile kernel launched through
+    task_detachable_kernel_launch (the host dataflow team runs them). The grid it reads back
+    equals the oracle's, bit for bit, on two repetitions."""
+    g = O.heat_init(nx, ny, seed=23)
+    g.tofile(tmp_path / "init.bin")
+    r = subprocess.run([CXX_EXE] + [str(a) for a in (nx, ny, ts, steps, 2, tmp_path / "init.bin", tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(l) for l in r.stdout.strip().splitlines()]
+    assert len(lines) == 2 and all(l["tasks"] == -(-nx // ts) * -(-ny // ts) * steps for l in lines)
+    assert lines[0]["checksum"] == lines[1]["checksum"]
+    out = np.fromfile(tmp_path / "out.bin").reshape(ny, nx)
+    np.testing.assert_array_equal(out, O.heat_run(g, nx, ny, steps, 0.2))

@@ -91,3 +91,29 @@ def test_f32_tiles_bit_exact(torch_cuda):
             xk.heat_tile(s, d, nx, ny, nx, tx, ty, ts, ts, C)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(d.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_heat_norms_fp64_checks(torch_cuda, dtype):
+    """xkb_heat_norms: boundary max, L2 norm and the step's residual in FP64, against numpy on
+    the same grids; the residual is 0 for FP64 storage and the float rounding for FP32."""
+    torch = torch_cuda
+    nx, ny = 300, 170
+    g = O.heat_init(nx, ny, seed=31)
+    npdt = np.float64 if dtype == "f64" else np.float32
+    src = torch.from_numpy(g.astype(npdt)).cuda()
+    dst = src.clone()
+    xk.heat_step(src, dst, nx, ny, nx, 0.2)
+    n = xk.heat_norms(src, dst, nx, ny, nx, 0.2)
+    d = dst.cpu().numpy().astype(np.float64)
+    exact = O.heat_step(g.astype(npdt).astype(np.float64), g.astype(np.float64).copy(), nx, ny, 0.2)
+    interior = d[1:-1, 1:-1]
+    assert n["boundary_max_abs"] == 0.0
+    assert abs(n["l2_norm"] - np.sqrt((interior ** 2).sum())) <= 1e-12 * n["l2_norm"]
+    assert n["interior_max_abs"] == np.abs(interior).max()
+    res = np.abs(interior - exact[1:-1, 1:-1]).max()
+    assert n["residual_max_abs"] == res
+    if dtype == "f64":
+        assert res == 0.0
+    else:
+        assert 0 < res <= 2.0 ** -24 * n["interior_max_abs"]

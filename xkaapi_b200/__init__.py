@@ -73,6 +73,7 @@ SIGNATURES = {
     "xkb_heat_tile": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step_cfg": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, ctypes.POINTER(HeatCfg), _vp]),
+    "xkb_heat_norms": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp, _vp]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
     "xkb_sched_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_sched_destroy": (_int, [_vp]),
@@ -166,6 +167,17 @@ def heat_step(src, dst, nx, ny, ld, c, stream=None, cfg=None):
                                          _stream(stream)))
     return check(lib().xkb_heat_step_cfg(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c,
                                          ctypes.byref(cfg), _stream(stream)))
+
+
+def heat_norms(src, dst, nx, ny, ld, c, stream=None):
+    """FP64 checks of the step src -> dst (torch CUDA grids of either storage type): the largest
+    |dst| on the boundary, the interior L2 norm, the step's residual max |dst - update(src)| and
+    the largest interior |dst| (xkb_heat_norms)."""
+    import torch
+    out = torch.zeros(4, dtype=torch.float64, device=src.device)
+    check(lib().xkb_heat_norms(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c, out.data_ptr(), _stream(stream)))
+    o = out.cpu().tolist()
+    return {"boundary_max_abs": o[0], "l2_norm": o[1] ** 0.5, "residual_max_abs": o[2], "interior_max_abs": o[3]}
 
 
 def axpby(a, x, b, y, stream=None):

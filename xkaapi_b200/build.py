@@ -100,6 +100,36 @@ def build_examples(verbose=False):
         if r.returncode != 0:
             raise RuntimeError(f"gcc failed on {src}:\n{r.stdout}\n{r.stderr}")
         out.append(exe)
+    # C++ programs (the reference's C++ source API, include/xkrt/) with their own CUDA kernels in
+    # <name>_kernel.cu
+    for f in sorted(os.listdir(EXAMPLES)):
+        if not f.endswith(".cc"):
+            continue
+        src, exe = os.path.join(EXAMPLES, f), os.path.join(EXAMPLES, f[:-3])
+        kern = os.path.join(EXAMPLES, f[:-3] + "_kernel.cu")
+        deps = [src, LIB] + ([kern] if os.path.exists(kern) else []) + \
+            [os.path.join(r, h) for r, _, hs in os.walk(os.path.join(REPO, "include", "xkrt")) for h in hs]
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(d) for d in deps):
+            out.append(exe)
+            continue
+        objs = []
+        if os.path.exists(kern):
+            kobj = os.path.join(BUILD, f[:-3] + "_kernel.o")
+            cmd = [nvcc()] + ARCH + ["-O3", "-Xcompiler", "-fPIC", "-c", kern, "-o", kobj]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {kern}:\n{r.stdout}\n{r.stderr}")
+            objs.append(kobj)
+        cuda = os.path.dirname(os.path.dirname(nvcc()))
+        cmd = ["g++", "-std=c++20", "-O2", "-Wall", "-Werror", "-I" + os.path.join(REPO, "include"), "-I" + os.path.join(cuda, "include"),
+               src] + objs + ["-o", exe, "-L" + PKG, "-lxkb200", "-L" + os.path.join(cuda, "lib64"), "-lcudart", "-lpthread",
+                              "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed on {src}:\n{r.stdout}\n{r.stderr}")
+        out.append(exe)
     return out
 
 

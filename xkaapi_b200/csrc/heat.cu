@@ -155,3 +155,71 @@ extern "C" int xkb_heat_step_cfg(int dtype, const void * src, void * dst, int64_
     return dtype == XKB_F64 ? launch_step<double>(src, dst, ld, nx, ny, c, k, xkb_stream(stream))
                             : launch_step<float>(src, dst, ld, nx, ny, c, k, xkb_stream(stream));
 }
+
+// ---- FP64 checks of a step's result ---------------------------------------------------------
+namespace {
+
+// Non-negative doubles order like their bit patterns, so an integer max is a double max.
+__device__ __forceinline__ void atomic_max_nonneg(double * p, double v)
+{
+    atomicMax((unsigned long long *) p, (unsigned long long) __double_as_longlong(v));
+}
+
+// out[0] max |dst| on the boundary, out[1] sum of dst^2 over the interior, out[2] max over the
+// interior of |dst - (src + c*lap(src))| with src promoted to double, out[3] max |dst| interior.
+// One block per column band; threads over rows; all arithmetic in double.
+template <typename T>
+__global__ void __launch_bounds__(256) heat_norms_kernel(const T * __restrict__ src, const T * __restrict__ dst, int64_t ld,
+                                                         int64_t nx, int64_t ny, double c, double * out)
+{
+    double bmax = 0, sum = 0, rmax = 0, vmax = 0;
+    for (int64_t j = blockIdx.x; j < ny; j += gridDim.x)
+        for (int64_t i = threadIdx.x; i < nx; i += blockDim.x)
+        {
+            const double d = (double) dst[j * ld + i];
+            if (i == 0 || j == 0 || i == nx - 1 || j == ny - 1) { bmax = fmax(bmax, fabs(d)); continue; }
+            const T * s = src + j * ld + i;
+            const double v = (double) s[0];
+            const double a = __dadd_rn(__dsub_rn((double) s[1], __dmul_rn(2.0, v)), (double) s[-1]);
+            const double b = __dadd_rn(__dsub_rn((double) s[ld], __dmul_rn(2.0, v)), (double) s[-ld]);
+            const double e = __dadd_rn(v, __dmul_rn(c, __dadd_rn(a, b)));
+            rmax = fmax(rmax, fabs(d - e));
+            vmax = fmax(vmax, fabs(d));
+            sum += d * d;
+        }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomic_max_nonneg(out + 0, bmax);
+        atomicAdd(out + 1, sum);
+        atomic_max_nonneg(out + 2, rmax);
+        atomic_max_nonneg(out + 3, vmax);
+    }
+}
+
+} // namespace
+
+extern "C" int xkb_heat_norms(int dtype, const void * src, const void * dst, int64_t ld, int64_t nx, int64_t ny, double c,
+                              double * out, void * stream)
+{
+    int rc = heat_check(dtype, src, dst, ld, nx, ny);
+    if (rc) return rc;
+    if (!out) return xkb_set_error(XKB_EINVAL, "heat_norms: null output");
+    cudaStream_t st = xkb_stream(stream);
+    XKB_CUDA_TRY(cudaMemsetAsync(out, 0, 4 * sizeof(double), st));
+    if (nx == 0 || ny == 0) return XKB_OK;
+    int dev = 0, sms = 148;
+    XKB_CUDA_TRY(cudaGetDevice(&dev));
+    XKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned grid = (unsigned) std::min<int64_t>(ny, (int64_t) sms * 8);
+    if (dtype == XKB_F64) heat_norms_kernel<double><<<grid, 256, 0, st>>>((const double *) src, (const double *) dst, ld, nx, ny, c, out);
+    else heat_norms_kernel<float><<<grid, 256, 0, st>>>((const float *) src, (const float *) dst, ld, nx, ny, c, out);
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}

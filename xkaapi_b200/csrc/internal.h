@@ -77,3 +77,9 @@ int xkb_internal_sched_run_window(xkb_sched_t * S, const xkb_task_desc_t * tasks
 int xkb_internal_sched_upload_window(xkb_sched_t * S, const xkb_task_desc_t * tasks, size_t ntasks);
 int xkb_internal_sched_launch_window(xkb_sched_t * S, const xkb_task_graph_t * g);
 int xkb_internal_sched_windows_wait(xkb_sched_t * S, uint64_t * executed);
+
+// The heat update of the cells [i0, i0 + w) x [j0, j0 + h) of an nx x ny grid (interior cells
+// only) on per-access replicas: src and dst point at cell (i0, j0) of theirs, each with its own
+// leading dimension (xkb_diffusion_views with an explicit box).
+int xkb_internal_diffusion_box(int dtype, cudaStream_t stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
+                               int64_t i0, int64_t j0, int64_t w, int64_t h, int64_t nx, int64_t ny, double c);

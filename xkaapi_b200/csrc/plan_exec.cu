@@ -20,6 +20,7 @@
 // src/dst point at the tile origin after the launcher's re-basing (main.cc:214-219), with their
 // own leading dimensions.
 #include "common.cuh"
+#include "internal.h"
 
 #include <algorithm>
 #include <vector>
@@ -227,18 +228,26 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
     return rc;
 }
 
+// The cells [i0, i0 + w) x [j0, j0 + h) of the grid (interior ones only), src and dst pointing at
+// cell (i0, j0) of their replicas.
+int xkb_internal_diffusion_box(int dtype, cudaStream_t stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
+                               int64_t i0, int64_t j0, int64_t w, int64_t h, int64_t nx, int64_t ny, double c)
+{
+    if ((dtype != XKB_F64 && dtype != XKB_F32) || !src || !dst || w <= 0 || h <= 0)
+        return xkb_set_error(XKB_EINVAL, "diffusion_views: bad arguments");
+    const dim3 block(256), grid((unsigned) ((w + 255) / 256), (unsigned) (h < 1024 ? h : 1024));
+    if (dtype == XKB_F64)
+        diffusion_views_kernel<double><<<grid, block, 0, stream>>>((const double *) src, ld_src, (double *) dst, ld_dst, i0, j0, w, h, nx, ny, c);
+    else
+        diffusion_views_kernel<float><<<grid, block, 0, stream>>>((const float *) src, ld_src, (float *) dst, ld_dst, i0, j0, w, h, nx, ny, c);
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
 extern "C" int xkb_diffusion_views(int dtype, void * stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
                                    int64_t tile_x, int64_t tile_y, int64_t tsx, int64_t tsy, int64_t nx, int64_t ny, double c)
 {
-    if ((dtype != XKB_F64 && dtype != XKB_F32) || !src || !dst || tsx <= 0 || tsy <= 0)
-        return xkb_set_error(XKB_EINVAL, "diffusion_views: bad arguments");
-    const dim3 block(256), grid((unsigned) ((tsx + 255) / 256), (unsigned) (tsy < 1024 ? tsy : 1024));
-    if (dtype == XKB_F64)
-        diffusion_views_kernel<double><<<grid, block, 0, xkb_stream(stream)>>>((const double *) src, ld_src, (double *) dst, ld_dst,
-                                                                             tile_x * tsx, tile_y * tsy, tsx, tsy, nx, ny, c);
-    else
-        diffusion_views_kernel<float><<<grid, block, 0, xkb_stream(stream)>>>((const float *) src, ld_src, (float *) dst, ld_dst,
-                                                                            tile_x * tsx, tile_y * tsy, tsx, tsy, nx, ny, c);
-    XKB_CUDA_TRY(cudaGetLastError());
-    return XKB_OK;
+    if (tsx <= 0 || tsy <= 0) return xkb_set_error(XKB_EINVAL, "diffusion_views: bad arguments");
+    return xkb_internal_diffusion_box(dtype, xkb_stream(stream), src, ld_src, dst, ld_dst, tile_x * tsx, tile_y * tsy, tsx, tsy, nx,
+                                      ny, c);
 }

@@ -210,6 +210,7 @@ struct xkb_runtime {
     std::vector<uint64_t> hextra;                     //   handles that get an extra writer task before it
     std::vector<uint32_t> dfirst;                     //   their first occurrences, in record order
     uint64_t cur_h2d = 0, cur_d2h = 0, cur_h2d_bytes = 0, cur_d2h_bytes = 0;   // copies of the batch in progress
+    uint64_t cur_d2d = 0;                             // device-to-device copies (reference mode)
     // page-locked descriptor slots of streamed windows (a slot is reused once its copy is done)
     struct DescSlot { xkb_task_desc_t * p = nullptr; size_t cap = 0; cudaEvent_t ev = nullptr; } dslot[2];
     int dslot_next = 0;
@@ -230,6 +231,11 @@ struct xkb_runtime {
     Driver drivers[2] = {{XKRT_DRIVER_TYPE_HOST, -1, &devices[0]}, {XKRT_DRIVER_TYPE_CUDA, 0, &devices[1]}};
     xkrt_task_format_id_t fmt_file[2] = {0, 0};       // file read / write tasks
     bool any_unified = false;
+    // XKB_PLANNER=reference: the reference's coherency decisions (per-access device allocations,
+    // H2D / D2D / D2H as its memory tree plans them) on the tasks run one at a time in spawn order
+    bool ref_mode = false;
+    std::vector<void *> allocs;                       //   device memory of each planner allocation
+    FILE * plan_record = nullptr;                     // XKB_PLAN_RECORD: every executed copy record
     void * cxx_rt = nullptr;                          // the C++ runtime_t bodies of C++ tasks receive
     bool cxx_task_first = false;                      // XKB_CXX_HOST_BODY=task: host bodies of C++ tasks get the task first
 };
@@ -319,6 +325,9 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     R->chunk = RESOLVE_CHUNK;
     if (const char * e = getenv("XKB_STREAM")) R->stream_on = atoi(e) != 0;
     if (const char * e = getenv("XKB_CXX_HOST_BODY")) R->cxx_task_first = strcmp(e, "task") == 0;
+    if (const char * e = getenv("XKB_PLANNER")) R->ref_mode = strcmp(e, "reference") == 0;
+    if (R->ref_mode) R->stream_on = false;
+    if (const char * e = getenv("XKB_PLAN_RECORD")) R->plan_record = fopen(e, "wb");
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
     // fixed pools (address space only; pages are backed when touched) let a worker thread read
@@ -336,7 +345,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
         for (int k = 0; k < 3; ++k) R->prefaulter[k] = std::thread(prefault_loop, R, k);
     }
     register_file_formats(R);
-    int rc = xkb_planner_create_resident(&R->planner);
+    int rc = R->ref_mode ? xkb_planner_create(&R->planner) : xkb_planner_create_resident(&R->planner);
     if (rc == XKB_OK && R->gpu)
     {
         if (cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_init: stream");
@@ -399,6 +408,8 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     for (auto & d : R->dslot) { if (d.ev) cudaEventDestroy(d.ev); if (d.p) cudaFreeHost(d.p); }
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
+    for (void * p : R->allocs) if (p) cudaFree(p);
+    if (R->plan_record) fclose(R->plan_record);
     if (R->stream) cudaStreamDestroy(R->stream);
     const int st = R->status;
     delete R;
@@ -424,10 +435,10 @@ static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, boo
 {
     std::lock_guard<std::mutex> lk(R->plan_mu);       // the worker may be streaming a window
     int32_t id = -1;
-    int rc = xkb_planner_add_region(R->planner, (uint64_t) ptr, size, &id);
+    int rc = R->ref_mode ? XKB_OK : xkb_planner_add_region(R->planner, (uint64_t) ptr, size, &id);
     if (rc) return rc;
     void * mirror = unified ? ptr : nullptr;          // unified memory: the device uses it in place
-    if (R->gpu && !unified)
+    if (R->gpu && !unified && !R->ref_mode)           // reference mode: per-access allocations instead
     {
         cudaError_t e = cudaMalloc(&mirror, size);
         if (e != cudaSuccess) return xkb_set_cuda_error(e);
@@ -983,6 +994,24 @@ static void * mirror_of(xkb_runtime * R, uint64_t host)
     return p;
 }
 
+// Reference mode: device memory for every allocation the planner made since the last call.
+static int ensure_allocs(xkb_runtime * R)
+{
+    size_t n = 0;
+    int rc = xkb_planner_allocations(R->planner, nullptr, 0, &n);
+    if (rc || n <= R->allocs.size()) return rc;
+    std::vector<uint64_t> sizes(n);
+    if ((rc = xkb_planner_allocations(R->planner, sizes.data(), n, &n))) return rc;
+    while (R->allocs.size() < n)
+    {
+        void * p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, std::max<uint64_t>(sizes[R->allocs.size()], 16));
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        R->allocs.push_back(p);
+    }
+    return XKB_OK;
+}
+
 static int run_copies(xkb_runtime * R, cudaStream_t stream)
 {
     size_t n = 0;
@@ -990,6 +1019,18 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
     if (rc || !n) return rc;
     std::vector<xkb_copy_t> c(n);
     if ((rc = xkb_planner_copies(R->planner, c.data(), n, &n, 1))) return rc;
+    if (R->plan_record) fwrite(c.data(), sizeof(xkb_copy_t), n, R->plan_record);
+    if (R->ref_mode)
+    {
+        if ((rc = ensure_allocs(R))) return rc;
+        for (const xkb_copy_t & k : c)
+        {
+            (k.kind == XKB_COPY_H2D ? R->cur_h2d : k.kind == XKB_COPY_D2H ? R->cur_d2h : R->cur_d2d) += 1;
+            if (k.kind != XKB_COPY_D2D)
+                (k.kind == XKB_COPY_H2D ? R->cur_h2d_bytes : R->cur_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
+        }
+        return xkb_plan_execute(c.data(), n, R->allocs.data(), R->allocs.size(), stream);
+    }
     std::vector<void *> ptrs(R->regions.size(), nullptr);
     for (auto & kv : R->regions) ptrs[kv.second.id] = kv.second.mirror;
     for (const xkb_copy_t & k : c)
@@ -1384,6 +1425,42 @@ static void bg_finish(xkb_runtime * R)
     R->res_stale = R->res != nullptr;     // kept with its buffers; reset when the next batch starts
 }
 
+// Reference mode: the leading dimension (in elements) of each device view of the task run_one is
+// making coherent on this thread (-1: the host layout's).
+thread_local std::vector<int64_t> g_view_ld;
+
+// Reference mode: a built-in body on the per-access allocations its accesses were fetched into --
+// heat: access 0 the halo-expanded source tile, access 1 the destination tile, re-based on the
+// tile's first cell as the reference's launcher does (examples/heat-diffusion-2d/src/main.cc:
+// 214-219); axpby: access 0 the x range, access 1 the y range.
+static int run_builtin_views(xkb_runtime * R, Task & T, size_t t, const xkb_access_rec_t * recs, xkb_task_desc_t d,
+                             cudaStream_t stream)
+{
+    if (d.kind == XKB_TASK_NOOP) return XKB_OK;
+    if (T.nacc < 2) return xkb_set_error(XKB_EINVAL, "built-in task %zu: needs its two data accesses in reference mode", t);
+    const xkb_access_rec_t & r0 = recs[T.acc_off], & r1 = recs[T.acc_off + 1];
+    uint8_t * p0 = (uint8_t *) R->replica_pool[T.acc_off], * p1 = (uint8_t *) R->replica_pool[T.acc_off + 1];
+    if (!p0 || !p1) return xkb_set_error(XKB_EINVAL, "built-in task %zu: accesses without device views", t);
+    if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
+    {
+        const auto & h = d.u.heat;
+        const int64_t es = d.kind == XKB_TASK_HEAT_F64 ? 8 : 4, l0 = g_view_ld[0], l1 = g_view_ld[1];
+        if (r0.type != XKB_ACCESS_TYPE_BLAS_MATRIX || r1.type != XKB_ACCESS_TYPE_BLAS_MATRIX || l0 <= 0 || l1 <= 0)
+            return xkb_set_error(XKB_EINVAL, "heat task %zu: accesses 0 and 1 must be matrix tiles in reference mode", t);
+        const uint8_t * src = p0 + (((int64_t) h.x0 - (int64_t) r0.offset_m) + ((int64_t) h.y0 - (int64_t) r0.offset_n) * l0) * es;
+        uint8_t * dst = p1 + (((int64_t) h.x0 - (int64_t) r1.offset_m) + ((int64_t) h.y0 - (int64_t) r1.offset_n) * l1) * es;
+        return xkb_internal_diffusion_box(d.kind == XKB_TASK_HEAT_F64 ? XKB_F64 : XKB_F32, stream, src, l0, dst, l1, h.x0, h.y0,
+                                          (int64_t) h.x1 - h.x0, (int64_t) h.y1 - h.y0, h.nx, h.ny, h.c);
+    }
+    if (d.kind == XKB_TASK_AXPBY)
+    {
+        d.u.axpby.x = (uint64_t) (uintptr_t) (p0 - d.u.axpby.lo * 8);
+        d.u.axpby.y = (uint64_t) (uintptr_t) (p1 - d.u.axpby.lo * 8);
+        return xkb_internal_launch_task(&d, stream);
+    }
+    return xkb_set_error(XKB_EINVAL, "built-in task %zu: unknown kind %u", t, d.kind);
+}
+
 // The body of a task built with the C++ source API: each access's device_view points at the
 // access's first element where the body runs (its leading dimension in elements), then the
 // format's function is called as f(runtime, device, task) with the program's runtime_t and
@@ -1396,7 +1473,8 @@ static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStrea
     {
         const uintptr_t addr = (uintptr_t) R->replica_pool[T.acc_off + a];
         const xkrt::memory_view_t & h = acc[a].host_view;
-        acc[a].device_view = xkrt::memory_replica_view_t(addr, acc[a].type == ACCESS_TYPE_BLAS_MATRIX ? h.ld : h.m);
+        const int64_t vld = a < g_view_ld.size() ? g_view_ld[a] : -1;
+        acc[a].device_view = xkrt::memory_replica_view_t(addr, vld >= 0 ? (size_t) vld : acc[a].type == ACCESS_TYPE_BLAS_MATRIX ? h.ld : h.m);
         acc[a].state = xkrt::ACCESS_STATE_FETCHED;
     }
     task->state.value = xkrt::TASK_STATE_EXECUTING;
@@ -1430,6 +1508,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     Task & T = R->pending[t];
     const bool dev = is_device(R, T);
     int rc = XKB_OK;
+    g_view_ld.assign(T.nacc, -1);
     {
         std::lock_guard<std::mutex> lk(R->plan_mu);
         for (uint32_t a = 0; a < T.nacc && rc == XKB_OK; ++a)
@@ -1438,6 +1517,21 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
             if (r.type == REC_NONE) continue;
             if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
             const uint64_t begin = rec_begin(r);
+            if (R->ref_mode)
+            {
+                // the reference's decisions: the access's own device allocation (its view), the
+                // copies its memory tree plans; a host access reads the host memory in place
+                xkb_view_t v;
+                if ((rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v))) break;
+                if (dev)
+                {
+                    if ((rc = ensure_allocs(R))) break;
+                    R->replica_pool[T.acc_off + a] = (uint8_t *) R->allocs[v.alloc] + v.off;
+                    g_view_ld[a] = v.ld;
+                }
+                else R->replica_pool[T.acc_off + a] = (void *) begin;
+                continue;
+            }
             R->replica_pool[T.acc_off + a] = dev ? mirror_of(R, begin) : (void *) begin;
             // a host task on memory no region covers: that memory never has a device copy;
             // unified memory needs no copy either way
@@ -1461,6 +1555,12 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
         {
             xkb_task_desc_t d;
             if (T.nargs < sizeof(d)) rc = xkb_set_error(XKB_EINVAL, "built-in task %zu: args are not an xkb_task_desc_t", t);
+            else if (R->ref_mode)
+            {
+                memcpy(&d, R->args_pool.data() + T.args_off, sizeof(d));
+                d.kind = (uint32_t) f.builtin;
+                rc = run_builtin_views(R, T, t, recs, d, stream);
+            }
             else
             {
                 memcpy(&d, R->args_pool.data() + T.args_off, sizeof(d));
@@ -1545,6 +1645,7 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
     size_t nw = std::thread::hardware_concurrency();
     if (const char * e = getenv("XKB_HOST_THREADS")) nw = strtoul(e, nullptr, 10);
     nw = std::max<size_t>(1, std::min<size_t>({nw ? nw : 1, 64, nt}));
+    if (R->ref_mode) nw = 1;             // one task at a time, in spawn order: the canonical schedule
     while (R->wstreams.size() < nw)
     {
         cudaStream_t st;
@@ -1576,7 +1677,13 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
                     }
                     continue;
                 }
-                t = D.ready.front(); D.ready.pop_front();
+                if (R->ref_mode)
+                {
+                    // the ready task spawned first (with one worker: the next one in spawn order)
+                    auto it = std::min_element(D.ready.begin(), D.ready.end());
+                    t = *it; D.ready.erase(it);
+                }
+                else { t = D.ready.front(); D.ready.pop_front(); }
             }
             const int rc = run_one(R, base + t, recs, R->wstreams[k]);
             if (rc)
@@ -1804,7 +1911,7 @@ static int wait_batch(xkb_runtime * R)
         fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms, %zu of %zu tasks streamed\n", nacc, records_ms,
                 R->last_ms[0] - records_ms, P, ntasks);
 
-    bool fused = true;
+    bool fused = !R->ref_mode;       // reference mode: every task through the dataflow path, one at a time
     for (size_t t = P; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
 
     const bool all_streamed = fused && P == ntasks;
@@ -1879,8 +1986,25 @@ static int wait_batch(xkb_runtime * R)
     {
         t0 = std::chrono::steady_clock::now();
         // every block whose only coherent copy is on the GPU (exactly the blocks device tasks
-        // wrote: each wait leaves the host coherent), one walk over the planner's partition
-        rc = xkb_planner_flush_to_host(R->planner);
+        // wrote: each wait leaves the host coherent), one walk over the planner's partition;
+        // reference mode: the reference's fetch to the host of every written access
+        // (memory_coherent_async's host reads, src/memory/coherent.cc:137-231), in spawn order
+        if (R->ref_mode)
+        {
+            for (size_t t = P; t < ntasks && rc == XKB_OK; ++t)
+            {
+                const Task & T = R->pending[t];
+                if (!is_device(R, T)) continue;
+                for (uint32_t a = 0; a < T.nacc && rc == XKB_OK; ++a)
+                {
+                    const xkb_access_rec_t & r = recs[T.acc_off + a];
+                    if ((r.type == XKB_ACCESS_TYPE_BLAS_MATRIX || r.type == XKB_ACCESS_TYPE_SEGMENT) && (r.mode & XKB_ACCESS_MODE_W))
+                        rc = xkb_planner_fetch(R->planner, &r, a, 0, nullptr);
+                }
+            }
+        }
+        else
+            rc = xkb_planner_flush_to_host(R->planner);
         const double fetch_ms = ms_since(t0);
         if (rc == XKB_OK) rc = run_copies(R, R->stream);
         if (all_streamed)
@@ -1932,7 +2056,7 @@ extern "C" void xkrt_task_wait(xkrt_runtime_t * runtime)
     bg_finish(R);
     if (getenv("XKB_TRACE_WAIT")) fprintf(stderr, "xkrt_task_wait: %.1f ms in all, %.1f ms to finish\n", wb_ms, ms_since(w0) - wb_ms);
     R->last_h2d = R->cur_h2d; R->last_d2h = R->cur_d2h; R->last_h2d_bytes = R->cur_h2d_bytes; R->last_d2h_bytes = R->cur_d2h_bytes;
-    R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = 0;
+    R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = R->cur_d2d = 0;
     R->in_wait = false;
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
     R->args_dense = true;

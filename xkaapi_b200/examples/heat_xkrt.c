@@ -16,7 +16,8 @@
  *   F32 = 1: FP32 storage (the FP32 tile body); init.bin / out.bin hold FP64 grids (NX*NY,
  *   row-major) -- the FP32 grid starts from the FP64 values rounded to float.
  * Output: one JSON line per repetition {rep, tasks, seconds, tasks_per_s, spawn_s, resolve_ms,
- * coherency_ms, run_ms, writeback_ms, edges, h2d, d2h (copies), h2d_bytes, d2h_bytes, fused, checksum}. */
+ * coherency_ms, run_ms, writeback_ms, edges, h2d, d2h (copies), h2d_bytes, d2h_bytes, fused, checksum, grid_a,
+ * grid_b}. */
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -154,10 +155,11 @@ int main(int argc, char ** argv)
         if (xkrt_deinit(rt) != 0) { fprintf(stderr, "xkrt_deinit: %s\n", xkb_last_error()); return 1; }
         printf("{\"rep\": %d, \"tasks\": %llu, \"seconds\": %.6f, \"tasks_per_s\": %.1f, \"spawn_s\": %.6f, "
                "\"resolve_ms\": %.3f, \"coherency_ms\": %.3f, \"run_ms\": %.3f, \"writeback_ms\": %.3f, \"edges\": %llu, "
-               "\"h2d\": %llu, \"d2h\": %llu, \"h2d_bytes\": %llu, \"d2h_bytes\": %llu, \"fused\": %d, \"checksum\": %.17g}\n",
+               "\"h2d\": %llu, \"d2h\": %llu, \"h2d_bytes\": %llu, \"d2h_bytes\": %llu, \"fused\": %d, \"checksum\": %.17g, "
+               "\"grid_a\": %llu, \"grid_b\": %llu}\n",
                rep, (unsigned long long) tasks, t2 - t0, (double) tasks / (t2 - t0), t1 - t0, ms[0], ms[1], ms[2], ms[3],
                (unsigned long long) edges, (unsigned long long) h2d, (unsigned long long) d2h, (unsigned long long) h2d_bytes,
-               (unsigned long long) d2h_bytes, fused, checksum);
+               (unsigned long long) d2h_bytes, fused, checksum, (unsigned long long) (uintptr_t) a, (unsigned long long) (uintptr_t) b);
         fflush(stdout);
     }
     free(init);
