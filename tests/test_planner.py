@@ -204,3 +204,154 @@ def test_flush_to_host_matches_write_back_fetches(seed):
     assert _copied_bytes(a) == _copied_bytes(b)
     P2.flush_to_host()
     assert len(P2.copies(take=True)) == 0
+
+
+def _byte_set(copies, kind):
+    """Host byte intervals (merged) that the copies of one kind read (H2D) or write (D2H)."""
+    col = 5 if kind == xk.COPY_H2D else 9
+    ldc = 6 if kind == xk.COPY_H2D else 10
+    iv = []
+    for c in copies[copies[:, 2] == kind]:
+        base, ld, m, n, s = int(c[col]), int(c[ldc]), int(c[11]), int(c[12]), int(c[13])
+        for r in range(n):
+            a = base + r * ld * s if ld else base
+            iv.append((a, a + m * s))
+    iv.sort()
+    out = []
+    for a, b in iv:
+        if out and a <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], b))
+        else:
+            out.append((a, b))
+    return out
+
+
+def _spans(recs):
+    """Merged host byte spans the records touch (regions for the resident planner)."""
+    iv = []
+    for r in recs:
+        if r["type"] == 1:                                          # segment [addr, ld)
+            iv.append((int(r["addr"]), int(r["ld"])))
+        else:
+            s = int(r["sizeof_type"])
+            a = int(r["addr"]) + (int(r["offset_n"]) * int(r["ld"]) + int(r["offset_m"])) * s
+            iv.append((a, a + ((int(r["n"]) - 1) * int(r["ld"]) + int(r["m"])) * s))
+    iv.sort()
+    out = []
+    for a, b in iv:
+        if out and a <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], b))
+        else:
+            out.append((a, b))
+    return out
+
+
+def _minus(a, b):
+    """Interval set difference a - b (both merged, sorted)."""
+    out, j = [], 0
+    for lo, hi in a:
+        cur = lo
+        while j < len(b) and b[j][1] <= cur:
+            j += 1
+        k = j
+        while k < len(b) and b[k][0] < hi:
+            if b[k][0] > cur:
+                out.append((cur, b[k][0]))
+            cur = max(cur, b[k][1])
+            k += 1
+        if cur < hi:
+            out.append((cur, hi))
+    return out
+
+
+def _device_written(recs):
+    """Merged host byte spans of the device fetches with W mode (rows of matrices, segments)."""
+    iv = []
+    for r in recs:
+        if (r["reserved"] & 1) or not (r["mode"] & 2):
+            continue
+        if r["type"] == 1:
+            iv.append((int(r["addr"]), int(r["ld"])))
+        else:
+            s, ld = int(r["sizeof_type"]), int(r["ld"])
+            a = int(r["addr"]) + (int(r["offset_n"]) * ld + int(r["offset_m"])) * s
+            iv += [(a + k * ld * s, a + k * ld * s + int(r["m"]) * s) for k in range(int(r["n"]))]
+    iv.sort()
+    out = []
+    for a, b in iv:
+        if out and a <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], b))
+        else:
+            out.append((a, b))
+    return out
+
+
+def _rec_bytes(r):
+    """Merged host byte spans of one record."""
+    if r["type"] == 1:
+        return [(int(r["addr"]), int(r["ld"]))]
+    s, ld = int(r["sizeof_type"]), int(r["ld"])
+    a = int(r["addr"]) + (int(r["offset_n"]) * ld + int(r["offset_m"])) * s
+    iv = sorted((a + k * ld * s, a + k * ld * s + int(r["m"]) * s) for k in range(int(r["n"])))
+    out = []
+    for lo, hi in iv:
+        if out and lo <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], hi))
+        else:
+            out.append((lo, hi))
+    return out
+
+
+def _union(a, b):
+    out = []
+    for lo, hi in sorted(a + b):
+        if out and lo <= out[-1][1]:
+            out[-1] = (out[-1][0], max(out[-1][1], hi))
+        else:
+            out.append((lo, hi))
+    return out
+
+
+def _inter(a, b):
+    return _minus(a, _minus(a, b))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_resident_copy_set_derives_from_reference_plan(case):
+    """The resident mode (the C API's default layout: one mirror per registered region) moves the
+    host bytes the reference's memory tree moves, on every golden stream:
+    * H2D: the set of host bytes its copies read equals the set the reference's copies read (the
+      reference may read a byte again into another allocation view; one mirror needs it once);
+    * D2H, fetch by fetch: the bytes it copies back for a host access that reads are exactly the
+      bytes of the access that a device access wrote since the host last had them (none for a host
+      access that only writes) -- and the reference copies those too; what the reference copies besides is data the host already holds: bytes the GPU
+      only read (its memory tree does not keep the host's bit when it copies a block to the device,
+      memory-tree.hpp:1110-1215) or bytes a host access wrote since (the memory tree treats a host
+      fetch as a read and leaves the device views coherent).
+    The reference's D2D copies between allocation views have no counterpart: one mirror holds
+    every view of a block."""
+    recs = G[case + "__stream"]
+    ref = G[case + "__plan"]
+    P = xk.Planner(resident=True)
+    for a, b in _spans(recs):
+        P.add_region(a, b - a)
+    for i in range(len(recs)):
+        first = i if i == 0 or recs[i]["task"] != recs[i - 1]["task"] else first
+        P.fetch(recs[i], i - first, 0 if recs[i]["reserved"] & 1 else 1)
+    res = P.copies()
+    assert not (res[:, 2] == xk.COPY_D2D).any()
+    assert _byte_set(res, xk.COPY_H2D) == _byte_set(ref, xk.COPY_H2D)
+    fresh = []                    # bytes whose newest data is on the GPU only
+    for i in range(len(recs)):
+        r = recs[i]
+        first = i if i == 0 or recs[i]["task"] != recs[i - 1]["task"] else first
+        span = _rec_bytes(r)
+        if not r["reserved"] & 1:
+            if r["mode"] & 2:
+                fresh = _union(fresh, span)
+            continue
+        key = lambda q: q[(q[:, 0] == int(r["task"])) & (q[:, 1] == i - first)]
+        mine, theirs = _byte_set(key(res), xk.COPY_D2H), _byte_set(key(ref), xk.COPY_D2H)
+        assert mine == (_inter(span, fresh) if r["mode"] & 1 else []), i     # a host write needs no data
+        assert _minus(mine, theirs) == [], i
+        fresh = _minus(fresh, span)           # the host holds the newest data of the access now
