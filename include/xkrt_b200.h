@@ -206,6 +206,23 @@ XKB_API int xkb_planner_copies(xkb_planner_t * planner, xkb_copy_t * out, size_t
 /* Byte size of every device allocation made so far, in allocation order. */
 XKB_API int xkb_planner_allocations(xkb_planner_t * planner, uint64_t * sizes, size_t cap, size_t * n);
 
+/* Device budget of a planner in the reference's mode (before its first fetch): every device
+ * allocation gets an offset in one region of `bytes` bytes, handed out best fit (the reference's
+ * area allocator, src/driver/device.cc:185-280; 256-byte rounding). When an allocation does not
+ * fit, allocations the task being fetched does not use are evicted, oldest first: each block
+ * loses its view on them, and a block whose only coherent copy was such a view is first copied
+ * back to the host (a D2H record of the fetch that needed the room). The reference evicts only
+ * blocks coherent elsewhere (memory-tree.hpp:1221-1324) and aborts when that is not enough;
+ * XKB_ENOMEM here when the task's own allocations leave no room. */
+XKB_API int xkb_planner_set_device_budget(xkb_planner_t * planner, uint64_t bytes);
+/* Offset of each allocation in the budget, in allocation order, and whether it is still live
+ * (either array may be NULL). An evicted allocation keeps its offset: the copies planned by the
+ * fetch that evicted it read it before the room is reused (run each fetch's copies before the
+ * next fetch). */
+XKB_API int xkb_planner_allocation_offsets(xkb_planner_t * planner, int64_t * offsets, uint8_t * live, size_t cap, size_t * n);
+/* Allocations evicted and blocks written back to the host by evictions so far. */
+XKB_API int xkb_planner_eviction_stats(xkb_planner_t * planner, uint64_t * evicted, uint64_t * written_back);
+
 /* Resident mode (the B200 layout): every host region registered with xkb_planner_add_region
  * has ONE device mirror with the host layout (allocation ordinal = region index, byte offset =
  * offset in the region). A fetch to the GPU copies (H2D) only the blocks of the access the

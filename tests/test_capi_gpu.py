@@ -135,3 +135,13 @@ def test_heat_many_waits_one_runtime(torch_cuda, tmp_path, chunk, nx, ny, ts, st
     assert r.returncode == 0, r.stderr
     assert json.loads(r.stdout)["waits"] == waits
     np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), O.heat_run(g, nx, ny, steps, 0.2))
+
+
+def test_spawn_generic_detachable_count_and_ocr(torch_cuda, tmp_path):
+    """xkrt_task_spawn_generic: a detachable task spawned with an initial counter of 2 completes
+    only after two xkrt_task_detachable_decr from another thread (its successor sees both), one
+    with counter 0 completes when its body returns, and device tasks spawned with a non-default
+    ocr_access run and compute the right y (one GPU owns every access)."""
+    r = subprocess.run([build("spawn_generic_capi", tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == {"order": 1, "early": 1, "axpby": 1}

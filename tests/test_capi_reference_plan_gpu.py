@@ -81,3 +81,19 @@ def test_capi_reference_plan_and_grid(torch_cuda, tmp_path, exe):
     # the write-back: the reference's fetch to the host of every written access moves the interior
     # of both grids back once (the later fetches of a block already on the host copy nothing)
     assert int((wb[:, 11] * wb[:, 12] * wb[:, 13]).sum()) == 2 * (N - 2) * (N - 2) * 8
+
+
+@pytest.mark.parametrize("exe,budget", [("heat_cxx", "12M"), ("heat_xkrt", "12M"), ("heat_xkrt", "3M")])
+def test_capi_device_budget_smaller_than_the_grids(torch_cuda, tmp_path, exe, budget):
+    """Reference mode with XKB_DEVICE_BUDGET below the two grids (2 x 8 MiB): the per-access
+    allocations share one budget, old ones are evicted (blocks whose only copy they hold written
+    back to the host first) and the grid is still the oracle's, bit for bit."""
+    n, ts, steps = 1024, 128, 8
+    g = O.heat_init(n, n, seed=12)
+    g.tofile(tmp_path / "init.bin")
+    env = dict(os.environ, XKB_PLANNER="reference", XKB_DEVICE_BUDGET=budget)
+    args = [n, n, ts, steps, 1] + ([] if exe == "heat_cxx" else [0]) + [tmp_path / "init.bin", tmp_path / "out.bin"]
+    r = subprocess.run([os.path.join(REPO, "xkaapi_b200", "examples", exe)] + [str(a) for a in args], capture_output=True,
+                       text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(n, n), O.heat_run(g, n, n, steps, 0.2))

@@ -355,3 +355,75 @@ def test_resident_copy_set_derives_from_reference_plan(case):
         assert mine == (_inter(span, fresh) if r["mode"] & 1 else []), i     # a host write needs no data
         assert _minus(mine, theirs) == [], i
         fresh = _minus(fresh, span)           # the host holds the newest data of the access now
+
+
+def _run_plan_on_bytes(copies, host, base, dev, offs):
+    """Execute copy records on byte arrays: `host` holds the host memory from address `base`,
+    `dev` the device budget (allocation k at offs[k])."""
+    for c in copies:
+        kind, m, n, s = int(c[2]), int(c[11]), int(c[12]), int(c[13])
+        w = m * s
+        def rows(dev_side, alloc, off, ld):
+            buf, b0 = (dev, int(offs[alloc]) + off) if dev_side else (host, off - base)
+            pitch = ld * s if ld else w
+            return [(buf, b0 + r * pitch) for r in range(n)]
+        src = rows(kind != 0, int(c[4]), int(c[5]), int(c[6]))
+        dst = rows(kind != 1, int(c[8]), int(c[9]), int(c[10]))
+        for (sb, so), (db, do) in zip(src, dst):
+            db[do:do + w] = sb[so:so + w]
+
+
+@pytest.mark.parametrize("budget_mb,steps", [(12, 6), (3, 4)])
+def test_budget_eviction_runs_heat_bit_exact_on_cpu(budget_mb, steps):
+    """Reference mode with a device budget smaller than the two grids (2 x 8 MiB): the planner's
+    allocations stay inside the budget without overlapping, evictions write dirty blocks back to
+    the host, and executing its copies on byte arrays with each tile computed on its device views
+    gives the oracle's grid, bit for bit."""
+    import sys
+    import streams as S
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import kernels_oracle as O
+    n, ts = 1024, 128
+    base = 1 << 30
+    recs = S.heat_stream(n, n, ts, ts, steps, base_src=base, base_dst=base + n * n * 8)
+    g = O.heat_init(n, n, seed=8)
+    host = np.zeros(2 * n * n * 8, np.uint8)
+    host[:n * n * 8] = g.view(np.uint8).ravel()
+    host[n * n * 8:] = g.view(np.uint8).ravel()
+    budget = budget_mb << 20
+    dev = np.zeros(budget, np.uint8)
+    P = xk.Planner(budget=budget)
+    live = {}
+    for t in range(len(recs) // 2):
+        views = []
+        for a in range(2):          # each fetch's copies run before the next fetch (as the runtime does)
+            views.append(P.fetch(recs[2 * t + a], a, 1))
+            offs, live = P.offsets()
+            sizes = P.allocations()
+            spans = sorted((int(offs[k]), int(offs[k]) + (int(sizes[k]) + 255) // 256 * 256) for k in range(len(offs)) if live[k])
+            assert all(e <= budget for _, e in spans)
+            assert all(spans[i][1] <= spans[i + 1][0] for i in range(len(spans) - 1))
+            _run_plan_on_bytes(P.copies(take=True), host, base, dev, offs)
+        # the tile body on the task's two device views (src: halo tile, dst: interior tile)
+        r0, r1 = recs[2 * t], recs[2 * t + 1]
+        (a0, o0, l0), (a1, o1, l1) = views
+        src = dev[offs[a0] + o0:].view(np.float64) if (offs[a0] + o0) % 8 == 0 else None
+        assert src is not None
+        m0, n0 = int(r0["m"]), int(r0["n"])
+        S0 = np.lib.stride_tricks.as_strided(src, shape=(n0, m0), strides=(l0 * 8, 8))
+        D = O._update(S0.astype(np.float64), 0.2)         # interior of the halo tile = the W tile
+        dst = dev[offs[a1] + o1:].view(np.float64)
+        m1, n1 = int(r1["m"]), int(r1["n"])
+        D1 = np.lib.stride_tricks.as_strided(dst, shape=(n1, m1), strides=(l1 * 8, 8))
+        ox, oy = int(r1["offset_m"]) - int(r0["offset_m"]) - 1, int(r1["offset_n"]) - int(r0["offset_n"]) - 1
+        D1[:, :] = D[oy:oy + n1, ox:ox + m1]
+    # write-back of every written access, in spawn order
+    for t in range(len(recs) // 2):
+        w = recs[2 * t + 1].copy()
+        w["mode"] = S.R
+        P.fetch(w, 1, 0)
+    _run_plan_on_bytes(P.copies(take=True), host, base, dev, P.offsets()[0])
+    final = host[(steps % 2) * n * n * 8:][:n * n * 8].view(np.float64).reshape(n, n)
+    np.testing.assert_array_equal(final, O.heat_run(g, n, n, steps, 0.2))
+    evicted, written = P.eviction_stats()
+    assert evicted > 0 and written > 0

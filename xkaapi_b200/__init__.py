@@ -74,6 +74,9 @@ SIGNATURES = {
     "xkb_heat_step": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp]),
     "xkb_heat_step_cfg": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, ctypes.POINTER(HeatCfg), _vp]),
     "xkb_heat_norms": (_int, [_int, _vp, _vp, _i64, _i64, _i64, _dbl, _vp, _vp]),
+    "xkb_planner_set_device_budget": (_int, [_vp, ctypes.c_uint64]),
+    "xkb_planner_allocation_offsets": (_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "xkb_planner_eviction_stats": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
     "xkb_sched_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_sched_destroy": (_int, [_vp]),
@@ -324,12 +327,28 @@ class Planner:
     an (n, 14) int64 array: task, access, kind, src_dev, src_alloc, src_off, src_ld, dst_dev,
     dst_alloc, dst_off, dst_ld, m, n, sizeof."""
 
-    def __init__(self, resident=False):
+    def __init__(self, resident=False, budget=0):
         self._h = ctypes.c_void_p()
         if resident:
             check(lib().xkb_planner_create_resident(ctypes.byref(self._h)))
         else:
             check(lib().xkb_planner_create(ctypes.byref(self._h)))
+            if budget:
+                check(lib().xkb_planner_set_device_budget(self._h, budget))
+
+    def offsets(self):
+        """(offset, live) of every allocation in the device budget."""
+        import numpy as np
+        n = ctypes.c_size_t()
+        check(lib().xkb_planner_allocation_offsets(self._h, None, None, 0, ctypes.byref(n)))
+        out, live = np.zeros(n.value, dtype=np.int64), np.zeros(n.value, dtype=np.uint8)
+        check(lib().xkb_planner_allocation_offsets(self._h, out.ctypes.data, live.ctypes.data, n.value, ctypes.byref(n)))
+        return out, live.astype(bool)
+
+    def eviction_stats(self):
+        e, w = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().xkb_planner_eviction_stats(self._h, ctypes.byref(e), ctypes.byref(w)))
+        return e.value, w.value
 
     def add_region(self, base, size):
         r = ctypes.c_int32()

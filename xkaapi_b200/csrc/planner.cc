@@ -224,11 +224,59 @@ void rinsert(RFrame & f, const Rect & r, std::vector<RPartite> & out)
     }
 }
 
+// Device memory of a budget, handed out best fit from a free list: the smallest free piece that
+// fits, split when what remains is at least half the request (else given whole), neighbouring
+// free pieces merged again -- the reference's area allocator (src/driver/device.cc:185-280),
+// with 256-byte rounding instead of 8 so that every allocation suits vector loads.
+struct Arena {
+    uint64_t cap = 0;
+    std::map<uint64_t, uint64_t> free_at;              // offset -> size
+    void init(uint64_t bytes) { cap = bytes; free_at.clear(); if (bytes) free_at[0] = bytes; }
+    // offset of `size` bytes (*got: the bytes taken), or false
+    bool take(uint64_t size, uint64_t & off, uint64_t & got)
+    {
+        size = (size + 255) & ~(uint64_t) 255;
+        auto best = free_at.end();
+        for (auto it = free_at.begin(); it != free_at.end(); ++it)
+            if (it->second >= size && (best == free_at.end() || it->second < best->second)) best = it;
+        if (best == free_at.end()) return false;
+        off = best->first;
+        const uint64_t rest = best->second - size;
+        free_at.erase(best);
+        if (rest >= size / 2 && rest > 0) { free_at[off + size] = rest; got = size; }
+        else got = size + rest;
+        return true;
+    }
+    void give(uint64_t off, uint64_t size)
+    {
+        auto it = free_at.emplace(off, size).first;
+        auto nx = std::next(it);
+        if (nx != free_at.end() && it->first + it->second == nx->first) { it->second += nx->second; free_at.erase(nx); }
+        if (it != free_at.begin())
+        {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; free_at.erase(it); }
+        }
+    }
+    uint64_t largest() const { uint64_t m = 0; for (auto & kv : free_at) m = std::max(m, kv.second); return m; }
+};
+
 } // namespace
 
 struct xkb_planner {
     std::map<std::pair<uint64_t, uint64_t>, std::unique_ptr<Frame>> frames;
     std::vector<uint64_t> allocs;
+    // device budget (0: none): each allocation gets an offset in it; allocations not used by the
+    // task being fetched are evicted, oldest first, when a new one does not fit
+    uint64_t budget = 0;
+    Arena arena;
+    std::vector<int64_t> alloc_off;                   // offset in the budget (kept once evicted: the copies
+                                                      // planned before the eviction still read it)
+    std::vector<uint64_t> alloc_got;                  // bytes taken from the budget
+    std::vector<uint8_t> alloc_live;                  // 0 once evicted
+    int64_t cur_task = -1;
+    std::vector<int32_t> pinned;                      // allocations of the current task's views
+    uint64_t evicted = 0, written_back = 0;
     std::vector<xkb_copy_t> copies;
     std::vector<Partite> scratch;
     // resident mode: one device mirror per registered host region (base -> (size, index))
@@ -331,6 +379,75 @@ static int resident_fetch(xkb_planner * P, const xkb_access_rec_t & a, int64_t a
     return XKB_OK;
 }
 
+// Evict allocation k: every block with a view on it loses that view; a block whose only coherent
+// copy is that view (the host's is stale) is first copied back to the host (D2H, recorded for the
+// fetch that needs the room). The reference only evicts blocks coherent elsewhere and gives up
+// on the rest (memory-tree.hpp:1221-1324); writing them back lets any working set that fits one
+// task at a time run.
+static void evict(xkb_planner * P, int32_t k, int64_t task, int64_t access_index)
+{
+    for (auto & fk : P->frames)
+    {
+        Frame & f = *fk.second;
+        const bool seg = f.ld == ~0ull;
+        const uint64_t stride = seg ? 0 : f.ld * f.s;
+        for (auto & sk : f.slabs)
+            for (auto & bk : sk.second.blocks)
+            {
+                State & st = bk.second.st;
+                int vi = -1;
+                for (int q = 0; q < st.nviews; ++q) if (st.views[q].alloc == k) { vi = q; break; }
+                if (vi < 0) continue;
+                const View v = st.views[vi];
+                if (st.coh == (1u << vi) && !(st.dev & DEV_HOST))
+                {
+                    Partite p{sk.first, sk.second.x1, bk.first, bk.second.y1, &st};
+                    push_copy(P, task, access_index, XKB_COPY_D2H, p, f.ld, f.s, k, view_off(v, p.x0, p.y0, f.s),
+                              seg ? 0 : (int64_t) v.ld, -1, (int64_t) (p.x0 + p.y0 * stride), seg ? 0 : (int64_t) f.ld);
+                    st.dev |= DEV_HOST;
+                    ++P->written_back;
+                }
+                for (int q = vi; q + 1 < st.nviews; ++q) st.views[q] = st.views[q + 1];
+                --st.nviews;
+                st.coh = (uint8_t) ((st.coh & ((1u << vi) - 1)) | ((st.coh >> (vi + 1)) << vi));
+                if (!st.coh) st.dev = (uint8_t) ((st.dev & ~DEV_GPU) | DEV_HOST);
+            }
+    }
+    P->arena.give((uint64_t) P->alloc_off[k], P->alloc_got[k]);
+    P->alloc_live[k] = 0;
+    ++P->evicted;
+}
+
+// A new allocation of `bytes` (its ordinal in *out): with a budget, room is made by evicting the
+// oldest allocations the current task does not use.
+static int new_allocation(xkb_planner * P, uint64_t bytes, int64_t task, int64_t access_index, int32_t * out)
+{
+    const int32_t id = (int32_t) P->allocs.size();
+    if (P->budget)
+    {
+        uint64_t off = 0, got = 0;
+        int32_t next = 0;
+        while (!P->arena.take(bytes, off, got))
+        {
+            while (next < id && (!P->alloc_live[next] ||
+                                 std::find(P->pinned.begin(), P->pinned.end(), next) != P->pinned.end()))
+                ++next;
+            if (next >= id)
+                return xkb_set_error(XKB_ENOMEM, "planner: %llu bytes do not fit the device budget of %llu bytes next to the "
+                                                 "current task's own allocations (largest free piece %llu)",
+                                     (unsigned long long) bytes, (unsigned long long) P->budget,
+                                     (unsigned long long) P->arena.largest());
+            evict(P, next++, task, access_index);
+        }
+        P->alloc_off.push_back((int64_t) off);
+        P->alloc_got.push_back(got);
+        P->alloc_live.push_back(1);
+    }
+    P->allocs.push_back(bytes);
+    *out = id;
+    return XKB_OK;
+}
+
 static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access_index, int device, xkb_view_t * view)
 {
     if (P->resident) return resident_fetch(P, a, access_index, device, view);
@@ -368,6 +485,7 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
         return XKB_OK;
     }
     if (device != 1) return xkb_set_error(XKB_EINVAL, "planner: device must be 0 (host) or 1 (GPU)");
+    if ((int64_t) a.task != P->cur_task) { P->cur_task = (int64_t) a.task; P->pinned.clear(); }
 
     for (int k = 0; k < nr; ++k) insert(f, rr[k]);
     P->scratch.clear();
@@ -404,8 +522,9 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
             if (p.st->nviews >= MAX_VIEWS)
                 return xkb_set_error(XKB_ERANGE, "planner: a block would need more than %d allocations on the device "
                                                  "(the reference stops here too)", MAX_VIEWS);
-        alloc = (int32_t) P->allocs.size();
-        P->allocs.push_back(seg ? (r.x1 - r.x0) : a.m * a.n * a.sizeof_type);
+        // (eviction removes views from blocks, never blocks: `parts` stays valid)
+        if ((rc = new_allocation(P, seg ? (r.x1 - r.x0) : a.m * a.n * a.sizeof_type, (int64_t) a.task, access_index, &alloc)))
+            return rc;
         for (size_t k = 0; k < parts.size(); ++k)
         {
             State & st = *parts[k].st;
@@ -413,6 +532,7 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
         }
     }
     auto view_idx = [&](const State & st) { for (int q = 0; q < st.nviews; ++q) if (st.views[q].alloc == alloc) return q; return -1; };
+    P->pinned.push_back(alloc);
     // (4) the access's device view: its corner block's view
     for (const Partite & p : parts)
         if (p.x0 == r.x0 && p.y0 == r.y0)
@@ -502,6 +622,33 @@ extern "C" int xkb_planner_allocations(xkb_planner_t * P, uint64_t * sizes, size
     if (!sizes) return XKB_OK;
     if (cap < P->allocs.size()) return xkb_set_error(XKB_ERANGE, "planner_allocations: %zu entries needed", P->allocs.size());
     if (!P->allocs.empty()) memcpy(sizes, P->allocs.data(), P->allocs.size() * sizeof(uint64_t));
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_set_device_budget(xkb_planner_t * P, uint64_t bytes)
+{
+    if (!P || P->resident || !P->allocs.empty()) return xkb_set_error(XKB_EINVAL, "planner_set_device_budget: a fresh planner of the reference mode");
+    P->budget = bytes;
+    P->arena.init(bytes);
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_allocation_offsets(xkb_planner_t * P, int64_t * offs, uint8_t * live, size_t cap, size_t * n)
+{
+    if (!P || !n || !P->budget) return xkb_set_error(XKB_EINVAL, "planner_allocation_offsets: needs a planner with a device budget");
+    *n = P->alloc_off.size();
+    if (!offs && !live) return XKB_OK;
+    if (cap < P->alloc_off.size()) return xkb_set_error(XKB_ERANGE, "planner_allocation_offsets: %zu entries needed", P->alloc_off.size());
+    if (offs && !P->alloc_off.empty()) memcpy(offs, P->alloc_off.data(), P->alloc_off.size() * sizeof(int64_t));
+    if (live && !P->alloc_live.empty()) memcpy(live, P->alloc_live.data(), P->alloc_live.size());
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_eviction_stats(xkb_planner_t * P, uint64_t * evicted, uint64_t * written_back)
+{
+    if (!P) return xkb_set_error(XKB_EINVAL, "planner_eviction_stats: null planner");
+    if (evicted) *evicted = P->evicted;
+    if (written_back) *written_back = P->written_back;
     return XKB_OK;
 }
 

@@ -235,6 +235,8 @@ struct xkb_runtime {
     // H2D / D2D / D2H as its memory tree plans them) on the tasks run one at a time in spawn order
     bool ref_mode = false;
     std::vector<void *> allocs;                       //   device memory of each planner allocation
+    uint64_t budget = 0;                              //   XKB_DEVICE_BUDGET: one region the allocations share,
+    uint8_t * budget_base = nullptr;                  //   evicting old ones when a new one does not fit
     FILE * plan_record = nullptr;                     // XKB_PLAN_RECORD: every executed copy record
     void * cxx_rt = nullptr;                          // the C++ runtime_t bodies of C++ tasks receive
     bool cxx_task_first = false;                      // XKB_CXX_HOST_BODY=task: host bodies of C++ tasks get the task first
@@ -327,6 +329,15 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     if (const char * e = getenv("XKB_CXX_HOST_BODY")) R->cxx_task_first = strcmp(e, "task") == 0;
     if (const char * e = getenv("XKB_PLANNER")) R->ref_mode = strcmp(e, "reference") == 0;
     if (R->ref_mode) R->stream_on = false;
+    if (const char * e = getenv("XKB_DEVICE_BUDGET"))
+    {
+        char * end = nullptr;
+        double v = strtod(e, &end);
+        if (end && (*end == 'k' || *end == 'K')) v *= 1024.0;
+        else if (end && (*end == 'm' || *end == 'M')) v *= 1024.0 * 1024.0;
+        else if (end && (*end == 'g' || *end == 'G')) v *= 1024.0 * 1024.0 * 1024.0;
+        R->budget = v > 0 ? (uint64_t) v : 0;
+    }
     if (const char * e = getenv("XKB_PLAN_RECORD")) R->plan_record = fopen(e, "wb");
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
@@ -346,6 +357,12 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     }
     register_file_formats(R);
     int rc = R->ref_mode ? xkb_planner_create(&R->planner) : xkb_planner_create_resident(&R->planner);
+    if (rc == XKB_OK && R->ref_mode && R->budget)
+    {
+        if ((rc = xkb_planner_set_device_budget(R->planner, R->budget)) == XKB_OK && R->gpu &&
+            cudaMalloc((void **) &R->budget_base, R->budget) != cudaSuccess)
+            rc = xkb_set_error(XKB_ENOMEM, "xkrt_init: device budget of %llu bytes", (unsigned long long) R->budget);
+    }
     if (rc == XKB_OK && R->gpu)
     {
         if (cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_init: stream");
@@ -408,7 +425,8 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     for (auto & d : R->dslot) { if (d.ev) cudaEventDestroy(d.ev); if (d.p) cudaFreeHost(d.p); }
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
-    for (void * p : R->allocs) if (p) cudaFree(p);
+    if (R->budget_base) cudaFree(R->budget_base);
+    else for (void * p : R->allocs) if (p) cudaFree(p);
     if (R->plan_record) fclose(R->plan_record);
     if (R->stream) cudaStreamDestroy(R->stream);
     const int st = R->status;
@@ -997,6 +1015,17 @@ static void * mirror_of(xkb_runtime * R, uint64_t host)
 // Reference mode: device memory for every allocation the planner made since the last call.
 static int ensure_allocs(xkb_runtime * R)
 {
+    if (R->budget_base)
+    {
+        // every allocation lives at its offset in the budget (evicted ones keep theirs until reused)
+        size_t n = 0;
+        int rc = xkb_planner_allocation_offsets(R->planner, nullptr, nullptr, 0, &n);
+        if (rc || n <= R->allocs.size()) return rc;
+        std::vector<int64_t> off(n);
+        if ((rc = xkb_planner_allocation_offsets(R->planner, off.data(), nullptr, n, &n))) return rc;
+        while (R->allocs.size() < n) R->allocs.push_back(R->budget_base + off[R->allocs.size()]);
+        return XKB_OK;
+    }
     size_t n = 0;
     int rc = xkb_planner_allocations(R->planner, nullptr, 0, &n);
     if (rc || n <= R->allocs.size()) return rc;
@@ -1523,6 +1552,9 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
                 // copies its memory tree plans; a host access reads the host memory in place
                 xkb_view_t v;
                 if ((rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v))) break;
+                // each fetch's copies before the next fetch: an eviction by the next one may
+                // reuse the memory these copies read
+                if ((rc = run_copies(R, stream))) break;
                 if (dev)
                 {
                     if ((rc = ensure_allocs(R))) break;
