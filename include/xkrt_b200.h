@@ -362,10 +362,13 @@ typedef struct xkb_server_cfg_t {
 } xkb_server_cfg_t;
 
 /* One heat-diffusion request: nx x ny grid, ts x ts tiles, `steps` Jacobi steps, f32 = 1 for
- * FP32 storage, seed of its U[0,1) initial interior (boundary 0), coefficient c; arrival_s is
- * when it arrives (seconds after xkb_server_run starts, non-decreasing); result (optional,
- * host memory of nx*ny elements) receives the final grid. start_s / finish_s are filled in:
- * admission time and completion time as the host observed it. */
+ * FP32 storage, coefficient c; arrival_s is when it arrives (seconds after xkb_server_run
+ * starts, non-decreasing). input (optional, host memory of nx*ny elements of the storage type;
+ * page-locked memory makes its copy asynchronous) is the initial grid, copied in when the
+ * request is admitted; without it the server builds the grid from `seed` (U[0,1) interior from
+ * splitmix64 of seed * 0x100000001b3 + cell index, boundary 0). result (optional, host memory
+ * of nx*ny elements) receives the final grid. start_s / finish_s are filled in: admission time,
+ * and the time the host saw the result in `result` (or the run end). */
 typedef struct xkb_request_t {
     double arrival_s;
     int64_t nx, ny, ts;
@@ -373,14 +376,19 @@ typedef struct xkb_request_t {
     uint64_t seed;
     double c;
     void * result;
+    const void * input;
     double start_s, finish_s;
 } xkb_request_t;
 
 /* The serving loop of the path: requests are admitted in arrival order as soon as a slot is
- * free and their grids fit in the budget (best-fit allocation with split/merge, as the
- * reference's device allocator, src/driver/device.cc:49-280); each runs its whole graph on the
- * device (two-step windows of its resolved dependency graph on the persistent scheduler) while
- * later arrivals are admitted and run beside it. */
+ * free and their memory fits in the budget (best-fit allocation with split/merge, as the
+ * reference's device allocator, src/driver/device.cc:49-280). ONE persistent kernel, launched
+ * for the whole trace, runs the tile tasks of every admitted request: the host copies a request's
+ * input grid in and writes its slot record; the kernel's idle teams set the request up (wait
+ * counters, queue, second grid) and then take ready tasks from whichever request has some; the
+ * host copies each result out as its last task ends. The graph of every request shape is
+ * resolved (two-step windows, periodic form) before the loop starts. XKB_SERVE_MODE=launch in
+ * the environment runs each request as its own persistent launch on its slot's stream instead. */
 XKB_API int xkb_server_create(xkb_server_t ** server, const xkb_server_cfg_t * cfg);
 XKB_API int xkb_server_destroy(xkb_server_t * server);
 /* Serve a whole arrival trace; returns when every request has completed. */

@@ -56,7 +56,8 @@ class Request(ctypes.Structure):
     """xkb_request_t: one heat-diffusion request of a served stream."""
     _fields_ = [("arrival_s", ctypes.c_double), ("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("ts", ctypes.c_int64),
                 ("steps", ctypes.c_int32), ("f32", ctypes.c_int32), ("seed", ctypes.c_uint64), ("c", ctypes.c_double),
-                ("result", ctypes.c_void_p), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
+                ("result", ctypes.c_void_p), ("input", ctypes.c_void_p), ("start_s", ctypes.c_double),
+                ("finish_s", ctypes.c_double)]
 
 
 class PeriodicGraph(ctypes.Structure):

@@ -83,3 +83,41 @@ int xkb_internal_sched_windows_wait(xkb_sched_t * S, uint64_t * executed);
 // leading dimension (xkb_diffusion_views with an explicit box).
 int xkb_internal_diffusion_box(int dtype, cudaStream_t stream, const void * src, int64_t ld_src, void * dst, int64_t ld_dst,
                                int64_t i0, int64_t j0, int64_t w, int64_t h, int64_t nx, int64_t ny, double c);
+
+// ---- device-resident serving loop (one persistent kernel for every admitted request) --------
+// One admitted request, in device memory. The host writes it, then the slot's counters, then the
+// slot's state word (three copies in stream order), so a team that sees the state sees the rest.
+struct XkbSrvSlot {
+    const xkb_task_desc_t * tasks;       // the periodic window's `period` descriptors
+    const uint32_t * succ_ptr, * succ, * xsucc_ptr, * xsucc, * npred_first, * npred_next;
+    int * wc;                            // ntasks wait counters
+    int * queue;                         // ntasks ready-queue slots
+    const uint8_t * copy_src;            // the grid the host copied in ...
+    uint8_t * copy_dst;                  //   ... duplicated here by the set-up chunks (second grid)
+    uint64_t copy_bytes;
+    uint32_t period, ntasks;
+    uint32_t nchunks;                    // set-up chunks (wait counters, queue slots, grid copy)
+    uint32_t gen;                        // admission number, reported back when the request ends
+    uint32_t seed_later;                 // 1: some task of a later window has no predecessor
+    int32_t pfd;
+};
+// The slot's counters (device memory): state 0 idle, 1 admitted (set-up pending), 2 running,
+// 3 done; set-up chunks claimed / finished; ready-queue head and tail; tasks executed.
+struct XkbSrvCtl { unsigned state, init_next, init_done, head, tail, executed, pad[2]; };
+struct XkbSrvArgs {
+    XkbSrvSlot * slots;
+    XkbSrvCtl * ctl;
+    int nslots;
+    volatile unsigned * host_done;       // mapped host memory: gen of the last request each slot ended
+    unsigned * status;                   // [0] first error (XKB_ETIMEDOUT), [1] tasks executed,
+                                         // [2] set by the host: 1 once no request will come,
+                                         //     2 to stop at once (the host gave up)
+    uint64_t run_ns;                     // how long a team may run before it gives up
+    uint64_t timeout_ns;                 // longest wait for one published queue slot
+};
+// Tasks per set-up chunk of a served request, and at most this many bytes of its grid copy.
+constexpr uint32_t XKB_SRV_CHUNK = 16384;
+constexpr uint64_t XKB_SRV_COPY_CHUNK = uint64_t(256) << 10;
+// Launch the serving kernel (grid CTAs of 256 threads, warps_per_task 1, 2, 4 or 8).
+int xkb_internal_server_launch(const XkbSrvArgs & a, int grid, int warps_per_task, cudaStream_t stream);
+

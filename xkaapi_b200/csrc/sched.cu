@@ -887,6 +887,218 @@ extern "C" int xkb_sched_run_noalloc(const xkb_task_desc_t * tasks, const xkb_ta
     return XKB_OK;
 }
 
+// ------------------------------------------------------------------------------------------
+// Device-resident serving loop: ONE persistent kernel runs the tile tasks of every admitted
+// request. The host admits a request by writing its slot record (descriptors, periodic graph,
+// counter and queue arrays, the grid to duplicate) and then the slot's state word; any idle team
+// of the kernel then takes the slot's set-up chunks (wait counters, queue slots, second grid),
+// the team that finishes the last chunk publishes the request's first ready tasks, and from then
+// on teams take ready tasks from whichever slot has some -- a small request does not hold SMs it
+// cannot use, and requests admitted while others run share the device at once. The team that
+// executes a request's last task marks the slot done and reports the admission number to mapped
+// host memory; the host copies the result out. Teams stop when the host has said no request will
+// come and every slot is idle or done, on an error, or at the time limit; every wait is bounded.
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned * p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned * p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void srv_publish(const XkbSrvSlot & S, XkbSrvCtl * c, uint32_t t)
+{
+    const unsigned pos = atomicAdd(&c->tail, 1u);
+    xkb_st_release(S.queue + pos, (int) t);
+}
+
+template <int TEAM_WARPS>
+__global__ void __launch_bounds__(SCHED_THREADS, XKB_SCHED_MINB) server_kernel(XkbSrvArgs a)
+{
+    constexpr int NTEAMS = (SCHED_THREADS / 32) / TEAM_WARPS;
+    constexpr int TEAM_THREADS = TEAM_WARPS * 32;
+    __shared__ int job_kind[NTEAMS];           // 0 stop, 1 task, 2 set-up chunk, -1 nothing yet
+    __shared__ int job_slot[NTEAMS];
+    __shared__ int job_idx[NTEAMS];            // task id, or chunk index
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int team = warp / TEAM_WARPS, twarp = warp % TEAM_WARPS;
+    const int bar = 1 + team, tthread = twarp * 32 + lane;
+    const int gteam = blockIdx.x * NTEAMS + team;
+    unsigned executed = 0;
+    uint32_t nap = 32;
+    const uint64_t t_start = xkb_globaltimer();
+    for (;;)
+    {
+        if (tthread == 0)
+        {
+            int kind = -1, slot = -1, idx = -1;
+            if (*(volatile unsigned *) (a.status + 2) >= 2) kind = 0;     // the host gave up: stop now
+            for (int k = 0; k < a.nslots && kind < 0; ++k)
+            {
+                const int sl = (gteam + k) % a.nslots;
+                XkbSrvCtl * c = a.ctl + sl;
+                const unsigned st = ld_acquire_u32(&c->state);
+                if (st == 1)
+                {
+                    if (*(volatile unsigned *) &c->init_next < a.slots[sl].nchunks)
+                    {
+                        const unsigned ch = atomicAdd(&c->init_next, 1u);
+                        if (ch < a.slots[sl].nchunks) { kind = 2; slot = sl; idx = (int) ch; }
+                    }
+                }
+                else if (st == 2)
+                {
+                    unsigned h = *(volatile unsigned *) &c->head;
+                    while (h < *(volatile unsigned *) &c->tail)
+                    {
+                        const unsigned got = atomicCAS(&c->head, h, h + 1);
+                        if (got == h) { kind = 1; slot = sl; break; }
+                        h = got;
+                    }
+                    if (kind == 1)
+                    {
+                        // the id at that position was published (tail counts it) or is about to be
+                        const int * q = a.slots[sl].queue + h;
+                        const uint64_t t0 = xkb_globaltimer();
+                        uint32_t spins = 0;
+                        int t;
+                        while ((t = xkb_ld_acquire(q)) < 0)
+                        {
+                            if ((++spins & 63) == 0 && xkb_globaltimer() - t0 > a.timeout_ns)
+                            {
+                                atomicCAS(a.status, 0u, (unsigned) -XKB_ETIMEDOUT);
+                                break;
+                            }
+                        }
+                        if (t < 0) kind = 0; else idx = t;
+                    }
+                }
+            }
+            if (kind < 0)
+            {
+                if (*(volatile unsigned *) a.status != 0) kind = 0;
+                else if (xkb_globaltimer() - t_start > a.run_ns) { atomicCAS(a.status, 0u, (unsigned) -XKB_ETIMEDOUT); kind = 0; }
+                else if (*(volatile unsigned *) (a.status + 2))
+                {
+                    bool busy = false;
+                    for (int sl = 0; sl < a.nslots && !busy; ++sl)
+                    {
+                        const unsigned st = ld_acquire_u32(&a.ctl[sl].state);
+                        busy = st == 1 || st == 2;
+                    }
+                    if (!busy) kind = 0;
+                }
+                if (kind < 0) { __nanosleep(nap); if (nap < 8192) nap *= 2; }
+            }
+            else nap = 32;
+            job_kind[team] = kind; job_slot[team] = slot; job_idx[team] = idx;
+        }
+        team_sync(bar, TEAM_THREADS);
+        const int kind = job_kind[team], sl = job_slot[team], idx = job_idx[team];
+        if (kind == 0) break;
+        if (kind == 2)
+        {
+            // set-up chunk: wait counters and empty queue slots of its tasks, and its share of the
+            // second grid (a copy of the first, which the host copied in)
+            const XkbSrvSlot & S = a.slots[sl];
+            const uint32_t t0 = (uint32_t) idx * XKB_SRV_CHUNK, t1 = min(S.ntasks, t0 + XKB_SRV_CHUNK);
+            for (uint32_t t = t0 + tthread; t < t1; t += TEAM_THREADS)
+            {
+                S.queue[t] = -1;
+                const uint32_t w = t / S.period, l = t - w * S.period;
+                S.wc[t] = (int) (w == 0 ? S.npred_first[l] : S.npred_next[l]);
+            }
+            const uint64_t per = ((S.copy_bytes + S.nchunks - 1) / S.nchunks + 15) & ~(uint64_t) 15;
+            const uint64_t b0 = min(S.copy_bytes, (uint64_t) idx * per), b1 = min(S.copy_bytes, b0 + per);
+            const uint4 * src = (const uint4 *) (S.copy_src + b0);
+            uint4 * dst = (uint4 *) (S.copy_dst + b0);
+            const uint64_t nv = (b1 - b0) / 16;
+            uint64_t k = tthread;
+            for (; k + 3 * TEAM_THREADS < nv; k += 4 * TEAM_THREADS)     // four 16-byte loads in flight per lane
+            {
+                const uint4 v0 = __ldcg(src + k), v1 = __ldcg(src + k + TEAM_THREADS), v2 = __ldcg(src + k + 2 * TEAM_THREADS),
+                            v3 = __ldcg(src + k + 3 * TEAM_THREADS);
+                dst[k] = v0; dst[k + TEAM_THREADS] = v1; dst[k + 2 * TEAM_THREADS] = v2; dst[k + 3 * TEAM_THREADS] = v3;
+            }
+            for (; k < nv; k += TEAM_THREADS) dst[k] = __ldcg(src + k);
+            for (uint64_t r = ((b1 - b0) & ~(uint64_t) 15) + tthread; r < b1 - b0; r += TEAM_THREADS)
+                S.copy_dst[b0 + r] = S.copy_src[b0 + r];
+            __threadfence();
+            team_sync(bar, TEAM_THREADS);
+            if (tthread == 0)
+            {
+                XkbSrvCtl * c = a.ctl + sl;
+                if (atomicAdd(&c->init_done, 1u) + 1 == S.nchunks)
+                {
+                    // every chunk is done: publish the tasks with no predecessor, then run
+                    for (uint32_t l = 0; l < S.period && l < S.ntasks; ++l)
+                        if (S.npred_first[l] == 0) srv_publish(S, c, l);
+                    if (S.seed_later)
+                        for (uint32_t t = S.period; t < S.ntasks; ++t)
+                            if (S.npred_next[t % S.period] == 0) srv_publish(S, c, t);
+                    st_release_u32(&c->state, 2u);
+                }
+            }
+        }
+        else if (kind == 1)
+        {
+            const XkbSrvSlot & S = a.slots[sl];
+            const uint32_t t = (uint32_t) idx, w = t / S.period, l = t - w * S.period;
+            run_task_team(S.tasks[l], twarp, TEAM_WARPS, S.pfd);
+            __threadfence();
+            team_sync(bar, TEAM_THREADS);
+            if (twarp == 0)
+            {
+                XkbSrvCtl * c = a.ctl + sl;
+                const uint32_t base = w * S.period;
+                for (uint32_t i = S.succ_ptr[l] + lane; i < S.succ_ptr[l + 1]; i += 32)
+                {
+                    const uint32_t u = base + S.succ[i];
+                    if (u < S.ntasks && atom_add_acq_rel(S.wc + u, -1) == 1) srv_publish(S, c, u);
+                }
+                if (S.xsucc_ptr)
+                    for (uint32_t i = S.xsucc_ptr[l] + lane; i < S.xsucc_ptr[l + 1]; i += 32)
+                    {
+                        const uint32_t u = base + S.period + S.xsucc[i];
+                        if (u < S.ntasks && atom_add_acq_rel(S.wc + u, -1) == 1) srv_publish(S, c, u);
+                    }
+                __syncwarp();
+                if (lane == 0)
+                {
+                    ++executed;
+                    if (atomicAdd(&c->executed, 1u) + 1 == S.ntasks)
+                    {
+                        st_release_u32(&c->state, 3u);
+                        __threadfence_system();
+                        a.host_done[sl] = S.gen;
+                    }
+                }
+            }
+        }
+        team_sync(bar, TEAM_THREADS);           // job_* are rewritten only after every thread read them
+    }
+    if (tthread == 0 && executed) atomicAdd(a.status + 1, executed);
+}
+
+int xkb_internal_server_launch(const XkbSrvArgs & a, int grid, int warps_per_task, cudaStream_t stream)
+{
+    switch (warps_per_task)
+    {
+        case 1: server_kernel<1><<<grid, SCHED_THREADS, 0, stream>>>(a); break;
+        case 2: server_kernel<2><<<grid, SCHED_THREADS, 0, stream>>>(a); break;
+        case 4: server_kernel<4><<<grid, SCHED_THREADS, 0, stream>>>(a); break;
+        case 8: server_kernel<8><<<grid, SCHED_THREADS, 0, stream>>>(a); break;
+        default: return xkb_set_error(XKB_EINVAL, "server: warps per task must be 1, 2, 4 or 8");
+    }
+    XKB_CUDA_TRY(cudaGetLastError());
+    return XKB_OK;
+}
+
 int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream)
 {
     if (d->kind == XKB_TASK_NOOP) return XKB_OK;
