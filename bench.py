@@ -494,11 +494,29 @@ def serve_trace(ngraphs, seed, ts=128):
     return side, steps, f32, np.cumsum(gaps), bytes_
 
 
-def serve_requests(xk, side, steps, f32, arrivals):
+_SERVE_IO = {}
+
+
+def serve_io(torch):
+    """Page-locked host buffers every served request reads its initial grid from and writes its
+    result to: one input of the largest grid (seeded U[0,1) values; a request takes its first
+    nx*ny elements) and one result buffer that concurrent results overwrite (only the time of
+    the transfers matters here; the parity tests check results)."""
+    if not _SERVE_IO:
+        n = 8192 * 8192
+        inp = torch.empty(n, dtype=torch.float64).pin_memory()
+        inp.numpy()[:] = np.random.default_rng(SEED).random(n)
+        _SERVE_IO["in"] = inp
+        _SERVE_IO["out"] = torch.empty(n, dtype=torch.float64).pin_memory()
+    return _SERVE_IO["in"].data_ptr(), _SERVE_IO["out"].data_ptr()
+
+
+def serve_requests(xk, side, steps, f32, arrivals, io=None):
     reqs = (xk.Request * len(side))()
     for k, r in enumerate(reqs):
         r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32 = float(arrivals[k]), int(side[k]), int(side[k]), 128, int(steps[k]), int(f32[k])
-        r.seed, r.c, r.result = 7000 + k, COEF, None
+        r.seed, r.c = 7000 + k, COEF
+        r.input, r.result = (io if io else (None, None))
     return reqs
 
 
@@ -506,18 +524,27 @@ def serve_study(xk, torch, ngraphs=2000, slots=16, load=0.8):
     side, steps, f32, unit_arrivals, bytes_ = serve_trace(ngraphs, 2026)
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150e9, free - 8e9))
+    io = serve_io(torch)
     srv = xk.Server(budget_bytes=budget, slots=slots)
     # capacity: the first graphs of the trace all arriving at once (closed loop), measured on the
-    # second pass, after the first has resolved the periodic graph of every shape they use
+    # second pass, after the first has resolved the periodic graph of every shape they use; the
+    # same with one persistent launch per request (the former serving loop) for comparison
     cal = min(300, ngraphs)
     for _ in range(2):
-        reqs = serve_requests(xk, side[:cal], steps[:cal], f32[:cal], np.zeros(cal))
+        reqs = serve_requests(xk, side[:cal], steps[:cal], f32[:cal], np.zeros(cal), io)
         srv.run(reqs)
     capacity = float(bytes_[:cal].sum()) / max(r.finish_s for r in reqs)          # bytes/s served
+    os.environ["XKB_SERVE_MODE"] = "launch"
+    try:
+        reqs = serve_requests(xk, side[:cal], steps[:cal], f32[:cal], np.zeros(cal), io)
+        srv.run(reqs)
+        capacity_launch = float(bytes_[:cal].sum()) / max(r.finish_s for r in reqs)
+    finally:
+        del os.environ["XKB_SERVE_MODE"]
     # the trace: Poisson arrivals whose offered HBM traffic is `load` x the capacity
     rate = load * capacity / float(bytes_.mean())                                  # graphs/s
     arrivals = unit_arrivals / rate
-    reqs = serve_requests(xk, side, steps, f32, arrivals)
+    reqs = serve_requests(xk, side, steps, f32, arrivals, io)
     t0 = time.perf_counter()
     srv.run(reqs)
     wall = time.perf_counter() - t0
@@ -530,11 +557,16 @@ def serve_study(xk, torch, ngraphs=2000, slots=16, load=0.8):
             "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_ms": round(float(lat.mean()), 3),
             "admission_wait_p99_ms": round(float(np.percentile(wait, 99)), 3),
             "tasks": tasks, "tasks_per_s": round(tasks / fin), "GBps": round(float(bytes_.sum()) / fin / 1e9, 1),
-            "capacity_GBps": round(capacity / 1e9, 1), "offered_load": load, "rate_graphs_per_s": round(rate, 1),
+            "capacity_GBps": round(capacity / 1e9, 1), "capacity_frac": round(capacity / 1e9 / peaks()[0], 3),
+            "capacity_launch_mode_GBps": round(capacity_launch / 1e9, 1), "offered_load": load,
+            "rate_graphs_per_s": round(rate, 1),
             "span_s": round(float(arrivals[-1]), 3), "makespan_s": round(fin, 3), "wall_s": round(wall, 3),
             "budget_GB": round(budget / 1e9, 1), "slots": slots,
             "trace": "Poisson arrivals, side log-uniform 256-8192 (multiple of 128), steps U{10..200}, FP64/FP32 50/50, "
-                     "128^2 tiles; load calibrated on a closed-loop run of the first 300 graphs (second pass, shapes resolved)"}
+                     "128^2 tiles; load calibrated on a closed-loop run of the first 300 graphs (second pass, shapes resolved)",
+            "latency": "arrival -> result in host memory: the input grid copied in from page-locked host memory at "
+                       "admission and the result copied out are inside it",
+            "loop": "one persistent kernel for the whole trace runs every admitted request's tile tasks"}
 
 
 def main():
