@@ -17,8 +17,13 @@ sorted copy records are stored.
 axpby fixtures: oracle/_ref/ref_axpby (the reference's host-only runtime running the seeded
 axpby task chains with segment accesses, oracle/ref/ref_axpby.cc); the final y of each case is
 stored with its parameters, pinning the oracle's restatement of the chain generator and update.
-Run: python tests/golden/make_golden.py [deps] [plan] [axpby]   (default: all; needs the binaries
-of oracle/ref/build_ref.sh)
+wrap fixtures: streams with matrix tiles that wrap the leading dimension (tests/streams.py
+mixed_stream), where the reference's dependency tree is not point-wise
+(include/xkrt/memory/access/blas/dependency-tree.hpp:228-256 applies a PUT to whole split-off
+nodes that meet the access's other rect): the reference's edges and the point-wise edges of the
+oracle restatement (oracle/_bin/deps_oracle) are both stored, so the exact difference is pinned.
+Run: python tests/golden/make_golden.py [deps] [plan] [axpby] [wrap]   (default: all; needs the
+binaries of oracle/ref/build_ref.sh and oracle/Makefile)
 """
 import os, subprocess, sys, tempfile
 import numpy as np
@@ -185,8 +190,30 @@ def ref_axpby(n, passes, seed, cmin, cmax):
         return np.fromfile(out), json.loads(r.stdout.strip().splitlines()[-1])["tasks"]
 
 
+WRAP_SEEDS = (0, 14, 17, 21, 25, 43, 54, 171, 1, 2)      # the first eight diverge, the last two agree
+
+
+def pointwise_edges(recs):
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "s.bin")
+        S.write_stream(p, recs)
+        subprocess.run([os.path.join(REPO, "oracle/_bin/deps_oracle"), p, os.path.join(d, "o")],
+                       check=True, capture_output=True)
+        return S.read_edges(os.path.join(d, "o.edges"))
+
+
 def main():
-    which = set(sys.argv[1:]) or {"deps", "plan", "axpby"}
+    which = set(sys.argv[1:]) or {"deps", "plan", "axpby", "wrap"}
+    if "wrap" in which:
+        out = {}
+        for seed in WRAP_SEEDS:
+            recs = S.mixed_stream(40, seed)
+            name = f"wrap_{seed}"
+            out[name + "__stream"] = recs
+            out[name + "__ref_edges"] = ref_edges(recs)
+            out[name + "__pointwise_edges"] = pointwise_edges(recs)
+            print(f"{name}: {len(out[name + '__ref_edges'])} reference edges, {len(out[name + '__pointwise_edges'])} point-wise")
+        np.savez_compressed(os.path.join(HERE, "wrap_golden.npz"), **out)
     if "axpby" in which:
         out = {}
         for name, n, passes, seed, cmin, cmax in AXPBY_CASES:

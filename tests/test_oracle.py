@@ -94,3 +94,38 @@ def test_axpby_chain_oracle_matches_reference_runtime(case):
     x, y, chunks = O.axpby_chain(n, passes, seed, cmin, cmax)
     assert len(chunks) == int(AXPBY_GOLDEN[case + "__tasks"][0])
     np.testing.assert_array_equal(O.axpby_chain_run(x, y, chunks), AXPBY_GOLDEN[case + "__y"])
+
+
+WRAP = np.load(os.path.join(REPO, "tests", "golden", "wrap_golden.npz"))
+WRAP_CASES = sorted(k[:-len("__stream")] for k in WRAP.files if k.endswith("__stream"))
+
+
+def _closure(edges, n):
+    reach = [set() for _ in range(n)]
+    succ = [[] for _ in range(n)]
+    for p, s in edges:
+        succ[p].append(s)
+    for t in range(n - 1, -1, -1):
+        for s in succ[t]:
+            reach[t].add(s)
+            reach[t] |= reach[s]
+    return reach
+
+
+@pytest.mark.parametrize("case", WRAP_CASES)
+def test_wrapped_tiles_pinned_divergence(case, tmp_path):
+    """Tiles that wrap the leading dimension: the reference's tree is not point-wise there
+    (include/xkrt/memory/access/blas/dependency-tree.hpp:228-256 applies a PUT to whole split-off
+    nodes that meet the access's other rect), the restatement and the GPU resolver are. The
+    fixture holds both edge sets; the restatement reproduces its point-wise set exactly, so the
+    difference to the reference is exactly the recorded one -- and every edge only the point-wise
+    set has is one the reference orders too, through other tasks."""
+    recs = WRAP[case + "__stream"]
+    mine = run_oracle(recs, tmp_path)
+    np.testing.assert_array_equal(mine, WRAP[case + "__pointwise_edges"])
+    ref = set(map(tuple, WRAP[case + "__ref_edges"].tolist()))
+    ours = set(map(tuple, mine.tolist()))
+    n = int(recs["task"].max()) + 1
+    reach = _closure(ref, n)
+    assert all(s in reach[p] for p, s in ours - ref)
+    assert any(int(r["offset_m"]) + int(r["m"]) > int(r["ld"]) for r in recs if r["type"] == S.MATRIX)

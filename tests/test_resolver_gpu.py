@@ -1,5 +1,7 @@
 """GPU dependency resolver: bit-exact unique edge sets against the reference's own trees
 (golden fixtures) and against the oracle restatement on larger seeded streams."""
+import os
+
 import numpy as np
 import pytest
 
@@ -56,9 +58,20 @@ def test_incremental_batches_equal_one_shot(torch_cuda, case, batches):
 @pytest.mark.parametrize("seed", range(4))
 def test_mixed_streams_vs_oracle(torch_cuda, seed):
     recs = S.mixed_stream(300, seed + 100)
-    # the oracle and the GPU agree on every stream; (the reference itself diverges only for
-    # matrix tiles that wrap the leading dimension, which the golden fixtures exclude)
+    # the oracle and the GPU agree on every stream (the reference itself diverges where matrix
+    # tiles wrap the leading dimension; tests/golden/wrap_golden.npz pins that difference)
     np.testing.assert_array_equal(gpu_edges(recs), U.oracle_edges(recs))
+
+
+_WRAP = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "wrap_golden.npz"))
+
+
+@pytest.mark.parametrize("case", sorted(k[:-len("__stream")] for k in _WRAP.files if k.endswith("__stream")))
+def test_wrapped_tiles_gpu_edges_are_the_pinned_pointwise_set(torch_cuda, case):
+    """On streams with tiles that wrap the leading dimension the GPU resolver gives exactly the
+    point-wise edge set the fixture records beside the reference's (their difference is pinned
+    by tests/test_oracle.py)."""
+    np.testing.assert_array_equal(gpu_edges(_WRAP[case + "__stream"]), _WRAP[case + "__pointwise_edges"])
 
 
 def test_microbench_16k_vs_oracle(torch_cuda):
