@@ -454,8 +454,7 @@ static int admit(xkb_server * S, int k, xkb_request_t & q, uint8_t * mem, Window
     const void * in = q.input;
     if (!in)
     {
-        int rc = grow_pinned(sl.hinput, sl.hinput_cap, bytes);
-        if (rc) return rc;
+        if (sl.hinput_cap < bytes) return xkb_set_error(XKB_EINVAL, "server_run: input staging was not sized for the trace");
         seeded_host_grid(q, sl.hinput);
         in = sl.hinput;
     }
@@ -475,8 +474,7 @@ static int admit(xkb_server * S, int k, xkb_request_t & q, uint8_t * mem, Window
     int * queue = (int *) ((uint8_t *) wc + ((ntasks * 4 + 255) & ~(uint64_t) 255));
     std::vector<xkb_task_desc_t> d;
     heat_descs(sh, 2, (uint64_t) a, (uint64_t) b, q.c, d);
-    int rc = grow_pinned(sl.hdesc, sl.hdesc_cap, d.size() * sizeof(xkb_task_desc_t));
-    if (rc) return rc;
+    if (sl.hdesc_cap < d.size() * sizeof(xkb_task_desc_t)) return xkb_set_error(XKB_EINVAL, "server_run: descriptor staging was not sized for the trace");
     memcpy(sl.hdesc, d.data(), d.size() * sizeof(xkb_task_desc_t));
     XKB_CUDA_TRY(cudaMemcpyAsync(desc, sl.hdesc, d.size() * sizeof(xkb_task_desc_t), cudaMemcpyHostToDevice, sl.stream));
     XkbSrvSlot & r = *sl.hslot;
@@ -530,6 +528,21 @@ static int server_run_device(xkb_server * S, xkb_request_t * reqs, size_t n)
             XKB_CUDA_TRY(cudaHostAlloc((void **) &sl.hslot, sizeof(XkbSrvSlot) + sizeof(XkbSrvCtl) + 64, cudaHostAllocDefault));
             sl.hctl = (XkbSrvCtl *) (sl.hslot + 1);
             sl.hstate = (unsigned *) (sl.hctl + 1);
+        }
+    }
+    // page-locked staging sized for the whole trace up front: no host allocation or release runs
+    // while the kernel does (releasing page-locked memory may wait for the device)
+    {
+        size_t desc_bytes = 0, input_bytes = 0;
+        for (size_t i = 0; i < n; ++i)
+        {
+            if (win[i]) desc_bytes = std::max<size_t>(desc_bytes, 2 * win[i]->per_step * sizeof(xkb_task_desc_t));
+            if (!reqs[i].input) input_bytes = std::max<size_t>(input_bytes, (size_t) (reqs[i].nx * reqs[i].ny * (reqs[i].f32 ? 4 : 8)));
+        }
+        for (Slot & sl : S->slots)
+        {
+            if (desc_bytes && (rc = grow_pinned(sl.hdesc, sl.hdesc_cap, desc_bytes))) return rc;
+            if (input_bytes && (rc = grow_pinned(sl.hinput, sl.hinput_cap, input_bytes))) return rc;
         }
     }
     XKB_CUDA_TRY(cudaMemsetAsync(S->d_ctl, 0, ns * sizeof(XkbSrvCtl), S->kstream));
