@@ -211,6 +211,7 @@ struct xkb_runtime {
     std::vector<uint32_t> dfirst;                     //   their first occurrences, in record order
     uint64_t cur_h2d = 0, cur_d2h = 0, cur_h2d_bytes = 0, cur_d2h_bytes = 0;   // copies of the batch in progress
     uint64_t cur_d2d = 0;                             // device-to-device copies (reference mode)
+    uint64_t copy_calls = 0;                          // run_copies calls that issued copies (under plan_mu)
     // page-locked descriptor slots of streamed windows (a slot is reused once its copy is done)
     struct DescSlot { xkb_task_desc_t * p = nullptr; size_t cap = 0; cudaEvent_t ev = nullptr; } dslot[2];
     int dslot_next = 0;
@@ -1048,6 +1049,7 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
     if (rc || !n) return rc;
     std::vector<xkb_copy_t> c(n);
     if ((rc = xkb_planner_copies(R->planner, c.data(), n, &n, 1))) return rc;
+    ++R->copy_calls;
     if (R->plan_record) fwrite(c.data(), sizeof(xkb_copy_t), n, R->plan_record);
     if (R->ref_mode)
     {
@@ -1540,6 +1542,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     g_view_ld.assign(T.nacc, -1);
     {
         std::lock_guard<std::mutex> lk(R->plan_mu);
+        const uint64_t calls0 = R->copy_calls;
         for (uint32_t a = 0; a < T.nacc && rc == XKB_OK; ++a)
         {
             const xkb_access_rec_t & r = recs[T.acc_off + a];
@@ -1573,7 +1576,10 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
             rc = xkb_planner_fetch(R->planner, &r, a, dev ? 1 : 0, &v);
         }
         if (rc == XKB_OK) rc = run_copies(R, stream);
-        if (rc == XKB_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: copies");
+        // the task's copies complete before the planner is released (its state then describes data
+        // in place); a task that issued none has nothing to wait for
+        if (rc == XKB_OK && R->copy_calls != calls0 && cudaStreamSynchronize(stream) != cudaSuccess)
+            rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: copies");
     }
     if (rc) return rc;
     const Format & f = R->formats[T.fmtid];
