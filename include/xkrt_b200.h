@@ -220,6 +220,11 @@ XKB_API int xkb_planner_set_device_budget(xkb_planner_t * planner, uint64_t byte
  * fetch that evicted it read it before the room is reused (run each fetch's copies before the
  * next fetch). */
 XKB_API int xkb_planner_allocation_offsets(xkb_planner_t * planner, int64_t * offsets, uint8_t * live, size_t cap, size_t * n);
+/* Host fetches of a planner in the reference's mode copy from the largest allocation's view of a
+ * block, as the reference does (memory-tree.hpp:1110-1160), even when that view is not coherent:
+ * the host then receives stale data. on != 0: copy from the largest COHERENT view instead (what
+ * the C API's reference mode does, so that host memory is right after xkrt_task_wait). */
+XKB_API int xkb_planner_set_writeback_coherent(xkb_planner_t * planner, int on);
 /* Allocations evicted and blocks written back to the host by evictions so far. */
 XKB_API int xkb_planner_eviction_stats(xkb_planner_t * planner, uint64_t * evicted, uint64_t * written_back);
 

@@ -427,3 +427,49 @@ def test_budget_eviction_runs_heat_bit_exact_on_cpu(budget_mb, steps):
     np.testing.assert_array_equal(final, O.heat_run(g, n, n, steps, 0.2))
     evicted, written = P.eviction_stats()
     assert evicted > 0 and written > 0
+
+
+@pytest.mark.parametrize("coherent", [False, True])
+def test_reference_writeback_pick_and_the_coherent_one(coherent):
+    """Executing the reference's plan for 4 heat steps (1024^2, 128^2 tiles) on byte arrays, then
+    its host fetch of every written access: with the reference's pick of the source view (the
+    largest allocation, memory-tree.hpp:1110-1160) 14,259 cells of the host grid are stale; with
+    xkb_planner_set_writeback_coherent (what the C API's reference mode sets) the grid is the
+    oracle's, bit for bit. The device-side plan is the same either way."""
+    import sys
+    import streams as S
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import kernels_oracle as O
+    n, ts, steps, base = 1024, 128, 4, 1 << 30
+    recs = S.heat_stream(n, n, ts, ts, steps, base_src=base, base_dst=base + n * n * 8)
+    g = O.heat_init(n, n, seed=4)
+    host = np.concatenate([g.view(np.uint8).ravel()] * 2)
+    P = xk.Planner()
+    if coherent:
+        xk.check(xk.lib().xkb_planner_set_writeback_coherent(P._h, 1))
+    dev = np.zeros(64 << 20, np.uint8)
+
+    def offsets():
+        sizes = P.allocations()
+        return np.concatenate([[0], np.cumsum((sizes.astype(np.int64) + 255) // 256 * 256)])[:len(sizes)]
+    for t in range(len(recs) // 2):
+        views = []
+        for a in range(2):
+            views.append(P.fetch(recs[2 * t + a], a, 1))
+            _run_plan_on_bytes(P.copies(take=True), host, base, dev, offsets())
+        offs = offsets()
+        r0, r1 = recs[2 * t], recs[2 * t + 1]
+        (a0, o0, l0), (a1, o1, l1) = views
+        S0 = np.lib.stride_tricks.as_strided(dev[offs[a0] + o0:].view(np.float64), shape=(int(r0["n"]), int(r0["m"])), strides=(l0 * 8, 8))
+        D = O._update(S0.astype(np.float64), 0.2)
+        D1 = np.lib.stride_tricks.as_strided(dev[offs[a1] + o1:].view(np.float64), shape=(int(r1["n"]), int(r1["m"])), strides=(l1 * 8, 8))
+        ox, oy = int(r1["offset_m"]) - int(r0["offset_m"]) - 1, int(r1["offset_n"]) - int(r0["offset_n"]) - 1
+        D1[:, :] = D[oy:oy + int(r1["n"]), ox:ox + int(r1["m"])]
+    for t in range(len(recs) // 2):
+        w = recs[2 * t + 1].copy()
+        w["mode"] = S.R
+        P.fetch(w, 1, 0)
+    _run_plan_on_bytes(P.copies(take=True), host, base, dev, offsets())
+    final = host[(steps % 2) * n * n * 8:][:n * n * 8].view(np.float64).reshape(n, n)
+    stale = int((final != O.heat_run(g, n, n, steps, 0.2)).sum())
+    assert stale == (0 if coherent else 14259)

@@ -78,6 +78,7 @@ SIGNATURES = {
     "xkb_planner_set_device_budget": (_int, [_vp, ctypes.c_uint64]),
     "xkb_planner_allocation_offsets": (_int, [_vp, _vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_planner_eviction_stats": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "xkb_planner_set_writeback_coherent": (_int, [_vp, _int]),
     "xkb_axpby": (_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
     "xkb_sched_create": (_int, [ctypes.POINTER(_vp), _vp]),
     "xkb_sched_destroy": (_int, [_vp]),
@@ -179,7 +180,9 @@ def heat_norms(src, dst, nx, ny, ld, c, stream=None):
     the largest interior |dst| (xkb_heat_norms)."""
     import torch
     out = torch.zeros(4, dtype=torch.float64, device=src.device)
+    torch.cuda.current_stream().synchronize()        # the zeros are in place before the library's stream clears them
     check(lib().xkb_heat_norms(_dtype_code(src), src.data_ptr(), dst.data_ptr(), ld, nx, ny, c, out.data_ptr(), _stream(stream)))
+    getattr(stream, "synchronize", torch.cuda.synchronize)()
     o = out.cpu().tolist()
     return {"boundary_max_abs": o[0], "l2_norm": o[1] ** 0.5, "residual_max_abs": o[2], "interior_max_abs": o[3]}
 

@@ -277,6 +277,7 @@ struct xkb_planner {
     int64_t cur_task = -1;
     std::vector<int32_t> pinned;                      // allocations of the current task's views
     uint64_t evicted = 0, written_back = 0;
+    bool coherent_writeback = false;                  // host fetches copy from a coherent view
     std::vector<xkb_copy_t> copies;
     std::vector<Partite> scratch;
     // resident mode: one device mirror per registered host region (base -> (size, index))
@@ -476,6 +477,14 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
             int src = 0;
             for (int i = 1; i < st.nviews; ++i)
                 if (P->allocs[st.views[src].alloc] < P->allocs[st.views[i].alloc]) src = i;
+            if (P->coherent_writeback && !(st.coh & (1u << src)))
+            {
+                // the largest COHERENT view instead (the reference's pick may hold stale data)
+                int best = -1;
+                for (int i = 0; i < st.nviews; ++i)
+                    if ((st.coh & (1u << i)) && (best < 0 || P->allocs[st.views[best].alloc] < P->allocs[st.views[i].alloc])) best = i;
+                if (best >= 0) src = best;
+            }
             const View & v = st.views[src];
             push_copy(P, a.task, access_index, XKB_COPY_D2H, p, ld, s, v.alloc, view_off(v, p.x0, p.y0, s),
                       seg ? 0 : (int64_t) v.ld, -1, host_addr(p), seg ? 0 : (int64_t) ld);
@@ -641,6 +650,13 @@ extern "C" int xkb_planner_allocation_offsets(xkb_planner_t * P, int64_t * offs,
     if (cap < P->alloc_off.size()) return xkb_set_error(XKB_ERANGE, "planner_allocation_offsets: %zu entries needed", P->alloc_off.size());
     if (offs && !P->alloc_off.empty()) memcpy(offs, P->alloc_off.data(), P->alloc_off.size() * sizeof(int64_t));
     if (live && !P->alloc_live.empty()) memcpy(live, P->alloc_live.data(), P->alloc_live.size());
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_set_writeback_coherent(xkb_planner_t * P, int on)
+{
+    if (!P || P->resident) return xkb_set_error(XKB_EINVAL, "planner_set_writeback_coherent: a planner of the reference mode");
+    P->coherent_writeback = on != 0;
     return XKB_OK;
 }
 

@@ -358,6 +358,8 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
     }
     register_file_formats(R);
     int rc = R->ref_mode ? xkb_planner_create(&R->planner) : xkb_planner_create_resident(&R->planner);
+    // the reference's write-back may copy a stale view to the host; the runtime copies coherent data
+    if (rc == XKB_OK && R->ref_mode) rc = xkb_planner_set_writeback_coherent(R->planner, 1);
     if (rc == XKB_OK && R->ref_mode && R->budget)
     {
         if ((rc = xkb_planner_set_device_budget(R->planner, R->budget)) == XKB_OK && R->gpu &&
