@@ -93,6 +93,8 @@ int main(void)
     xkrt_task_spawn_generic(rt, HOST_DEVICE_GLOBAL_ID, TASK_FLAG_DEPENDENT, esucc, NULL, 0, &b, 1, UNSPECIFIED_TASK_ACCESS, 0);
     xkrt_task_wait(rt);
     pthread_join(th, NULL);
+    const int st1 = xkb_runtime_status(rt);
+    if (st1 != 0) { fprintf(stderr, "host batch: status %d: %s\n", st1, xkb_last_error()); return 1; }
 
     /* device tasks with ocr_access = 1 (the y access) */
     enum { N = 1 << 16 };
@@ -112,10 +114,11 @@ int main(void)
         xkrt_task_spawn_generic(rt, 1, TASK_FLAG_DEVICE | TASK_FLAG_DEPENDENT, ax, &d, sizeof(d), acc, 2, 1, 0);
     }
     xkrt_task_wait(rt);
+    const int st2 = xkb_runtime_status(rt);
+    if (st2 != 0) { fprintf(stderr, "device batch: status %d: %s\n", st2, xkb_last_error()); return 1; }
     int ax_ok = 1;
     for (int i = 0; i < N; ++i) if (y[i] != 2.0 * i + 3.0) { ax_ok = 0; break; }
-    const int st = xkb_runtime_status(rt);
-    if (xkrt_deinit(rt) != 0 || st != 0) { fprintf(stderr, "status %d: %s\n", st, xkb_last_error()); return 1; }
+    if (xkrt_deinit(rt) != 0) { fprintf(stderr, "deinit: %s\n", xkb_last_error()); return 1; }
     printf("{\"order\": %d, \"early\": %d, \"axpby\": %d}\n", succ_saw == 2, early_succ_saw == 1, ax_ok);
     return succ_saw == 2 && early_succ_saw == 1 && ax_ok ? 0 : 1;
 }

@@ -35,7 +35,7 @@ def _oracle_run(g, dtype):
     """STEPS double-buffered Jacobi steps of the C oracle on all host threads."""
     L = O.c_oracle()
     step = L.xk_oracle_heat_step_f64 if dtype == np.float64 else L.xk_oracle_heat_step_f32
-    a = np.ascontiguousarray(g, dtype=dtype)
+    a = np.array(g, dtype=dtype, copy=True)          # the oracle steps in place: never on the caller's grid
     b = a.copy()
     nt = _threads()
     for _ in range(STEPS):
