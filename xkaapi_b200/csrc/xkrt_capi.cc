@@ -65,11 +65,15 @@ struct Task {
     uint32_t nargs = 0, nacc = 0;
     size_t args_off = 0, acc_off = 0;
     xkrt_task_func_t func = nullptr;      // team / plain function spawns
-    void * user_data = nullptr;
+    void * user_data = nullptr;           // their argument; without func: the task_t of a task built
+                                          // with the C++ source API (null otherwise)
     int detach = 0;                       // references (atomic builtins): the running body's, plus each
                                           // xkrt_task_detachable_incr; the task completes at 0
-    void * cxx = nullptr;                 // the task_t of a task built with the C++ source API
 };
+static_assert(sizeof(Task) == 64, "a spawned task record is one cache line");
+
+// The task_t of a task built with the C++ source API, or null.
+static inline void * cxx_of(const Task & T) { return T.func ? nullptr : T.user_data; }
 
 struct Region { uint64_t size; void * mirror; bool pinned_by_us; int32_t id; bool unified; };
 
@@ -741,11 +745,12 @@ static void spawn_task(xkb_runtime * R, xkrt_device_global_id_t device, xkrt_tas
 {
     Task t;
     t.rt = R; t.fmtid = fmtid; t.flags = flags; t.device = device;
-    t.cxx = cxx; t.detach = detach0;
+    t.detach = detach0;
     t.nargs = (uint32_t) args_size; t.nacc = (uint32_t) nacc;
     t.args_off = (R->args_pool.size() + 15) & ~(size_t) 15;
     t.acc_off = R->acc_pool.size();
-    t.func = func; t.user_data = ud;
+    t.func = func; t.user_data = cxx ? cxx : ud;       // C++ tasks have no func
+    
     const size_t args_end = args_size ? t.args_off + args_size : R->args_pool.size();
     if (!R->args_pool.resize(args_end) || !R->acc_pool.resize(t.acc_off + nacc) || !R->pending.push_back(t))
     {
@@ -1500,7 +1505,7 @@ static int run_builtin_views(xkb_runtime * R, Task & T, size_t t, const xkb_acce
 // task_t (a CUDA-target body on the worker's stream; a device task without format runs nothing).
 static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStream_t stream)
 {
-    xkrt::task_t * task = (xkrt::task_t *) T.cxx;
+    xkrt::task_t * task = (xkrt::task_t *) cxx_of(T);
     xkrt::access_t * acc = (task->flags & TASK_FLAG_DEPENDENT) ? xkrt::TASK_ACCESSES(task) : nullptr;
     for (uint32_t a = 0; a < T.nacc && acc; ++a)
     {
@@ -1587,7 +1592,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     const Format & f = R->formats[T.fmtid];
     __atomic_add_fetch(&T.detach, 1, __ATOMIC_ACQ_REL);        // the body's own reference
     g_current = &T;
-    if (T.cxx) rc = run_cxx_body(R, T, t, dev, stream);
+    if (cxx_of(T)) rc = run_cxx_body(R, T, t, dev, stream);
     else if (dev && T.fmtid == XKRT_TASK_FORMAT_NULL) {}         // placement only
     else if (dev)
     {
@@ -1645,7 +1650,7 @@ struct Dataflow {
 // queued (src/task.cc:160-245, __task_complete).
 static void task_completed(::xkb_runtime * R, Task & T)
 {
-    if (T.cxx) ((xkrt::task_t *) T.cxx)->state.value = xkrt::TASK_STATE_COMPLETED;
+    if (void * c = cxx_of(T)) ((xkrt::task_t *) c)->state.value = xkrt::TASK_STATE_COMPLETED;
     Dataflow * D = R ? R->df.load(std::memory_order_acquire) : nullptr;
     if (!D) return;
     const size_t g = (size_t) (&T - R->pending.data());
@@ -2155,7 +2160,7 @@ extern "C" void xkb_cxx_detachable(xkrt_runtime_t * runtime, void * task, int de
 {
     xkb_runtime * R = RT(runtime);
     xkrt::task_t * t = (xkrt::task_t *) task;
-    if (!R || !t || t->magic != xkrt::TASK_MAGIC || t->impl >= R->pending.size() || R->pending[t->impl].cxx != task)
+    if (!R || !t || t->magic != xkrt::TASK_MAGIC || t->impl >= R->pending.size() || cxx_of(R->pending[t->impl]) != task)
     {
         fail(R, xkb_set_error(XKB_EINVAL, "task_detachable: not a committed task of this runtime"));
         return;
