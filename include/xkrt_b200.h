@@ -228,6 +228,15 @@ XKB_API int xkb_planner_set_writeback_coherent(xkb_planner_t * planner, int on);
 /* Allocations evicted and blocks written back to the host by evictions so far. */
 XKB_API int xkb_planner_eviction_stats(xkb_planner_t * planner, uint64_t * evicted, uint64_t * written_back);
 
+/* Forget every device copy: the host's copy of every block is the only coherent one again and
+ * the next fetch of a block copies it from the host (the reference's runtime_t::reset drops the
+ * coherency controllers and the device memory, src/memory/invalidate.cc:66-133). Reference mode:
+ * the allocations are forgotten too (the next one is allocation 0 again, at offset 0 of a
+ * budget); resident mode: the regions and their mirrors stay. Blocks whose only copy is on the
+ * device are lost, as in the reference: write them back first (xkb_planner_flush_to_host in
+ * resident mode). XKB_EINVAL while planned copies have not been taken. */
+XKB_API int xkb_planner_invalidate(xkb_planner_t * planner);
+
 /* Resident mode (the B200 layout): every host region registered with xkb_planner_add_region
  * has ONE device mirror with the host layout (allocation ordinal = region index, byte offset =
  * offset in the region). A fetch to the GPU copies (H2D) only the blocks of the access the

@@ -3,7 +3,10 @@
  * the runtime's resolver reused, host memory coherent between batches), and the program
  * re-initialises no data between waits. WAIT_EVERY < 0: a wait after steps 1, 2, 4, 8, ... (and
  * the last), so every batch is larger than the one before.
- * usage: heat_waits_capi NX NY TS STEPS WAIT_EVERY init.bin out.bin */
+ * With a ninth argument "reset": after every wait but the last the program halves the source
+ * grid in host memory, outside any task, and calls xkrt_reset, which makes the runtime forget its
+ * device copies; the next batch then reads the halved grid (not the device's copy of the old one).
+ * usage: heat_waits_capi NX NY TS STEPS WAIT_EVERY init.bin out.bin [reset] */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -27,6 +30,7 @@ int main(int argc, char ** argv)
     if (argc < 8) return 2;
     const long NX = atol(argv[1]), NY = atol(argv[2]), TS = atol(argv[3]);
     const int steps = atoi(argv[4]), every = atoi(argv[5]);
+    const int reset = argc > 8 && strcmp(argv[8], "reset") == 0;
     xkrt_runtime_t * rt;
     if (xkrt_init(&rt) != 0) return 1;
     double * a = (double *) malloc(NX * NY * sizeof(double)), * b = (double *) malloc(NX * NY * sizeof(double));
@@ -61,7 +65,16 @@ int main(int argc, char ** argv)
             }
         double * t = src; src = dst; dst = t;
         const int at = every > 0 ? (s + 1) % every == 0 : ((s + 1) & s) == 0;
-        if (at || s + 1 == steps) { xkrt_task_wait(rt); ++waits; }
+        if (at || s + 1 == steps)
+        {
+            xkrt_task_wait(rt);
+            ++waits;
+            if (reset && s + 1 < steps)
+            {
+                for (long i = 0; i < NX * NY; ++i) src[i] *= 0.5;
+                xkrt_reset(rt);
+            }
+        }
     }
     f = fopen(argv[7], "wb");
     fwrite(src, sizeof(double), NX * NY, f);

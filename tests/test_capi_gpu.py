@@ -137,6 +137,31 @@ def test_heat_many_waits_one_runtime(torch_cuda, tmp_path, chunk, nx, ny, ts, st
     np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), O.heat_run(g, nx, ny, steps, 0.2))
 
 
+@pytest.mark.parametrize("planner", ["resident", "reference"])
+def test_reset_forgets_device_copies(torch_cuda, tmp_path, planner):
+    """xkrt_reset between waits (the reference's runtime_t::reset, src/memory/invalidate.cc:66-133):
+    the program halves the source grid in host memory after each wait, then resets; every batch
+    reads the halved grid, so the result is the oracle's with the same halvings (the device's
+    copies of the grid, coherent before the host write, are forgotten)."""
+    nx, ny, ts, steps, every = 260, 190, 64, 9, 3
+    g = O.heat_init(nx, ny, seed=31)
+    g.tofile(tmp_path / "init.bin")
+    env = dict(os.environ)
+    if planner == "reference":
+        env["XKB_PLANNER"] = "reference"
+    r = subprocess.run([build("heat_waits_capi", tmp_path), str(nx), str(ny), str(ts), str(steps), str(every),
+                        str(tmp_path / "init.bin"), str(tmp_path / "out.bin"), "reset"], capture_output=True, text=True,
+                       env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout)["waits"] == 3
+    want = g
+    for k in range(steps // every):
+        want = O.heat_run(want, nx, ny, every, 0.2)
+        if k + 1 < steps // every:
+            want = want * 0.5
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), want)
+
+
 def test_spawn_generic_detachable_count_and_ocr(torch_cuda, tmp_path):
     """xkrt_task_spawn_generic: a detachable task spawned with an initial counter of 2 completes
     only after two xkrt_task_detachable_decr from another thread (its successor sees both), one

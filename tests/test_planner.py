@@ -473,3 +473,38 @@ def test_reference_writeback_pick_and_the_coherent_one(coherent):
     final = host[(steps % 2) * n * n * 8:][:n * n * 8].view(np.float64).reshape(n, n)
     stale = int((final != O.heat_run(g, n, n, steps, 0.2)).sum())
     assert stale == (0 if coherent else 14259)
+
+
+@pytest.mark.parametrize("resident", [False, True])
+def test_invalidate_fetches_from_the_host_again(resident):
+    """After xkb_planner_invalidate (what xkrt_reset does to the coherency state, the reference's
+    runtime_t::reset, src/memory/invalidate.cc:66-133) the same reads copy the same bytes from
+    the host again; without it they copy nothing. Reference mode restarts its allocations."""
+    import streams as S
+    base = 1 << 30
+    recs = S.from_tuples([[("m", S.R, base, 256, 0, 0, 64, 32, 8)], [("m", S.RW, base, 256, 64, 0, 64, 32, 8)]])
+    P = xk.Planner(resident=resident)
+    if resident:
+        P.add_region(base, 256 * 64 * 8)
+    for i, r in enumerate(recs):
+        P.fetch(r, 0, 1)
+    first = P.copies(take=True)
+    assert len(first) and (first[:, 2] == 0).all()
+    allocs0 = P.allocations()
+    for r in recs:
+        P.fetch(r, 0, 1)
+    assert len(P.copies(take=True)) == 0             # both reads already coherent on the device
+    P.invalidate()
+    for r in recs:
+        P.fetch(r, 0, 1)
+    again = P.copies(take=True)
+    np.testing.assert_array_equal(again, first)
+    np.testing.assert_array_equal(P.allocations(), allocs0)
+
+
+def test_invalidate_refuses_untaken_copies():
+    import streams as S
+    P = xk.Planner()
+    P.fetch(S.from_tuples([[("m", S.R, 1 << 30, 256, 0, 0, 64, 32, 8)]])[0], 0, 1)
+    with pytest.raises(xk.XkbError):
+        P.invalidate()

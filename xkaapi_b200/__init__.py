@@ -97,6 +97,7 @@ SIGNATURES = {
     "xkb_planner_create_resident": (_int, [ctypes.POINTER(_vp)]),
     "xkb_planner_add_region": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
     "xkb_planner_flush_to_host": (_int, [_vp]),
+    "xkb_planner_invalidate": (_int, [_vp]),
     "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),
     "xkb_planner_plan": (_int, [_vp, _vp, ctypes.c_size_t, _int, _vp]),
     "xkb_planner_copies": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _int]),
@@ -361,6 +362,10 @@ class Planner:
 
     def flush_to_host(self):
         check(lib().xkb_planner_flush_to_host(self._h))
+
+    def invalidate(self):
+        """Forget every device copy (the host's is the only coherent one again)."""
+        check(lib().xkb_planner_invalidate(self._h))
 
     def plan(self, recs, device=1):
         import numpy as np

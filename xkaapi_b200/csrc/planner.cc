@@ -724,6 +724,18 @@ extern "C" int xkb_planner_flush_to_host(xkb_planner_t * P)
     return XKB_OK;
 }
 
+extern "C" int xkb_planner_invalidate(xkb_planner_t * P)
+{
+    if (!P) return xkb_set_error(XKB_EINVAL, "planner_invalidate: null planner");
+    if (!P->copies.empty()) return xkb_set_error(XKB_EINVAL, "planner_invalidate: %zu planned copies not taken", P->copies.size());
+    if (P->resident) { P->rframes.clear(); return XKB_OK; }       // the regions' mirrors stay, holding nothing
+    P->frames.clear();
+    P->allocs.clear(); P->alloc_off.clear(); P->alloc_got.clear(); P->alloc_live.clear(); P->pinned.clear();
+    P->arena.init(P->budget);
+    P->cur_task = -1;
+    return XKB_OK;
+}
+
 extern "C" int xkb_planner_add_region(xkb_planner_t * P, uint64_t host_base, uint64_t size, int32_t * region)
 {
     if (!P || !P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_add_region: needs a resident planner and a size");

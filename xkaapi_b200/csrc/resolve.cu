@@ -94,6 +94,22 @@ __device__ __forceinline__ int spill_alloc(int * spill, unsigned * ctr, unsigned
     return (int) c;
 }
 
+// Pairs are staged per warp in shared memory and appended to a.emit EMIT_BUF - 32 or more at a
+// time, with one atomic on the batch's counter per flush instead of one per emitting step.
+constexpr int EMIT_BUF = 256;
+
+// Append this warp's n staged pairs to a.emit (coalesced); every lane of the warp calls it.
+__device__ __forceinline__ void emit_flush(const ResolveArgs & a, const unsigned long long * buf, int n, int lane)
+{
+    __syncwarp();
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(a.emit_count, (unsigned long long) n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int j = lane; j < n; j += 32)
+        if (base + j < a.emit_cap) a.emit[base + j] = buf[j];
+    __syncwarp();
+}
+
 // BINNED: the CTA's ops come from its region's list (op indices in op order, built by the
 // binning kernels below) instead of a scan of every op of the batch.
 template <int RX, int RY, bool BINNED>
@@ -107,6 +123,7 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
     __shared__ DOp list[CHUNK];
     __shared__ int wcount[NW];
     __shared__ int nlist_s;
+    __shared__ unsigned long long ebuf[NW][EMIT_BUF];   // each warp's pairs not yet in a.emit
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int rx = blockIdx.x % a.nrx, ry = blockIdx.x / a.nrx;
@@ -117,6 +134,7 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
     const size_t cell = valid ? (size_t) cy * a.ncx + cx : 0;
 
     int writer = -1, nr = 0, head = -1, tail = -1;
+    int nbuf = 0;                                // pairs in this warp's ebuf (same in every lane)
     if (valid)
     {
         const int * st = a.state_in + cell * STRIDE;
@@ -190,15 +208,10 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
                     const unsigned peers = __match_any_sync(0xffffffffu, p);
                     const bool leader = p >= 0 && lane == __ffs(peers) - 1;
                     const unsigned em = __ballot_sync(0xffffffffu, leader);
-                    unsigned long long slot0 = 0;
-                    if (lane == __ffs(em) - 1 && em) slot0 = atomicAdd(a.emit_count, (unsigned long long) __popc(em));
-                    slot0 = __shfl_sync(0xffffffffu, slot0, em ? __ffs(em) - 1 : 0);
                     if (leader)
-                    {
-                        const unsigned long long slot = slot0 + __popc(em & ((1u << lane) - 1));
-                        if (slot < a.emit_cap)
-                            a.emit[slot] = ((unsigned long long) (uint32_t) p << 32) | (uint32_t) op.task;
-                    }
+                        ebuf[warp][nbuf + __popc(em & ((1u << lane) - 1))] = ((unsigned long long) (uint32_t) p << 32) | (uint32_t) op.task;
+                    nbuf += __popc(em);
+                    if (nbuf > EMIT_BUF - 32) { emit_flush(a, ebuf[warp], nbuf, lane); nbuf = 0; }
                 }
             }
             else if (in)
@@ -225,6 +238,7 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
         __syncthreads();
     }
 
+    if (nbuf) emit_flush(a, ebuf[warp], nbuf, lane);
     if (valid)
     {
         int * st = a.state_out + cell * STRIDE;
@@ -347,17 +361,26 @@ __global__ void dedupe_kernel(const unsigned long long * __restrict__ emit, size
     if (i >= n) return;
     const unsigned long long key = emit[i];
     unsigned long long h = mix64(key) & mask;
+    bool fresh = false;
     for (unsigned long long probe = 0; probe <= mask; ++probe)
     {
         const unsigned long long prev = atomicCAS(table + h, EDGE_EMPTY, key);
-        if (prev == EDGE_EMPTY)
-        {
-            const unsigned long long s = atomicAdd(nuniq, 1ull);
-            if (s < uniq_cap) uniq[s] = key;
-            return;
-        }
-        if (prev == key) return;
+        if (prev == EDGE_EMPTY) { fresh = true; break; }
+        if (prev == key) break;
         h = (h + 1) & mask;
+    }
+    // one atomic per warp on the shared counter for the warp's new pairs
+    const unsigned act = __activemask();
+    const unsigned nb = __ballot_sync(act, fresh);
+    if (!nb) return;
+    const int lane = threadIdx.x & 31, first = __ffs(nb) - 1;
+    unsigned long long base = 0;
+    if (lane == first) base = atomicAdd(nuniq, (unsigned long long) __popc(nb));
+    base = __shfl_sync(act, base, first);
+    if (fresh)
+    {
+        const unsigned long long s = base + __popc(nb & ((1u << lane) - 1));
+        if (s < uniq_cap) uniq[s] = key;
     }
 }
 

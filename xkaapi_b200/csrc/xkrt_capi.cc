@@ -454,6 +454,25 @@ extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
     R->pending.clear(); R->args_pool.clear(); R->acc_pool.clear(); R->replica_pool.clear(); R->recs.clear();
     R->args_dense = true;
     R->cur_h2d = R->cur_d2h = R->cur_h2d_bytes = R->cur_d2h_bytes = 0;
+    // the coherency state goes too (src/memory/invalidate.cc:66-133 drops the memory controllers
+    // and the device memory): the next task fetches every block from the host again. Each wait
+    // left the host coherent, so the host holds everything completed tasks wrote.
+    if (R->planner)
+    {
+        size_t n = 0;                                                   // copies planned for dropped tasks
+        if (xkb_planner_copies(R->planner, nullptr, 0, &n, 0) == XKB_OK && n)
+        {
+            std::vector<xkb_copy_t> drop(n);
+            xkb_planner_copies(R->planner, drop.data(), n, &n, 1);
+        }
+        if (xkb_planner_invalidate(R->planner) != XKB_OK) fail(R, XKB_EINVAL);
+    }
+    if (R->ref_mode)
+    {
+        if (R->gpu) cudaStreamSynchronize(R->stream);
+        if (!R->budget_base) for (void * p : R->allocs) if (p) cudaFree(p);
+        R->allocs.clear();
+    }
 }
 
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, bool unified = false)
