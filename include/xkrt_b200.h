@@ -228,6 +228,19 @@ XKB_API int xkb_planner_set_writeback_coherent(xkb_planner_t * planner, int on);
 /* Allocations evicted and blocks written back to the host by evictions so far. */
 XKB_API int xkb_planner_eviction_stats(xkb_planner_t * planner, uint64_t * evicted, uint64_t * written_back);
 
+/* Registration-overflow protection of the reference's default build (XKRT_MEMORY_REGISTER_-
+ * OVERFLOW_PROTECTION with protect_registered_memory_overflow on): host memory [ptr, ptr + size)
+ * got registered / unregistered. The range is rounded out to pages; register takes the pieces not
+ * registered yet, unregister every registered interval the range meets; each is inserted into
+ * every (ld, sizeof) frame (and into frames made later, while registered) as its 1-3 rects, so no
+ * block and no copy straddles a registration boundary (memory-tree.hpp:2184-2240,
+ * src/memory/register.cc:89-262). The blocks' state is unchanged. Reference mode only.
+ * Divergence: where a registration meets two or more registered intervals, the reference walks
+ * them in tree order (its IntervalSet::find is not sorted, an assert of its debug build says
+ * they should be); this planner walks them in address order. */
+XKB_API int xkb_planner_register(xkb_planner_t * planner, uint64_t ptr, uint64_t size);
+XKB_API int xkb_planner_unregister(xkb_planner_t * planner, uint64_t ptr, uint64_t size);
+
 /* Forget every device copy: the host's copy of every block is the only coherent one again and
  * the next fetch of a block copies it from the host (the reference's runtime_t::reset drops the
  * coherency controllers and the device memory, src/memory/invalidate.cc:66-133). Reference mode:

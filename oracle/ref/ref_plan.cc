@@ -17,6 +17,16 @@
 //        <out>.allocs: int64 {bytes} per allocation, in allocation order
 //        <out>.views : int64 {task, access, alloc, off, ld} -- the device view each access gets
 //        stdout      : one JSON line of counts
+//
+// Optional third argument: a file of int64 registration events {before_task, kind (1 register,
+// 2 unregister), ptr, size}, applied before the first fetch of task `before_task` the way
+// runtime_t::memory_register / memory_unregister (src/memory/register.cc:89-262) tell the trees
+// of the calling task's domain under the reference's default build (overflow protection, page
+// rounding and assisted registration on; one driver that registers host memory): the range is
+// rounded out to pages (include/xkrt/memory/pageas.h), only its pieces not yet registered
+// (register) or its registered intervals (unregister) go to every existing tree
+// (KBLASMemoryTree::registered / unregistered, memory-tree.hpp:2184-2240), and a tree created
+// later first receives every registered piece (src/task/task.cc:88-94, 127-133).
 #include <xkrt/runtime.h>
 #include <xkrt/task/task.hpp>
 #include <xkrt/memory/access/access.hpp>
@@ -30,6 +40,12 @@
 #include <string>
 #include <utility>
 #include <vector>
+
+#include <xkrt/memory/access/common/interval-set.hpp>
+#include <xkrt/memory/pageas.h>
+
+#include <algorithm>
+#include <array>
 
 #include "../access_stream.h"
 #include "seams.h"
@@ -91,11 +107,65 @@ static area_chunk_t * hook_allocate(runtime_t *, device_global_id_t, size_t size
 static void hook_deallocate(runtime_t *, device_global_id_t, area_chunk_t *) {}
 static void hook_execute(runtime_t *, device_t *, task_t *) {}
 
+using Trees = std::map<std::pair<size_t, size_t>, BLASMemoryTree *>;
+static IntervalSet<uintptr_t> g_pages;                  // runtime_t::registered_pages
+static std::map<uintptr_t, size_t> g_registered;        // runtime_t::registered_memory
+
+static void apply_register(Trees & trees, uintptr_t ptr, size_t size)
+{
+    uintptr_t a; size_t sz;
+    pageas((void *) ptr, size, &a, &sz);
+    const uintptr_t b = a + sz;
+    std::vector<Interval> iv;
+    g_pages.find(a, b, iv);
+    unsigned i = 0;
+    uintptr_t p1 = a;
+    while (1)
+    {
+        const uintptr_t p2 = (i == iv.size()) ? b : iv[i].a;
+        if (p1 < p2)
+        {
+            g_registered[p1] = p2 - p1;
+            for (auto & kv : trees) kv.second->registered(p1, p2 - p1);
+        }
+        if (i == iv.size()) break;
+        p1 = iv[i].b;
+        ++i;
+    }
+    g_pages.fill(a, b);
+}
+
+static void apply_unregister(Trees & trees, uintptr_t ptr, size_t size)
+{
+    uintptr_t a; size_t sz;
+    pageas((void *) ptr, size, &a, &sz);
+    const uintptr_t b = a + sz;
+    std::vector<Interval> iv;
+    g_pages.find(a, b, iv);
+    std::sort(iv.begin(), iv.end());
+    for (const Interval & v : iv)
+    {
+        g_registered.erase(v.a);
+        for (auto & kv : trees) kv.second->unregistered(v.a, v.b - v.a);
+    }
+    g_pages.unfill(a, b);
+}
+
 int main(int argc, char ** argv)
 {
-    if (argc < 3) { fprintf(stderr, "usage: %s <stream.bin> <out-prefix>\n", argv[0]); return 2; }
+    if (argc < 3) { fprintf(stderr, "usage: %s <stream.bin> <out-prefix> [events.bin]\n", argv[0]); return 2; }
     std::vector<xk_stream_rec_t> recs;
     if (xk_stream_read(argv[1], recs)) { fprintf(stderr, "cannot read %s\n", argv[1]); return 2; }
+    std::vector<std::array<int64_t, 4>> events;
+    if (argc > 3)
+    {
+        FILE * ef = fopen(argv[3], "rb");
+        if (!ef) { fprintf(stderr, "cannot read %s\n", argv[3]); return 2; }
+        std::array<int64_t, 4> e;
+        while (fread(e.data(), 8, 4, ef) == 4) events.push_back(e);
+        fclose(ef);
+    }
+    size_t next_event = 0;
 
     xk_seam_hooks.copy2d = hook_copy2d;
     xk_seam_hooks.copy1d = hook_copy1d;
@@ -108,7 +178,7 @@ int main(int argc, char ** argv)
     runtime_t * runtime = (runtime_t *) calloc(1, sizeof(runtime_t));
     new (&runtime->router) RouterAffinity();
 
-    std::map<std::pair<size_t, size_t>, BLASMemoryTree *> trees;
+    Trees trees;
     std::vector<std::array<int64_t, 5>> views;
     const device_global_id_t GPU = 1;
 
@@ -116,6 +186,12 @@ int main(int argc, char ** argv)
     while (i < recs.size())
     {
         const uint32_t tid = recs[i].task;
+        while (next_event < events.size() && events[next_event][0] <= (int64_t) tid)
+        {
+            const auto & e = events[next_event++];
+            if (e[1] == 1) apply_register(trees, (uintptr_t) e[2], (size_t) e[3]);
+            else apply_unregister(trees, (uintptr_t) e[2], (size_t) e[3]);
+        }
         size_t j = i;
         while (j < recs.size() && recs[j].task == tid) ++j;
         const task_access_counter_t AC = (task_access_counter_t) (j - i);
@@ -139,7 +215,11 @@ int main(int argc, char ** argv)
             access_t * acc = accesses + a;
             const size_t ld = acc->host_view.ld, s = acc->host_view.sizeof_type;
             BLASMemoryTree *& tree = trees[{ld, s}];
-            if (!tree) tree = new BLASMemoryTree(runtime, ld, s, false);
+            if (!tree)
+            {
+                tree = new BLASMemoryTree(runtime, ld, s, false);
+                for (const auto & [p, n] : g_registered) tree->registered(p, n);
+            }
             g_task = tid; g_access = (int64_t) a;
             // record field `reserved` bit 0 selects the host (device 0) as the fetch target
             const device_global_id_t target = (recs[i + a].reserved & 1) ? HOST_DEVICE_GLOBAL_ID : GPU;

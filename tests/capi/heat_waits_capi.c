@@ -7,6 +7,7 @@
  * grid in host memory, outside any task, and calls xkrt_reset, which makes the runtime forget its
  * device copies; the next batch then reads the halved grid (not the device's copy of the old one).
  * usage: heat_waits_capi NX NY TS STEPS WAIT_EVERY init.bin out.bin [reset] */
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -81,6 +82,7 @@ int main(int argc, char ** argv)
     fclose(f);
     const int st = xkb_runtime_status(rt);
     if (xkrt_deinit(rt) != 0 || st != 0) { fprintf(stderr, "status %d: %s\n", st, xkb_last_error()); return 1; }
-    printf("{\"waits\": %d}\n", waits);
+    printf("{\"waits\": %d, \"grid_a\": %llu, \"grid_b\": %llu}\n", waits, (unsigned long long) (uintptr_t) a,
+           (unsigned long long) (uintptr_t) b);
     return 0;
 }

@@ -22,7 +22,10 @@ mixed_stream), where the reference's dependency tree is not point-wise
 (include/xkrt/memory/access/blas/dependency-tree.hpp:228-256 applies a PUT to whole split-off
 nodes that meet the access's other rect): the reference's edges and the point-wise edges of the
 oracle restatement (oracle/_bin/deps_oracle) are both stored, so the exact difference is pinned.
-Run: python tests/golden/make_golden.py [deps] [plan] [axpby] [wrap]   (default: all; needs the
+register fixtures: ref_plan with registration events (the reference's default build splits its
+trees at registered pages, memory-tree.hpp:2184-2240); each case's plan is stored with the
+plan of the same stream without registrations so the splits' effect is visible.
+Run: python tests/golden/make_golden.py [deps] [plan] [axpby] [wrap] [register]   (default: all; needs the
 binaries of oracle/ref/build_ref.sh and oracle/Makefile)
 """
 import os, subprocess, sys, tempfile
@@ -174,6 +177,53 @@ def plan_cases():
         yield f"plan_seg_{seed}", np.array(rows, dtype=S.REC)
 
 
+def ref_plan_registered(recs, events):
+    """ref_plan with registration events (int64 rows {before_task, kind 1 register / 2 unregister,
+    ptr, size}): the reference's trees split at the registered pages."""
+    with tempfile.TemporaryDirectory() as d:
+        p, e = os.path.join(d, "s.bin"), os.path.join(d, "e.bin")
+        S.write_stream(p, recs)
+        np.asarray(events, dtype="<i8").reshape(-1, 4).tofile(e)
+        subprocess.run([os.path.join(REPO, "oracle/_ref/ref_plan"), p, os.path.join(d, "o"), e],
+                       check=True, capture_output=True)
+        plan = np.fromfile(os.path.join(d, "o.plan"), dtype="<i8").reshape(-1, 14)
+        allocs = np.fromfile(os.path.join(d, "o.allocs"), dtype="<i8")
+        views = np.fromfile(os.path.join(d, "o.views"), dtype="<i8").reshape(-1, 5)
+    if len(plan):
+        plan = plan[np.lexsort(tuple(plan[:, k] for k in range(13, -1, -1)))]
+    return plan, allocs, views
+
+
+def register_cases():
+    """(name, stream, events) for the registration-overflow fixtures: grids registered whole,
+    unaligned, in two overlapping pieces, between tasks and unregistered; ld 200 (1600-byte
+    columns) puts page boundaries inside columns; a segment stream; write-backs."""
+    REG, UNREG = 1, 2
+    n = 256 * 256 * 8
+    heat = S.heat_stream(256, 256, 64, 64, 4, base_src=1 << 20, base_dst=1 << 21)
+    yield "reg_heat_256_both", heat, [(0, REG, 1 << 20, n), (0, REG, 1 << 21, n)]
+    una = S.heat_stream(256, 256, 64, 64, 4, base_src=(1 << 20) + 1024, base_dst=(1 << 22) + 512)
+    yield "reg_heat_256_unaligned", una, [(0, REG, (1 << 20) + 1024, n), (0, REG, (1 << 22) + 512, n)]
+    yield "reg_heat_256_pieces", heat, [(0, REG, 1 << 20, 300000), (0, REG, (1 << 20) + 300000, n - 300000),
+                                        (0, REG, (1 << 21) + 5000, 70000)]
+    m = 200 * 160 * 8
+    ld200 = S.heat_stream(200, 160, 48, 48, 5, base_src=1 << 20, base_dst=(1 << 20) + m + 100)
+    yield "reg_heat_ld200_midstream", ld200, [(3, REG, (1 << 20) + 777, 90000), (20, REG, (1 << 20) + m + 100, m),
+                                              (41, UNREG, (1 << 20) + 777, 90000), (60, REG, (1 << 20) + 20000, 9000)]
+    rng = np.random.default_rng(5)
+    rows = []
+    for t in range(24):
+        for _ in range(int(rng.integers(1, 3))):
+            a = (1 << 16) + int(rng.integers(0, 4096)) * 8
+            b = a + int(rng.integers(1, 2048)) * 8
+            rows.append((t, S.SEGMENT, [S.R, S.W, S.RW][int(rng.integers(0, 3))], int(rng.random() < 0.2), a, b, 0, 0, 0, 0, 0))
+    yield "reg_seg", np.array(rows, dtype=S.REC), [(0, REG, (1 << 16) + 10000, 12000), (9, REG, (1 << 16) + 30000, 5000),
+                                                   (15, UNREG, (1 << 16) + 10000, 100)]
+    wb = S.microbench_stream(20, 3, n=256, ld=256, align=16, max_side_units=6)
+    wb["reserved"] = (np.random.default_rng(1003).random(len(wb)) < 0.25).astype(np.uint16)
+    yield "reg_mat_wb", wb, [(0, REG, (1 << 30) + 12345, 200000), (10, REG, (1 << 30) + 300000, 100000)]
+
+
 AXPBY_CASES = [  # name, n, passes, seed, cmin bytes, cmax bytes
     ("axpby_20000_p3", 20000, 3, 11, 512, 65536),
     ("axpby_12345_p5", 12345, 5, 29, 64, 16384),
@@ -203,7 +253,20 @@ def pointwise_edges(recs):
 
 
 def main():
-    which = set(sys.argv[1:]) or {"deps", "plan", "axpby", "wrap"}
+    which = set(sys.argv[1:]) or {"deps", "plan", "axpby", "wrap", "register"}
+    if "register" in which:
+        out = {}
+        for name, recs, events in register_cases():
+            plan, allocs, views = ref_plan_registered(recs, events)
+            out[name + "__stream"] = recs
+            out[name + "__events"] = np.asarray(events, dtype=np.int64).reshape(-1, 4)
+            out[name + "__plan"] = plan
+            out[name + "__allocs"] = allocs
+            out[name + "__views"] = views
+            out[name + "__plan_noreg"] = ref_plan(recs)[0]
+            print(f"{name}: {len(recs)} accesses, {len(events)} events, {len(plan)} copies "
+                  f"({len(out[name + '__plan_noreg'])} without them), {len(allocs)} allocations")
+        np.savez_compressed(os.path.join(HERE, "register_golden.npz"), **out)
     if "wrap" in which:
         out = {}
         for seed in WRAP_SEEDS:

@@ -162,6 +162,51 @@ def test_reset_forgets_device_copies(torch_cuda, tmp_path, planner):
     np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), want)
 
 
+@pytest.mark.parametrize("protect", ["1", "0"])
+def test_reference_mode_registration_splits(torch_cuda, tmp_path, protect):
+    """Reference mode on user memory registered with xkrt_memory_register (the grids come from
+    malloc, so they are not page-aligned): with the reference's default registration-overflow
+    protection the copies the C API executes (XKB_PLAN_RECORD) are the planner's plan for the
+    same stream after the two registrations -- the planner's splits are pinned to the reference's
+    memory tree by tests/test_planner.py -- and they differ from the plan without them;
+    XKAAPI_MEMORY_REGISTER_PROTECT_OVERFLOW=0 gives the plan without them. The grid is the
+    oracle's either way."""
+    import streams as S
+    import xkaapi_b200 as xk
+    nx, ny, ts, steps = 200, 136, 64, 5
+    g = O.heat_init(nx, ny, seed=41)
+    g.tofile(tmp_path / "init.bin")
+    env = dict(os.environ, XKB_PLANNER="reference", XKB_PLAN_RECORD=str(tmp_path / "plan.bin"),
+               XKAAPI_MEMORY_REGISTER_PROTECT_OVERFLOW=protect)
+    r = subprocess.run([build("heat_waits_capi", tmp_path), str(nx), str(ny), str(ts), str(steps), str(steps),
+                        str(tmp_path / "init.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.bin").reshape(ny, nx), O.heat_run(g, nx, ny, steps, 0.2))
+    recs = S.heat_stream(nx, ny, ts, ts, steps, base_src=out["grid_a"], base_dst=out["grid_b"])
+
+    def plan(registered):
+        P = xk.Planner()
+        if registered:
+            P.register(out["grid_a"], nx * ny * 8)
+            P.register(out["grid_b"], nx * ny * 8)
+        first = 0
+        for i in range(len(recs)):
+            if i == 0 or recs[i]["task"] != recs[i - 1]["task"]:
+                first = i
+            P.fetch(recs[i], i - first, 1)
+        for i in range(len(recs)):                  # the wait's write-back: every written access, spawn order
+            if recs[i]["mode"] & S.W:
+                P.fetch(recs[i], 1, 0)
+        return P.copies()
+
+    key = lambda q: q[np.lexsort(tuple(q[:, k] for k in range(13, -1, -1)))]
+    done = key(np.fromfile(tmp_path / "plan.bin", dtype=np.int64).reshape(-1, 14))
+    with_reg, without = key(plan(True)), key(plan(False))
+    assert len(with_reg) != len(without)
+    np.testing.assert_array_equal(done, with_reg if protect == "1" else without)
+
+
 def test_spawn_generic_detachable_count_and_ocr(torch_cuda, tmp_path):
     """xkrt_task_spawn_generic: a detachable task spawned with an initial counter of 2 completes
     only after two xkrt_task_detachable_decr from another thread (its successor sees both), one

@@ -508,3 +508,39 @@ def test_invalidate_refuses_untaken_copies():
     P.fetch(S.from_tuples([[("m", S.R, 1 << 30, 256, 0, 0, 64, 32, 8)]])[0], 0, 1)
     with pytest.raises(xk.XkbError):
         P.invalidate()
+
+
+RG = np.load(os.path.join(REPO, "tests", "golden", "register_golden.npz"))
+REG_CASES = sorted(k[:-len("__stream")] for k in RG.files if k.endswith("__stream"))
+
+
+@pytest.mark.parametrize("case", REG_CASES)
+def test_registration_splits_match_reference(case):
+    """Registration-overflow protection (the reference's default build): host ranges registered
+    or unregistered before given tasks split the partition at their pages; every copy, allocation
+    and device view equals the reference's memory tree fed the same events (golden from
+    oracle/_ref/ref_plan), and differs from the plan without the registrations."""
+    recs, events = RG[case + "__stream"], RG[case + "__events"]
+    P = xk.Planner()
+    views, first, e = [], 0, 0
+    for i in range(len(recs)):
+        if i == 0 or recs[i]["task"] != recs[i - 1]["task"]:
+            first = i
+            while e < len(events) and events[e][0] <= recs[i]["task"]:
+                (P.register if events[e][1] == 1 else P.unregister)(int(events[e][2]), int(events[e][3]))
+                e += 1
+        views.append(P.fetch(recs[i], i - first, 0 if recs[i]["reserved"] & 1 else 1))
+    q = P.copies()
+    q = q[np.lexsort(tuple(q[:, k] for k in range(13, -1, -1)))]
+    np.testing.assert_array_equal(q, RG[case + "__plan"])
+    np.testing.assert_array_equal(P.allocations().astype(np.int64), RG[case + "__allocs"])
+    dev = (recs["reserved"] & 1) == 0
+    np.testing.assert_array_equal(np.array(views)[dev], RG[case + "__views"][dev][:, 2:])
+    assert len(q) > len(RG[case + "__plan_noreg"])
+    np.testing.assert_array_equal(plan_of(recs)[0], RG[case + "__plan_noreg"])
+
+
+def test_registration_refused_in_resident_mode():
+    P = xk.Planner(resident=True)
+    with pytest.raises(xk.XkbError):
+        P.register(1 << 20, 4096)

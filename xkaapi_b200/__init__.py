@@ -98,6 +98,8 @@ SIGNATURES = {
     "xkb_planner_add_region": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
     "xkb_planner_flush_to_host": (_int, [_vp]),
     "xkb_planner_invalidate": (_int, [_vp]),
+    "xkb_planner_register": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64]),
+    "xkb_planner_unregister": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64]),
     "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),
     "xkb_planner_plan": (_int, [_vp, _vp, ctypes.c_size_t, _int, _vp]),
     "xkb_planner_copies": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _int]),
@@ -362,6 +364,13 @@ class Planner:
 
     def flush_to_host(self):
         check(lib().xkb_planner_flush_to_host(self._h))
+
+    def register(self, ptr, size):
+        """Host memory [ptr, ptr + size) registered (registration-overflow protection)."""
+        check(lib().xkb_planner_register(self._h, ptr, size))
+
+    def unregister(self, ptr, size):
+        check(lib().xkb_planner_unregister(self._h, ptr, size))
 
     def invalidate(self):
         """Forget every device copy (the host's is the only coherent one again)."""

@@ -30,7 +30,13 @@
 //  * Host fetch (write-back): no copy if no device holds the block, or the host already does;
 //    else D2H from the view on the LARGEST allocation of the block (first one of maximal size,
 //    coherent or not -- as the reference selects it, :1110-1160); completion sets the host bit.
+//  * Registration-overflow protection (the reference's default build): a registered host range,
+//    rounded out to pages, is inserted into every frame as 1-3 rects, so that no block, hence no
+//    copy, straddles a registration boundary (memory-tree.hpp:2184-2240, src/memory/register.cc,
+//    src/task/task.cc:88-94, 127-133). Only the partition changes; blocks keep their state.
 #include "common.cuh"
+
+#include <unistd.h>
 
 #include <algorithm>
 #include <cstring>
@@ -285,7 +291,34 @@ struct xkb_planner {
     std::map<uint64_t, std::pair<uint64_t, int32_t>> regions;
     std::map<std::pair<uint64_t, uint64_t>, std::unique_ptr<RFrame>> rframes;
     std::vector<RPartite> rscratch;
+    // registration-overflow protection: the registered page intervals (start -> end, disjoint,
+    // overlapping ones merged, adjacent ones not) and the pieces every new frame receives
+    std::map<uint64_t, uint64_t> reg_pages;
+    std::map<uint64_t, uint64_t> registered;          // start -> size
 };
+
+// The rects of the bytes [a, a + size) in a frame (interval_to_rects, access.hpp:77-139): one in
+// the segment frame; in an (ld, sizeof) frame the head of the first column, the whole columns, the
+// tail of the last (empty ones dropped, as the tree ignores them).
+static int interval_rects(uint64_t a, uint64_t size, uint64_t ld, uint64_t s, Rect out[3])
+{
+    if (ld == ~0ull) { out[0] = {a, a + size, 0, 1}; return 1; }
+    const uint64_t LDs = ld * s;
+    const uint64_t x0 = a % LDs, x1 = std::min(x0 + size, LDs), dx10 = x1 - x0;
+    const uint64_t x3 = (size - dx10) % LDs;
+    const uint64_t y0 = a / LDs, y1 = y0 + 1, y3 = y0 + (size - dx10 - x3) / LDs + 2, y2 = y3 - 1;
+    const Rect r[3] = {{x0, x1, y0, y1}, {0, LDs, y1, y2}, {0, x3, y2, y3}};
+    int n = 0;
+    for (const Rect & q : r) if (q.x0 < q.x1 && q.y0 < q.y1) out[n++] = q;
+    return n;
+}
+
+static void split_frame_at(Frame & f, uint64_t a, uint64_t size)
+{
+    Rect r[3];
+    const int n = interval_rects(a, size, f.ld, f.s, r);
+    for (int k = 0; k < n; ++k) insert(f, r[k]);
+}
 
 // The access's rects in its (ld, sizeof) frame (access.hpp:204-287): one rect, or two when the
 // tile wraps the leading dimension; `origin` is where each rect's view origin lies so that
@@ -457,7 +490,13 @@ static int fetch_one(xkb_planner * P, const xkb_access_rec_t & a, int64_t access
     if (rc) return rc;
     const Rect & r = rr[0];
     std::unique_ptr<Frame> & fp = P->frames[{ld, s}];
-    if (!fp) { fp.reset(new (std::nothrow) Frame()); if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory"); fp->ld = ld; fp->s = s; }
+    if (!fp)
+    {
+        fp.reset(new (std::nothrow) Frame());
+        if (!fp) return xkb_set_error(XKB_ENOMEM, "planner: out of memory");
+        fp->ld = ld; fp->s = s;
+        for (const auto & kv : P->registered) split_frame_at(*fp, kv.first, kv.second);   // task.cc:88-94, 127-133
+    }
     Frame & f = *fp;
     const bool seg = ld == ~0ull;
     const uint64_t host_stride = seg ? 0 : ld * s;
@@ -720,6 +759,69 @@ extern "C" int xkb_planner_flush_to_host(xkb_planner_t * P)
                 k = e + 1;
             }
         }
+    }
+    return XKB_OK;
+}
+
+// The page interval of [ptr, ptr + size) (pageas, include/xkrt/memory/pageas.h).
+static void page_round(uint64_t ptr, uint64_t size, uint64_t & a, uint64_t & b)
+{
+    static const uint64_t page = (uint64_t) sysconf(_SC_PAGESIZE);
+    a = ptr - ptr % page;
+    const uint64_t e = ptr + size;
+    b = e + (page - e % page) % page;
+}
+
+// Registered page intervals meeting [a, b), in address order.
+static std::vector<std::pair<uint64_t, uint64_t>> reg_find(const xkb_planner * P, uint64_t a, uint64_t b)
+{
+    std::vector<std::pair<uint64_t, uint64_t>> out;
+    auto it = P->reg_pages.upper_bound(a);
+    if (it != P->reg_pages.begin()) { auto p = std::prev(it); if (p->second > a) out.push_back(*p); }
+    for (; it != P->reg_pages.end() && it->first < b; ++it) out.push_back(*it);
+    return out;
+}
+
+extern "C" int xkb_planner_register(xkb_planner_t * P, uint64_t ptr, uint64_t size)
+{
+    if (!P || P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_register: a planner of the reference mode and a size");
+    uint64_t a, b;
+    page_round(ptr, size, a, b);
+    // the pieces of [a, b) not registered yet (src/memory/register.cc:121-166), each split into
+    // every frame and remembered for frames made later
+    const auto iv = reg_find(P, a, b);
+    uint64_t p1 = a;
+    for (size_t i = 0; i <= iv.size(); ++i)
+    {
+        const uint64_t p2 = i == iv.size() ? b : iv[i].first;
+        if (p1 < p2)
+        {
+            P->registered[p1] = p2 - p1;
+            for (auto & kv : P->frames) split_frame_at(*kv.second, p1, p2 - p1);
+        }
+        if (i < iv.size()) p1 = iv[i].second;
+    }
+    // IntervalSet::fill: merge with every interval it overlaps (adjacent ones stay apart)
+    uint64_t lo = a, hi = b;
+    for (const auto & v : iv) { lo = std::min(lo, v.first); hi = std::max(hi, v.second); P->reg_pages.erase(v.first); }
+    P->reg_pages[lo] = hi;
+    return XKB_OK;
+}
+
+extern "C" int xkb_planner_unregister(xkb_planner_t * P, uint64_t ptr, uint64_t size)
+{
+    if (!P || P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_unregister: a planner of the reference mode and a size");
+    uint64_t a, b;
+    page_round(ptr, size, a, b);
+    // every registered interval it meets, whole (src/memory/register.cc:199-262), then
+    // IntervalSet::unfill of [a, b)
+    for (const auto & v : reg_find(P, a, b))
+    {
+        P->registered.erase(v.first);
+        for (auto & kv : P->frames) split_frame_at(*kv.second, v.first, v.second - v.first);
+        P->reg_pages.erase(v.first);
+        if (v.first < a) P->reg_pages[v.first] = a;
+        if (v.second > b) P->reg_pages[b] = v.second;
     }
     return XKB_OK;
 }

@@ -243,6 +243,13 @@ struct xkb_runtime {
     uint64_t budget = 0;                              //   XKB_DEVICE_BUDGET: one region the allocations share,
     uint8_t * budget_base = nullptr;                  //   evicting old ones when a new one does not fit
     FILE * plan_record = nullptr;                     // XKB_PLAN_RECORD: every executed copy record
+    // registration-overflow protection (reference mode; XKAAPI_MEMORY_REGISTER_PROTECT_OVERFLOW=0
+    // turns it off, as in the reference): (un)registrations, applied to the planner before the
+    // fetches of the task spawned next after the call, in spawn order
+    bool protect_overflow = true;
+    struct RegEvent { size_t before; bool reg; uint64_t ptr, size; };
+    std::vector<RegEvent> reg_events;
+    size_t reg_next = 0;
     void * cxx_rt = nullptr;                          // the C++ runtime_t bodies of C++ tasks receive
     bool cxx_task_first = false;                      // XKB_CXX_HOST_BODY=task: host bodies of C++ tasks get the task first
 };
@@ -344,6 +351,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
         R->budget = v > 0 ? (uint64_t) v : 0;
     }
     if (const char * e = getenv("XKB_PLAN_RECORD")) R->plan_record = fopen(e, "wb");
+    if (const char * e = getenv("XKAAPI_MEMORY_REGISTER_PROTECT_OVERFLOW")) R->protect_overflow = atoi(e) != 0;
     if (const char * c = getenv("XKB_RESOLVE_CHUNK"))      // smaller batches (tests, memory-tight hosts)
         R->chunk = std::max<size_t>(16, strtoull(c, nullptr, 10));
     // fixed pools (address space only; pages are backed when touched) let a worker thread read
@@ -443,6 +451,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
 
 static void bg_finish(xkb_runtime * R);
 static void bg_wait_done(xkb_runtime * R);
+static int apply_registrations(xkb_runtime * R, size_t upto);
 
 extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
 {
@@ -459,6 +468,7 @@ extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
     // left the host coherent, so the host holds everything completed tasks wrote.
     if (R->planner)
     {
+        if (R->ref_mode) apply_registrations(R, SIZE_MAX);             // registrations outlive the reset
         size_t n = 0;                                                   // copies planned for dropped tasks
         if (xkb_planner_copies(R->planner, nullptr, 0, &n, 0) == XKB_OK && n)
         {
@@ -492,12 +502,35 @@ static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, boo
     return XKB_OK;
 }
 
+// Reference mode: the registration reaches the planner before the fetches of the next task
+// spawned (the tasks spawned before it were fetched first under the canonical schedule).
+static void note_registration(xkb_runtime * R, bool reg, void * ptr, size_t size)
+{
+    if (!R->ref_mode || !R->protect_overflow || !size) return;
+    std::lock_guard<std::mutex> lk(R->plan_mu);
+    R->reg_events.push_back({R->pending.size(), reg, (uint64_t) ptr, (uint64_t) size});
+}
+
+// Registrations noted before task `upto` (every one with upto = SIZE_MAX) into the planner.
+static int apply_registrations(xkb_runtime * R, size_t upto)
+{
+    int rc = XKB_OK;
+    while (rc == XKB_OK && R->reg_next < R->reg_events.size() && R->reg_events[R->reg_next].before <= upto)
+    {
+        const auto & e = R->reg_events[R->reg_next++];
+        rc = e.reg ? xkb_planner_register(R->planner, e.ptr, e.size) : xkb_planner_unregister(R->planner, e.ptr, e.size);
+    }
+    if (R->reg_next == R->reg_events.size()) { R->reg_events.clear(); R->reg_next = 0; }
+    return rc;
+}
+
 extern "C" int xkrt_memory_register(xkrt_runtime_t * runtime, void * ptr, size_t size)
 {
     xkb_runtime * R = RT(runtime);
     if (!R || !ptr || !size) return xkb_set_error(XKB_EINVAL, "xkrt_memory_register: bad arguments");
     if (R->gpu) cudaHostRegister(ptr, size, cudaHostRegisterDefault);     // pinned copies when possible
     cudaGetLastError();
+    note_registration(R, true, ptr, size);
     return add_region(R, ptr, size, false);
 }
 
@@ -505,8 +538,8 @@ extern "C" int xkrt_memory_unregister(xkrt_runtime_t * runtime, void * ptr, size
 {
     xkb_runtime * R = RT(runtime);
     if (!R || !ptr) return xkb_set_error(XKB_EINVAL, "xkrt_memory_unregister: bad arguments");
-    (void) size;
     if (R->gpu) { cudaHostUnregister(ptr); cudaGetLastError(); }
+    note_registration(R, false, ptr, size);
     return XKB_OK;                       // the mirror stays until xkrt_deinit
 }
 
@@ -1569,6 +1602,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     {
         std::lock_guard<std::mutex> lk(R->plan_mu);
         const uint64_t calls0 = R->copy_calls;
+        if (R->ref_mode) rc = apply_registrations(R, t);
         for (uint32_t a = 0; a < T.nacc && rc == XKB_OK; ++a)
         {
             const xkb_access_rec_t & r = recs[T.acc_off + a];
@@ -2055,6 +2089,7 @@ static int wait_batch(xkb_runtime * R)
         // (memory_coherent_async's host reads, src/memory/coherent.cc:137-231), in spawn order
         if (R->ref_mode)
         {
+            rc = apply_registrations(R, SIZE_MAX);
             for (size_t t = P; t < ntasks && rc == XKB_OK; ++t)
             {
                 const Task & T = R->pending[t];
