@@ -106,6 +106,11 @@ typedef struct xkb_task_graph_t {
  * include/xkrt/thread/thread.h:159-196). */
 XKB_API int xkb_resolver_create(xkb_resolver_t ** resolver, void * stream);
 XKB_API int xkb_resolver_destroy(xkb_resolver_t * resolver);
+/* Forget every task, edge and domain (the next add starts a new graph at task 0) but keep the
+ * device and page-locked working buffers, so the next graph resolves without allocating them
+ * again -- what a runtime does between waits (the reference drops its dependency domains with the
+ * implicit task's, src/memory/invalidate.cc:103-121). */
+XKB_API int xkb_resolver_reset(xkb_resolver_t * resolver);
 
 /* Resolve a batch of host-resident access records (tasks dense, in spawn order, the first
  * one numbered like the number of tasks added so far). Replaces, for each task of the batch,

@@ -117,6 +117,7 @@ SIGNATURES = {
     "xkb_handle_map_destroy": (_int, [_vp]),
     "xkb_handle_map_expand": (_int, [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_resolver_add": (_int, [_vp, _vp, ctypes.c_size_t]),
+    "xkb_resolver_reset": (_int, [_vp]),
     "xkb_resolver_graph": (_int, [_vp, ctypes.POINTER(TaskGraph)]),
     "xkb_resolver_edges": (_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "xkb_resolver_stats": (_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
@@ -224,6 +225,10 @@ class Resolver:
         g = TaskGraph()
         check(lib().xkb_resolver_graph(self._h, ctypes.byref(g)))
         return g
+
+    def reset(self):
+        """Forget every task and edge; keep the working buffers."""
+        check(lib().xkb_resolver_reset(self._h))
 
     def periodic(self, period):
         g = PeriodicGraph()

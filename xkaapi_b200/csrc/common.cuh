@@ -11,8 +11,10 @@
         if (_e != cudaSuccess) return xkb_set_cuda_error(_e); \
     } while (0)
 
-// Records the CUDA error string for xkb_last_error() and returns XKB_ECUDA.
-int xkb_set_cuda_error(cudaError_t e);
+// Records the CUDA error string and the source line that met it for xkb_last_error() and returns
+// XKB_ECUDA (XKB_ENODEV / XKB_ENOMEM for a missing device / device memory).
+int xkb_set_cuda_error_at(cudaError_t e, const char * file, int line);
+#define xkb_set_cuda_error(e) xkb_set_cuda_error_at((e), __FILE__, __LINE__)
 int xkb_set_error(int code, const char * fmt, ...);
 
 static inline cudaStream_t xkb_stream(void * s) { return (cudaStream_t) s; }

@@ -15,13 +15,13 @@ int xkb_set_error(int code, const char * fmt, ...)
     return code;
 }
 
-int xkb_set_cuda_error(cudaError_t e)
+int xkb_set_cuda_error_at(cudaError_t e, const char * file, int line)
 {
-    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
-        return xkb_set_error(XKB_ENODEV, "CUDA: %s", cudaGetErrorString(e));
-    if (e == cudaErrorMemoryAllocation)
-        return xkb_set_error(XKB_ENOMEM, "CUDA: %s", cudaGetErrorString(e));
-    return xkb_set_error(XKB_ECUDA, "CUDA: %s", cudaGetErrorString(e));
+    const char * base = file;
+    for (const char * p = file; *p; ++p) if (*p == '/') base = p + 1;
+    const int code = (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? XKB_ENODEV
+                   : e == cudaErrorMemoryAllocation ? XKB_ENOMEM : XKB_ECUDA;
+    return xkb_set_error(code, "CUDA: %s (%s:%d)", cudaGetErrorString(e), base, line);
 }
 
 extern "C" const char * xkb_last_error(void) { return g_last_error; }

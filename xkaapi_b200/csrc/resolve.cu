@@ -604,6 +604,7 @@ struct xkb_resolver {
     bool graph_valid = false;
     double last_device_ms = 0;
     double last_ops_ms = 0, last_compress_ms = 0;   // host phases of the last batch
+    double emit_per_op = 32.0;                  // emitted-pair estimate per op (from the last batch)
     // parallel host passes (validation, op build): the host team and the page-locked staging buffer
     std::unique_ptr<WorkPool> pool;
     HostStage stage;
@@ -1129,7 +1130,9 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
 
     static const bool trace = getenv("XKB_TRACE_RESOLVE") != nullptr;
     const size_t realloc0 = g_realloc_bytes;
-    size_t emit_guess = std::max<size_t>(1 << 16, total * 8);
+    // an emit buffer too small costs a second pass of the region kernel: size it from the pairs per
+    // op the last batch emitted (32 per op before the first), within 2^28 pairs
+    size_t emit_guess = std::max<size_t>(1 << 16, std::min<size_t>(size_t(1) << 28, (size_t) (total * R->emit_per_op)));
     for (int attempt = 0; attempt < 16; ++attempt)
     {
         const auto ta = clk::now();
@@ -1160,6 +1163,7 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
         const auto tb = clk::now();
         if (nemit > R->emit.cap) { emit_guess = (size_t) nemit; continue; }
         R->spill_used = sp[0];
+        if (total) R->emit_per_op = std::max(2.0, 1.25 * (double) nemit / (double) total);
 
         // success: unique the emitted pairs into the accumulated edge list
         if (nemit)
@@ -1299,6 +1303,11 @@ int xkb_internal_resolver_reset(xkb_resolver_t * R)
     for (size_t & n : R->useg_n) n = 0;
     R->spill_used = 0;
     return XKB_OK;
+}
+
+extern "C" int xkb_resolver_reset(xkb_resolver_t * R)
+{
+    return xkb_internal_resolver_reset(R);
 }
 
 extern "C" int xkb_resolver_add(xkb_resolver_t * R, const xkb_access_rec_t * recs, size_t n)
