@@ -187,6 +187,7 @@ def test_reference_mode_registration_splits(torch_cuda, tmp_path, protect):
 
     def plan(registered):
         P = xk.Planner()
+        xk.check(xk.lib().xkb_planner_set_writeback_coherent(P._h, 1))   # what the reference mode sets
         if registered:
             P.register(out["grid_a"], nx * ny * 8)
             P.register(out["grid_b"], nx * ny * 8)

@@ -125,13 +125,8 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
         }
     };
 
-    // west and current columns kept in FP64: every loaded value is widened once
-    double west[VEC], cur[VEC];
-    {
-        const Cells<T, VEC> w0c = load(cy0 - 1), c0 = load(cy0);
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) { west[e] = (double) w0c.v[e]; cur[e] = (double) c0.v[e]; }
-    }
+    Cells<T, VEC> west = load(cy0 - 1);
+    Cells<T, VEC> cur  = load(cy0);
     for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
     {
         if (pf_on && lane < PF)
@@ -149,18 +144,16 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
         {
             const int64_t jc = j0 + k;
             if (jc >= cy1) break;                        // warp-uniform
-            double east[VEC];
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) east[e] = (double) nxt[k].v[e];
-            const double north = __shfl_up_sync(0xffffffffu, cur[VEC - 1], 1);
-            const double south = __shfl_down_sync(0xffffffffu, cur[0], 1);
+            const T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
+            const T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
             Cells<T, VEC> out;
 #pragma unroll
             for (int e = 0; e < VEC; ++e)
             {
-                const double up = e == 0 ? north : cur[e - 1];
-                const double dn = e == VEC - 1 ? south : cur[e + 1];
-                out.v[e] = (T) heat_update(cur[e], up, dn, west[e], east[e], c);
+                const double sv = (double) cur.v[e];
+                const double up = (double) (e == 0 ? north : cur.v[e - 1]);
+                const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
+                out.v[e] = (T) heat_update(sv, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
             }
             T * q = dp + jc * ld;
             if (full_store)
@@ -179,8 +172,8 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
                 for (int e = 0; e < VEC; ++e)
                     if (r + e >= w0 && r + e < w1) q[e] = out.v[e];
             }
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) { west[e] = cur[e]; cur[e] = east[e]; }
+            west = cur;
+            cur = nxt[k];
         }
     }
 }
@@ -259,14 +252,8 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
             return ld_cells<T, VEC, CG>(src, ld, nx, r, j, vec_ok);
         }
     };
-    // the sweep keeps the west and current columns in FP64: with FP32 storage every loaded value is
-    // widened once (the conversion pipe, not HBM, otherwise bounds the FP32 body)
-    double west[VEC], cur[VEC];
-    {
-        const Cells<T, VEC> w0 = load(cy0 - 1), c0 = load(cy0);
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) { west[e] = (double) w0.v[e]; cur[e] = (double) c0.v[e]; }
-    }
+    Cells<T, VEC> west = load(cy0 - 1);
+    Cells<T, VEC> cur  = load(cy0);
     for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
     {
         if (pf_on && lane < PF)
@@ -289,22 +276,20 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
         {
             const int64_t jc = j0 + k;
             if (jc >= cy1) break;                        // warp-uniform
-            double east[VEC];
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) east[e] = (double) nxt[k].v[e];
-            double north = __shfl_up_sync(0xffffffffu, cur[VEC - 1], 1);
-            double south = __shfl_down_sync(0xffffffffu, cur[0], 1);
-            if (lane == 0)  north = (double) hn[k];
-            if (lane == 31) south = (double) hs[k];
+            T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
+            T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
+            if (lane == 0)  north = hn[k];
+            if (lane == 31) south = hs[k];
             if (lane_rows)
             {
                 Cells<T, VEC> out;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e)
                 {
-                    const double up = e == 0 ? north : cur[e - 1];
-                    const double dn = e == VEC - 1 ? south : cur[e + 1];
-                    out.v[e] = (T) heat_update(cur[e], up, dn, west[e], east[e], c);
+                    const double sv = (double) cur.v[e];
+                    const double up = (double) (e == 0 ? north : cur.v[e - 1]);
+                    const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
+                    out.v[e] = (T) heat_update(sv, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
                 }
                 T * q = dp + jc * ld;
                 if (full_store)
@@ -324,8 +309,8 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
                         if (r + e >= rx0 && r + e < rx1) q[e] = out.v[e];
                 }
             }
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) { west[e] = cur[e]; cur[e] = east[e]; }
+            west = cur;
+            cur = nxt[k];
         }
     }
 }

@@ -147,7 +147,11 @@ static int issue_host_copies(std::vector<HostCopy> & v, cudaMemcpyKind kind, cud
         cudaError_t e = flat ? cudaMemcpyAsync((void *) c.dst, (const void *) c.src, (size_t) (c.width * c.rows), kind, st)
                              : cudaMemcpy2DAsync((void *) c.dst, (size_t) c.dp, (const void *) c.src, (size_t) c.sp,
                                                  (size_t) c.width, (size_t) c.rows, kind, st);
-        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        if (e != cudaSuccess)
+            return xkb_set_error(e == cudaErrorMemoryAllocation ? XKB_ENOMEM : XKB_ECUDA,
+                                 "CUDA: %s (%s of %lld x %lld bytes, %p pitch %lld -> %p pitch %lld)", cudaGetErrorString(e),
+                                 kind == cudaMemcpyHostToDevice ? "H2D" : "D2H", (long long) c.rows, (long long) c.width,
+                                 (const void *) c.src, (long long) c.sp, (void *) c.dst, (long long) c.dp);
     }
     v.clear();
     return XKB_OK;

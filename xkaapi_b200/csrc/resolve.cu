@@ -65,6 +65,9 @@ struct DOp {            // one op in cell coordinates (24 bytes)
 // any number of readers (a region that is read every step and never written) while the state
 // and the region kernel's shared memory stay small. Chunks of a chain that a write clears are
 // not reused.
+#ifndef XKB_REGION_RY
+#define XKB_REGION_RY 8                 // cell rows of a 2-D region (8 columns each): 8 = two warps per CTA
+#endif
 constexpr int RCAP = 32;
 constexpr int SHDR = 4;
 constexpr int STRIDE = SHDR + RCAP;
@@ -1041,7 +1044,7 @@ static int launch_domain(xkb_resolver * R, Domain & d, size_t op_offset, size_t 
         a.nrx = (ncx + RX - 1) / RX;
         return launch_region<RX, RY>(R, a, a.nrx);
     }
-    constexpr int RX = 8, RY = 8;
+    constexpr int RX = 8, RY = XKB_REGION_RY;
     a.nrx = (ncx + RX - 1) / RX;
     const int nry = (ncy + RY - 1) / RY;
     return launch_region<RX, RY>(R, a, a.nrx * nry);
