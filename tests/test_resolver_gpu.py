@@ -182,3 +182,34 @@ def test_rejects_bad_streams(torch_cuda):
     r.add(ok)
     np.testing.assert_array_equal(r.edges(), [[0, 1]])
     r.close()
+
+
+def _readers_stream(nreaders):
+    tasks = [[("m", S.W, 1 << 20, 256, 0, 0, 64, 8, 8)]]
+    tasks += [[("m", S.R, 1 << 20, 256, 0, 0, 64, 8, 8)] for _ in range(nreaders)]
+    tasks += [[("m", S.W, 1 << 20, 256, 16, 2, 8, 2, 8)], [("m", S.W, 1 << 20, 256, 40, 5, 4, 1, 8)]]
+    tasks += [[("m", S.R, 1 << 20, 256, 0, 0, 64, 8, 8)] for _ in range(nreaders // 2)]
+    tasks += [[("m", S.RW, 1 << 20, 256, 0, 0, 64, 8, 8)]]
+    return S.from_tuples(tasks)
+
+
+@pytest.mark.parametrize("nseg", [2, 3, 8])
+def test_time_split_resolution_same_edges(torch_cuda, monkeypatch, nseg):
+    """Every region's op list cut into nseg segments (XKB_RESOLVE_SEGMENTS forces the time-split
+    kernels: one pass of PUT ops writing the state at each cut, then one CTA per region and
+    segment emitting its LINK ops' edges): the reference's golden edges, the oracle's edges on
+    seeded streams and in several batches, and reader lists past the inline ones (spilled before a
+    cut, across cuts, added inside a segment, over several batches) give the same edge sets."""
+    monkeypatch.setenv("XKB_RESOLVE_SEGMENTS", str(nseg))
+    for case in CASES:
+        np.testing.assert_array_equal(gpu_edges(expanded(GOLDEN[case + "__stream"])), GOLDEN[case + "__edges"], err_msg=case)
+    for case in ("heat_1024_t128_s3", "microbench_1024_2000", "mixed_segmat_0"):
+        np.testing.assert_array_equal(gpu_edges(GOLDEN[case + "__stream"], 3, seed=nseg), GOLDEN[case + "__edges"], err_msg=case)
+    for seed in range(2):
+        recs = S.mixed_stream(300, seed + 100)
+        np.testing.assert_array_equal(gpu_edges(recs), U.oracle_edges(recs))
+    recs = S.microbench_stream(16384, 12345)
+    np.testing.assert_array_equal(gpu_edges(recs), U.oracle_edges(recs))
+    for nreaders, batches in ((100, 1), (3000, 1), (3000, 4)):
+        recs = _readers_stream(nreaders)
+        np.testing.assert_array_equal(gpu_edges(recs, batches, seed=7), U.oracle_edges(recs), err_msg=f"{nreaders} readers")

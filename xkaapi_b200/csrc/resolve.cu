@@ -34,6 +34,7 @@
 #include "workpool.h"
 
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -250,6 +251,199 @@ resolve_region_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const i
     }
 }
 
+// ---- time-split resolution of a region ---------------------------------------------------------
+// A region's op list is cut into nseg segments (cut s at lo + (hi - lo) * s / nseg). The cell
+// state before each cut is all a segment needs to emit its edges, and only PUT ops change the
+// state, so:
+//  * resolve_puts_kernel (one CTA per region) applies the PUT ops of the whole list -- the
+//    cheap half of the work -- writing the state before every cut to `snap` and the final state
+//    to state_out; it owns the reader spill chains, exactly as resolve_region_kernel does;
+//  * resolve_links_kernel (one CTA per region and segment, nseg times the CTAs) replays its
+//    segment from that state: PUT ops update a private copy of the state and LINK ops emit
+//    the edges. Readers past RCAP that were in the state at the cut are read from the chain the
+//    snapshot names (resolve_puts_kernel only ever appends to a chain past the snapshot's count,
+//    and a write drops a chain without reusing it, so the first nr entries stay as they were);
+//    readers the segment itself adds past RCAP go to a private chain (chunks from the same pool,
+//    never linked into the kept state).
+// The edges are those of resolve_region_kernel over the whole list (the same LINK ops see the
+// same states); only the order in which pairs reach a.emit differs, which the dedupe ignores.
+
+__device__ __forceinline__ int seg_cut(int lo, int hi, int s, int nseg)
+{
+    return lo + (int) ((long long) (hi - lo) * s / nseg);
+}
+
+template <int RX, int RY>
+__global__ void __launch_bounds__(RX * RY)
+resolve_puts_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const int * __restrict__ rlist, int nseg,
+                    int * __restrict__ snap, size_t ncells)
+{
+    constexpr int NT = RX * RY;
+    constexpr int CHUNK = NT * RES_CHUNK_PER_THREAD;
+    extern __shared__ int rd[];                  // readers: rd[k * NT + tid]
+    __shared__ DOp list[CHUNK];
+
+    const int tid = threadIdx.x;
+    const int rx = blockIdx.x % a.nrx, ry = blockIdx.x / a.nrx;
+    const int cx = rx * RX + tid % RX, cy = ry * RY + tid / RX;
+    const bool valid = cx < a.ncx && cy < a.ncy;
+    const size_t cell = valid ? (size_t) cy * a.ncx + cx : 0;
+
+    int writer = -1, nr = 0, head = -1, tail = -1;
+    if (valid)
+    {
+        const int * st = a.state_in + cell * STRIDE;
+        writer = st[0]; nr = st[1]; head = st[2]; tail = st[3];
+        for (int k = 0; k < nr && k < RCAP; ++k) rd[k * NT + tid] = st[SHDR + k];
+    }
+    auto snapshot = [&](int s) {
+        if (!valid) return;
+        int * st = snap + ((size_t) (s - 1) * ncells + cell) * STRIDE;
+        st[0] = writer; st[1] = nr; st[2] = head; st[3] = tail;
+        for (int k = 0; k < nr && k < RCAP; ++k) st[SHDR + k] = rd[k * NT + tid];
+    };
+
+    const int lo = (int) roff[blockIdx.x], hi = (int) roff[blockIdx.x + 1];
+    int seg = 1, cut = nseg > 1 ? seg_cut(lo, hi, 1, nseg) : INT_MAX;
+    for (int base = lo; base < hi; base += CHUNK)
+    {
+        const int n = min(CHUNK, hi - base);
+        for (int j = tid; j < n; j += NT) list[j] = a.ops[rlist[base + j]];
+        __syncthreads();
+        for (int k = 0; k < n; ++k)
+        {
+            while (base + k == cut) { snapshot(seg); ++seg; cut = seg < nseg ? seg_cut(lo, hi, seg, nseg) : INT_MAX; }
+            const DOp op = list[k];
+            if (op.link) continue;
+            const bool in = valid && op.cx0 <= cx && cx < op.cx1 && op.cy0 <= cy && cy < op.cy1;
+            if (!in) continue;
+            if (op.mode & M_W) { writer = op.task; nr = 0; head = tail = -1; }
+            else if (op.mode == M_R)
+            {
+                if (nr < RCAP) rd[nr * NT + tid] = op.task;
+                else
+                {
+                    const int slot = (nr - RCAP) % SPILL_R;
+                    if (slot == 0)
+                    {
+                        const int c = spill_alloc(a.spill, a.spill_ctr, a.spill_cap);
+                        if (c >= 0) { if (tail >= 0) a.spill[(size_t) tail * SPILL] = c; else head = c; }
+                        tail = c;
+                    }
+                    if (tail >= 0) a.spill[(size_t) tail * SPILL + 1 + slot] = op.task;
+                }
+                ++nr;
+            }
+        }
+        __syncthreads();
+    }
+    while (seg < nseg) { snapshot(seg); ++seg; }          // cuts at the end of the list
+    if (valid)
+    {
+        int * st = a.state_out + cell * STRIDE;
+        st[0] = writer; st[1] = nr; st[2] = head; st[3] = tail;
+        for (int k = 0; k < nr && k < RCAP; ++k) st[SHDR + k] = rd[k * NT + tid];
+    }
+}
+
+template <int RX, int RY>
+__global__ void __launch_bounds__(RX * RY)
+resolve_links_kernel(ResolveArgs a, const unsigned * __restrict__ roff, const int * __restrict__ rlist, int nseg,
+                     const int * __restrict__ snap, size_t ncells)
+{
+    constexpr int NT = RX * RY;
+    constexpr int NW = NT / 32;
+    constexpr int CHUNK = NT * RES_CHUNK_PER_THREAD;
+    extern __shared__ int rd[];
+    __shared__ DOp list[CHUNK];
+    __shared__ unsigned long long ebuf[NW][EMIT_BUF];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int region = blockIdx.x / nseg, s = blockIdx.x % nseg;
+    const int rx = region % a.nrx, ry = region / a.nrx;
+    const int cx = rx * RX + tid % RX, cy = ry * RY + tid / RX;
+    const bool valid = cx < a.ncx && cy < a.ncy;
+    const size_t cell = valid ? (size_t) cy * a.ncx + cx : 0;
+
+    int writer = -1, nr = 0, shead = -1;
+    if (valid)
+    {
+        const int * st = s == 0 ? a.state_in + cell * STRIDE : snap + ((size_t) (s - 1) * ncells + cell) * STRIDE;
+        writer = st[0]; nr = st[1]; shead = st[2];
+        for (int k = 0; k < nr && k < RCAP; ++k) rd[k * NT + tid] = st[SHDR + k];
+    }
+    int nsnap = nr;                              // readers [RCAP, nsnap) are on the snapshot's chain
+    int phead = -1, ptail = -1;                  // readers the segment adds past RCAP
+    int nbuf = 0;
+
+    const int lo = (int) roff[region], hi = (int) roff[region + 1];
+    const int from = seg_cut(lo, hi, s, nseg), to = seg_cut(lo, hi, s + 1, nseg);
+    for (int base = from; base < to; base += CHUNK)
+    {
+        const int n = min(CHUNK, to - base);
+        for (int j = tid; j < n; j += NT) list[j] = a.ops[rlist[base + j]];
+        __syncthreads();
+        for (int k = 0; k < n; ++k)
+        {
+            const DOp op = list[k];
+            const bool in = valid && op.cx0 <= cx && cx < op.cx1 && op.cy0 <= cy && cy < op.cy1;
+            const int pbase = max(RCAP, nsnap);  // first reader position on the private chain
+            if (op.link)
+            {
+                const bool from_readers = in && (op.mode & M_W) && nr > 0;
+                const int cnt = from_readers ? nr : ((in && writer >= 0) ? 1 : 0);
+                const int maxcnt = __reduce_max_sync(0xffffffffu, cnt);
+                int chunk = shead, ci = 0;
+                for (int q = 0; q < maxcnt; ++q)
+                {
+                    int p = -1;
+                    if (q < cnt)
+                    {
+                        if (!from_readers) p = writer;
+                        else if (q < RCAP) p = rd[q * NT + tid];
+                        else
+                        {
+                            if (q == pbase) { chunk = phead; ci = 0; }
+                            else if (ci == SPILL_R) { chunk = chunk >= 0 ? a.spill[(size_t) chunk * SPILL] : -1; ci = 0; }
+                            p = chunk >= 0 ? a.spill[(size_t) chunk * SPILL + 1 + ci] : -1;   // -1: pool ran out, batch redone
+                            ++ci;
+                        }
+                    }
+                    const unsigned peers = __match_any_sync(0xffffffffu, p);
+                    const bool leader = p >= 0 && lane == __ffs(peers) - 1;
+                    const unsigned em = __ballot_sync(0xffffffffu, leader);
+                    if (leader)
+                        ebuf[warp][nbuf + __popc(em & ((1u << lane) - 1))] = ((unsigned long long) (uint32_t) p << 32) | (uint32_t) op.task;
+                    nbuf += __popc(em);
+                    if (nbuf > EMIT_BUF - 32) { emit_flush(a, ebuf[warp], nbuf, lane); nbuf = 0; }
+                }
+            }
+            else if (in)
+            {
+                if (op.mode & M_W) { writer = op.task; nr = 0; nsnap = 0; phead = ptail = -1; }
+                else if (op.mode == M_R)
+                {
+                    if (nr < RCAP) rd[nr * NT + tid] = op.task;
+                    else
+                    {
+                        const int slot = (nr - pbase) % SPILL_R;
+                        if (slot == 0)
+                        {
+                            const int c = spill_alloc(a.spill, a.spill_ctr, a.spill_cap);
+                            if (c >= 0) { if (ptail >= 0) a.spill[(size_t) ptail * SPILL] = c; else phead = c; }
+                            ptail = c;
+                        }
+                        if (ptail >= 0) a.spill[(size_t) ptail * SPILL + 1 + slot] = op.task;
+                    }
+                    ++nr;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (nbuf) emit_flush(a, ebuf[warp], nbuf, lane);
+}
+
 // ---- binning of ops to regions ----------------------------------------------------------------
 // The regions of an op: the RX x RY cell blocks its cell rect overlaps.
 __global__ void bin_count_kernel(const DOp * __restrict__ ops, int nops, int RX, int RY, int nrx, unsigned * rcount)
@@ -278,6 +472,7 @@ __global__ void bin_fill_kernel(const DOp * __restrict__ ops, int nops, int RX, 
         }
 }
 
+constexpr int MAX_SEGMENTS = 8;              // time-split segments per region (resolve_links_kernel)
 constexpr int BIN_SORT_THREADS = 1024;
 constexpr int BIN_SORT_CAP = 16384;          // ops of one region sortable in one CTA (64 KB of shared memory)
 
@@ -604,6 +799,7 @@ struct xkb_resolver {
     DevBuf<uint32_t> periodic;                  // packed arrays of the periodic form
     DevBuf<unsigned> bin_off, bin_cur;          // ops binned to regions: offsets, fill cursors
     DevBuf<int> bin_list, bin_flag;             // op indices per region; region-too-long flag
+    DevBuf<int> snap;                           // cell states at the time-split cuts (resolve_puts_kernel)
     bool graph_valid = false;
     double last_device_ms = 0;
     double last_ops_ms = 0, last_compress_ms = 0;   // host phases of the last batch
@@ -1015,7 +1211,23 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
         XKB_CUDA_TRY(cudaStreamSynchronize(st));
         binned = !too_long;
     }
-    if (binned)
+    // time split: segments per region from the mean list length (a segment of a few hundred ops
+    // still amortises its state load); XKB_RESOLVE_SEGMENTS overrides (1 = one pass per region)
+    const char * seg_s = getenv("XKB_RESOLVE_SEGMENTS");
+    const int seg_env = seg_s ? atoi(seg_s) : 0;
+    int nseg = seg_env > 0 ? seg_env : (int) std::min<size_t>(MAX_SEGMENTS, std::max<size_t>(1, (size_t) total / nregions / 512));
+    nseg = std::max(1, std::min(nseg, MAX_SEGMENTS));
+    if (binned && nseg > 1)
+    {
+        const size_t ncells = (size_t) a.ncx * a.ncy;
+        if ((rc = R->snap.reserve((size_t) (nseg - 1) * ncells * STRIDE))) return rc;
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_puts_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_links_kernel<RX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        resolve_puts_kernel<RX, RY><<<(unsigned) nregions, RX * RY, smem, st>>>(a, R->bin_off.p, R->bin_list.p, nseg, R->snap.p, ncells);
+        resolve_links_kernel<RX, RY><<<(unsigned) (nregions * nseg), RX * RY, smem, st>>>(a, R->bin_off.p, R->bin_list.p, nseg,
+                                                                                      R->snap.p, ncells);
+    }
+    else if (binned)
     {
         XKB_CUDA_TRY(cudaFuncSetAttribute(resolve_region_kernel<RX, RY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         resolve_region_kernel<RX, RY, true><<<(unsigned) nregions, RX * RY, smem, st>>>(a, R->bin_off.p, R->bin_list.p);
