@@ -103,7 +103,9 @@ struct XkbSrvSlot {
 };
 // The slot's counters (device memory): state 0 idle, 1 admitted (set-up pending), 2 running,
 // 3 done; set-up chunks claimed / finished; ready-queue head and tail; tasks executed.
-struct XkbSrvCtl { unsigned state, init_next, init_done, head, tail, executed, pad[2]; };
+// claimers: teams between their check that the slot runs (state 2) and their claim on `head`;
+// the team that ends the request waits for none to be left before the host may reuse the slot.
+struct XkbSrvCtl { unsigned state, init_next, init_done, head, tail, executed, claimers, pad; };
 struct XkbSrvArgs {
     XkbSrvSlot * slots;
     XkbSrvCtl * ctl;

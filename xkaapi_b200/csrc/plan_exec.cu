@@ -88,7 +88,10 @@ using namespace xkb;
 
 // One host copy: rows x width bytes from src (pitch sp) to dst (pitch dp). A byte range of a
 // segment has no pitch (sp = dp = 0): such ranges merge whenever they continue each other.
-struct HostCopy { uintptr_t src, dst; int64_t sp, dp, width, rows; };
+// `alloc`: the device allocation the copy touches -- copies of different allocations never merge
+// (adjacent allocations, host or device, are still separate allocations to the driver, and a
+// copy may not run across the end of one).
+struct HostCopy { uintptr_t src, dst; int64_t sp, dp, width, rows; int64_t alloc; };
 
 static size_t coalesce(std::vector<HostCopy> & v)
 {
@@ -96,6 +99,7 @@ static size_t coalesce(std::vector<HostCopy> & v)
     // side by side: same rows and pitches, each continuing the previous one in both spaces (byte
     // ranges: any widths)
     std::sort(v.begin(), v.end(), [](const HostCopy & a, const HostCopy & b) {
+        if (a.alloc != b.alloc) return a.alloc < b.alloc;
         if (a.sp != b.sp) return a.sp < b.sp;
         if (a.dp != b.dp) return a.dp < b.dp;
         if (a.rows != b.rows) return a.rows < b.rows;
@@ -107,7 +111,7 @@ static size_t coalesce(std::vector<HostCopy> & v)
         HostCopy & a = v[k];
         const HostCopy & b = v[i];
         const bool range = a.sp == 0 && a.dp == 0;
-        if (a.sp == b.sp && a.dp == b.dp && a.rows == b.rows && b.src == a.src + (uintptr_t) a.width &&
+        if (a.alloc == b.alloc && a.sp == b.sp && a.dp == b.dp && a.rows == b.rows && b.src == a.src + (uintptr_t) a.width &&
             b.dst == a.dst + (uintptr_t) a.width && (range || a.rows == 1 || a.width + b.width <= std::min(a.sp, a.dp)))
         {
             a.width += b.width;
@@ -118,6 +122,7 @@ static size_t coalesce(std::vector<HostCopy> & v)
     v.resize(k + 1);
     // stacked: same width and pitches, each starting one pitch x rows below the previous one
     std::sort(v.begin(), v.end(), [](const HostCopy & a, const HostCopy & b) {
+        if (a.alloc != b.alloc) return a.alloc < b.alloc;
         if (a.sp != b.sp) return a.sp < b.sp;
         if (a.dp != b.dp) return a.dp < b.dp;
         if (a.width != b.width) return a.width < b.width;
@@ -128,7 +133,7 @@ static size_t coalesce(std::vector<HostCopy> & v)
     {
         HostCopy & a = v[k];
         const HostCopy & b = v[i];
-        if (a.sp == b.sp && a.dp == b.dp && a.width == b.width && a.width <= std::min(a.sp, a.dp) &&
+        if (a.alloc == b.alloc && a.sp == b.sp && a.dp == b.dp && a.width == b.width && a.width <= std::min(a.sp, a.dp) &&
             b.src == a.src + (uintptr_t) (a.rows * a.sp) && b.dst == a.dst + (uintptr_t) (a.rows * a.dp))
             a.rows += b.rows;
         else v[++k] = b;
@@ -213,14 +218,14 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
             uint8_t * d = dev_ptr(c.dst_alloc, c.dst_off);
             if (!d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
             const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
-            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n});
+            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n, c.dst_alloc});
         }
         else if (c.kind == XKB_COPY_D2H)
         {
             const uint8_t * s = dev_ptr(c.src_alloc, c.src_off);
             if (!s) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
             const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
-            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n});
+            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n, c.src_alloc});
         }
         else { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu has an unknown kind", i); break; }
         hkind = c.kind;

@@ -63,7 +63,7 @@ constexpr int SCHED_THREADS = 256;
 
 constexpr int SCHED_BULK_NBUF = 8;       // staged columns in flight per warp (bulk tile body)
 #ifndef XKB_TILE_PF
-#define XKB_TILE_PF 4                    // east columns an FP32 tile strip loads ahead into registers
+#define XKB_TILE_PF 6                    // east columns an FP32 tile strip loads ahead into registers
 #endif
 #ifndef XKB_F64_VEC
 #define XKB_F64_VEC 4                    // rows per lane of the FP64 tile body: one warp covers 128 rows
@@ -951,15 +951,22 @@ __global__ void __launch_bounds__(SCHED_THREADS, XKB_SCHED_MINB) server_kernel(X
                         if (ch < a.slots[sl].nchunks) { kind = 2; slot = sl; idx = (int) ch; }
                     }
                 }
-                else if (st == 2)
+                else if (st == 2 && *(volatile unsigned *) &c->head < *(volatile unsigned *) &c->tail)
                 {
-                    unsigned h = *(volatile unsigned *) &c->head;
-                    while (h < *(volatile unsigned *) &c->tail)
+                    // claim the next queue position with one atomicAdd (a compare-and-swap loop on
+                    // `head` serialises the teams on it); the position may be published a little
+                    // later, which the wait below covers. The claim counts in `claimers` while the
+                    // state is re-checked, so the team ending the request can tell when no claim
+                    // on this request's counters is left.
+                    atomicAdd(&c->claimers, 1u);
+                    __threadfence();
+                    unsigned h = 0;
+                    if (ld_acquire_u32(&c->state) == 2)
                     {
-                        const unsigned got = atomicCAS(&c->head, h, h + 1);
-                        if (got == h) { kind = 1; slot = sl; break; }
-                        h = got;
+                        h = atomicAdd(&c->head, 1u);
+                        if (h < a.slots[sl].ntasks) { kind = 1; slot = sl; }
                     }
+                    atomicSub(&c->claimers, 1u);
                     if (kind == 1)
                     {
                         // the id at that position was published (tail counts it) or is about to be
@@ -1074,6 +1081,17 @@ __global__ void __launch_bounds__(SCHED_THREADS, XKB_SCHED_MINB) server_kernel(X
                     if (atomicAdd(&c->executed, 1u) + 1 == S.ntasks)
                     {
                         st_release_u32(&c->state, 3u);
+                        __threadfence();
+                        // teams that saw state 2 before the store above claim past the last task
+                        // and leave; wait (bounded) until none is between its check and its claim
+                        const uint64_t tw = xkb_globaltimer();
+                        uint32_t spins = 0;
+                        while (*(volatile unsigned *) &c->claimers != 0)
+                            if ((++spins & 63) == 0 && xkb_globaltimer() - tw > a.timeout_ns)
+                            {
+                                atomicCAS(a.status, 0u, (unsigned) -XKB_ETIMEDOUT);
+                                break;
+                            }
                         __threadfence_system();
                         a.host_done[sl] = S.gen;
                     }
