@@ -481,6 +481,42 @@ def microbench_stream(ntasks, seed, n=8192, ld=8192, align=64, max_units=32, bas
     return recs
 
 
+def resolver_microbench(xk, torch, stream, recs, hbm_peak, reps=3):
+    """The dependency microbench through the GPU resolver: a fresh resolver's first add + graph
+    (its working buffers allocated inside the timing), then the same resolver reset and reused,
+    as the runtime keeps its resolver between waits (best of `reps`). Returns (line, edges)."""
+    r3 = xk.Resolver(stream)
+    t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
+    dt_first = time.perf_counter() - t0
+    nfirst = int(g3.nedges)
+    dts = []
+    for _ in range(reps):
+        r3.reset()
+        t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
+        dts.append(time.perf_counter() - t0)
+    dt = min(dts) if dts else dt_first
+    phases = r3.timing()
+    nedges = int(g3.nedges)
+    r3.close()
+    ntasks = int(recs["task"].max()) + 1
+    visits = int(((recs["m"] // 64) * (recs["n"] // 64)).sum())          # 64 x 64-element cells per access
+    mb_bytes = 32.0 * len(recs) + 8.0 * nedges + 16.0 * visits
+    line = {"tasks": ntasks, "accesses": int(len(recs)), "unique_edges": nedges,
+            "seconds": round(dt, 4), "tasks_per_s": round(ntasks / dt),
+            "seconds_fresh_resolver": round(dt_first, 4),
+            "same_edges_fresh_and_reused": nfirst == nedges,
+            "phases_ms": {"host_ops": round(phases[0], 2), "compress": round(phases[1], 2),
+                          "batch_device": round(phases[2], 2)},
+            "timing": "wall time of add + graph on a reset, reused resolver (best of %d); "
+                      "seconds_fresh_resolver: the first add + graph of a new resolver" % reps,
+            "roofline": {"bound": "hbm", "achieved": round(mb_bytes / dt / 1e9, 2), "peak": hbm_peak,
+                         "unit": "GB/s", "frac": round(mb_bytes / dt / 1e9 / hbm_peak, 5),
+                         "algorithmic_bytes": mb_bytes, "cell_visits": visits,
+                         "what": "32 B per access + 8 B per unique edge + 16 B per visit of a "
+                                 "64 x 64-element cell, over the wall time of add + graph"}}
+    return line, nedges
+
+
 def serve_trace(ngraphs, seed, ts=128):
     """Served-stream trace: grid side log-uniform in [256, 8192] rounded to a multiple of the
     tile; steps uniform in {10..200}; FP64 / FP32 storage 50/50; Poisson arrival order."""
@@ -569,6 +605,69 @@ def serve_study(xk, torch, ngraphs=2000, slots=16, load=0.8):
             "loop": "one persistent kernel for the whole trace runs every admitted request's tile tasks"}
 
 
+def run_study(args):
+    """One study alone on cuda:0, its JSON line on stdout (no headline, no CPU baseline)."""
+    import torch
+    import xkaapi_b200 as xk
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    hbm_peak, _ = peaks()
+    if args.study == "resolver":
+        recs = microbench_stream(args.tasks, 12345)
+        line, _ = resolver_microbench(xk, torch, stream, recs, hbm_peak, reps=args.steps)
+        print(json.dumps({"study": "resolver", **line}), flush=True)
+        return 0
+    if args.study == "graph":
+        n, steps, esz = NX, STEPS, (4 if args.f32 else 8)
+        g = torch.rand((n, n), dtype=torch.float64, generator=torch.Generator().manual_seed(SEED))
+        g[0, :] = 0; g[-1, :] = 0; g[:, 0] = 0; g[:, -1] = 0
+        a = g.to(device="cuda", dtype=torch.float32 if args.f32 else torch.float64); b = a.clone()
+        del g
+        res, graph, _ = build_heat_graph(xk, torch, a, b, n, n, TS, steps, stream, esize=esz)
+        d = xk.heat_task_descs((a.data_ptr(), b.data_ptr()), n, n, n, TS, TS, steps, COEF, f32=args.f32)
+        sch = xk.Scheduler(stream); sch.set_team(1); sch.set_tasks(d); del d
+        if args.prefetch:
+            sch.set_prefetch(args.prefetch)
+        runs = []
+        for k in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                sch.run(graph); sch.wait()
+            if k >= args.warmup:
+                runs.append(sch.kernel_ms())
+        best = min(runs)
+        print(json.dumps({"study": "graph", "size": n, "steps": steps, "dtype": "f32" if args.f32 else "f64",
+                          "tasks": int(graph.ntasks), "kernel_ms": [round(x, 3) for x in runs],
+                          "GBps_best": round(2.0 * esz * cells_all(n, n) * steps / (best / 1e3) / 1e9, 1)}), flush=True)
+        sch.close(); res.close()
+        return 0
+    # serve: closed-loop capacity of a few shapes, device loop and one launch per request
+    io = serve_io(torch)
+    free, _ = torch.cuda.mem_get_info()
+    srv = xk.Server(budget_bytes=int(min(150e9, free - 8e9)), slots=16)
+    side, steps, f32, _, _ = serve_trace(2000, 2026)
+    cases = {"8 x 4096^2 FP64 x 100 steps": (np.full(8, 4096), np.full(8, 100), np.zeros(8, np.int64)),
+             "first 300 graphs of the trace": (side[:300], steps[:300], f32[:300])}
+    for name, (sd, st, f) in cases.items():
+        nbytes = float(((sd.astype(np.float64) - 2) ** 2 * st * np.where(f == 1, 8.0, 16.0)).sum())
+        for mode in ("device", "launch"):
+            if mode == "launch":
+                os.environ["XKB_SERVE_MODE"] = "launch"
+            else:
+                os.environ.pop("XKB_SERVE_MODE", None)
+            for withio in (True, False):
+                for _ in range(2):          # the second pass: every shape's graph already resolved
+                    reqs = serve_requests(xk, sd, st, f, np.zeros(len(sd)), io if withio else None)
+                    srv.run(reqs)
+                fin = max(r.finish_s for r in reqs)
+                print(json.dumps({"study": "serve", "case": name, "mode": mode, "host_io": withio,
+                                  "GBps": round(nbytes / fin / 1e9, 1), "makespan_s": round(fin, 3),
+                                  "p50_ms": round(float(np.percentile([(r.finish_s - r.start_s) * 1e3 for r in reqs], 50)), 2)}),
+                      flush=True)
+    os.environ.pop("XKB_SERVE_MODE", None)
+    srv.close()
+    return 0
+
+
 def main():
     global NX, NY, STEPS
     ap = argparse.ArgumentParser()
@@ -581,11 +680,21 @@ def main():
                     help="run only the headline measurement (no forms / stencil / resolver / CPU side studies)")
     ap.add_argument("--size", type=int, default=NX, help="grid side (default 16384)")
     ap.add_argument("--graph-steps", type=int, default=STEPS, help="Jacobi steps in the graph (default 500)")
+    ap.add_argument("--study", choices=["resolver", "graph", "serve"],
+                    help="run one study alone and print its JSON (the commands of the profile summaries): "
+                         "resolver = the dependency microbench (--tasks); graph = the heat graph on the "
+                         "persistent scheduler (--size, --graph-steps, --f32, --prefetch, --steps); "
+                         "serve = serving capacity with and without host I/O, device loop and one launch per request")
+    ap.add_argument("--tasks", type=int, default=65536, help="--study resolver: tasks of the microbench")
+    ap.add_argument("--f32", action="store_true", help="--study graph: FP32 storage")
+    ap.add_argument("--prefetch", type=int, default=0, help="--study graph: L2 prefetch distance (0: the default)")
     args = ap.parse_args()
     NX = NY = args.size
     STEPS = args.graph_steps
     if args.impl == "reference":
         return run_reference(args)
+    if args.study:
+        return run_study(args)
 
     import torch
     import xkaapi_b200 as xk
@@ -772,38 +881,10 @@ def main():
         # resolver microbench
         mb_tasks = 16384 if args.quick else 65536
         recs = microbench_stream(mb_tasks, 12345)
-        r3 = xk.Resolver(stream)
-        # first: a fresh resolver (its working buffers allocated inside the timing); then the same
-        # resolver reset and reused, as the runtime keeps its resolver between waits (best of 3)
-        t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
-        dt_first = time.perf_counter() - t0
-        nfirst = int(g3.nedges)
-        dts = []
-        for _ in range(3):
-            r3.reset()
-            t0 = time.perf_counter(); r3.add(recs); g3 = r3.graph(); torch.cuda.synchronize()
-            dts.append(time.perf_counter() - t0)
-        dt = min(dts)
-        phases = r3.timing()
-        visits = int(((recs["m"] // 64) * (recs["n"] // 64)).sum())          # 64 x 64-element cells per access
-        mb_bytes = 32.0 * len(recs) + 8.0 * int(g3.nedges) + 16.0 * visits
-        extra["resolver_microbench"] = {"tasks": mb_tasks, "accesses": int(len(recs)), "unique_edges": int(g3.nedges),
-                                        "seconds": round(dt, 4), "tasks_per_s": round(mb_tasks / dt),
-                                        "seconds_fresh_resolver": round(dt_first, 4),
-                                        "same_edges_fresh_and_reused": nfirst == int(g3.nedges),
-                                        "phases_ms": {"host_ops": round(phases[0], 2), "compress": round(phases[1], 2),
-                                                      "batch_device": round(phases[2], 2)},
-                                        "timing": "wall time of add + graph on a reset, reused resolver (best of 3); "
-                                                  "seconds_fresh_resolver: the first add + graph of a new resolver",
-                                        "roofline": {"bound": "hbm", "achieved": round(mb_bytes / dt / 1e9, 2), "peak": hbm_peak,
-                                                     "unit": "GB/s", "frac": round(mb_bytes / dt / 1e9 / hbm_peak, 5),
-                                                     "algorithmic_bytes": mb_bytes, "cell_visits": visits,
-                                                     "what": "32 B per access + 8 B per unique edge + 16 B per visit of a "
-                                                             "64 x 64-element cell, over the wall time of add + graph"}}
-        r3.close()
+        extra["resolver_microbench"], nedges = resolver_microbench(xk, torch, stream, recs, hbm_peak)
         ref = ref_deps_time(recs)
         if ref:
-            ref["same_unique_edges"] = ref.pop("unique_edges") == int(g3.nedges)
+            ref["same_unique_edges"] = ref.pop("unique_edges") == nedges
             extra["resolver_microbench"]["reference_cpu"] = ref
 
     # ---------------- served stream (after releasing the headline graph's memory) -----------
