@@ -911,7 +911,7 @@ def main():
         # resolver microbench
         mb_tasks = 16384 if args.quick else 65536
         recs = microbench_stream(mb_tasks, 12345)
-        extra["resolver_microbench"], nedges = resolver_microbench(xk, torch, stream, recs, hbm_peak)
+        extra["resolver_microbench"], nedges = resolver_microbench(xk, torch, stream, recs, hbm_peak, reps=5)
         ref = ref_deps_time(recs)
         if ref:
             ref["same_unique_edges"] = ref.pop("unique_edges") == nedges

@@ -193,14 +193,17 @@ def _readers_stream(nreaders):
     return S.from_tuples(tasks)
 
 
-@pytest.mark.parametrize("nseg", [2, 3, 8])
-def test_time_split_resolution_same_edges(torch_cuda, monkeypatch, nseg):
+@pytest.mark.parametrize("nseg,global_bins", [(2, False), (3, True), (8, False), (1, True)])
+def test_time_split_resolution_same_edges(torch_cuda, monkeypatch, nseg, global_bins):
     """Every region's op list cut into nseg segments (XKB_RESOLVE_SEGMENTS forces the time-split
     kernels: one pass of PUT ops writing the state at each cut, then one CTA per region and
     segment emitting its LINK ops' edges): the reference's golden edges, the oracle's edges on
     seeded streams and in several batches, and reader lists past the inline ones (spilled before a
-    cut, across cuts, added inside a segment, over several batches) give the same edge sets."""
+    cut, across cuts, added inside a segment, over several batches) give the same edge sets; with
+    the global-atomic binning too (what domains of more than 12,288 regions use)."""
     monkeypatch.setenv("XKB_RESOLVE_SEGMENTS", str(nseg))
+    if global_bins:                     # the binning without block-local counts (domains of many regions)
+        monkeypatch.setenv("XKB_RESOLVE_BIN_GLOBAL", "1")
     for case in CASES:
         np.testing.assert_array_equal(gpu_edges(expanded(GOLDEN[case + "__stream"])), GOLDEN[case + "__edges"], err_msg=case)
     for case in ("heat_1024_t128_s3", "microbench_1024_2000", "mixed_segmat_0"):

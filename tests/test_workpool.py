@@ -21,3 +21,13 @@ def test_handle_map_decisions(tmp_path):
                     "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr
+
+
+def test_pool_arrays_and_parked_reservations(tmp_path):
+    """The spawn pools (xkaapi_b200/csrc/pool.h): fixed reservations, growth by remapping, and a
+    released fixed reservation reused by the next one of the same size (pages still backed)."""
+    exe = str(tmp_path / "pool_test")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-pthread", os.path.join(REPO, "tests", "cpp", "pool_test.cc"),
+                    "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stderr

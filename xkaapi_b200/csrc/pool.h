@@ -9,10 +9,48 @@
 #include <sys/mman.h>
 
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 namespace xkb {
+
+// Fixed reservations given back by released arrays are parked for the next reserve_fixed of the
+// same size in this process, their pages still backed: a program that makes one runtime after
+// another (xkrt_init ... xkrt_deinit in a loop) then spawns into memory that is already faulted
+// in instead of faulting and zeroing it again. At most PARKED_MAX reservations are kept (the
+// oldest is unmapped); XKB_POOL_CACHE=0 unmaps at release instead.
+class ParkedReservations {
+public:
+    static ParkedReservations & get() { static ParkedReservations p; return p; }
+    void * take(size_t bytes)
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (size_t i = 0; i < v_.size(); ++i)
+            if (v_[i].second == bytes)
+            {
+                void * q = v_[i].first;
+                v_.erase(v_.begin() + (long) i);
+                return q;
+            }
+        return nullptr;
+    }
+    void give(void * p, size_t bytes)
+    {
+        static const bool on = !(getenv("XKB_POOL_CACHE") && atoi(getenv("XKB_POOL_CACHE")) == 0);
+        if (!on) { munmap(p, bytes); return; }
+        std::lock_guard<std::mutex> lk(mu_);
+        v_.push_back({p, bytes});
+        if (v_.size() > PARKED_MAX) { munmap(v_.front().first, v_.front().second); v_.erase(v_.begin()); }
+    }
+private:
+    static constexpr size_t PARKED_MAX = 8;
+    std::mutex mu_;
+    std::vector<std::pair<void *, size_t>> v_;
+};
 
 template <typename T>
 class PoolArray {
@@ -56,7 +94,8 @@ public:
     void clear() { n_ = 0; }
     void release()
     {
-        if (p_) munmap(p_, bytes_);
+        if (p_ && fixed_) ParkedReservations::get().give(p_, bytes_);
+        else if (p_) munmap(p_, bytes_);
         p_ = nullptr; n_ = 0; bytes_ = 0; fixed_ = false;
     }
     // Reserve `max_elems` elements of address space up front (pages are only backed when first
@@ -66,9 +105,13 @@ public:
     {
         if (p_) return false;
         const size_t nb = max_elems * sizeof(T);
-        void * q = mmap(nullptr, nb, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
-        if (q == MAP_FAILED) return false;
-        madvise(q, nb, MADV_HUGEPAGE);
+        void * q = ParkedReservations::get().take(nb);
+        if (!q)
+        {
+            q = mmap(nullptr, nb, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+            if (q == MAP_FAILED) return false;
+            madvise(q, nb, MADV_HUGEPAGE);
+        }
         p_ = (T *) q; bytes_ = nb; fixed_ = true;
         return true;
     }

@@ -472,6 +472,68 @@ __global__ void bin_fill_kernel(const DOp * __restrict__ ops, int nops, int RX, 
         }
 }
 
+// Block-local binning: with at most BIN_SMEM_REGIONS regions, a block of the count / fill kernels
+// counts its ops' regions in shared memory and touches each region's global counter once (the
+// kernels above do one global atomic per (op, region) on a few hundred shared counters).
+constexpr int BIN_SMEM_REGIONS = 12288;
+
+__global__ void bin_count_smem_kernel(const DOp * __restrict__ ops, int nops, int RX, int RY, int nrx, int nregions,
+                                      unsigned * rcount)
+{
+    extern __shared__ unsigned h[];
+    for (int r = threadIdx.x; r < nregions; r += blockDim.x) h[r] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += gridDim.x * blockDim.x)
+    {
+        const DOp o = ops[i];
+        if (o.cx0 >= o.cx1 || o.cy0 >= o.cy1) continue;
+        for (int ry = o.cy0 / RY; ry <= (o.cy1 - 1) / RY; ++ry)
+            for (int rx = o.cx0 / RX; rx <= (o.cx1 - 1) / RX; ++rx)
+                atomicAdd(h + ry * nrx + rx, 1u);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nregions; r += blockDim.x)
+        if (h[r]) atomicAdd(rcount + r, h[r]);
+}
+
+// Each block counts its own ops' regions, reserves one range per region with one global atomic,
+// and places its ops inside its ranges (any op-to-block split works: each region's list is put
+// back in op order afterwards).
+__global__ void bin_fill_smem_kernel(const DOp * __restrict__ ops, int nops, int RX, int RY, int nrx, int nregions,
+                                     const unsigned * __restrict__ roff, unsigned * cursor, int * list)
+{
+    extern __shared__ unsigned h[];                       // [nregions] counts, then [nregions] bases
+    unsigned * base = h + nregions;
+    for (int r = threadIdx.x; r < nregions; r += blockDim.x) h[r] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += gridDim.x * blockDim.x)
+    {
+        const DOp o = ops[i];
+        if (o.cx0 >= o.cx1 || o.cy0 >= o.cy1) continue;
+        for (int ry = o.cy0 / RY; ry <= (o.cy1 - 1) / RY; ++ry)
+            for (int rx = o.cx0 / RX; rx <= (o.cx1 - 1) / RX; ++rx)
+                atomicAdd(h + ry * nrx + rx, 1u);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nregions; r += blockDim.x)
+    {
+        base[r] = h[r] ? roff[r] + atomicAdd(cursor + r, h[r]) : 0u;
+        h[r] = 0;
+    }
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += gridDim.x * blockDim.x)
+    {
+        const DOp o = ops[i];
+        if (o.cx0 >= o.cx1 || o.cy0 >= o.cy1) continue;
+        for (int ry = o.cy0 / RY; ry <= (o.cy1 - 1) / RY; ++ry)
+            for (int rx = o.cx0 / RX; rx <= (o.cx1 - 1) / RX; ++rx)
+            {
+                const int r = ry * nrx + rx;
+                list[base[r] + atomicAdd(h + r, 1u)] = i;
+            }
+    }
+}
+
 constexpr int MAX_SEGMENTS = 8;              // time-split segments per region (resolve_links_kernel)
 constexpr int BIN_SORT_THREADS = 1024;
 constexpr int BIN_SORT_CAP = 16384;          // ops of one region sortable in one CTA (64 KB of shared memory)
@@ -1194,7 +1256,22 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
     XKB_CUDA_TRY(cudaMemsetAsync(R->bin_cur.p, 0, nb * sizeof(unsigned), st));
     XKB_CUDA_TRY(cudaMemsetAsync(R->bin_flag.p, 0, sizeof(int), st));
     const unsigned g = (unsigned) ((a.nops + 255) / 256);
-    bin_count_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p);
+    // block-local binning: a grid of a few blocks per SM, each walking its share of the ops
+    const char * gb = getenv("XKB_RESOLVE_BIN_GLOBAL");             // 1: the global-atomic binning (tests)
+    const bool smem_bins = nregions <= BIN_SMEM_REGIONS && !(gb && atoi(gb) == 1);
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned gs = std::min<unsigned>(g, (unsigned) (2 * sms));
+    if (smem_bins)
+    {
+        XKB_CUDA_TRY(cudaFuncSetAttribute(bin_count_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          BIN_SMEM_REGIONS * (int) sizeof(unsigned)));
+        bin_count_smem_kernel<<<gs, 256, (size_t) nregions * sizeof(unsigned), st>>>(a.ops, a.nops, RX, RY, a.nrx, nregions,
+                                                                                   R->bin_off.p);
+    }
+    else
+        bin_count_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p);
     if ((rc = device_exclusive_scan(R->bin_off.p, R->bin_off.p, nb, R->tmp.p, nullptr, st))) return rc;
     unsigned total = 0;
     XKB_CUDA_TRY(cudaMemcpyAsync(&total, R->bin_off.p + nregions, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -1203,7 +1280,15 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
     if (binned)
     {
         if ((rc = R->bin_list.reserve(total))) return rc;
-        bin_fill_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p, R->bin_cur.p, R->bin_list.p);
+        if (smem_bins)
+        {
+            XKB_CUDA_TRY(cudaFuncSetAttribute(bin_fill_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              2 * BIN_SMEM_REGIONS * (int) sizeof(unsigned)));
+            bin_fill_smem_kernel<<<gs, 256, 2 * (size_t) nregions * sizeof(unsigned), st>>>(a.ops, a.nops, RX, RY, a.nrx, nregions,
+                                                                                         R->bin_off.p, R->bin_cur.p, R->bin_list.p);
+        }
+        else
+            bin_fill_kernel<<<g, 256, 0, st>>>(a.ops, a.nops, RX, RY, a.nrx, R->bin_off.p, R->bin_cur.p, R->bin_list.p);
         XKB_CUDA_TRY(cudaFuncSetAttribute(bin_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BIN_SORT_CAP * (int) sizeof(int)));
         bin_sort_kernel<<<(unsigned) nregions, BIN_SORT_THREADS, BIN_SORT_CAP * sizeof(int), st>>>(R->bin_off.p, R->bin_list.p, R->bin_flag.p);
         int too_long = 0;
