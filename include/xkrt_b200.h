@@ -262,6 +262,11 @@ XKB_API int xkb_planner_invalidate(xkb_planner_t * planner);
  * the writer's copy the only coherent one. Blocks are the same canonical partition as above. */
 XKB_API int xkb_planner_create_resident(xkb_planner_t ** planner);
 XKB_API int xkb_planner_add_region(xkb_planner_t * planner, uint64_t host_base, uint64_t size, int32_t * region);
+/* Resident mode: the regions inside [host_base, host_base + size) (none may cross its ends) are
+ * replaced by one region covering it, with a new allocation ordinal: what registering memory
+ * that overlaps registered memory does (the union becomes one region). The blocks keep their
+ * coherency states; the caller moves the old mirrors' bytes into the new mirror. */
+XKB_API int xkb_planner_replace_regions(xkb_planner_t * planner, uint64_t host_base, uint64_t size, int32_t * region);
 /* Resident mode: make the host coherent again for every block whose only coherent copy is on
  * the GPU -- what fetching every record device tasks wrote back to the host does, without the
  * records (one walk over the partition). Blocks that follow one another in a slab and in the

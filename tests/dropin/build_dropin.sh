@@ -26,7 +26,9 @@ LIBDIR="$REPO/xkaapi_b200"
 RPATH='-Wl,-rpath,$ORIGIN/../../../xkaapi_b200'
 CXXFLAGS="-std=c++20 -O2 -I$REPO/include -I$CUDA/include"
 
-for t in task-dependency task-dependency-interval task-dependency-interval-matrix task-dependency-handle task-format-host; do
+for t in task-dependency task-dependency-interval task-dependency-interval-matrix task-dependency-handle task-format-host \
+         init deinit sync task-format task-gpu-empty memory-register-async-legacy memory-register-assisted \
+         memory-register-assisted-unregister; do
     g++ $CXXFLAGS -o "$OUT/$t" "$REF/tests/$t.cc" -L"$LIBDIR" -lxkb200 "$RPATH"
 done
 gcc -std=c11 -O2 -I"$REPO/include" -o "$OUT/task-with-access" "$REF/tests/api/c/task-with-access.c" -L"$LIBDIR" -lxkb200 "$RPATH"

@@ -13,6 +13,17 @@ present), run on the GPU.
   reference itself these asserts read the runtime object instead of the task and fail. This
   library calls bodies the same way by default; XKB_CXX_HOST_BODY=task passes the task first
   instead, which is what these older programs expect, and makes their order checks meaningful.
+* tests/init.cc, deinit.cc, sync.cc, task-format.cc: runtime start and end, a wait with nothing
+  spawned, an empty task format.
+* tests/task-gpu-empty.cc: a hand-built DEVICE task (RW matrix access on malloc'd memory) whose
+  format has only a host function. The reference runs the host function when the device's target
+  has none (src/task.cc:322-330); here such a task runs as a host task on the host team.
+* tests/memory-register-async-legacy.cc: memory_register_async of an unaligned malloc'd range,
+  then a wait.
+* tests/memory-register-assisted.cc, -assisted-unregister.cc: three overlapping registrations of
+  one buffer (the reference registers only the new pages each time), the whole buffer distributed
+  to the GPU by distribute_async over its union, then overlapping unregistrations (one twice).
+  Here overlapping registrations merge into one region.
 * tests/api/c/task-with-access.c: a C team task with a segment access (api/c/include/xkrt/xkrt.h).
 * examples/heat-diffusion-2d: the whole example (32 x 32 FP32 grid, 1000 steps, placement through
   distribute_async, a CUDA-target tile body launched by task_detachable_kernel_launch on the
@@ -45,7 +56,9 @@ def _run(name, tmp_path, env_extra=None):
     return r
 
 
-@pytest.mark.parametrize("name", ["task-dependency", "task-format-host"])
+@pytest.mark.parametrize("name", ["task-dependency", "task-format-host", "init", "deinit", "sync", "task-format",
+                                  "task-gpu-empty", "memory-register-async-legacy", "memory-register-assisted",
+                                  "memory-register-assisted-unregister"])
 def test_reference_task_programs(torch_cuda, tmp_path, name):
     _run(name, tmp_path)
 

@@ -544,3 +544,25 @@ def test_registration_refused_in_resident_mode():
     P = xk.Planner(resident=True)
     with pytest.raises(xk.XkbError):
         P.register(1 << 20, 4096)
+
+
+def test_replace_regions_keeps_block_states():
+    """Resident mode: two regions replaced by their union (what overlapping registrations do in the
+    C API): blocks made coherent on the GPU before stay coherent (no copy), new blocks copy from
+    the host, and copies name the new region's ordinal and offsets in it."""
+    import streams as S
+    base = 1 << 30
+    P = xk.Planner(resident=True)
+    P.add_region(base, 4096)
+    P.add_region(base + 4096, 4096)
+    P.fetch(S.from_tuples([[("s", S.R, base, base + 1024)]])[0], 0, 1)
+    assert len(P.copies(take=True)) == 1
+    with pytest.raises(xk.XkbError):
+        P.replace_regions(base + 8, 4096)                # a region would cross the range's start
+    rid = P.replace_regions(base, 8192)
+    assert rid == 2
+    P.fetch(S.from_tuples([[("s", S.R, base, base + 1024)]])[0], 0, 1)
+    assert len(P.copies(take=True)) == 0                 # still coherent on the GPU
+    P.fetch(S.from_tuples([[("s", S.R, base + 4000, base + 5000)]])[0], 0, 1)
+    q = P.copies(take=True)
+    assert len(q) == 1 and q[0, 2] == 0 and q[0, 8] == rid and q[0, 9] == 4000 and q[0, 11] == 1000

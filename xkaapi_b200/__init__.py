@@ -98,6 +98,7 @@ SIGNATURES = {
     "xkb_planner_add_region": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
     "xkb_planner_flush_to_host": (_int, [_vp]),
     "xkb_planner_invalidate": (_int, [_vp]),
+    "xkb_planner_replace_regions": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
     "xkb_planner_register": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64]),
     "xkb_planner_unregister": (_int, [_vp, ctypes.c_uint64, ctypes.c_uint64]),
     "xkb_planner_fetch": (_int, [_vp, _vp, ctypes.c_uint32, _int, _vp]),
@@ -365,6 +366,12 @@ class Planner:
     def add_region(self, base, size):
         r = ctypes.c_int32()
         check(lib().xkb_planner_add_region(self._h, base, size, ctypes.byref(r)))
+        return r.value
+
+    def replace_regions(self, base, size):
+        """Resident mode: the regions inside [base, base + size) become one region (new ordinal)."""
+        r = ctypes.c_int32()
+        check(lib().xkb_planner_replace_regions(self._h, base, size, ctypes.byref(r)))
         return r.value
 
     def flush_to_host(self):

@@ -826,6 +826,27 @@ extern "C" int xkb_planner_unregister(xkb_planner_t * P, uint64_t ptr, uint64_t 
     return XKB_OK;
 }
 
+extern "C" int xkb_planner_replace_regions(xkb_planner_t * P, uint64_t base, uint64_t size, int32_t * region)
+{
+    if (!P || !P->resident || !size) return xkb_set_error(XKB_EINVAL, "planner_replace_regions: needs a resident planner and a size");
+    const uint64_t end = base + size;
+    auto it = P->regions.lower_bound(base);          // first region starting at or after base
+    if (it != P->regions.begin())
+    {
+        auto p = std::prev(it);
+        if (p->first + p->second.first > base) return xkb_set_error(XKB_EINVAL, "planner_replace_regions: a region starts before the range");
+    }
+    for (auto q = it; q != P->regions.end() && q->first < end; ++q)
+        if (q->first + q->second.first > end) return xkb_set_error(XKB_EINVAL, "planner_replace_regions: a region ends after the range");
+    while (it != P->regions.end() && it->first < end)
+        it = P->regions.erase(it);
+    const int32_t id = (int32_t) P->allocs.size();
+    P->allocs.push_back(size);
+    P->regions[base] = {size, id};
+    if (region) *region = id;
+    return XKB_OK;
+}
+
 extern "C" int xkb_planner_invalidate(xkb_planner_t * P)
 {
     if (!P) return xkb_set_error(XKB_EINVAL, "planner_invalidate: null planner");

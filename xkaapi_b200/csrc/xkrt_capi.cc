@@ -201,6 +201,7 @@ struct xkb_runtime {
     // registration per growth, and an upload never spans two of them)
     size_t args_pinned = 0;
     std::vector<std::pair<void *, size_t>> pinned_ranges;
+    std::map<uint64_t, uint64_t> user_pinned;         // page-locked pieces of registered memory: start -> end
     std::atomic<bool> args_dense{true};               // every task's args: one descriptor, back to back
     // streaming: while the program spawns, the worker hands each resolved window of a batch made
     // only of built-in device tasks to the GPU (coherency, descriptors, one persistent launch)
@@ -437,6 +438,7 @@ extern "C" int xkrt_deinit(xkrt_runtime_t * runtime)
     }
     for (cudaStream_t w : R->wstreams) cudaStreamDestroy(w);
     for (auto & r : R->pinned_ranges) cudaHostUnregister(r.first);
+    for (auto & r : R->user_pinned) cudaHostUnregister((void *) r.first);
     for (auto & d : R->dslot) { if (d.ev) cudaEventDestroy(d.ev); if (d.p) cudaFreeHost(d.p); }
     if (R->sched) xkb_sched_destroy(R->sched);
     if (R->planner) xkb_planner_destroy(R->planner);
@@ -485,9 +487,69 @@ extern "C" void xkrt_reset(xkrt_runtime_t * runtime)
     }
 }
 
+// Registering memory that overlaps registered memory (the reference's assisted registration,
+// src/memory/register.cc:121-166, registers only the pages not registered yet): the union of the
+// range and the regions it meets becomes one region, so an access over the union has one mirror.
+// The old mirrors' bytes move into the new one; the blocks keep their coherency states.
+static int merge_regions(xkb_runtime * R, const std::vector<uint64_t> & over, uint64_t lo, uint64_t hi, bool unified)
+{
+    if (over.size() == 1)
+    {
+        const Region & g = R->regions[over[0]];
+        if (over[0] == lo && g.size == hi - lo) return XKB_OK;     // inside one region already
+    }
+    for (uint64_t k : over)
+    {
+        const Region & g = R->regions[k];
+        if (unified || g.unified || g.pinned_by_us)
+            return xkb_set_error(XKB_EINVAL, "memory registration: the range overlaps memory the runtime allocated");
+    }
+    if (!R->pending.empty())
+        return xkb_set_error(XKB_EINVAL, "memory registration: the range overlaps registered memory while %zu spawned tasks "
+                                         "wait; register it before spawning them or after xkrt_task_wait", R->pending.size());
+    int32_t id = -1;
+    if (!R->ref_mode)
+    {
+        const int rc = xkb_planner_replace_regions(R->planner, lo, hi - lo, &id);
+        if (rc) return rc;
+    }
+    void * mirror = nullptr;
+    if (R->gpu && !R->ref_mode)
+    {
+        cudaError_t e = cudaMalloc(&mirror, hi - lo);
+        if (e != cudaSuccess) return xkb_set_cuda_error(e);
+        for (uint64_t k : over)
+        {
+            const Region & g = R->regions[k];
+            if (g.mirror && (e = cudaMemcpyAsync((uint8_t *) mirror + (k - lo), g.mirror, g.size, cudaMemcpyDeviceToDevice,
+                                                 R->stream)) != cudaSuccess)
+                return xkb_set_cuda_error(e);
+        }
+        if ((e = cudaStreamSynchronize(R->stream)) != cudaSuccess) return xkb_set_cuda_error(e);
+        for (uint64_t k : over) if (R->regions[k].mirror) cudaFree(R->regions[k].mirror);
+    }
+    for (uint64_t k : over) R->regions.erase(k);
+    R->regions[lo] = Region{hi - lo, mirror, false, id, false};
+    R->last_base = R->last_end = 0; R->last_mirror = nullptr;     // the lookup hint may name a freed mirror
+    return XKB_OK;
+}
+
 static int add_region(xkb_runtime * R, void * ptr, size_t size, bool pinned, bool unified = false)
 {
     std::lock_guard<std::mutex> lk(R->plan_mu);       // the worker may be streaming a window
+    {
+        const uint64_t b = (uint64_t) ptr, e = b + size;
+        uint64_t lo = b, hi = e;
+        std::vector<uint64_t> over;
+        auto it = R->regions.upper_bound(b);
+        if (it != R->regions.begin()) { auto p = std::prev(it); if (p->first + p->second.size > b) it = p; }
+        for (; it != R->regions.end() && it->first < e; ++it)
+        {
+            over.push_back(it->first);
+            lo = std::min(lo, it->first); hi = std::max(hi, it->first + it->second.size);
+        }
+        if (!over.empty()) return merge_regions(R, over, lo, hi, unified);
+    }
     int32_t id = -1;
     int rc = R->ref_mode ? XKB_OK : xkb_planner_add_region(R->planner, (uint64_t) ptr, size, &id);
     if (rc) return rc;
@@ -528,8 +590,25 @@ extern "C" int xkrt_memory_register(xkrt_runtime_t * runtime, void * ptr, size_t
 {
     xkb_runtime * R = RT(runtime);
     if (!R || !ptr || !size) return xkb_set_error(XKB_EINVAL, "xkrt_memory_register: bad arguments");
-    if (R->gpu) cudaHostRegister(ptr, size, cudaHostRegisterDefault);     // pinned copies when possible
-    cudaGetLastError();
+    if (R->gpu)
+    {
+        // page-lock (faster copies, when the driver allows) the parts not page-locked by an
+        // earlier registration: the driver refuses a range that overlaps a locked one
+        std::lock_guard<std::mutex> lk(R->plan_mu);
+        const uint64_t b = (uint64_t) ptr, e = b + size;
+        uint64_t at = b;
+        auto it = R->user_pinned.upper_bound(b);
+        if (it != R->user_pinned.begin() && std::prev(it)->second > b) at = std::prev(it)->second;
+        for (;; ++it)
+        {
+            const uint64_t gap_end = (it != R->user_pinned.end() && it->first < e) ? it->first : e;
+            if (at < gap_end && cudaHostRegister((void *) at, gap_end - at, cudaHostRegisterDefault) == cudaSuccess)
+                R->user_pinned[at] = gap_end;
+            cudaGetLastError();
+            if (it == R->user_pinned.end() || it->first >= e) break;
+            at = std::max(at, it->second);
+        }
+    }
     note_registration(R, true, ptr, size);
     return add_region(R, ptr, size, false);
 }
@@ -538,9 +617,20 @@ extern "C" int xkrt_memory_unregister(xkrt_runtime_t * runtime, void * ptr, size
 {
     xkb_runtime * R = RT(runtime);
     if (!R || !ptr) return xkb_set_error(XKB_EINVAL, "xkrt_memory_unregister: bad arguments");
-    if (R->gpu) { cudaHostUnregister(ptr); cudaGetLastError(); }
+    if (R->gpu)
+    {
+        // unlock the page-locked pieces inside the range (the mirror stays until xkrt_deinit)
+        std::lock_guard<std::mutex> lk(R->plan_mu);
+        const uint64_t b = (uint64_t) ptr, e = b + size;
+        for (auto it = R->user_pinned.lower_bound(b); it != R->user_pinned.end() && it->second <= e;)
+        {
+            cudaHostUnregister((void *) it->first);
+            cudaGetLastError();
+            it = R->user_pinned.erase(it);
+        }
+    }
     note_registration(R, false, ptr, size);
-    return XKB_OK;                       // the mirror stays until xkrt_deinit
+    return XKB_OK;
 }
 
 extern "C" void * xkrt_memory_host_allocate(xkrt_runtime_t * runtime, xkrt_device_global_id_t device, size_t size)
@@ -1121,8 +1211,10 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
         }
         return xkb_plan_execute(c.data(), n, R->allocs.data(), R->allocs.size(), stream);
     }
-    std::vector<void *> ptrs(R->regions.size(), nullptr);
-    for (auto & kv : R->regions) ptrs[kv.second.id] = kv.second.mirror;
+    int32_t maxid = -1;                               // ids of merged-away regions are not reused
+    for (auto & kv : R->regions) maxid = std::max(maxid, kv.second.id);
+    std::vector<void *> ptrs((size_t) (maxid + 1), nullptr);
+    for (auto & kv : R->regions) if (kv.second.id >= 0) ptrs[kv.second.id] = kv.second.mirror;
     for (const xkb_copy_t & k : c)
     {
         (k.kind == XKB_COPY_H2D ? R->cur_h2d : R->cur_d2h) += 1;
