@@ -216,3 +216,13 @@ def test_spawn_generic_detachable_count_and_ocr(torch_cuda, tmp_path):
     r = subprocess.run([build("spawn_generic_capi", tmp_path)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr + r.stdout
     assert json.loads(r.stdout.strip().splitlines()[-1]) == {"order": 1, "early": 1, "axpby": 1}
+
+
+def test_partly_locked_registration_and_range_checks(torch_cuda, tmp_path):
+    """A registration made while tasks are pending, touching locked memory, stays unlocked except
+    the page it shares with the locked piece; axpby tasks on a vector starting in that page run
+    and are exact (copies are cut at the locked piece's end). An axpby whose element range leaves
+    its vector's region is refused with XKB_EINVAL instead of running past the region's mirror."""
+    r = subprocess.run([build("register_pieces_capi", tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == {"ok": 1, "refused": 1}

@@ -257,10 +257,14 @@ struct xkb_runtime {
 
 static xkb_runtime * RT(xkrt_runtime_t * r) { return (xkb_runtime *) r; }
 
+// Records the runtime's first failure (xkb_runtime_status; xkrt_deinit returns it). With
+// XKB_TRACE_ERRORS set, the failure's text is printed on stderr when it is recorded -- programs
+// written for the reference only see the status.
 static void fail(xkb_runtime * R, int rc)
 {
     int ok = XKB_OK;
-    if (R && rc != XKB_OK) R->status.compare_exchange_strong(ok, rc);
+    if (R && rc != XKB_OK && R->status.compare_exchange_strong(ok, rc) && getenv("XKB_TRACE_ERRORS"))
+        fprintf(stderr, "[xkrt] error %d: %s\n", rc, xkb_last_error());
 }
 
 // The prefault helpers (one per spawn pool): while the program spawns, they fault in the pages
@@ -592,21 +596,29 @@ extern "C" int xkrt_memory_register(xkrt_runtime_t * runtime, void * ptr, size_t
     if (!R || !ptr || !size) return xkb_set_error(XKB_EINVAL, "xkrt_memory_register: bad arguments");
     if (R->gpu)
     {
-        // page-lock (faster copies, when the driver allows) the parts not page-locked by an
-        // earlier registration: the driver refuses a range that overlaps a locked one
+        // page-lock the range (faster copies): the pages of [ptr, ptr + size) and of every locked
+        // piece they meet or touch become ONE locked piece -- the driver refuses a range sharing a
+        // page with a locked one. Tasks in flight may be copying from the pieces met, so then
+        // only a range that meets none is locked. Copies never run across a piece's end
+        // (run_copies splits them), so partly locked memory is safe either way.
         std::lock_guard<std::mutex> lk(R->plan_mu);
+        static const uint64_t page = (uint64_t) sysconf(_SC_PAGESIZE);
         const uint64_t b = (uint64_t) ptr, e = b + size;
-        uint64_t at = b;
-        auto it = R->user_pinned.upper_bound(b);
-        if (it != R->user_pinned.begin() && std::prev(it)->second > b) at = std::prev(it)->second;
-        for (;; ++it)
+        uint64_t lo = b - b % page, hi = (e + page - 1) / page * page;
+        std::vector<uint64_t> meet;
+        auto it = R->user_pinned.upper_bound(lo);
+        if (it != R->user_pinned.begin() && std::prev(it)->second >= lo) it = std::prev(it);
+        for (; it != R->user_pinned.end() && it->first <= hi; ++it)
         {
-            const uint64_t gap_end = (it != R->user_pinned.end() && it->first < e) ? it->first : e;
-            if (at < gap_end && cudaHostRegister((void *) at, gap_end - at, cudaHostRegisterDefault) == cudaSuccess)
-                R->user_pinned[at] = gap_end;
+            meet.push_back(it->first);
+            lo = std::min(lo, it->first); hi = std::max(hi, it->second);
+        }
+        const bool covered = meet.size() == 1 && meet[0] <= b - b % page && R->user_pinned[meet[0]] >= e;
+        if (!covered && (meet.empty() || R->pending.empty()))
+        {
+            for (uint64_t m : meet) { cudaHostUnregister((void *) m); R->user_pinned.erase(m); }
+            if (cudaHostRegister((void *) lo, hi - lo, cudaHostRegisterDefault) == cudaSuccess) R->user_pinned[lo] = hi;
             cudaGetLastError();
-            if (it == R->user_pinned.end() || it->first >= e) break;
-            at = std::max(at, it->second);
         }
     }
     note_registration(R, true, ptr, size);
@@ -621,7 +633,8 @@ extern "C" int xkrt_memory_unregister(xkrt_runtime_t * runtime, void * ptr, size
     {
         // unlock the page-locked pieces inside the range (the mirror stays until xkrt_deinit)
         std::lock_guard<std::mutex> lk(R->plan_mu);
-        const uint64_t b = (uint64_t) ptr, e = b + size;
+        static const uint64_t page = (uint64_t) sysconf(_SC_PAGESIZE);
+        const uint64_t b = (uint64_t) ptr - (uint64_t) ptr % page, e = ((uint64_t) ptr + size + page - 1) / page * page;
         for (auto it = R->user_pinned.lower_bound(b); it != R->user_pinned.end() && it->second <= e;)
         {
             cudaHostUnregister((void *) it->first);
@@ -1191,6 +1204,61 @@ static int ensure_allocs(xkb_runtime * R)
     return XKB_OK;
 }
 
+// A host copy whose host bytes run across an end of a page-locked piece of registered memory
+// (locked and pageable memory, or two pieces, in one copy: the driver refuses it) becomes one
+// copy per column, each cut at those ends -- what the reference's registration-overflow
+// protection does by splitting its partition (memory-tree.hpp:2184-2240).
+static void split_at_locked_ends(const xkb_runtime * R, std::vector<xkb_copy_t> & c)
+{
+    if (R->user_pinned.empty()) return;
+    auto cuts_inside = [&](uint64_t lo, uint64_t hi, std::vector<uint64_t> * out) {
+        bool any = false;
+        auto it = R->user_pinned.upper_bound(lo);
+        if (it != R->user_pinned.begin()) --it;
+        for (; it != R->user_pinned.end() && it->first < hi; ++it)
+            for (uint64_t x : {it->first, it->second})
+                if (lo < x && x < hi) { any = true; if (out) out->push_back(x); }
+        return any;
+    };
+    std::vector<xkb_copy_t> out;
+    bool changed = false;
+    for (const xkb_copy_t & k : c)
+    {
+        if (k.kind == XKB_COPY_D2D) { out.push_back(k); continue; }
+        const bool h2d = k.kind == XKB_COPY_H2D;
+        const uint64_t hbase = (uint64_t) (h2d ? k.src_off : k.dst_off);
+        const int64_t row = k.m * k.sizeof_type;
+        const int64_t hld = (h2d ? k.src_ld : k.dst_ld) * k.sizeof_type, dld = (h2d ? k.dst_ld : k.src_ld) * k.sizeof_type;
+        const uint64_t span = (uint64_t) ((k.n - 1) * hld + row);
+        bool straddles = false;                      // a cut inside a column, not only between two
+        if (cuts_inside(hbase, hbase + span, nullptr))
+            for (int64_t j = 0; j < k.n && !straddles; ++j)
+                straddles = cuts_inside(hbase + (uint64_t) (j * hld), hbase + (uint64_t) (j * hld + row), nullptr);
+        if (!straddles) { out.push_back(k); continue; }
+        changed = true;
+        const int64_t dbase = h2d ? k.dst_off : k.src_off;
+        for (int64_t j = 0; j < k.n; ++j)
+        {
+            const uint64_t h0 = hbase + (uint64_t) (j * hld);
+            std::vector<uint64_t> cut;
+            cuts_inside(h0, h0 + (uint64_t) row, &cut);
+            std::sort(cut.begin(), cut.end());
+            uint64_t a = h0;
+            cut.push_back(h0 + (uint64_t) row);
+            for (uint64_t x : cut)
+            {
+                xkb_copy_t q = k;
+                q.m = (int64_t) (x - a); q.n = 1; q.sizeof_type = 1; q.src_ld = q.dst_ld = 0;
+                const int64_t d = dbase + j * dld + (int64_t) (a - h0);
+                if (h2d) { q.src_off = (int64_t) a; q.dst_off = d; } else { q.dst_off = (int64_t) a; q.src_off = d; }
+                out.push_back(q);
+                a = x;
+            }
+        }
+    }
+    if (changed) c.swap(out);
+}
+
 static int run_copies(xkb_runtime * R, cudaStream_t stream)
 {
     size_t n = 0;
@@ -1199,7 +1267,9 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
     std::vector<xkb_copy_t> c(n);
     if ((rc = xkb_planner_copies(R->planner, c.data(), n, &n, 1))) return rc;
     ++R->copy_calls;
-    if (R->plan_record) fwrite(c.data(), sizeof(xkb_copy_t), n, R->plan_record);
+    if (R->plan_record) fwrite(c.data(), sizeof(xkb_copy_t), n, R->plan_record);      // the planner's records
+    split_at_locked_ends(R, c);
+    n = c.size();
     if (R->ref_mode)
     {
         if ((rc = ensure_allocs(R))) return rc;
@@ -1226,19 +1296,37 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
 // Point a built-in descriptor's host addresses at the device mirrors.
 // false when a pointer lies outside every registered region (no error text: callable from
 // several threads at once)
+// The mirror of host bytes [host, host + bytes), or null unless one region holds all of them (a
+// body indexes its grid or vector from the translated base, so every byte it may touch must be
+// in that region's mirror).
+static void * mirror_range(const xkb_runtime * R, uint64_t host, uint64_t bytes, RegionHint & h)
+{
+    uint8_t * m = (uint8_t *) mirror_lookup(R, host, h);
+    return m && bytes <= h.end - host ? m : nullptr;
+}
+
 static bool translate_hint(const xkb_runtime * R, xkb_task_desc_t & d, RegionHint & h)
 {
     if (d.kind == XKB_TASK_HEAT_F64 || d.kind == XKB_TASK_HEAT_F32)
     {
-        void * s = mirror_lookup(R, d.u.heat.src, h), * t = mirror_lookup(R, d.u.heat.dst, h);
+        // the whole grid: the tile's strips may read any row of its columns and their neighbours
+        const auto & g = d.u.heat;
+        if (g.nx <= 0 || g.ny <= 0 || g.ld < g.nx) return false;
+        const uint64_t esz = d.kind == XKB_TASK_HEAT_F64 ? 8 : 4;
+        const uint64_t bytes = ((uint64_t) (g.ny - 1) * (uint64_t) g.ld + (uint64_t) g.nx) * esz;
+        void * s = mirror_range(R, g.src, bytes, h), * t = mirror_range(R, g.dst, bytes, h);
         if (!s || !t) return false;
         d.u.heat.src = (uint64_t) s; d.u.heat.dst = (uint64_t) t;
     }
     else if (d.kind == XKB_TASK_AXPBY)
     {
-        void * x = mirror_lookup(R, d.u.axpby.x, h), * y = mirror_lookup(R, d.u.axpby.y, h);
+        const auto & v = d.u.axpby;
+        if (v.lo < 0 || v.hi < v.lo) return false;
+        const uint64_t off = (uint64_t) v.lo * 8, bytes = (uint64_t) (v.hi - v.lo) * 8;
+        // x and y are the vectors' bases; the task touches elements [lo, hi) of each
+        void * x = mirror_range(R, v.x + off, bytes, h), * y = mirror_range(R, v.y + off, bytes, h);
         if (!x || !y) return false;
-        d.u.axpby.x = (uint64_t) x; d.u.axpby.y = (uint64_t) y;
+        d.u.axpby.x = (uint64_t) x - off; d.u.axpby.y = (uint64_t) y - off;
     }
     return true;
 }
