@@ -9,6 +9,10 @@
 
 // Launch one task descriptor as its own kernel (the plain per-task form) on `stream`.
 int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream);
+// xkb_plan_execute with host cuts (sorted addresses): no two copies whose host bytes lie on
+// different sides of a cut are merged into one (each copy given must lie between two cuts).
+int xkb_internal_plan_execute_cut(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs,
+                                  cudaStream_t stream, const uint64_t * cuts, size_t ncuts);
 
 // Set a scheduler's descriptors on the device only (persistent forms only; no host copy).
 // checked: the caller validated every descriptor with xkb_internal_task_valid.

@@ -88,9 +88,10 @@ using namespace xkb;
 
 // One host copy: rows x width bytes from src (pitch sp) to dst (pitch dp). A byte range of a
 // segment has no pitch (sp = dp = 0): such ranges merge whenever they continue each other.
-// `alloc`: the device allocation the copy touches -- copies of different allocations never merge
+// `alloc`: the device allocation the copy touches, and in its high bits the span of host memory
+// between two cuts its host bytes lie in -- copies of different allocations or spans never merge
 // (adjacent allocations, host or device, are still separate allocations to the driver, and a
-// copy may not run across the end of one).
+// copy may not run across the end of one; the cuts are the ends of page-locked pieces).
 struct HostCopy { uintptr_t src, dst; int64_t sp, dp, width, rows; int64_t alloc; };
 
 static size_t coalesce(std::vector<HostCopy> & v)
@@ -162,10 +163,14 @@ static int issue_host_copies(std::vector<HostCopy> & v, cudaMemcpyKind kind, cud
     return XKB_OK;
 }
 
-extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, void * stream)
+static int plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, cudaStream_t st,
+                        const uint64_t * cuts, size_t ncuts)
 {
     if (n && (!copies || !alloc_ptrs)) return xkb_set_error(XKB_EINVAL, "plan_execute: bad arguments");
-    cudaStream_t st = xkb_stream(stream);
+    auto tag = [&](int64_t alloc, uint64_t host) -> int64_t {
+        const int64_t span = cuts ? (int64_t) (std::upper_bound(cuts, cuts + ncuts, host) - cuts) : 0;
+        return (span << 32) | (alloc & 0xffffffff);
+    };
     auto dev_ptr = [&](int64_t alloc, int64_t off) -> uint8_t * {
         return (alloc >= 0 && (size_t) alloc < nallocs) ? (uint8_t *) alloc_ptrs[alloc] + off : nullptr;
     };
@@ -218,14 +223,16 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
             uint8_t * d = dev_ptr(c.dst_alloc, c.dst_off);
             if (!d) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
             const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
-            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n, c.dst_alloc});
+            hrun.push_back({(uintptr_t) c.src_off, (uintptr_t) d, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n,
+                            tag(c.dst_alloc, (uint64_t) c.src_off)});
         }
         else if (c.kind == XKB_COPY_D2H)
         {
             const uint8_t * s = dev_ptr(c.src_alloc, c.src_off);
             if (!s) { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu names an unknown allocation", i); break; }
             const bool range = c.src_ld == 0 && c.dst_ld == 0 && c.n == 1;
-            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n, c.src_alloc});
+            hrun.push_back({(uintptr_t) s, (uintptr_t) c.dst_off, range ? 0 : sp, range ? 0 : dp, row_bytes, c.n,
+                            tag(c.src_alloc, (uint64_t) c.dst_off)});
         }
         else { rc = xkb_set_error(XKB_EINVAL, "plan_execute: copy %zu has an unknown kind", i); break; }
         hkind = c.kind;
@@ -235,6 +242,17 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
     if (rc == XKB_OK) rc = flush();
     if (dbatch) { cudaStreamSynchronize(st); cudaFree(dbatch); }
     return rc;
+}
+
+extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs, void * stream)
+{
+    return plan_execute(copies, n, alloc_ptrs, nallocs, xkb_stream(stream), nullptr, 0);
+}
+
+int xkb_internal_plan_execute_cut(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs,
+                                  cudaStream_t stream, const uint64_t * cuts, size_t ncuts)
+{
+    return plan_execute(copies, n, alloc_ptrs, nallocs, stream, ncuts ? cuts : nullptr, ncuts);
 }
 
 // The cells [i0, i0 + w) x [j0, j0 + h) of the grid (interior ones only), src and dst pointing at

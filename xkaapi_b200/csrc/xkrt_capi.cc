@@ -1230,11 +1230,7 @@ static void split_at_locked_ends(const xkb_runtime * R, std::vector<xkb_copy_t> 
         const int64_t row = k.m * k.sizeof_type;
         const int64_t hld = (h2d ? k.src_ld : k.dst_ld) * k.sizeof_type, dld = (h2d ? k.dst_ld : k.src_ld) * k.sizeof_type;
         const uint64_t span = (uint64_t) ((k.n - 1) * hld + row);
-        bool straddles = false;                      // a cut inside a column, not only between two
-        if (cuts_inside(hbase, hbase + span, nullptr))
-            for (int64_t j = 0; j < k.n && !straddles; ++j)
-                straddles = cuts_inside(hbase + (uint64_t) (j * hld), hbase + (uint64_t) (j * hld + row), nullptr);
-        if (!straddles) { out.push_back(k); continue; }
+        if (!cuts_inside(hbase, hbase + span, nullptr)) { out.push_back(k); continue; }
         changed = true;
         const int64_t dbase = h2d ? k.dst_off : k.src_off;
         for (int64_t j = 0; j < k.n; ++j)
@@ -1270,6 +1266,8 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
     if (R->plan_record) fwrite(c.data(), sizeof(xkb_copy_t), n, R->plan_record);      // the planner's records
     split_at_locked_ends(R, c);
     n = c.size();
+    std::vector<uint64_t> cuts;                       // locked-piece ends: copies are not merged across them
+    for (auto & kv : R->user_pinned) { cuts.push_back(kv.first); cuts.push_back(kv.second); }
     if (R->ref_mode)
     {
         if ((rc = ensure_allocs(R))) return rc;
@@ -1279,7 +1277,7 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
             if (k.kind != XKB_COPY_D2D)
                 (k.kind == XKB_COPY_H2D ? R->cur_h2d_bytes : R->cur_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
         }
-        return xkb_plan_execute(c.data(), n, R->allocs.data(), R->allocs.size(), stream);
+        return xkb_internal_plan_execute_cut(c.data(), n, R->allocs.data(), R->allocs.size(), stream, cuts.data(), cuts.size());
     }
     int32_t maxid = -1;                               // ids of merged-away regions are not reused
     for (auto & kv : R->regions) maxid = std::max(maxid, kv.second.id);
@@ -1290,7 +1288,7 @@ static int run_copies(xkb_runtime * R, cudaStream_t stream)
         (k.kind == XKB_COPY_H2D ? R->cur_h2d : R->cur_d2h) += 1;
         (k.kind == XKB_COPY_H2D ? R->cur_h2d_bytes : R->cur_d2h_bytes) += (uint64_t) (k.m * k.n * k.sizeof_type);
     }
-    return xkb_plan_execute(c.data(), n, ptrs.data(), ptrs.size(), stream);
+    return xkb_internal_plan_execute_cut(c.data(), n, ptrs.data(), ptrs.size(), stream, cuts.data(), cuts.size());
 }
 
 // Point a built-in descriptor's host addresses at the device mirrors.
