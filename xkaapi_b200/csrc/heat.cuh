@@ -315,108 +315,6 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
     }
 }
 
-#ifndef XKB_F32X8
-#define XKB_F32X8 1                      // FP32 tile strips with eight rows per lane (0: four)
-#endif
-#ifndef XKB_F32X8_PF
-#define XKB_F32X8_PF 2                   // east columns the eight-rows-per-lane FP32 strip loads ahead
-#endif
-
-// FP32 storage, eight rows per lane: a half-warp (16 lanes x 8 rows) covers the 128-row strip and
-// the warp's two halves sweep the two halves of its columns (the second at most one column
-// shorter), so every load moves 32 bytes per lane -- 1 KiB per warp instruction, as the FP64 body
-// with four rows per lane -- and every step updates 8 cells per lane. North/south neighbours come
-// from the adjacent lanes of the same half (16-wide shuffles), the strip's halo rows from lanes 0
-// and 15 of each half. Same update and rounding as the other bodies. Needs vec_ok,
-// 0 <= rbase and rbase + 128 <= nx.
-template <int PF, bool CG>
-__device__ __forceinline__ void heat_strip_halo_f32x8(const float * __restrict__ src, float * __restrict__ dst, int64_t ld,
-                                                      int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
-                                                      int64_t cy0, int64_t cy1, double c, int pfd)
-{
-    constexpr int VEC = 8;
-    const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4;
-    const int64_t r = rbase + (int64_t) hl * VEC;
-    const int64_t rn = rbase - 1, rs = rbase + 16 * VEC;
-    const bool has_n = hl == 0 && rn >= 0, has_s = hl == 15 && rs < nx;
-    const bool lane_rows = (r + VEC > rx0) && (r < rx1);
-    const bool full_store = r >= rx0 && r + VEC <= rx1;
-    const int64_t steps = (cy1 - cy0 + 1) / 2;            // columns of the first half
-    const int64_t c0 = half ? cy0 + steps : cy0, c1 = half ? cy1 : cy0 + steps;
-    // L2 prefetch of a column: the strip's rows and four halo rows on each side (16-byte aligned)
-    const int64_t pf_lo = rbase >= 4 ? rbase - 4 : 0;
-    int64_t pf_hi = rbase + 16 * VEC + 4; if (pf_hi > nx) pf_hi = nx;
-    const uint32_t pf_bytes = (uint32_t) (((pf_hi - pf_lo) * (int64_t) sizeof(float)) & ~(int64_t) 15);
-    const bool pf_on = pfd > 0 && pf_bytes > 0;
-    const float * __restrict__ sp = src + r;
-    float * __restrict__ dp = dst + r;
-    auto load = [&](int64_t j) -> Cells<float, VEC> {
-        Cells<float, VEC> q;
-        const float4 * p = (const float4 *) (sp + j * ld);
-        const float4 a = CG ? __ldcg(p) : __ldg(p), b = CG ? __ldcg(p + 1) : __ldg(p + 1);
-        q.v[0] = a.x; q.v[1] = a.y; q.v[2] = a.z; q.v[3] = a.w; q.v[4] = b.x; q.v[5] = b.y; q.v[6] = b.z; q.v[7] = b.w;
-        return q;
-    };
-    if (steps <= 0) return;
-    Cells<float, VEC> west = load(c0 - 1);
-    Cells<float, VEC> cur = c0 < c1 ? load(c0) : west;
-    for (int64_t i0 = 0; i0 < steps; i0 += PF)
-    {
-        const int64_t j0 = c0 + i0;
-        if (pf_on && hl < PF)
-        {
-            const int64_t jp = j0 + pfd + hl;
-            if (jp <= c1) l2_prefetch_bulk(src + jp * ld + pf_lo, pf_bytes);
-        }
-        Cells<float, VEC> nxt[PF];
-        float hn[PF], hs[PF];
-#pragma unroll
-        for (int k = 0; k < PF; ++k)
-        {
-            const int64_t jc = j0 + k;
-            nxt[k] = jc + 1 <= c1 ? load(jc + 1) : cur;
-            hn[k] = (has_n && jc < c1) ? ld_scalar<CG>(src + jc * ld + rn) : 0.0f;
-            hs[k] = (has_s && jc < c1) ? ld_scalar<CG>(src + jc * ld + rs) : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < PF; ++k)
-        {
-            if (i0 + k >= steps) break;                  // warp-uniform: both halves count `steps`
-            const int64_t jc = j0 + k;
-            float north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1, 16);
-            float south = __shfl_down_sync(0xffffffffu, cur.v[0], 1, 16);
-            if (hl == 0)  north = hn[k];
-            if (hl == 15) south = hs[k];
-            if (lane_rows && jc < c1)
-            {
-                Cells<float, VEC> out;
-#pragma unroll
-                for (int e = 0; e < VEC; ++e)
-                {
-                    const double sv = (double) cur.v[e];
-                    const double up = (double) (e == 0 ? north : cur.v[e - 1]);
-                    const double dn = (double) (e == VEC - 1 ? south : cur.v[e + 1]);
-                    out.v[e] = (float) heat_update(sv, up, dn, (double) west.v[e], (double) nxt[k].v[e], c);
-                }
-                float * q = dp + jc * ld;
-                if (full_store)
-                {
-                    ((float4 *) q)[0] = make_float4(out.v[0], out.v[1], out.v[2], out.v[3]);
-                    ((float4 *) q)[1] = make_float4(out.v[4], out.v[5], out.v[6], out.v[7]);
-                }
-                else
-                {
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e)
-                        if (r + e >= rx0 && r + e < rx1) q[e] = out.v[e];
-                }
-            }
-            west = cur;
-            cur = nxt[k];
-        }
-    }
-}
-
 template <typename T, int VEC, int PF, bool CG>
 __device__ __noinline__ void heat_strip_halo_edge(const T * __restrict__ src, T * __restrict__ dst, int64_t ld,
                                                   int64_t nx, int64_t rbase, int64_t rx0, int64_t rx1,
@@ -431,12 +329,7 @@ __device__ __forceinline__ void heat_strip_halo(const T * __restrict__ src, T * 
                                                 int64_t cy0, int64_t cy1, double c, bool vec_ok, int pfd)
 {
     if (vec_ok && rbase >= 0 && rbase + 32 * VEC <= nx)
-    {
-        if constexpr (sizeof(T) == 4 && VEC == 4 && XKB_F32X8)
-            heat_strip_halo_f32x8<XKB_F32X8_PF, CG>((const float *) src, (float *) dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, pfd);
-        else
-            heat_strip_halo_impl<T, VEC, PF, CG, true>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
-    }
+        heat_strip_halo_impl<T, VEC, PF, CG, true>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
     else
         heat_strip_halo_edge<T, VEC, PF, CG>(src, dst, ld, nx, rbase, rx0, rx1, cy0, cy1, c, vec_ok, pfd);
 }
