@@ -643,7 +643,7 @@ def run_study(args):
     # serve: closed-loop capacity of a few shapes, device loop and one launch per request
     io = serve_io(torch)
     free, _ = torch.cuda.mem_get_info()
-    srv = xk.Server(budget_bytes=int(min(150e9, free - 8e9)), slots=16)
+    srv = xk.Server(budget_bytes=int(min(150e9, free - 8e9)), slots=args.slots)
     side, steps, f32, _, _ = serve_trace(2000, 2026)
     cases = {"8 x 4096^2 FP64 x 100 steps": (np.full(8, 4096), np.full(8, 100), np.zeros(8, np.int64)),
              "first 300 graphs of the trace": (side[:300], steps[:300], f32[:300])}
@@ -688,6 +688,7 @@ def main():
     ap.add_argument("--tasks", type=int, default=65536, help="--study resolver: tasks of the microbench")
     ap.add_argument("--f32", action="store_true", help="--study graph: FP32 storage")
     ap.add_argument("--prefetch", type=int, default=0, help="--study graph: L2 prefetch distance (0: the default)")
+    ap.add_argument("--slots", type=int, default=16, help="served stream: requests on the device at once")
     args = ap.parse_args()
     NX = NY = args.size
     STEPS = args.graph_steps
@@ -937,7 +938,7 @@ def main():
         extra["e2e_user_body"] = user_body_study(local)
         extra["axpby_chains"] = axpby_study(local)
     if rank == 0 and not args.no_side:
-        extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000)
+        extra["serve"] = serve_study(xk, torch, ngraphs=400 if args.quick else 2000, slots=args.slots)
 
     # ---------------- CPU baseline (rank 0, N=1) ----------------------------------------------
     cpu = None
