@@ -547,10 +547,22 @@ def serve_io(torch):
     return _SERVE_IO["in"].data_ptr(), _SERVE_IO["out"].data_ptr()
 
 
-def serve_requests(xk, side, steps, f32, arrivals, io=None):
+def serve_tiles(side, policy):
+    """Tile side of each served graph: 128 ("128"), or 256 for grids of 2048 and more, whose
+    128^2 tiles would be 256 or more per step ("256from2048"); the trace fixes the graphs, the
+    runtime chooses their tiling (the batched configuration tunes the tile over 128-1024)."""
+    side = np.asarray(side)
+    if policy == "256from2048":
+        return np.where(side >= 2048, 256, 128)
+    return np.full(len(side), 128)
+
+
+def serve_requests(xk, side, steps, f32, arrivals, io=None, tiles=None):
     reqs = (xk.Request * len(side))()
+    tiles = np.full(len(side), 128) if tiles is None else tiles
     for k, r in enumerate(reqs):
-        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32 = float(arrivals[k]), int(side[k]), int(side[k]), 128, int(steps[k]), int(f32[k])
+        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32 = (float(arrivals[k]), int(side[k]), int(side[k]), int(tiles[k]),
+                                                         int(steps[k]), int(f32[k]))
         r.seed, r.c = 7000 + k, COEF
         r.input, r.result = (io if io else (None, None))
     return reqs
@@ -649,20 +661,20 @@ def run_study(args):
              "first 300 graphs of the trace": (side[:300], steps[:300], f32[:300])}
     for name, (sd, st, f) in cases.items():
         nbytes = float(((sd.astype(np.float64) - 2) ** 2 * st * np.where(f == 1, 8.0, 16.0)).sum())
-        for mode in ("device", "launch"):
+        for mode, withio, policy in (("device", True, "128"), ("device", True, "256from2048"), ("device", False, "128"),
+                                     ("launch", True, "128"), ("launch", False, "128")):
             if mode == "launch":
                 os.environ["XKB_SERVE_MODE"] = "launch"
             else:
                 os.environ.pop("XKB_SERVE_MODE", None)
-            for withio in (True, False):
-                for _ in range(2):          # the second pass: every shape's graph already resolved
-                    reqs = serve_requests(xk, sd, st, f, np.zeros(len(sd)), io if withio else None)
-                    srv.run(reqs)
-                fin = max(r.finish_s for r in reqs)
-                print(json.dumps({"study": "serve", "case": name, "mode": mode, "host_io": withio,
-                                  "GBps": round(nbytes / fin / 1e9, 1), "makespan_s": round(fin, 3),
-                                  "p50_ms": round(float(np.percentile([(r.finish_s - r.start_s) * 1e3 for r in reqs], 50)), 2)}),
-                      flush=True)
+            for _ in range(2):          # the second pass: every shape's graph already resolved
+                reqs = serve_requests(xk, sd, st, f, np.zeros(len(sd)), io if withio else None, serve_tiles(sd, policy))
+                srv.run(reqs)
+            fin = max(r.finish_s for r in reqs)
+            print(json.dumps({"study": "serve", "case": name, "mode": mode, "host_io": withio, "tiles": policy,
+                              "GBps": round(nbytes / fin / 1e9, 1), "makespan_s": round(fin, 3),
+                              "p50_ms": round(float(np.percentile([(r.finish_s - r.start_s) * 1e3 for r in reqs], 50)), 2)}),
+                  flush=True)
     os.environ.pop("XKB_SERVE_MODE", None)
     srv.close()
     return 0

@@ -12,13 +12,14 @@ import xkaapi_b200 as xk
 pytestmark = pytest.mark.gpu
 
 
-def make_requests(specs):
+def make_requests(specs, tiles=None):
     reqs = (xk.Request * len(specs))()
     bufs = []
-    for r, (t, n, steps, f32, seed) in zip(reqs, specs):
+    for k, (r, (t, n, steps, f32, seed)) in enumerate(zip(reqs, specs)):
         buf = np.zeros((n, n), dtype=np.float32 if f32 else np.float64)
         bufs.append(buf)
-        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32, r.seed, r.c = t, n, n, 64, steps, f32, seed, 0.2
+        ts = 64 if tiles is None else tiles[k]
+        r.arrival_s, r.nx, r.ny, r.ts, r.steps, r.f32, r.seed, r.c = t, n, n, ts, steps, f32, seed, 0.2
         r.result = buf.ctypes.data
     return reqs, bufs
 
@@ -89,3 +90,20 @@ def test_device_loop_with_inputs_equals_launch_mode(torch_cuda, monkeypatch):
         dt = np.float32 if f32 else np.float64
         np.testing.assert_array_equal(a, b)
         np.testing.assert_array_equal(a, O.heat_run(O.serve_init(n, n, seed, dt), n, n, steps, 0.2, dtype=dt))
+
+
+def test_tile_sides_of_a_stream_equal_the_oracle(torch_cuda):
+    """Requests of one stream tiled 64^2, 128^2 and 256^2 (a strip sweeps several 128-row pieces of
+    a 256^2 tile; ragged last tiles), FP64 and FP32 storage, in the device-resident loop: every
+    result equals the oracle bit for bit."""
+    specs, tiles = [], []
+    for k, (n, ts) in enumerate([(300, 256), (520, 256), (400, 128), (258, 64), (640, 256), (384, 128)]):
+        specs.append((0.001 * k, n, 3 + k, k % 2, 2000 + k))
+        tiles.append(ts)
+    srv = xk.Server(budget_bytes=64 << 20, slots=4, max_seconds=60.0)
+    reqs, bufs = make_requests(specs, tiles)
+    srv.run(reqs)
+    srv.close()
+    for (t, n, steps, f32, seed), buf in zip(specs, bufs):
+        dt = np.float32 if f32 else np.float64
+        np.testing.assert_array_equal(buf, O.heat_run(O.serve_init(n, n, seed, dt), n, n, steps, 0.2, dtype=dt))
