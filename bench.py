@@ -635,9 +635,9 @@ def run_study(args):
         g[0, :] = 0; g[-1, :] = 0; g[:, 0] = 0; g[:, -1] = 0
         a = g.to(device="cuda", dtype=torch.float32 if args.f32 else torch.float64); b = a.clone()
         del g
-        res, graph, _ = build_heat_graph(xk, torch, a, b, n, n, TS, steps, stream, esize=esz)
-        d = xk.heat_task_descs((a.data_ptr(), b.data_ptr()), n, n, n, TS, TS, steps, COEF, f32=args.f32)
-        sch = xk.Scheduler(stream); sch.set_team(1); sch.set_tasks(d); del d
+        res, graph, _ = build_heat_graph(xk, torch, a, b, n, n, args.tile, steps, stream, esize=esz)
+        d = xk.heat_task_descs((a.data_ptr(), b.data_ptr()), n, n, n, args.tile, args.tile, steps, COEF, f32=args.f32)
+        sch = xk.Scheduler(stream); sch.set_team(args.team); sch.set_tasks(d); del d
         if args.prefetch:
             sch.set_prefetch(args.prefetch)
         runs = []
@@ -648,6 +648,7 @@ def run_study(args):
                 runs.append(sch.kernel_ms())
         best = min(runs)
         print(json.dumps({"study": "graph", "size": n, "steps": steps, "dtype": "f32" if args.f32 else "f64",
+                          "tile": args.tile, "warps_per_task": args.team,
                           "tasks": int(graph.ntasks), "kernel_ms": [round(x, 3) for x in runs],
                           "GBps_best": round(2.0 * esz * cells_all(n, n) * steps / (best / 1e3) / 1e9, 1)}), flush=True)
         sch.close(); res.close()
@@ -701,6 +702,8 @@ def main():
     ap.add_argument("--f32", action="store_true", help="--study graph: FP32 storage")
     ap.add_argument("--prefetch", type=int, default=0, help="--study graph: L2 prefetch distance (0: the default)")
     ap.add_argument("--slots", type=int, default=16, help="served stream: requests on the device at once")
+    ap.add_argument("--tile", type=int, default=TS, help="--study graph: tile side")
+    ap.add_argument("--team", type=int, default=1, help="--study graph: warps per task (1, 2, 4, 8)")
     args = ap.parse_args()
     NX = NY = args.size
     STEPS = args.graph_steps
