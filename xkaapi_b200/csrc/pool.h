@@ -52,8 +52,11 @@ private:
     std::vector<std::pair<void *, size_t>> v_;
 };
 
+// The element count sits on a cache line of its own, away from the base pointer: the spawning
+// thread bumps the count of three arrays per task while worker threads read their base pointers
+// to convert earlier tasks, and one shared line would bounce between those cores on every spawn.
 template <typename T>
-class PoolArray {
+class alignas(64) PoolArray {
     static_assert(std::is_trivially_copyable<T>::value, "PoolArray holds trivially copyable elements");
 
 public:
@@ -152,8 +155,9 @@ private:
     }
 
     T * p_ = nullptr;
-    size_t n_ = 0, bytes_ = 0;
+    size_t bytes_ = 0;
     bool fixed_ = false;
+    alignas(64) size_t n_ = 0;
 };
 
 } // namespace xkb

@@ -367,6 +367,7 @@ extern "C" int xkrt_init(xkrt_runtime_t ** out)
                            R->acc_pool.reserve_fixed(MAXA) && R->recs.reserve_fixed(MAXA) && R->replica_pool.reserve_fixed(MAXA);
         if (!fixed) { R->pending.release(); R->args_pool.release(); R->acc_pool.release(); R->recs.release(); R->replica_pool.release(); }
         R->bg = R->gpu && fixed;
+        if (const char * e = getenv("XKB_BACKGROUND")) if (atoi(e) == 0) R->bg = false;   // resolution at the wait
     }
     if (R->pending.fixed())
     {
@@ -1551,17 +1552,20 @@ static int resolve_range(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_
     if (t0 >= t1) return XKB_OK;
     if (!R->recs.resize(a1)) return xkb_set_error(XKB_ENOMEM, "xkrt_task_wait: out of host memory");
     xkb_access_rec_t * recs = R->recs.data();
+    // the pools do not move while this runs (fixed reservations, or no spawn during the wait)
+    const Task * tasks = R->pending.data();
+    const xkrt_access_t * accs = R->acc_pool.data();
     std::atomic<bool> dense(true);
     parallel_chunks(t1 - t0, [&](size_t b, size_t e) {
         bool d = true;
         for (size_t t = t0 + b; t < t0 + e; ++t)
         {
-            const Task & T = R->pending[t];
+            const Task & T = tasks[t];
             bool any = false;
             for (uint32_t k = 0; k < T.nacc; ++k)
             {
                 xkb_access_rec_t & r = recs[T.acc_off + k];
-                if (to_rec(R->acc_pool[T.acc_off + k], (uint32_t) t, r)) any = true;
+                if (to_rec(accs[T.acc_off + k], (uint32_t) t, r)) any = true;
                 else { r.type = REC_NONE; d = false; }
             }
             d = d && any;
