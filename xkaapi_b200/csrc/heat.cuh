@@ -16,6 +16,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace xkb {
 
 template <typename T> struct HeatVec;
@@ -266,21 +268,23 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
     };
     Cells<T, VEC> west = load(cy0 - 1);
     Cells<T, VEC> cur  = load(cy0);
-    for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
-    {
+    // one block of PF columns from j0; FULL: all PF columns lie before cy1 (no per-column checks)
+    auto block = [&](const int64_t j0, auto full_tag) {
+        constexpr bool FULL = decltype(full_tag)::value;
         if (pf_on && lane < PF)
         {
             const int64_t jp = j0 + pfd + lane;
             if (jp <= cy1) l2_prefetch_bulk(src + jp * ld + pf_lo, pf_bytes);
         }
         Cells<T, VEC> nxt[PF];
-        T hv = T(0), hn[HALO_LANES ? 1 : PF], hs[HALO_LANES ? 1 : PF];
+        [[maybe_unused]] T hv = T(0);
+        [[maybe_unused]] T hn[HALO_LANES ? 1 : PF], hs[HALO_LANES ? 1 : PF];
         if constexpr (HALO_LANES)
             if (hk < PF && h_row_ok && j0 + hk < cy1) hv = ld_scalar<CG>(src + (j0 + hk) * ld + h_row);
 #pragma unroll
         for (int k = 0; k < PF; ++k)
         {
-            if (j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
+            if (FULL || j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
             if constexpr (!HALO_LANES)
             {
                 const int64_t jc = j0 + k;
@@ -292,7 +296,7 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
         for (int k = 0; k < PF; ++k)
         {
             const int64_t jc = j0 + k;
-            if (jc >= cy1) break;                        // warp-uniform
+            if (!FULL && jc >= cy1) break;               // warp-uniform
             T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
             T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
             T hnk, hsk;
@@ -332,7 +336,10 @@ __device__ __forceinline__ void heat_strip_halo_impl(const T * __restrict__ src,
             west = cur;
             cur = nxt[k];
         }
-    }
+    };
+    int64_t j0 = cy0;
+    for (; j0 + PF <= cy1; j0 += PF) block(j0, std::true_type{});
+    if (j0 < cy1) block(j0, std::false_type{});
 }
 
 template <typename T, int VEC, int PF, bool CG>
