@@ -129,8 +129,9 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
 
     Cells<T, VEC> west = load(cy0 - 1);
     Cells<T, VEC> cur  = load(cy0);
-    for (int64_t j0 = cy0; j0 < cy1; j0 += PF)
-    {
+    // one block of PF columns from j0; FULL: all PF columns lie before cy1 (no per-column checks)
+    auto block = [&](const int64_t j0, auto full_tag) {
+        constexpr bool FULL = decltype(full_tag)::value;
         if (pf_on && lane < PF)
         {
             // lane k prefetches column j0 + pfd + k of the strip into L2 with one bulk request
@@ -140,12 +141,12 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
         Cells<T, VEC> nxt[PF];
 #pragma unroll
         for (int k = 0; k < PF; ++k)
-            if (j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
+            if (FULL || j0 + k + 1 <= cy1) nxt[k] = load(j0 + k + 1);
 #pragma unroll
         for (int k = 0; k < PF; ++k)
         {
             const int64_t jc = j0 + k;
-            if (jc >= cy1) break;                        // warp-uniform
+            if (!FULL && jc >= cy1) break;               // warp-uniform
             const T north = __shfl_up_sync(0xffffffffu, cur.v[VEC - 1], 1);
             const T south = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
             Cells<T, VEC> out;
@@ -177,7 +178,10 @@ __device__ __forceinline__ void heat_strip_impl(const T * __restrict__ src, T * 
             west = cur;
             cur = nxt[k];
         }
-    }
+    };
+    int64_t j0 = cy0;
+    for (; j0 + PF <= cy1; j0 += PF) block(j0, std::true_type{});
+    if (j0 < cy1) block(j0, std::false_type{});
 }
 
 // Edge strips (grid bottom rows, unaligned grids) take a checked path kept out of line so the
