@@ -94,6 +94,27 @@ def test_f32_tiles_bit_exact(torch_cuda):
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("tsy", [1, 2, 3, 5, 6, 7, 12, 13, 17, 36, 128])
+def test_tile_column_blocks_bit_exact(torch_cuda, dtype, tsy):
+    """Tile strips sweep their columns in blocks (FP64: 2 columns, FP32: 6) -- whole blocks with
+    no per-column checks, then one checked block for the rest: tile widths that are multiples of
+    a block, one column past one, and shorter than one, FP64 and FP32 storage."""
+    torch = torch_cuda
+    nx, ny, tsx = 200, 149, 64
+    g = O.heat_init(nx, ny, seed=tsy)
+    if dtype == "f32":
+        g = g.astype(np.float32)
+    ref = g.copy()
+    s, d = to_dev(torch, g), to_dev(torch, g)
+    for tx in range(-(-nx // tsx)):
+        for ty in range(-(-ny // tsy)):
+            O.heat_tile(g, ref, nx, ny, tx, ty, tsx, tsy, C)
+            xk.heat_tile(s, d, nx, ny, nx, tx, ty, tsx, tsy, C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
 def test_heat_norms_fp64_checks(torch_cuda, dtype):
     """xkb_heat_norms: boundary max, L2 norm and the step's residual in FP64, against numpy on
     the same grids; the residual is 0 for FP64 storage and the float rounding for FP32."""
