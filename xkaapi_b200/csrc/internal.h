@@ -11,6 +11,8 @@
 int xkb_internal_launch_task(const xkb_task_desc_t * d, cudaStream_t stream);
 // xkb_plan_execute with host cuts (sorted addresses): no two copies whose host bytes lie on
 // different sides of a cut are merged into one (each copy given must lie between two cuts).
+// Host copies issued by the plan executor so far, after coalescing (traces).
+uint64_t xkb_internal_issued_host_copies();
 int xkb_internal_plan_execute_cut(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs,
                                   cudaStream_t stream, const uint64_t * cuts, size_t ncuts);
 

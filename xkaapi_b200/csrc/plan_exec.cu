@@ -23,6 +23,7 @@
 #include "internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 namespace xkb {
@@ -143,9 +144,12 @@ static size_t coalesce(std::vector<HostCopy> & v)
     return v.size();
 }
 
+static std::atomic<uint64_t> g_issued_host_copies{0};     // after coalescing (traces)
+
 static int issue_host_copies(std::vector<HostCopy> & v, cudaMemcpyKind kind, cudaStream_t st)
 {
     coalesce(v);
+    g_issued_host_copies.fetch_add(v.size(), std::memory_order_relaxed);
     for (const HostCopy & c : v)
     {
         // a contiguous range (one row, or full-pitch rows) as a plain copy, else pitched
@@ -248,6 +252,8 @@ extern "C" int xkb_plan_execute(const xkb_copy_t * copies, size_t n, void * cons
 {
     return plan_execute(copies, n, alloc_ptrs, nallocs, xkb_stream(stream), nullptr, 0);
 }
+
+uint64_t xkb_internal_issued_host_copies() { return g_issued_host_copies.load(std::memory_order_relaxed); }
 
 int xkb_internal_plan_execute_cut(const xkb_copy_t * copies, size_t n, void * const * alloc_ptrs, size_t nallocs,
                                   cudaStream_t stream, const uint64_t * cuts, size_t ncuts)

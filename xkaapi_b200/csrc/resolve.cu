@@ -36,9 +36,11 @@
 #include <algorithm>
 #include <climits>
 #include <chrono>
+#include <string>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <map>
 #include <memory>
 #include <new>
@@ -709,11 +711,59 @@ struct HOp { uint32_t task; uint8_t link; uint8_t mode; HRect r; };
 
 static size_t g_realloc_bytes = 0;               // device bytes allocated by reserve (trace)
 
+// Device memory pool of the resolver's work buffers on the current device (made on first use).
+// Buffers only the resolver's own stream touches are allocated from it in stream order, so
+// growing one neither waits for the whole device (as cudaFree does) nor asks the driver for
+// memory while copies and kernels of other streams run: a runtime streaming windows of tasks
+// had its resolution stall for up to 0.3 s in cudaMalloc / cudaFree of a domain's cell states.
+// Freed memory stays in the pool for the next resolver of the process, up to 4 GiB
+// (XKB_POOL_CACHE=0: none).
+static cudaMemPool_t resolver_pool()
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[256];
+    static bool made[256];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) { cudaGetLastError(); return nullptr; }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!made[dev])
+    {
+        made[dev] = true;
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if (cudaMemPoolCreate(&pools[dev], &props) != cudaSuccess) { cudaGetLastError(); pools[dev] = nullptr; }
+        else
+        {
+            const char * e = getenv("XKB_POOL_CACHE");
+            uint64_t keep = (e && atoi(e) == 0) ? 0 : (uint64_t(4) << 30);
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
+    return pools[dev];
+}
+
 template <typename T>
 struct DevBuf {
     T * p = nullptr;
     size_t cap = 0;
-    ~DevBuf() { if (p) cudaFree(p); }
+    cudaStream_t st = nullptr;       // pooled: the one stream that uses the buffer
+    bool pooled = false;
+    ~DevBuf()
+    {
+        if (!p) return;
+        if (!pooled) cudaFree(p);
+        else if (cudaFreeAsync(p, st) != cudaSuccess) { cudaGetLastError(); cudaFree(p); }
+    }
+    // Allocate from the resolver's pool in the order of `s` (before the first allocation only).
+    void use_pool(cudaStream_t s)
+    {
+        if (p) return;
+        pooled = resolver_pool() != nullptr;
+        st = s;
+    }
     int reserve(size_t n)
     {
         if (n <= cap) return XKB_OK;
@@ -721,9 +771,18 @@ struct DevBuf {
         while (c < n) c *= 2;
         T * q = nullptr;
         g_realloc_bytes += c * sizeof(T);
-        cudaError_t e = cudaMalloc(&q, c * sizeof(T));
-        if (e != cudaSuccess) return xkb_set_cuda_error(e);
-        if (p) cudaFree(p);
+        if (pooled)
+        {
+            cudaError_t e = cudaMallocFromPoolAsync((void **) &q, c * sizeof(T), resolver_pool(), st);
+            if (e != cudaSuccess) return xkb_set_cuda_error(e);
+            if (p) cudaFreeAsync(p, st);      // after the stream's work queued so far
+        }
+        else
+        {
+            cudaError_t e = cudaMalloc(&q, c * sizeof(T));
+            if (e != cudaSuccess) return xkb_set_cuda_error(e);
+            if (p) cudaFree(p);
+        }
         p = q; cap = c;
         return XKB_OK;
     }
@@ -1021,6 +1080,7 @@ static int build_ops_staged(xkb_resolver * R, const xkb_access_rec_t * recs, siz
                 if (R->blas_index.count(key)) continue;
                 std::unique_ptr<Domain> d(new Domain());
                 d->ld = key.first; d->s = key.second;
+                d->state[0].use_pool(R->stream); d->state[1].use_pool(R->stream);
                 R->blas.push_back(std::move(d));
                 R->blas_index.emplace(key, R->blas.size() - 1);
             }
@@ -1115,6 +1175,7 @@ static void build_ops(xkb_resolver * R, const xkb_access_rec_t * recs, size_t n)
                 {
                     std::unique_ptr<Domain> d(new Domain());
                     d->ld = r.ld; d->s = r.sizeof_type;
+                    d->state[0].use_pool(R->stream); d->state[1].use_pool(R->stream);
                     for (auto k = R->segments.rbegin(); k != R->segments.rend(); ++k) push_ops(*d, false, *k);
                     R->blas.push_back(std::move(d));
                     it = R->blas_index.emplace(key, R->blas.size() - 1).first;
@@ -1191,6 +1252,26 @@ static int spill_check(xkb_resolver * R, bool & redo)
     return XKB_OK;
 }
 
+// XKB_TRACE_RESOLVE=2: the time each step of a batch's compression and region pass takes
+// (host clock, so a step that synchronises includes the device work queued before it).
+struct PhaseTrace {
+    const bool on;
+    const char * what;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    std::string line;
+    explicit PhaseTrace(const char * w) : on(trace_level() >= 2), what(w) {}
+    static int trace_level() { static const int l = getenv("XKB_TRACE_RESOLVE") ? atoi(getenv("XKB_TRACE_RESOLVE")) : 0; return l; }
+    void mark(const char * step)
+    {
+        if (!on) return;
+        const auto n = std::chrono::steady_clock::now();
+        char b[96];
+        snprintf(b, sizeof(b), " %s %.1f", step, std::chrono::duration<double, std::milli>(n - t).count());
+        line += b; t = n;
+    }
+    ~PhaseTrace() { if (on) fprintf(stderr, "  %s (ms):%s\n", what, line.c_str()); }
+};
+
 static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & xs, std::vector<uint64_t> & ys)
 {
     if (xs.size() < 2 || ys.size() < 2) { d.xs = xs; d.ys = ys; return XKB_OK; }
@@ -1198,8 +1279,10 @@ static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & x
     const size_t ncx = xs.size() - 1, ncy = ys.size() - 1, ncells = ncx * ncy;
     if (same && d.ncells == ncells) return XKB_OK;
     int rc;
+    PhaseTrace pt("refine");
     DevBuf<int> & out = d.state[d.cur ^ 1];
     if ((rc = out.reserve(ncells * STRIDE))) return rc;
+    pt.mark("state-reserve");
     if (d.ncells == 0)
     {
         init_state_kernel<<<(unsigned) ((ncells + 255) / 256), 256, 0, R->stream>>>(out.p, ncells);
@@ -1222,7 +1305,9 @@ static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & x
         if ((rc = dm.reserve(ncx + ncy))) return rc;
         XKB_CUDA_TRY(cudaMemcpyAsync(dm.p, mx.data(), ncx * sizeof(int), cudaMemcpyHostToDevice, R->stream));
         XKB_CUDA_TRY(cudaMemcpyAsync(dm.p + ncx, my.data(), ncy * sizeof(int), cudaMemcpyHostToDevice, R->stream));
+        pt.mark("maps");
         if ((rc = spill_reserve(R, 1))) return rc;
+        pt.mark("spill-reserve");
         for (bool redo = true; redo;)
         {
             if ((rc = reset_spill(R))) return rc;
@@ -1231,6 +1316,7 @@ static int refine_domain(xkb_resolver * R, Domain & d, std::vector<uint64_t> & x
                 (unsigned) R->spill_chunks);
             XKB_CUDA_TRY(cudaGetLastError());
             if ((rc = spill_check(R, redo))) return rc;   // synchronises: dm is freed on return
+            pt.mark("refine-kernel+sync");
         }
     }
     XKB_CUDA_TRY(cudaGetLastError());
@@ -1249,9 +1335,11 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
     cudaStream_t st = R->stream;
     const size_t nb = (size_t) nregions + 1;
     int rc;
+    PhaseTrace pt("regions");
     if ((rc = R->bin_off.reserve(nb)) || (rc = R->bin_cur.reserve(nb)) ||
         (rc = R->tmp.reserve(nb / SCAN_TILE + 2)) || (rc = R->bin_flag.reserve(1)))
         return rc;
+    pt.mark("reserve");
     XKB_CUDA_TRY(cudaMemsetAsync(R->bin_off.p, 0, nb * sizeof(unsigned), st));
     XKB_CUDA_TRY(cudaMemsetAsync(R->bin_cur.p, 0, nb * sizeof(unsigned), st));
     XKB_CUDA_TRY(cudaMemsetAsync(R->bin_flag.p, 0, sizeof(int), st));
@@ -1276,6 +1364,7 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
     unsigned total = 0;
     XKB_CUDA_TRY(cudaMemcpyAsync(&total, R->bin_off.p + nregions, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    pt.mark("count+sync");
     bool binned = total > 0;
     if (binned)
     {
@@ -1294,6 +1383,7 @@ static int launch_region(xkb_resolver * R, ResolveArgs & a, int nregions)
         int too_long = 0;
         XKB_CUDA_TRY(cudaMemcpyAsync(&too_long, R->bin_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         XKB_CUDA_TRY(cudaStreamSynchronize(st));
+        pt.mark("fill+sort+sync");
         binned = !too_long;
     }
     // time split: segments per region from the mean list length (a segment of a few hundred ops
@@ -1356,7 +1446,9 @@ static int compress_domain(xkb_resolver * R, Domain & d, const HOp * hops, DOp *
     size_t cap = 1024;
     while (cap < 4 * nops) cap *= 2;
     int rc;
+    PhaseTrace pt("compress");
     if ((rc = R->hset.reserve(2 * cap)) || (rc = R->ukeys.reserve(4 * nops)) || (rc = R->ucount.reserve(3))) return rc;
+    pt.mark("reserve");
     XKB_CUDA_TRY(cudaMemsetAsync(R->hset.p, 0xff, 2 * cap * sizeof(uint64_t), st));
     XKB_CUDA_TRY(cudaMemsetAsync(R->ucount.p, 0, 3 * sizeof(unsigned), st));
     const unsigned g = (unsigned) ((nops + 255) / 256);
@@ -1366,6 +1458,7 @@ static int compress_domain(xkb_resolver * R, Domain & d, const HOp * hops, DOp *
     unsigned cnt[3];
     XKB_CUDA_TRY(cudaMemcpyAsync(cnt, R->ucount.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
     XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    pt.mark("collect+sync");
     std::vector<uint64_t> xs(d.xs.size() + cnt[0] + 1), ys(d.ys.size() + cnt[1] + 1);
     std::copy(d.xs.begin(), d.xs.end(), xs.begin());
     std::copy(d.ys.begin(), d.ys.end(), ys.begin());
@@ -1379,7 +1472,9 @@ static int compress_domain(xkb_resolver * R, Domain & d, const HOp * hops, DOp *
         std::sort(v->begin(), v->end());
         v->erase(std::unique(v->begin(), v->end()), v->end());
     }
+    pt.mark("keys+sort");
     if ((rc = refine_domain(R, d, xs, ys))) return rc;
+    pt.mark("refine");
     if ((rc = R->bounds.reserve(d.xs.size() + d.ys.size()))) return rc;
     XKB_CUDA_TRY(cudaMemcpyAsync(R->bounds.p, d.xs.data(), d.xs.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     XKB_CUDA_TRY(cudaMemcpyAsync(R->bounds.p + d.xs.size(), d.ys.data(), d.ys.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
@@ -1388,6 +1483,7 @@ static int compress_domain(xkb_resolver * R, Domain & d, const HOp * hops, DOp *
     XKB_CUDA_TRY(cudaGetLastError());
     // the host vectors above die on return: the copies out of them must be done
     XKB_CUDA_TRY(cudaStreamSynchronize(st));
+    pt.mark("map+sync");
     return XKB_OK;
 }
 
@@ -1474,6 +1570,7 @@ static int resolve_batch(xkb_resolver * R, const xkb_access_rec_t * recs, size_t
             if (R->useg.empty() || R->useg.back()->cap - R->useg_n.back() < nemit)
             {
                 std::unique_ptr<DevBuf<unsigned long long>> seg(new (std::nothrow) DevBuf<unsigned long long>());
+                if (seg) seg->use_pool(R->stream);
                 if (!seg) return xkb_set_error(XKB_ENOMEM, "resolver: out of host memory");
                 // segments double in size, so a long stream allocates a few of them, not one per batch
                 const size_t last = R->useg.empty() ? 0 : R->useg.back()->cap;
@@ -1546,6 +1643,15 @@ extern "C" int xkb_resolver_create(xkb_resolver_t ** out, void * stream)
     R->interval.interval = true;
     R->handles.interval = true;
     R->stream = (cudaStream_t) stream;
+    // work buffers only this resolver's stream touches come from the pool in stream order; the
+    // graph it hands out (succ_ptr, succ, npred, window graphs, periodic form) stays in plain
+    // allocations, as a caller may read it on other streams
+    for (Domain * d : {&R->interval, &R->handles}) { d->state[0].use_pool(R->stream); d->state[1].use_pool(R->stream); }
+    R->dops.use_pool(R->stream); R->hops.use_pool(R->stream);
+    R->hset.use_pool(R->stream); R->ukeys.use_pool(R->stream); R->bounds.use_pool(R->stream); R->ucount.use_pool(R->stream);
+    R->emit.use_pool(R->stream); R->table.use_pool(R->stream); R->counters.use_pool(R->stream);
+    R->tmp.use_pool(R->stream); R->bin_off.use_pool(R->stream); R->bin_cur.use_pool(R->stream);
+    R->bin_list.use_pool(R->stream); R->bin_flag.use_pool(R->stream); R->snap.use_pool(R->stream);
     *out = R;
     return XKB_OK;
 }
@@ -1582,6 +1688,7 @@ int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops)
     if (R->useg.empty())
     {
         std::unique_ptr<DevBuf<unsigned long long>> seg(new (std::nothrow) DevBuf<unsigned long long>());
+        if (seg) seg->use_pool(R->stream);
         if (!seg) return xkb_set_error(XKB_ENOMEM, "resolver: out of host memory");
         if ((rc = seg->reserve(std::max<size_t>(emit, size_t(1) << 24)))) return rc;
         R->useg.push_back(std::move(seg));

@@ -1436,6 +1436,13 @@ static double ms_since(std::chrono::steady_clock::time_point t0)
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Trace clock: milliseconds since the process's first trace line.
+static double trace_clock_ms()
+{
+    static const auto epoch = std::chrono::steady_clock::now();
+    return ms_since(epoch);
+}
+
 // Device array owned by the runtime (freed when replaced or at deinit).
 struct DevArray {
     void * p = nullptr;
@@ -1642,8 +1649,8 @@ static void bg_worker(xkb_runtime * R)
         if (!failed && rc == XKB_OK && streamed) rc = stream_launch(R, mark);
         if (rc) streamed = false;
         if (trace)
-            fprintf(stderr, "worker: tasks [%zu, %zu) prepared and resolved in %.1f ms, %s in %.1f ms\n", t0, t1, res_ms,
-                    streamed ? "launched" : "kept", ms_since(w0) - res_ms);
+            fprintf(stderr, "worker: tasks [%zu, %zu) prepared and resolved in %.1f ms, %s in %.1f ms (at %.1f ms)\n", t0, t1, res_ms,
+                    streamed ? "launched" : "kept", ms_since(w0) - res_ms, trace_clock_ms());
         {
             std::lock_guard<std::mutex> lk(R->mu);
             if (rc && R->bg_rc == XKB_OK) { R->bg_rc = rc; R->bg_err = xkb_last_error(); }
@@ -1670,6 +1677,8 @@ static void bg_hand_over(xkb_runtime * R, bool final)
         R->handed = nt; R->handed_acc = nacc;
         R->hand_q.emplace_back(nt, nacc);
     }
+    static const bool trace = getenv("XKB_TRACE_WAIT") != nullptr;
+    if (trace) fprintf(stderr, "hand-over: tasks up to %zu (at %.1f ms)\n", nt, trace_clock_ms());
     if (!R->worker.joinable()) R->worker = std::thread(bg_worker, R);
     R->cv.notify_all();
 }
@@ -2108,8 +2117,18 @@ static int stream_prepare(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size
     std::lock_guard<std::mutex> lk(R->plan_mu);
     static const bool trace = getenv("XKB_TRACE_WAIT") != nullptr;
     const auto w0 = std::chrono::steady_clock::now();
+    const uint64_t issued0 = trace ? xkb_internal_issued_host_copies() : 0;
     int rc = fetch_new_to_device(R, a0, a1);
-    const double f_ms = ms_since(w0);
+    double f_ms = ms_since(w0), copy_ms = 0;
+    if (trace && rc == XKB_OK)
+    {
+        // traces only: wait for the window's copies to see how long they take
+        cudaStreamSynchronize(R->stream);
+        copy_ms = ms_since(w0) - f_ms;
+        fprintf(stderr, "  window coherency: %llu host copies issued, done %.1f ms after issue\n",
+                (unsigned long long) (xkb_internal_issued_host_copies() - issued0), copy_ms);
+        f_ms = ms_since(w0);
+    }
     // a slot whose previous copy is done
     xkb_runtime::DescSlot & sl = R->dslot[R->dslot_next];
     R->dslot_next ^= 1;
@@ -2188,8 +2207,8 @@ static int wait_batch(xkb_runtime * R)
     R->last_edges = P == 0 ? g.nedges : xkb_internal_resolver_nedges(res);
     R->last_ms[0] = ms_since(t0);
     if (getenv("XKB_TRACE_WAIT"))
-        fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms, %zu of %zu tasks streamed\n", nacc, records_ms,
-                R->last_ms[0] - records_ms, P, ntasks);
+        fprintf(stderr, "xkrt_task_wait: %zu records %.1f ms, resolver %.1f ms, %zu of %zu tasks streamed (at %.1f ms)\n", nacc,
+                records_ms, R->last_ms[0] - records_ms, P, ntasks, trace_clock_ms());
 
     bool fused = !R->ref_mode;       // reference mode: every task through the dataflow path, one at a time
     for (size_t t = P; t < ntasks && fused; ++t) fused = is_device(R, R->pending[t]) && R->formats[R->pending[t].fmtid].builtin >= 0;
