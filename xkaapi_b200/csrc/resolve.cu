@@ -1643,15 +1643,18 @@ extern "C" int xkb_resolver_create(xkb_resolver_t ** out, void * stream)
     R->interval.interval = true;
     R->handles.interval = true;
     R->stream = (cudaStream_t) stream;
-    // work buffers only this resolver's stream touches come from the pool in stream order; the
-    // graph it hands out (succ_ptr, succ, npred, window graphs, periodic form) stays in plain
-    // allocations, as a caller may read it on other streams
+    // work buffers only this resolver's stream touches come from the pool in stream order (the
+    // window graphs too: the runtime runs them on this stream); the graph it hands out
+    // (succ_ptr, succ, npred, periodic form) stays in plain allocations, as a caller may read it
+    // on other streams
     for (Domain * d : {&R->interval, &R->handles}) { d->state[0].use_pool(R->stream); d->state[1].use_pool(R->stream); }
     R->dops.use_pool(R->stream); R->hops.use_pool(R->stream);
     R->hset.use_pool(R->stream); R->ukeys.use_pool(R->stream); R->bounds.use_pool(R->stream); R->ucount.use_pool(R->stream);
     R->emit.use_pool(R->stream); R->table.use_pool(R->stream); R->counters.use_pool(R->stream);
     R->tmp.use_pool(R->stream); R->bin_off.use_pool(R->stream); R->bin_cur.use_pool(R->stream);
     R->bin_list.use_pool(R->stream); R->bin_flag.use_pool(R->stream); R->snap.use_pool(R->stream);
+    R->win_ptr.use_pool(R->stream); R->win_succ.use_pool(R->stream); R->win_npred.use_pool(R->stream);
+    R->win_tmp.use_pool(R->stream);
     *out = R;
     return XKB_OK;
 }
