@@ -823,10 +823,17 @@ __global__ void collect_bounds_kernel(const HOp * __restrict__ ops, int n, uint6
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const HRect r = ops[i].r;
-    hset_insert(tx, mask, r.x0, ux, counts + 0, counts + 2, 1u);
-    hset_insert(tx, mask, r.x1, ux, counts + 0, counts + 2, 1u);
-    hset_insert(ty, mask, r.y0, uy, counts + 1, counts + 2, 2u);
-    hset_insert(ty, mask, r.y1, uy, counts + 1, counts + 2, 2u);
+    // neighbouring ops mostly share their boundaries (tiles of one grid): one lane per distinct
+    // key of the warp probes the table
+    const unsigned act = __activemask(), lane = threadIdx.x & 31;
+    auto once = [&](uint64_t key, uint64_t * tab, uint64_t * out, unsigned * count, unsigned bit) {
+        const unsigned same = __match_any_sync(act, key);
+        if ((unsigned) (__ffs(same) - 1) == lane) hset_insert(tab, mask, key, out, count, counts + 2, bit);
+    };
+    once(r.x0, tx, ux, counts + 0, 1u);
+    once(r.x1, tx, ux, counts + 0, 1u);
+    once(r.y0, ty, uy, counts + 1, 2u);
+    once(r.y1, ty, uy, counts + 1, 2u);
 }
 
 __device__ __forceinline__ int32_t lower_index(const uint64_t * __restrict__ v, int n, uint64_t key)
