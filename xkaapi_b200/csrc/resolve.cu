@@ -1687,7 +1687,8 @@ int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops)
     }
     size_t cap = 1024;
     while (cap < 4 * nops) cap *= 2;
-    const size_t emit = std::max<size_t>(1 << 16, nops * 8);
+    // edge pairs: about 9 per op on tile stencils (the emit estimate after the first batches)
+    const size_t emit = std::max<size_t>(1 << 16, nops * 12);
     size_t tcap = 1024;
     while (tcap < 2 * emit) tcap *= 2;
     int rc;
@@ -1703,6 +1704,14 @@ int xkb_internal_resolver_prepare(xkb_resolver_t * R, size_t nops)
         if ((rc = seg->reserve(std::max<size_t>(emit, size_t(1) << 24)))) return rc;
         R->useg.push_back(std::move(seg));
         R->useg_n.push_back(0);
+    }
+    // the buffers still to come (cell states of each domain, region bins, time-split snapshots,
+    // window graphs) grow from the pool: give it room now rather than while batches run
+    if (cudaMemPool_t pool = resolver_pool())
+    {
+        void * w = nullptr;
+        if (cudaMallocFromPoolAsync(&w, size_t(256) << 20, pool, R->stream) == cudaSuccess) cudaFreeAsync(w, R->stream);
+        else cudaGetLastError();
     }
     XKB_CUDA_TRY(cudaStreamSynchronize(R->stream));
     return XKB_OK;
