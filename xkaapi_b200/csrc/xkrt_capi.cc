@@ -1746,7 +1746,7 @@ static int run_builtin_views(xkb_runtime * R, Task & T, size_t t, const xkb_acce
 // access's first element where the body runs (its leading dimension in elements), then the
 // format's function is called as f(runtime, device, task) with the program's runtime_t and
 // task_t (a CUDA-target body on the worker's stream; a device task without format runs nothing).
-static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStream_t stream)
+static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStream_t stream, bool * deferred)
 {
     xkrt::task_t * task = (xkrt::task_t *) cxx_of(T);
     xkrt::access_t * acc = (task->flags & TASK_FLAG_DEPENDENT) ? xkrt::TASK_ACCESSES(task) : nullptr;
@@ -1767,6 +1767,7 @@ static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStrea
         g_stream = stream;
         ((body3_t) f.f[XKRT_TASK_FORMAT_TARGET_CUDA])(R->cxx_rt, &R->devices[1], task);
         g_stream = nullptr;
+        if (deferred) { *deferred = true; return XKB_OK; }        // the caller tracks its completion
         if (cudaStreamSynchronize(stream) != cudaSuccess) return xkb_set_error(XKB_ECUDA, "task %zu: device body", t);
         return XKB_OK;
     }
@@ -1784,7 +1785,9 @@ static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStrea
 // state always describes data that is in place), then its body; a device body runs on the
 // worker's stream and is complete when this returns. The caller then drops the body's reference:
 // a task the body made detachable completes when its last reference goes, on whatever thread.
-static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cudaStream_t stream)
+// deferred (non-null): a device body's work may be left in flight on `stream`; *deferred is then
+// set and the caller completes the task once the stream has passed it.
+static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cudaStream_t stream, bool * deferred = nullptr)
 {
     Task & T = R->pending[t];
     const bool dev = is_device(R, T);
@@ -1836,7 +1839,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     const Format & f = R->formats[T.fmtid];
     __atomic_add_fetch(&T.detach, 1, __ATOMIC_ACQ_REL);        // the body's own reference
     g_current = &T;
-    if (cxx_of(T)) rc = run_cxx_body(R, T, t, dev, stream);
+    if (cxx_of(T)) rc = run_cxx_body(R, T, t, dev, stream, deferred);
     else if (dev && T.fmtid == XKRT_TASK_FORMAT_NULL) {}         // placement only
     else if (dev)
     {
@@ -1866,7 +1869,8 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
                 (xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[1], (xkrt_task_t *) &T);
             g_stream = nullptr;
         }
-        if (rc == XKB_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "task %zu: device body", t);
+        if (rc == XKB_OK && deferred) *deferred = true;
+        else if (rc == XKB_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "task %zu: device body", t);
     }
     else if (T.func) T.func((xkrt_runtime_t *) R, (xkrt_device_t *) &R->devices[0], (xkrt_task_t *) &T, T.user_data);
     else if (f.f[XKRT_TASK_FORMAT_TARGET_HOST])
@@ -1943,17 +1947,70 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
     }
     for (size_t t = 0; t < nt; ++t) if (D.wc[t] == 0) D.ready.push_back((uint32_t) t);
     R->df.store(&D, std::memory_order_release);
+    // A worker leaves up to MAX_INFLIGHT device bodies in flight on its stream (resident mode):
+    // it takes the next ready task while they run, and completes each one -- releasing its
+    // successors -- once the stream has passed the event recorded after it. It never sleeps on
+    // the ready queue while it holds work in flight: with nothing ready it waits for its oldest.
+    // Reference mode runs one task at a time (an eviction may reuse memory a body still reads).
+    constexpr size_t MAX_INFLIGHT = 4;
     auto worker = [&](size_t k) {
         cudaSetDevice(R->device);
         auto progress = std::chrono::steady_clock::now();
         size_t seen = 0;
+        std::vector<cudaEvent_t> evs;                         // this worker's events, reused
+        std::deque<std::pair<uint32_t, cudaEvent_t>> fl;      // bodies in flight, oldest first
+        auto fail_with = [&](int rc) {
+            std::lock_guard<std::mutex> lk(D.mu);
+            if (D.err == XKB_OK) { D.err = rc; D.err_text = xkb_last_error(); }
+            D.cv.notify_all();
+        };
+        auto leave = [&]() {                                  // nothing of this worker stays in flight
+            if (!fl.empty()) cudaStreamSynchronize(R->wstreams[k]);
+            for (auto & f : fl) evs.push_back(f.second);
+            fl.clear();
+            for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        };
+        // complete the bodies the stream has passed (all of them up to the oldest if `wait`)
+        auto retire = [&](bool wait) -> bool {
+            while (!fl.empty())
+            {
+                const cudaError_t e = wait ? cudaEventSynchronize(fl.front().second) : cudaEventQuery(fl.front().second);
+                if (e == cudaErrorNotReady) return true;
+                if (e != cudaSuccess) { fail_with(xkb_set_error(XKB_ECUDA, "task %u: device body: %s", (unsigned) (base + fl.front().first), cudaGetErrorString(e))); return false; }
+                const uint32_t done_t = fl.front().first;
+                evs.push_back(fl.front().second);
+                fl.pop_front();
+                wait = false;
+                if (task_unref(R->pending[base + done_t])) task_completed(R, R->pending[base + done_t]);
+            }
+            return true;
+        };
         for (;;)
         {
             uint32_t t;
+            if (!fl.empty())
+            {
+                if (!retire(fl.size() >= MAX_INFLIGHT)) { leave(); return; }
+                bool got = false;
+                {
+                    std::lock_guard<std::mutex> lk(D.mu);
+                    if (D.err != XKB_OK) got = false;
+                    else if (!D.ready.empty()) { t = D.ready.front(); D.ready.pop_front(); got = true; }
+                }
+                if (!got)
+                {
+                    bool err;
+                    { std::lock_guard<std::mutex> lk(D.mu); err = D.err != XKB_OK; }
+                    if (err) { leave(); return; }
+                    if (!retire(true)) { leave(); return; }
+                    continue;
+                }
+            }
+            else
             {
                 std::unique_lock<std::mutex> lk(D.mu);
                 D.cv.wait_for(lk, std::chrono::milliseconds(100), [&] { return D.err != XKB_OK || D.done == nt || !D.ready.empty(); });
-                if (D.err != XKB_OK || D.done == nt) return;
+                if (D.err != XKB_OK || D.done == nt) { lk.unlock(); leave(); return; }
                 if (D.ready.empty())
                 {
                     if (D.done != seen) { seen = D.done; progress = std::chrono::steady_clock::now(); }
@@ -1962,6 +2019,8 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
                         D.err = xkb_set_error(XKB_ETIMEDOUT, "xkrt_task_wait: %zu of %zu tasks completed, none for 600 s (a detached task never completed?)", D.done, nt);
                         D.err_text = xkb_last_error();
                         D.cv.notify_all();
+                        lk.unlock();
+                        leave();
                         return;
                     }
                     continue;
@@ -1974,13 +2033,22 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
                 }
                 else { t = D.ready.front(); D.ready.pop_front(); }
             }
-            const int rc = run_one(R, base + t, recs, R->wstreams[k]);
-            if (rc)
+            bool deferred = false;
+            const int rc = run_one(R, base + t, recs, R->wstreams[k], R->ref_mode ? nullptr : &deferred);
+            if (rc) { fail_with(rc); leave(); return; }
+            if (deferred)
             {
-                std::lock_guard<std::mutex> lk(D.mu);
-                if (D.err == XKB_OK) { D.err = rc; D.err_text = xkb_last_error(); }
-                D.cv.notify_all();
-                return;
+                cudaEvent_t ev = nullptr;
+                if (!evs.empty()) { ev = evs.back(); evs.pop_back(); }
+                else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ev = nullptr;
+                if (!ev || cudaEventRecord(ev, R->wstreams[k]) != cudaSuccess)
+                {
+                    if (ev) evs.push_back(ev);
+                    // no event: wait for the body here
+                    if (cudaStreamSynchronize(R->wstreams[k]) != cudaSuccess)
+                    { fail_with(xkb_set_error(XKB_ECUDA, "task %zu: device body", base + t)); leave(); return; }
+                }
+                else { fl.emplace_back(t, ev); continue; }
             }
             if (task_unref(R->pending[base + t])) task_completed(R, R->pending[base + t]);
         }
