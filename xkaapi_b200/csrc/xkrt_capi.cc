@@ -220,6 +220,7 @@ struct xkb_runtime {
     // page-locked descriptor slots of streamed windows (a slot is reused once its copy is done)
     struct DescSlot { xkb_task_desc_t * p = nullptr; size_t cap = 0; cudaEvent_t ev = nullptr; } dslot[2];
     int dslot_next = 0;
+    bool preplanned = false;                          // the batch's accesses were made coherent up front
     std::atomic<struct Dataflow *> df{nullptr};       // the batch being executed (detached completion)
     uint64_t last_base = 0, last_end = 0;             // region of the last mirror lookup
     uint8_t * last_mirror = nullptr;
@@ -1793,6 +1794,7 @@ static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cud
     const bool dev = is_device(R, T);
     int rc = XKB_OK;
     g_view_ld.assign(T.nacc, -1);
+    if (!R->preplanned)
     {
         std::lock_guard<std::mutex> lk(R->plan_mu);
         const uint64_t calls0 = R->copy_calls;
@@ -1916,12 +1918,46 @@ static void task_completed(::xkb_runtime * R, Task & T)
 // XKB_HOST_THREADS or one per hardware thread (at most 64) -- the reference's host team and
 // device threads executing ready tasks as their predecessors complete. A detached task holds no
 // thread; the batch ends when every task completed (600 s without progress is an error).
+static int fetch_new_to_device(xkb_runtime * R, size_t a0, size_t a1);
+
+// Tasks [t0, t1) (accesses [a0, a1)) when all of them run on the device and every access they
+// make lies in a registered region with a device mirror (or is a handle): their distinct records
+// are made coherent on the device now, in spawn order (copies complete on return), and each
+// access's replica pointer is set, so R->preplanned lets run_one skip the planner. Otherwise
+// nothing is done and each task plans its own coherency.
+static int preplan_device_batch(xkb_runtime * R, size_t t0, size_t t1, size_t a0, size_t a1)
+{
+    R->preplanned = false;
+    if (!R->gpu || t0 >= t1) return XKB_OK;
+    const xkb_access_rec_t * recs = R->recs.data();
+    std::lock_guard<std::mutex> lk(R->plan_mu);
+    for (size_t t = t0; t < t1; ++t)
+    {
+        const Task & T = R->pending[t];
+        if (!is_device(R, T)) return XKB_OK;
+        for (uint32_t a = 0; a < T.nacc; ++a)
+        {
+            const xkb_access_rec_t & r = recs[T.acc_off + a];
+            if (r.type == REC_NONE) continue;
+            if (r.type == XKB_ACCESS_TYPE_HANDLE) { R->replica_pool[T.acc_off + a] = (void *) (uintptr_t) r.addr; continue; }
+            if (in_unified(R, r)) return XKB_OK;
+            void * m = mirror_of(R, rec_begin(r));
+            if (!m) return XKB_OK;
+            R->replica_pool[T.acc_off + a] = m;
+        }
+    }
+    int rc = fetch_new_to_device(R, a0, a1);
+    if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: copies");
+    if (rc == XKB_OK) R->preplanned = true;
+    return rc;
+}
+
 static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_access_rec_t * recs, size_t base)
 {
     const size_t nt = R->pending.size() - base;
     // the replicas the bodies read (xkrt_task_access_replica): set as each task's accesses are
     // made coherent, null until then; only tasks run here have bodies that read them
-    if (nt)
+    if (nt && !R->preplanned)                      // preplanned: already set for every access
     {
         const size_t a0 = R->pending[base].acc_off;
         memset(R->replica_pool.data() + a0, 0, (R->acc_pool.size() - a0) * sizeof(void *));
@@ -2344,7 +2380,12 @@ static int wait_batch(xkb_runtime * R)
         // streamed windows (its completed predecessors) are done
         t0 = std::chrono::steady_clock::now();
         if (P) rc = xkb_internal_sched_windows_wait(R->sched, nullptr);
+        // a batch of device tasks only (program-defined CUDA bodies included): as for a fused
+        // batch, host data cannot change while it runs, so every access is made coherent on the
+        // device up front and the team's tasks skip the planner (and its lock)
+        if (rc == XKB_OK && !R->ref_mode) rc = preplan_device_batch(R, P, ntasks, a_P, nacc);
         if (rc == XKB_OK) rc = run_dataflow(R, g, recs, P);
+        R->preplanned = false;
         if (rc == XKB_OK && cudaStreamSynchronize(R->stream) != cudaSuccess) rc = xkb_set_error(XKB_ECUDA, "xkrt_task_wait: stream");
         R->last_ms[2] = ms_since(t0);
     }
