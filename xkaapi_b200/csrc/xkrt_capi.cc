@@ -1906,11 +1906,17 @@ static void task_completed(::xkb_runtime * R, Task & T)
     const size_t g = (size_t) (&T - R->pending.data());
     if (g < D->base || g - D->base >= D->nt) return;
     const size_t t = g - D->base;
-    std::lock_guard<std::mutex> lk(D->mu);
-    for (uint32_t i = D->ptr[t]; i < D->ptr[t + 1]; ++i)
-        if (--D->wc[D->succ[i]] == 0) D->ready.push_back(D->succ[i]);
-    ++D->done;
-    D->cv.notify_all();
+    size_t woke = 0;
+    bool last;
+    {
+        std::lock_guard<std::mutex> lk(D->mu);
+        for (uint32_t i = D->ptr[t]; i < D->ptr[t + 1]; ++i)
+            if (--D->wc[D->succ[i]] == 0) { D->ready.push_back(D->succ[i]); ++woke; }
+        last = ++D->done == D->nt;
+    }
+    // one sleeping worker per task made ready (all of them at the end, so that they leave)
+    if (last) D->cv.notify_all();
+    else for (size_t k = 0; k < woke; ++k) D->cv.notify_one();
 }
 
 // A non-fused batch (its tasks from `base` on; the earlier ones completed): ready tasks (all
