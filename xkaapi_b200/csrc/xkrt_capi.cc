@@ -1994,13 +1994,16 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
     // successors -- once the stream has passed the event recorded after it. It never sleeps on
     // the ready queue while it holds work in flight: with nothing ready it waits for its oldest.
     // Reference mode runs one task at a time (an eviction may reuse memory a body still reads).
-    constexpr size_t MAX_INFLIGHT = 4;
+    constexpr size_t MAX_INFLIGHT = 8, GROUP = 4;
     auto worker = [&](size_t k) {
         cudaSetDevice(R->device);
         auto progress = std::chrono::steady_clock::now();
         size_t seen = 0;
         std::vector<cudaEvent_t> evs;                         // this worker's events, reused
-        std::deque<std::pair<uint32_t, cudaEvent_t>> fl;      // bodies in flight, oldest first
+        // bodies in flight, oldest first; an event is recorded after every GROUP of them (and
+        // before the worker waits), and covers its entry and the ones before it
+        std::deque<std::pair<uint32_t, cudaEvent_t>> fl;
+        size_t open = 0;                                      // entries at the back with no event yet
         auto fail_with = [&](int rc) {
             std::lock_guard<std::mutex> lk(D.mu);
             if (D.err == XKB_OK) { D.err = rc; D.err_text = xkb_last_error(); }
@@ -2008,22 +2011,51 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
         };
         auto leave = [&]() {                                  // nothing of this worker stays in flight
             if (!fl.empty()) cudaStreamSynchronize(R->wstreams[k]);
-            for (auto & f : fl) evs.push_back(f.second);
-            fl.clear();
+            for (auto & f : fl) if (f.second) evs.push_back(f.second);
+            fl.clear(); open = 0;
             for (cudaEvent_t e : evs) cudaEventDestroy(e);
         };
-        // complete the bodies the stream has passed (all of them up to the oldest if `wait`)
-        auto retire = [&](bool wait) -> bool {
+        // an event after the entries that have none (false: none could be recorded; the worker
+        // then waits for its stream, and every entry is covered)
+        auto close = [&]() -> bool {
+            if (!open) return true;
+            cudaEvent_t ev = nullptr;
+            if (!evs.empty()) { ev = evs.back(); evs.pop_back(); }
+            else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) { cudaGetLastError(); ev = nullptr; }
+            if (ev && cudaEventRecord(ev, R->wstreams[k]) == cudaSuccess) { fl.back().second = ev; open = 0; return true; }
+            if (ev) evs.push_back(ev);
+            cudaGetLastError();
+            if (cudaStreamSynchronize(R->wstreams[k]) != cudaSuccess) return false;
+            // everything is done: complete it all
             while (!fl.empty())
             {
-                const cudaError_t e = wait ? cudaEventSynchronize(fl.front().second) : cudaEventQuery(fl.front().second);
-                if (e == cudaErrorNotReady) return true;
-                if (e != cudaSuccess) { fail_with(xkb_set_error(XKB_ECUDA, "task %u: device body: %s", (unsigned) (base + fl.front().first), cudaGetErrorString(e))); return false; }
-                const uint32_t done_t = fl.front().first;
-                evs.push_back(fl.front().second);
+                const uint32_t d = fl.front().first;
+                if (fl.front().second) evs.push_back(fl.front().second);
                 fl.pop_front();
+                if (task_unref(R->pending[base + d])) task_completed(R, R->pending[base + d]);
+            }
+            open = 0;
+            return true;
+        };
+        // complete the bodies the stream has passed (if `wait`, at least the oldest group)
+        auto retire = [&](bool wait) -> bool {
+            if (wait && !close()) { fail_with(xkb_set_error(XKB_ECUDA, "xkrt_task_wait: device body")); return false; }
+            while (!fl.empty())
+            {
+                size_t g = 0;
+                while (g < fl.size() && !fl[g].second) ++g;
+                if (g == fl.size()) return true;              // only the open group is left
+                const cudaError_t e = wait ? cudaEventSynchronize(fl[g].second) : cudaEventQuery(fl[g].second);
+                if (e == cudaErrorNotReady) return true;
+                if (e != cudaSuccess) { fail_with(xkb_set_error(XKB_ECUDA, "task %u: device body: %s", (unsigned) (base + fl[g].first), cudaGetErrorString(e))); return false; }
+                evs.push_back(fl[g].second);
+                for (size_t q = 0; q <= g; ++q)
+                {
+                    const uint32_t d = fl.front().first;
+                    fl.pop_front();
+                    if (task_unref(R->pending[base + d])) task_completed(R, R->pending[base + d]);
+                }
                 wait = false;
-                if (task_unref(R->pending[base + done_t])) task_completed(R, R->pending[base + done_t]);
             }
             return true;
         };
@@ -2080,17 +2112,10 @@ static int run_dataflow(xkb_runtime * R, const xkb_task_graph_t & g, const xkb_a
             if (rc) { fail_with(rc); leave(); return; }
             if (deferred)
             {
-                cudaEvent_t ev = nullptr;
-                if (!evs.empty()) { ev = evs.back(); evs.pop_back(); }
-                else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ev = nullptr;
-                if (!ev || cudaEventRecord(ev, R->wstreams[k]) != cudaSuccess)
-                {
-                    if (ev) evs.push_back(ev);
-                    // no event: wait for the body here
-                    if (cudaStreamSynchronize(R->wstreams[k]) != cudaSuccess)
-                    { fail_with(xkb_set_error(XKB_ECUDA, "task %zu: device body", base + t)); leave(); return; }
-                }
-                else { fl.emplace_back(t, ev); continue; }
+                fl.emplace_back(t, nullptr);
+                if (++open >= GROUP && !close())
+                { fail_with(xkb_set_error(XKB_ECUDA, "task %zu: device body", base + t)); leave(); return; }
+                continue;
             }
             if (task_unref(R->pending[base + t])) task_completed(R, R->pending[base + t]);
         }
