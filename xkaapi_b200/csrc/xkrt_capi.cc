@@ -1783,11 +1783,12 @@ static int run_cxx_body(xkb_runtime * R, Task & T, size_t t, bool dev, cudaStrea
 
 // One task of a non-fused batch on the calling worker: its accesses made coherent where it runs
 // (planner fetches and their copies, completed before the planner is released, so the planner's
-// state always describes data that is in place), then its body; a device body runs on the
-// worker's stream and is complete when this returns. The caller then drops the body's reference:
-// a task the body made detachable completes when its last reference goes, on whatever thread.
-// deferred (non-null): a device body's work may be left in flight on `stream`; *deferred is then
-// set and the caller completes the task once the stream has passed it.
+// state always describes data that is in place; skipped when the batch was made coherent up
+// front), then its body; a device body runs on the worker's stream and, with `deferred` null, is
+// complete when this returns. With `deferred` non-null a device body's work may be left in flight
+// on `stream`: *deferred is then set and the caller completes the task once the stream has passed
+// it. Completing drops the body's reference: a task the body made detachable completes when its
+// last reference goes, on whatever thread.
 static int run_one(xkb_runtime * R, size_t t, const xkb_access_rec_t * recs, cudaStream_t stream, bool * deferred = nullptr)
 {
     Task & T = R->pending[t];
